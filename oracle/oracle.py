@@ -1,0 +1,273 @@
+"""CPU oracle for the Acoular frequency-domain beamforming path.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline
+leg of ``bench.py``, always as the checker or the timed CPU reference -- never by the product
+package ``acoular_b200``.
+
+This module restates the reference's (Acoular 26.08) host-side glue for the path in numpy and
+calls the C restatement of its numba kernels in ``oracle_core.c`` (built into
+``oracle/lib/liboracle_acoular.so`` by ``oracle/build_oracle.sh``):
+
+* :func:`source_windows`   -- ``BaseSpectra._get_source_data``   acoular/spectra.py:171-184
+* :func:`num_blocks`       -- ``PowerSpectra._get_num_blocks``   acoular/spectra.py:281-283
+* :func:`fftfreq`          -- ``BaseSpectra.fftfreq``            acoular/spectra.py:128-168
+* :func:`calc_csm`         -- ``PowerSpectra.calc_csm``          acoular/spectra.py:366-416
+* :func:`dist_mat`         -- ``dist_mat``                       acoular/environments.py:65-103
+* :func:`beamformer_freq`  -- ``beamformerFreq`` (full CSM)      acoular/fastFuncs.py:61-214, 217-311
+* :func:`sig_loss_norm`    -- ``BeamformerBase.sig_loss_norm``   acoular/fbeamform.py:438-451
+* :func:`beamformer_calc`  -- ``BeamformerBase._calc``           acoular/fbeamform.py:475-510
+* :func:`synthetic`        -- ``BeamformerBase.synthetic``       acoular/fbeamform.py:512-593
+* :func:`L_p`              -- ``L_p``                            acoular/fbeamform.py:2412-2429
+
+Parity of the oracle itself is pinned by ``tests/test_oracle.py`` against goldens generated by
+running the reference's own code (``tests/golden/make_golden.py``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+from scipy import fft as sfft
+
+_HERE = Path(__file__).resolve().parent
+_LIB_PATH = _HERE / 'lib' / 'liboracle_acoular.so'
+_lib = None
+
+WINDOWS = {
+    'Rectangular': np.ones,
+    'Hanning': np.hanning,
+    'Hamming': np.hamming,
+    'Bartlett': np.bartlett,
+    'Blackman': np.blackman,
+}
+OVERLAPS = {'None': 1, '50%': 2, '75%': 4, '87.5%': 8}
+STEER_TYPES = {'classic': 1, 'inverse': 2, 'true level': 3, 'true location': 4}
+
+
+def build(force: bool = False) -> Path:
+    """Compile ``oracle_core.c`` with gcc (no GPU needed)."""
+    if force or not _LIB_PATH.exists() or _LIB_PATH.stat().st_mtime < (_HERE / 'oracle_core.c').stat().st_mtime:
+        subprocess.run(['bash', str(_HERE / 'build_oracle.sh')], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(str(_LIB_PATH))
+        dp = ctypes.POINTER(ctypes.c_double)
+        fp = ctypes.POINTER(ctypes.c_float)
+        i64 = ctypes.c_int64
+        L.orc_calc_csm_c128.argtypes = [dp, dp, i64, i64]
+        L.orc_calc_csm_c64.argtypes = [fp, fp, i64, i64]
+        L.orc_calc_csm_blocks_c128.argtypes = [dp, dp, i64, i64, i64]
+        L.orc_calc_csm_blocks_c64.argtypes = [fp, fp, i64, i64, i64]
+        L.orc_dist_mat.argtypes = [dp, dp, i64, i64, dp]
+        L.orc_beamformer_fullcsm.argtypes = [dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_int, i64, i64, dp, dp]
+        L.orc_num_threads.restype = ctypes.c_int
+        L.orc_set_num_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+# ----------------------------------------------------------------------------------------------
+# Stage A: cross-spectral matrix
+# ----------------------------------------------------------------------------------------------
+def _source_blocks(samples: np.ndarray, num: int):
+    """``TimeSamples.result(num)`` (acoular/sources.py:417-467): consecutive blocks, last one short."""
+    n = samples.shape[0]
+    i = 0
+    while i < n:
+        yield samples[i:i + num]
+        i += num
+
+
+def source_windows(samples: np.ndarray, block_size: int, overlap: int):
+    """Overlapped windows as yielded by ``_get_source_data`` (acoular/spectra.py:171-184)."""
+    bs = block_size
+    temp = np.empty((2 * bs, samples.shape[1]))
+    pos = bs
+    posinc = bs / overlap
+    for data_block in _source_blocks(samples, bs):
+        ns = data_block.shape[0]
+        temp[bs:bs + ns] = data_block
+        while pos + bs <= bs + ns:
+            yield temp[int(pos):int(pos + bs)]
+            pos += posinc
+        temp[0:bs] = temp[bs:]
+        pos -= bs
+
+
+def num_blocks(num_samples: int, block_size: int, overlap: int) -> float:
+    """acoular/spectra.py:281-283 -- a float formula, not a count."""
+    return overlap * num_samples / block_size - overlap + 1
+
+
+def fftfreq(block_size: int, sample_freq: float) -> np.ndarray:
+    """acoular/spectra.py:128-168."""
+    return abs(sfft.fftfreq(block_size, 1.0 / sample_freq)[: int(block_size / 2 + 1)])
+
+
+def calc_csm(samples: np.ndarray, block_size: int = 1024, window: str = 'Rectangular', overlap: str = 'None',
+             precision: str = 'complex128', return_spectra: bool = False):
+    """``PowerSpectra.calc_csm`` (acoular/spectra.py:366-416) with the C ``calcCSM``."""
+    ov = OVERLAPS[overlap]
+    wind = WINDOWS[window](block_size)
+    weight = np.dot(wind, wind)
+    wind = wind[np.newaxis, :].swapaxes(0, 1)
+    numfreq = int(block_size / 2 + 1)
+    M = samples.shape[1]
+    csm_upper = np.zeros((numfreq, M, M), dtype=precision)
+    L = lib()
+    spectra = []
+    for data in source_windows(samples, block_size, ov):
+        ft = np.ascontiguousarray(sfft.rfft(data * wind, None, 0).astype(precision))
+        if return_spectra:
+            spectra.append(ft.copy())
+        if precision == 'complex128':
+            L.orc_calc_csm_c128(_dp(csm_upper), _dp(ft), numfreq, M)
+        else:
+            L.orc_calc_csm_c64(_fp(csm_upper), _fp(ft), numfreq, M)
+    csm_lower = csm_upper.conj().transpose(0, 2, 1)
+    for f in range(csm_lower.shape[0]):
+        np.fill_diagonal(csm_lower[f], 0)
+    csm = csm_lower + csm_upper
+    out = csm * (2.0 / block_size / weight / num_blocks(samples.shape[0], block_size, ov))
+    if return_spectra:
+        return out, spectra
+    return out
+
+
+# ----------------------------------------------------------------------------------------------
+# Geometry
+# ----------------------------------------------------------------------------------------------
+def dist_mat(gpos: np.ndarray, mpos: np.ndarray) -> np.ndarray:
+    """acoular/environments.py:65-103; gpos (3, N), mpos (3, M) -> (N, M)."""
+    gpos = np.ascontiguousarray(gpos, dtype=np.float64)
+    mpos = np.ascontiguousarray(mpos, dtype=np.float64)
+    N, M = gpos.shape[1], mpos.shape[1]
+    rm = np.empty((N, M))
+    lib().orc_dist_mat(_dp(gpos), _dp(mpos), N, M, _dp(rm))
+    return rm
+
+
+def apparent_r(gpos, mpos=0.0):
+    """``Environment.apparent_r`` (acoular/environments.py:202-238)."""
+    if np.isscalar(mpos):
+        mpos = np.array((0, 0, 0), dtype=np.float64)[:, np.newaxis]
+    rm = dist_mat(gpos, mpos)
+    if rm.shape[1] == 1:
+        rm = rm[:, 0]
+    return rm
+
+
+def rect_grid_pos(x_min, x_max, y_min, y_max, z, increment):
+    """``RectGrid`` nxsteps/nysteps/pos (acoular/grids.py:332-358)."""
+    i = abs(increment)
+    nx = round((abs(x_max - x_min) + i) / i) if i != 0 else 1
+    ny = round((abs(y_max - y_min) + i) / i) if i != 0 else 1
+    bpos = np.mgrid[x_min:x_max:nx * 1j, y_min:y_max:ny * 1j, z:z + 0.1]
+    bpos.resize((3, nx * ny))
+    return bpos, (nx, ny)
+
+
+def rect_grid3d_pos(x_min, x_max, y_min, y_max, z_min, z_max, increment):
+    """``RectGrid3D`` (acoular/grids.py:523-560), scalar increment."""
+    i = abs(increment)
+    nx = round((abs(x_max - x_min) + i) / i)
+    ny = round((abs(y_max - y_min) + i) / i)
+    nz = round((abs(z_max - z_min) + i) / i)
+    bpos = np.mgrid[x_min:x_max:nx * 1j, y_min:y_max:ny * 1j, z_min:z_max:nz * 1j]
+    bpos.resize((3, nx * ny * nz))
+    return bpos, (nx, ny, nz)
+
+
+# ----------------------------------------------------------------------------------------------
+# Stage B: steered-response map
+# ----------------------------------------------------------------------------------------------
+def beamformer_freq(steer_type: str, r_diag: bool, norm: float, r0: np.ndarray, rm: np.ndarray, k: float,
+                    csm: np.ndarray):
+    """``beamformerFreq`` for the predefined steering types and a full CSM (fastFuncs.py:61-214)."""
+    csm = np.ascontiguousarray(csm, dtype=np.complex128)
+    r0 = np.ascontiguousarray(r0, dtype=np.float64)
+    rm = np.ascontiguousarray(rm, dtype=np.float64)
+    G, M = rm.shape
+    res = np.zeros(G)
+    nrm = np.zeros(G)
+    lib().orc_beamformer_fullcsm(_dp(csm), _dp(r0), _dp(rm), float(k), float(norm), int(bool(r_diag)),
+                                 STEER_TYPES[steer_type], G, M, _dp(res), _dp(nrm))
+    return res, nrm
+
+
+def sig_loss_norm(r_diag: bool, num_mics: int, r_diag_norm: float = 0.0) -> float:
+    """acoular/fbeamform.py:438-451."""
+    if not r_diag:
+        return 1.0
+    if r_diag_norm == 0.0:
+        n = float(num_mics)
+        return n / (n - 1)
+    return r_diag_norm
+
+
+def beamformer_calc(csm: np.ndarray, freqs: np.ndarray, ind, r0, rm, c: float, steer_type: str, r_diag: bool,
+                    r_diag_norm: float = 0.0, out: np.ndarray | None = None):
+    """``BeamformerBase._calc`` (acoular/fbeamform.py:475-510) for a plain ``SteeringVector``."""
+    G, M = rm.shape
+    if out is None:
+        out = np.zeros((csm.shape[0], G))
+    normfactor = sig_loss_norm(r_diag, M, r_diag_norm)
+    for i in ind:
+        c_i = np.array(csm[i], dtype='complex128')
+        b = beamformer_freq(steer_type, r_diag, normfactor, r0, rm, 2 * np.pi * freqs[i] / c, c_i)[0]
+        if r_diag:
+            b[np.sign(b) < 0] = 0.0
+        out[i] = b
+    return out
+
+
+def band_indices(freq: np.ndarray, f: float, num):
+    """Bin range of ``synthetic`` (acoular/fbeamform.py:566-577); ``(ind1, ind2)``."""
+    if isinstance(num, list):
+        f1, f2 = num[0], num[-1]
+    else:
+        f1 = f * 2.0 ** (-0.5 / num)
+        f2 = f * 2.0 ** (+0.5 / num)
+    return int(np.searchsorted(freq, f1)), int(np.searchsorted(freq, f2))
+
+
+def synthetic(result: np.ndarray, freq: np.ndarray, f: float, num=0, shape=None):
+    """``BeamformerBase.synthetic`` band sum (acoular/fbeamform.py:512-593) over a full result."""
+    if num == 0:
+        ind = int(np.searchsorted(freq, f))
+        h = np.zeros_like(result[0]) if ind >= len(freq) else result[ind]
+    else:
+        ind1, ind2 = band_indices(freq, f, num)
+        h = np.zeros_like(result[0]) if ind1 == ind2 else np.sum(result[ind1:ind2], 0)
+    return h if shape is None else h.reshape(shape)
+
+
+def L_p(x):
+    """acoular/fbeamform.py:2412-2429."""
+    return 10 * np.log10(np.clip(x / 4e-10, 1e-35, None))

@@ -1,0 +1,198 @@
+/*
+ * CPU oracle for the Acoular frequency-domain beamforming path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file restates, in plain C, the numba kernels that the
+ * reference (Acoular 26.08) runs on this path.  It is the checker for the CUDA kernels and the
+ * timed CPU baseline ("port") in the benchmark; no product code path may call it.
+ *
+ * Every function follows the reference's arithmetic order so that its results reproduce the
+ * reference's own numba results to rounding:
+ *   orc_calc_csm_c128 / _c64   acoular/fastFuncs.py:19-58     (calcCSM)
+ *   orc_dist_mat               acoular/environments.py:65-103 (dist_mat)
+ *   orc_beamformer_fullcsm     acoular/fastFuncs.py:217-311   (_freqBeamformer_FullCSM)
+ * Parity of this restatement is pinned against golden vectors produced by running the reference's
+ * own code (tests/golden/make_golden.py) and against the reference's committed regression arrays
+ * for Environment.apparent_r.
+ *
+ * Float32 phase semantics: the reference rounds k*r to float32 and evaluates np.cos / np.sin in
+ * float32, which numba lowers to the C library's cosf / sinf.  This file calls the same cosf / sinf.
+ *
+ * Build: oracle/build_oracle.sh (gcc -O2 -fopenmp -ffp-contract=off).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* calcCSM, complex128 signature (fastFuncs.py:19-58).
+ * csm: [F][M][M] interleaved (re, im) doubles, updated in place (upper triangle r <= c).
+ * spec: [F][M] interleaved.  csm[f,r,c] += conj(spec[f,c]) * spec[f,r]. */
+void orc_calc_csm_c128(double *csm, const double *spec, int64_t F, int64_t M)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < F; ++f) {
+        const double *s = spec + 2 * f * M;
+        double *c = csm + 2 * f * M * M;
+        for (int64_t col = 0; col < M; ++col) {
+            const double tr = s[2 * col], ti = -s[2 * col + 1]; /* temp = conj(spec[col]) */
+            for (int64_t row = 0; row <= col; ++row) {
+                const double xr = s[2 * row], xi = s[2 * row + 1];
+                /* csm += temp * spec[row]; the reference compiles this with fastmath, which LLVM
+                 * contracts into two chained FMAs per component in this order (verified bit-exact
+                 * against the reference's numba build). */
+                double *dst = c + 2 * (row * M + col);
+                dst[0] = fma(-ti, xi, fma(tr, xr, dst[0]));
+                dst[1] = fma(tr, xi, fma(ti, xr, dst[1]));
+            }
+        }
+    }
+}
+
+/* calcCSM, complex64 signature: same arithmetic in float32. */
+void orc_calc_csm_c64(float *csm, const float *spec, int64_t F, int64_t M)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < F; ++f) {
+        const float *s = spec + 2 * f * M;
+        float *c = csm + 2 * f * M * M;
+        for (int64_t col = 0; col < M; ++col) {
+            const float tr = s[2 * col], ti = -s[2 * col + 1];
+            for (int64_t row = 0; row <= col; ++row) {
+                const float xr = s[2 * row], xi = s[2 * row + 1];
+                float *dst = c + 2 * (row * M + col);
+                dst[0] = fmaf(-ti, xi, fmaf(tr, xr, dst[0]));
+                dst[1] = fmaf(tr, xi, fmaf(ti, xr, dst[1]));
+            }
+        }
+    }
+}
+
+/* Welch accumulation over K blocks of spectra [K][F][M] (one calcCSM call per block, the loop
+ * of PowerSpectra.calc_csm, spectra.py:407-410).  Used by the CPU baseline timing. */
+void orc_calc_csm_blocks_c128(double *csm, const double *spec, int64_t K, int64_t F, int64_t M)
+{
+    for (int64_t b = 0; b < K; ++b)
+        orc_calc_csm_c128(csm, spec + 2 * b * F * M, F, M);
+}
+
+void orc_calc_csm_blocks_c64(float *csm, const float *spec, int64_t K, int64_t F, int64_t M)
+{
+    for (int64_t b = 0; b < K; ++b)
+        orc_calc_csm_c64(csm, spec + 2 * b * F * M, F, M);
+}
+
+/* dist_mat (environments.py:65-103): rm[n, m] = |g_n - m_m|.  gpos [3][N], mpos [3][M]. */
+void orc_dist_mat(const double *gpos, const double *mpos, int64_t N, int64_t M, double *rm)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t n = 0; n < N; ++n) {
+        const double g0 = gpos[n], g1 = gpos[N + n], g2 = gpos[2 * N + n];
+        for (int64_t m = 0; m < M; ++m) {
+            const double d0 = g0 - mpos[m], d1 = g1 - mpos[M + m], d2 = g2 - mpos[2 * M + m];
+            /* fastmath contraction of d0^2 + d1^2 + d2^2 as numba emits it (bit-exact) */
+            rm[n * M + m] = sqrt(fma(d2, d2, fma(d1, d1, d0 * d0)));
+        }
+    }
+}
+
+/* _freqBeamformer_FullCSM (fastFuncs.py:217-311) for one frequency bin.
+ * csm: [M][M] interleaved complex128; r0: [G]; rm: [G][M]; k: wave number.
+ * steer_type: 1 classic, 2 inverse, 3 true level, 4 true location.
+ * Writes result[G] and normsteer[G]. */
+void orc_beamformer_fullcsm(const double *csm, const double *r0, const double *rm, double k, double norm,
+                            int r_diag, int steer_type, int64_t G, int64_t M, double *result, double *normsteer)
+{
+    const int st2 = steer_type == 2;
+    const int st34 = steer_type == 3 || steer_type == 4;
+#pragma omp parallel
+    {
+        double *vr = (double *)__builtin_alloca(sizeof(double) * M);
+        double *vi = (double *)__builtin_alloca(sizeof(double) * M);
+#pragma omp for schedule(static)
+        for (int64_t gi = 0; gi < G; ++gi) {
+            const double *r = rm + gi * M;
+            double help = 0.0;
+            for (int64_t m = 0; m < M; ++m) {
+                const float arg = (float)(k * r[m]);  /* np.float32(waveNumber * dist) */
+                vr[m] = (double)cosf(arg);            /* cos(arg) - 1j*sin(arg), float32 libm */
+                vi[m] = -(double)sinf(arg);
+            }
+            if (st2) {
+                help = 0.0;
+                for (int64_t m = 0; m < M; ++m) {
+                    help += r[m] * r[m];
+                    vr[m] *= r[m];
+                    vi[m] *= r[m];
+                }
+            }
+            if (st34) {
+                help = 0.0;
+                for (int64_t m = 0; m < M; ++m) {
+                    help += 1.0 / (r[m] * r[m]);
+                    vr[m] /= r[m];
+                    vi[m] /= r[m];
+                }
+            }
+            double scalar = 0.0;
+            for (int64_t b = 0; b < M; ++b) {
+                double lr = 0.0, li = 0.0;
+                for (int64_t a = 0; a < b; ++a) {
+                    /* csm[a, b] * conj(v[a]) */
+                    const double cr = csm[2 * (a * M + b)], ci = csm[2 * (a * M + b) + 1];
+                    const double hr = vr[a], hi = -vi[a];
+                    lr += cr * hr - ci * hi;
+                    li += cr * hi + ci * hr;
+                }
+                /* 2 * (left * v[b]).real */
+                scalar += 2.0 * (lr * vr[b] - li * vi[b]);
+            }
+            if (!r_diag) {
+                for (int64_t m = 0; m < M; ++m) {
+                    const double cr = csm[2 * (m * M + m)], ci = csm[2 * (m * M + m) + 1];
+                    const double hr = vr[m], hi = -vi[m];
+                    const double pr = cr * hr - ci * hi, pi = cr * hi + ci * hr;
+                    scalar += pr * vr[m] - pi * vi[m];
+                }
+            }
+            if (steer_type == 1) {
+                const double nf = (double)M;
+                normsteer[gi] = 1.0 / (double)M;
+                result[gi] = scalar / (nf * nf) * norm;
+            } else if (steer_type == 2) {
+                const double nf = (double)M * r0[gi];
+                const double nf2 = nf * nf;
+                normsteer[gi] = help / nf2;
+                result[gi] = scalar / nf2 * norm;
+            } else if (steer_type == 3) {
+                const double nf = r0[gi] * help;
+                normsteer[gi] = 1.0 / (r0[gi] * r0[gi]) / help;
+                result[gi] = scalar / (nf * nf) * norm;
+            } else {
+                const double nf = (double)M * help;
+                normsteer[gi] = 1.0 / (double)M;
+                result[gi] = scalar / nf * norm;
+            }
+        }
+    }
+}
+
+/* Number of OpenMP threads the library will use (reported as the baseline's core count). */
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_set_num_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}

@@ -1,0 +1,331 @@
+"""Generate the golden fixtures in this folder by running the reference's own code.
+
+Run once, in a container that holds the reference sources (default location below, or
+``ACOULAR_REFERENCE``)::
+
+    python tests/golden/make_golden.py
+
+The reference (Acoular 26.08) cannot be imported whole here (``traits``/``tables`` are absent), so
+this script loads its numba kernel module ``acoular/fastFuncs.py`` (+ ``internal.py``) under a stub
+package and executes the reference's own glue methods, extracted from the source by ``ast`` with
+their decorators removed, bound to plain stand-in objects:
+
+* ``BaseSpectra._get_source_data`` / ``fftfreq``      acoular/spectra.py:128-184
+* ``PowerSpectra._get_num_blocks`` / ``calc_csm``     acoular/spectra.py:281-283, 366-416
+* ``dist_mat`` (re-jitted ``njit(fastmath=True)``)    acoular/environments.py:65-103
+* ``Environment.apparent_r``                          acoular/environments.py:202-238
+* ``RectGrid`` / ``RectGrid3D`` ``_get_pos``          acoular/grids.py:350-358, 552-560
+* ``BeamformerBase.sig_loss_norm`` / ``_calc`` / ``synthetic``   acoular/fbeamform.py:438-593
+* ``WNoiseGenerator.signal``, ``SignalGenerator.usignal``, ``PointSource.result``,
+  ``_fill_mic_signal_block``, ``Mixer.result``        (fixture time data)
+
+Outputs (small ``.npz`` files) are committed; the tests never read the reference at run time.
+"""
+
+from __future__ import annotations
+
+import ast
+import importlib.util
+import os
+import sys
+import types
+import warnings
+from pathlib import Path
+from types import SimpleNamespace
+
+import numba as nb
+import numpy as np
+import scipy.linalg as spla
+from scipy import fft
+from scipy.signal import resample
+
+REF = Path(os.environ.get('ACOULAR_REFERENCE', '/root/reference'))
+OUT = Path(__file__).resolve().parent
+sys.path.insert(0, str(OUT.parent.parent))
+
+
+def _load_module(name):
+    pkg = sys.modules.get('acoular')
+    if pkg is None:
+        pkg = types.ModuleType('acoular')
+        pkg.__path__ = [str(REF / 'acoular')]
+        sys.modules['acoular'] = pkg
+    spec = importlib.util.spec_from_file_location(f'acoular.{name}', REF / 'acoular' / f'{name}.py')
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[f'acoular.{name}'] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+internal = _load_module('internal')
+fastFuncs = _load_module('fastFuncs')
+
+
+def _extract(relpath, qualname, ns, rename=None):
+    """Exec the source of ``Class.method`` or ``function`` from the reference, decorators removed."""
+    src = (REF / relpath).read_text()
+    tree = ast.parse(src)
+    parts = qualname.split('.')
+    body = tree.body
+    node = None
+    for p in parts:
+        node = next(n for n in body if isinstance(n, (ast.ClassDef, ast.FunctionDef)) and n.name == p)
+        body = node.body
+    node.decorator_list = []
+    if rename:
+        node.name = rename
+    mod = ast.Module(body=[node], type_ignores=[])
+    code = compile(ast.fix_missing_locations(mod), f'{relpath}:{qualname}', 'exec')
+    exec(code, ns)
+    return ns[node.name]
+
+
+NS = {'np': np, 'fft': fft, 'nb': nb, 'spla': spla, 'resample': resample, '_warn': warnings.warn,
+      'calcCSM': fastFuncs.calcCSM, 'beamformerFreq': fastFuncs.beamformerFreq,
+      'calcTransfer': fastFuncs.calcTransfer}
+
+dist_mat_py = _extract('acoular/environments.py', 'dist_mat', NS)
+dist_mat = nb.njit(fastmath=True)(dist_mat_py)
+NS['dist_mat'] = dist_mat
+apparent_r = _extract('acoular/environments.py', 'Environment.apparent_r', NS)
+rect_get_pos = _extract('acoular/grids.py', 'RectGrid._get_pos', NS, rename='rect_get_pos')
+rect3d_get_pos = _extract('acoular/grids.py', 'RectGrid3D._get_pos', NS, rename='rect3d_get_pos')
+get_source_data = _extract('acoular/spectra.py', 'BaseSpectra._get_source_data', NS)
+fftfreq_m = _extract('acoular/spectra.py', 'BaseSpectra.fftfreq', NS)
+get_num_blocks = _extract('acoular/spectra.py', 'PowerSpectra._get_num_blocks', NS)
+calc_csm = _extract('acoular/spectra.py', 'PowerSpectra.calc_csm', NS)
+sig_loss_norm = _extract('acoular/fbeamform.py', 'BeamformerBase.sig_loss_norm', NS)
+bf_calc = _extract('acoular/fbeamform.py', 'BeamformerBase._calc', NS)
+synthetic = _extract('acoular/fbeamform.py', 'BeamformerBase.synthetic', NS)
+w_signal = _extract('acoular/signals.py', 'WNoiseGenerator.signal', NS)
+usignal = _extract('acoular/signals.py', 'SignalGenerator.usignal', NS)
+fill_py = _extract('acoular/sources.py', '_fill_mic_signal_block', NS)
+NS['_fill_mic_signal_block'] = nb.njit(error_model='numpy')(fill_py)
+ps_result = _extract('acoular/sources.py', 'PointSource.result', NS)
+mixer_result = _extract('acoular/tprocess.py', 'Mixer.result', NS)
+
+WINDOWS = {'Rectangular': np.ones, 'Hanning': np.hanning, 'Hamming': np.hamming, 'Bartlett': np.bartlett,
+           'Blackman': np.blackman}
+OVERLAPS = {'None': 1, '50%': 2, '75%': 4, '87.5%': 8}
+
+
+# ---------------------------------------------------------------------------------------------- stand-ins
+class Env(SimpleNamespace):
+    def apparent_r(self, gpos, mpos=0.0):
+        return apparent_r(self, gpos, mpos)
+
+
+def make_rect_grid(x_min, x_max, y_min, y_max, z, increment):
+    i = abs(increment)
+    nx = round((abs(x_max - x_min) + i) / i)
+    ny = round((abs(y_max - y_min) + i) / i)
+    g = SimpleNamespace(x_min=x_min, x_max=x_max, y_min=y_min, y_max=y_max, z=z, increment=increment,
+                        nxsteps=nx, nysteps=ny, size=nx * ny, shape=(nx, ny))
+    g.pos = rect_get_pos(g)
+    return g
+
+
+def make_rect_grid3d(x_min, x_max, y_min, y_max, z_min, z_max, increment):
+    i = abs(increment)
+    nx = round((abs(x_max - x_min) + i) / i)
+    ny = round((abs(y_max - y_min) + i) / i)
+    nz = round((abs(z_max - z_min) + i) / i)
+    g = SimpleNamespace(x_min=x_min, x_max=x_max, y_min=y_min, y_max=y_max, z_min=z_min, z_max=z_max,
+                        nxsteps=nx, nysteps=ny, nzsteps=nz, size=nx * ny * nz, shape=(nx, ny, nz))
+    g.pos = rect3d_get_pos(g)
+    return g
+
+
+class WNoise(SimpleNamespace):
+    def signal(self):
+        return w_signal(self)
+
+    def usignal(self, factor):
+        return usignal(self, factor)
+
+
+class PSource(SimpleNamespace):
+    def _validate_locations(self):
+        pass
+
+    def result(self, num=128):
+        return ps_result(self, num)
+
+
+class Mix(SimpleNamespace):
+    def validate_sources(self):
+        pass
+
+    def result(self, num):
+        return mixer_result(self, num)
+
+
+class Samples(SimpleNamespace):
+    def result(self, num=128):
+        i = 0
+        while i < self.num_samples:
+            yield self.data[i:num + i]
+            i += num
+
+
+def reference_time_data(mpos, locs, seeds, rms, fs, nsamples, c=343.0, num=4096):
+    env = Env(c=c)
+    mics = SimpleNamespace(pos=mpos, num_mics=mpos.shape[1])
+    srcs = []
+    for loc, seed, r in zip(locs, seeds, rms):
+        sig = WNoise(seed=seed, rms=r, num_samples=nsamples, sample_freq=fs)
+        srcs.append(PSource(signal=sig, mics=mics, loc=np.asarray(loc, float).reshape(3, 1), env=env, start_t=0.0,
+                            start=0.0, up=16, prepadding='loop', num_samples=nsamples, sample_freq=fs,
+                            num_channels=mpos.shape[1]))
+    mix = Mix(source=srcs[0], sources=srcs[1:])
+    return np.concatenate([b.copy() for b in mix.result(num)])
+
+
+def reference_csm(data, fs, block_size, window, overlap, precision):
+    src = Samples(data=data, num_samples=data.shape[0], num_channels=data.shape[1], sample_freq=fs)
+    ps = SimpleNamespace(source=src, block_size=block_size, window_=WINDOWS[window], overlap_=OVERLAPS[overlap],
+                         precision=precision, num_channels=data.shape[1])
+    ps._get_source_data = lambda: get_source_data(ps)
+    ps.num_blocks = get_num_blocks(ps)
+    return calc_csm(ps), fftfreq_m(ps)
+
+
+class Steer(SimpleNamespace):
+    pass
+
+
+def reference_bf_result(csm, freqs, mpos, gpos, gshape, steer_type, r_diag, c=343.0, ref=None, r_diag_norm=0.0,
+                        ind=None):
+    """Run ``BeamformerBase._calc`` for bins ``ind`` (all if None); returns (F, G) and r0, rm."""
+    env = Env(c=c)
+    r0 = apparent_r(env, gpos) if ref is None else apparent_r(env, gpos, np.asarray(ref, float)[:, None])
+    rm = np.atleast_2d(apparent_r(env, gpos, mpos))
+    F, G = csm.shape[0], gpos.shape[1]
+    bf = SimpleNamespace(_f=freqs, r_diag=r_diag, r_diag_norm=r_diag_norm,
+                         freq_data=SimpleNamespace(num_channels=mpos.shape[1], csm=csm))
+    bf.sig_loss_norm = lambda: sig_loss_norm(bf)
+    bf._beamformer_params = lambda: (steer_type, lambda f: (r0, rm, 2 * np.pi * f / c))
+    bf._ac = np.zeros((F, G))
+    bf._fr = np.zeros(F, dtype='int8')
+    bf_calc(bf, np.arange(F) if ind is None else np.asarray(ind))
+    return bf._ac, r0, rm
+
+
+def reference_synthetic(ac_full, freqs, gshape, f, num):
+    bf = SimpleNamespace(result=ac_full, freq_data=SimpleNamespace(fftfreq=lambda: freqs),
+                         steer=SimpleNamespace(grid=SimpleNamespace(shape=gshape)))
+    NS['BeamformerAdaptiveGrid'] = type('BeamformerAdaptiveGrid', (), {})
+    NS['BeamformerSODIX'] = type('BeamformerSODIX', (), {})
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        return synthetic(bf, f, num)
+
+
+STEERS = ['classic', 'inverse', 'true level', 'true location']
+
+
+def golden_env():
+    """Environment.apparent_r on the reference's regression grid, checked against its committed array."""
+    g = make_rect_grid3d(-0.2, 0.2, -0.2, 0.2, 0.5, 0.9, 0.2)
+    mics = np.array(((0.5, 0.5, 0), (0, 0, 0), (-0.5, -0.5, 0)), dtype=float)
+    env = Env(c=343.0)
+    res_arr = np.vstack((apparent_r(env, g.pos, mics).T, apparent_r(env, g.pos).T))
+    res_sc = np.vstack((apparent_r(env, g.pos, 0.0).T, apparent_r(env, g.pos).T))
+    base = REF / 'tests/regression/_regtest_outputs'
+    exp_arr = np.load(base / 'test_environments.test_environment[RectGrid3D-mics-arr-default-Environment]__0/arrays.npy')
+    exp_sc = np.load(base / 'test_environments.test_environment[RectGrid3D-mics-scalar-default-Environment]__0/arrays.npy')
+    np.testing.assert_allclose(res_arr, exp_arr, rtol=1e-5, atol=1e-8)
+    np.testing.assert_allclose(res_sc, exp_sc, rtol=1e-5, atol=1e-8)
+    np.savez_compressed(OUT / 'env_apparent_r.npz', gpos=g.pos, mpos=mics, mics_arr=exp_arr, mics_scalar=exp_sc,
+                        rm_ref=apparent_r(env, g.pos, mics))
+    print('env_apparent_r.npz: matches the reference regression arrays')
+
+
+def golden_small():
+    """8 mics, 2000 samples of three monopoles: CSMs for several spectra settings + all maps."""
+    from acoular_b200.microphones import disk_mics
+    mpos = disk_mics(8, 0.5, seed=7).pos
+    fs = 51200.0
+    data = reference_time_data(mpos, [(-0.1, -0.1, -0.3), (0.15, 0, -0.3), (0, 0.1, -0.3)], [1, 2, 3],
+                               [1.0, 0.7, 0.5], fs, 2000)
+    out = {'mpos': mpos, 'data': data, 'fs': fs}
+    csm_cases = [(128, 'Hanning', '50%', 'complex128'), (256, 'Rectangular', 'None', 'complex128'),
+                 (128, 'Blackman', '75%', 'complex64'), (256, 'Hamming', '87.5%', 'complex128'),
+                 (128, 'Bartlett', '50%', 'complex64')]
+    for i, (bs, win, ov, prec) in enumerate(csm_cases):
+        csm, freqs = reference_csm(data, fs, bs, win, ov, prec)
+        out[f'csm{i}'] = csm
+        out[f'csm{i}_case'] = np.array([str(bs), win, ov, prec])
+        out[f'freqs{i}'] = freqs
+    g = make_rect_grid(-0.2, 0.2, -0.2, 0.2, -0.3, 0.05)
+    out['gpos'] = g.pos
+    out['gshape'] = np.array(g.shape)
+    csm, freqs = out['csm0'], out['freqs0']
+    ind = np.arange(10, 31)
+    out['bins'] = ind
+    for st in STEERS:
+        for rd in (False, True):
+            ac_full, r0, rm = reference_bf_result(csm, freqs, mpos, g.pos, g.shape, st, rd, ind=ind)
+            key = f'map_{st.replace(" ", "_")}_{int(rd)}'
+            out[key] = ac_full[ind]
+            out['syn_' + key] = reference_synthetic(ac_full, freqs, g.shape, 8000.0, 3)
+    # a non-origin reference position and a user r_diag_norm
+    ac_full, r0, _ = reference_bf_result(csm, freqs, mpos, g.pos, g.shape, 'true level', True,
+                                         ref=(0.1, -0.05, 0.02), r_diag_norm=1.25, ind=ind)
+    out['map_ref_rdn'] = ac_full[ind]
+    out['r0_ref'] = r0
+    np.savez_compressed(OUT / 'small_kat.npz', **out)
+    print('small_kat.npz written')
+
+
+def golden_rank1():
+    """Rank-1 CSM of one monopole (the reference's integrate test set-up, tests/unittests/test_integrate.py)."""
+    rng1 = np.random.RandomState(1)
+    mpos = rng1.normal(size=3 * 5).reshape((3, 5))
+    f = 2000.0
+    src = np.array([[0.0], [0.0], [1.0]])
+    env = Env(c=343.0)
+    r0 = apparent_r(env, src)
+    rm = np.atleast_2d(apparent_r(env, src, mpos))
+    transf = fastFuncs.calcTransfer(r0, rm, np.array(2 * np.pi * f / 343.0))
+    csm = (transf.T @ transf.T.conj().T)[None]  # (1, M, M)
+    g = make_rect_grid(-0.5, 0.5, -0.5, 0.5, 1.0, 0.25)
+    out = {'mpos': mpos, 'csm': csm, 'freqs': np.array([f]), 'gpos': g.pos, 'gshape': np.array(g.shape)}
+    for st in STEERS:
+        for rd in (False, True):
+            ac_full, _, _ = reference_bf_result(csm, np.array([f]), mpos, g.pos, g.shape, st, rd)
+            out[f'map_{st.replace(" ", "_")}_{int(rd)}'] = ac_full[0]
+    np.savez_compressed(OUT / 'rank1_kat.npz', **out)
+    print('rank1_kat.npz written')
+
+
+def golden_config1():
+    """The 64-mic three-source workload: CSM bins of the 8 kHz third-octave band and all 8 maps."""
+    from acoular_b200 import workloads
+    wl = workloads.three_sources_64()
+    data_ref = reference_time_data(wl.mics.pos, wl.locs, wl.seeds, wl.rms, wl.fs, wl.num_samples)
+    data_ours = wl.time_data()
+    diff = np.abs(data_ref - data_ours).max() / np.abs(data_ref).max()
+    print('config1 time data: restated generator vs reference max rel diff', diff)
+    assert diff < 1e-12
+    csm, freqs = reference_csm(data_ref, wl.fs, 128, 'Hanning', '50%', 'complex128')
+    g = wl.grid
+    out = {'freqs': freqs, 'band_bins': np.arange(18, 23), 'csm_band': csm[18:23],
+           'csm_diag': np.real(np.einsum('fmm->fm', csm)), 'csm_sum': csm.sum(axis=(1, 2)),
+           'data_stats': np.array([data_ref.sum(), (data_ref ** 2).sum(), data_ref[::997, ::7].sum()])}
+    for st in STEERS:
+        for rd in (False, True):
+            ac_full, _, _ = reference_bf_result(csm, freqs, wl.mics.pos, g.pos, g.shape, st, rd,
+                                                ind=np.arange(18, 23))
+            key = f'map_{st.replace(" ", "_")}_{int(rd)}'
+            out[key] = ac_full[18:23]
+            out['syn_' + key] = reference_synthetic(ac_full, freqs, g.shape, 8000.0, 3)
+    np.savez_compressed(OUT / 'config1_band.npz', **out)
+    print('config1_band.npz written')
+
+
+if __name__ == '__main__':
+    golden_env()
+    golden_small()
+    golden_rank1()
+    golden_config1()

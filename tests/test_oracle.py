@@ -1,0 +1,99 @@
+"""The CPU oracle against golden vectors produced by running the reference's own code.
+
+The oracle (``oracle/``) restates the reference's numba kernels in C and its glue in numpy; these
+tests pin it bit-for-bit (or to the stated tolerance) before it is trusted as the GPU checker.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+STEERS = ['classic', 'inverse', 'true level', 'true location']
+
+
+def test_apparent_r_matches_reference_regression(golden):
+    d = golden('env_apparent_r.npz')
+    res_arr = np.vstack((O.apparent_r(d['gpos'], d['mpos']).T, O.apparent_r(d['gpos']).T))
+    res_sc = np.vstack((O.apparent_r(d['gpos'], 0.0).T, O.apparent_r(d['gpos']).T))
+    # the reference's own snapshot tolerance (tests/regression/test_environments.py:66)
+    np.testing.assert_allclose(res_arr, d['mics_arr'], rtol=1e-5, atol=1e-8)
+    np.testing.assert_allclose(res_sc, d['mics_scalar'], rtol=1e-5, atol=1e-8)
+    assert np.array_equal(O.apparent_r(d['gpos'], d['mpos']), d['rm_ref'])
+
+
+@pytest.mark.parametrize('case', range(5))
+def test_calc_csm_bit_exact(golden, case):
+    d = golden('small_kat.npz')
+    bs, win, ov, prec = d[f'csm{case}_case']
+    csm = O.calc_csm(d['data'], int(bs), str(win), str(ov), str(prec))
+    ref = d[f'csm{case}']
+    assert csm.dtype == ref.dtype
+    assert np.array_equal(csm, ref)
+    np.testing.assert_array_equal(O.fftfreq(int(bs), float(d['fs'])), d[f'freqs{case}'])
+
+
+def test_num_blocks_formula():
+    # 2000 samples, block 128, 50 %: the formula gives 30.25 while 30 windows exist
+    assert O.num_blocks(2000, 128, 2) == 30.25
+    assert sum(1 for _ in O.source_windows(np.zeros((2000, 2)), 128, 2)) == 30
+    assert O.num_blocks(51200, 128, 2) == 799
+
+
+@pytest.mark.parametrize('steer', STEERS)
+@pytest.mark.parametrize('r_diag', [False, True])
+def test_beamformer_bit_exact(golden, steer, r_diag):
+    d = golden('small_kat.npz')
+    r0 = O.apparent_r(d['gpos'])
+    rm = O.apparent_r(d['gpos'], d['mpos'])
+    res = O.beamformer_calc(d['csm0'], d['freqs0'], d['bins'], r0, rm, 343.0, steer, r_diag)
+    key = f'map_{steer.replace(" ", "_")}_{int(r_diag)}'
+    assert np.array_equal(res[d['bins']], d[key])
+    syn = O.synthetic(res, d['freqs0'], 8000.0, 3, tuple(d['gshape']))
+    np.testing.assert_allclose(syn, d['syn_' + key], rtol=1e-14, atol=0)
+
+
+def test_reference_position_and_rdiag_norm(golden):
+    d = golden('small_kat.npz')
+    ref = np.array([0.1, -0.05, 0.02])
+    r0 = O.apparent_r(d['gpos'], ref[:, None])
+    np.testing.assert_array_equal(r0, d['r0_ref'])
+    rm = O.apparent_r(d['gpos'], d['mpos'])
+    res = O.beamformer_calc(d['csm0'], d['freqs0'], d['bins'], r0, rm, 343.0, 'true level', True, r_diag_norm=1.25)
+    assert np.array_equal(res[d['bins']], d['map_ref_rdn'])
+
+
+@pytest.mark.parametrize('steer', STEERS)
+@pytest.mark.parametrize('r_diag', [False, True])
+def test_rank1_known_answer(golden, steer, r_diag):
+    d = golden('rank1_kat.npz')
+    r0 = O.apparent_r(d['gpos'])
+    rm = O.apparent_r(d['gpos'], d['mpos'])
+    res = O.beamformer_calc(d['csm'], d['freqs'], [0], r0, rm, 343.0, steer, r_diag)
+    assert np.array_equal(res[0], d[f'map_{steer.replace(" ", "_")}_{int(r_diag)}'])
+    if steer == 'true level' and not r_diag:
+        # true-level steering recovers the source level at the source position (0, 0, 1)
+        g = int(np.argmin(np.sum((d['gpos'] - np.array([[0], [0], [1.0]])) ** 2, 0)))
+        assert abs(res[0, g] - 1.0) < 1e-6
+
+
+def test_config1_band_goldens(golden):
+    """The 64-mic three-source workload: restated time data, CSM band and all 8 maps."""
+    from acoular_b200 import workloads
+    d = golden('config1_band.npz')
+    wl = workloads.three_sources_64()
+    data = wl.time_data()
+    np.testing.assert_allclose([data.sum(), (data ** 2).sum(), data[::997, ::7].sum()], d['data_stats'], rtol=1e-12)
+    csm = O.calc_csm(data, 128, 'Hanning', '50%', 'complex128')
+    scale = np.abs(d['csm_band']).max()
+    assert np.abs(csm[18:23] - d['csm_band']).max() <= 1e-12 * scale
+    g = wl.grid
+    r0 = O.apparent_r(g.pos)
+    rm = O.apparent_r(g.pos, wl.mics.pos)
+    for steer in STEERS:
+        for r_diag in (False, True):
+            # only the band bins 18..22 are stored; pad the CSM so bin indices keep their wave numbers
+            res = O.beamformer_calc(np.concatenate([np.zeros((18, 64, 64), complex), d['csm_band']]), d['freqs'],
+                                    range(18, 23), r0, rm, 343.0, steer, r_diag)
+            key = f'map_{steer.replace(" ", "_")}_{int(r_diag)}'
+            assert np.array_equal(res[18:23], d[key])
