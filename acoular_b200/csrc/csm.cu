@@ -1,0 +1,360 @@
+// Stage A: cross-spectral matrix estimation (PowerSpectra.calc_csm, acoular/spectra.py:366-416).
+//
+// Data flow per chunk of windows (all on the device, samples resident in HBM):
+//   fft_window_kernel : samples [S][M] (f32|f64) -> window (FP64) -> rFFT (FP64, radix-2 in shared
+//                       memory) -> spectra [bin][window][mic] rounded to the CSM precision
+//   gram_kernel       : csm_upper[bin][r][c] += sum_w conj(X[bin][w][c]) * X[bin][w][r], r <= c,
+//                       64x64 upper-triangular tiles, windows streamed through shared memory
+//   finalize_kernel   : Hermitian completion and the 2/(N*sum(w^2)*num_blocks) scale
+//
+// The per-element accumulation runs sequentially over windows with the same two chained FMAs per
+// component that the reference's fastmath calcCSM (acoular/fastFuncs.py:53-57) compiles to, so
+// given identical spectra the Welch sums are bit-identical to the reference.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace acb {
+
+static thread_local std::string g_last_cuda_error;
+
+void set_cuda_error(cudaError_t e) { g_last_cuda_error = cudaGetErrorString(e); }
+
+// ------------------------------------------------------------------------------------------------
+// Windowed real FFT.  One CTA = one window x `mpb` mics; FFT of the N/2-point complex sequence
+// z[j] = x[2j] + i x[2j+1], then the split into the N/2+1 real-input bins.
+// ------------------------------------------------------------------------------------------------
+template <typename TS, bool C64>
+__global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ samples, int M, int N, int hop,
+                                                         int64_t w0, int64_t nw, int mpb,
+                                                         const double *__restrict__ window,
+                                                         const double2 *__restrict__ tw, int bin_lo, int nbins,
+                                                         void *__restrict__ out)
+{
+    extern __shared__ double2 zs[];  // [mpb][H]
+    const int H = N >> 1;
+    int logH = 0;
+    while ((1 << logH) < H) ++logH;
+    const int64_t w = w0 + blockIdx.y;
+    const int m0 = blockIdx.x * mpb;
+    const int nm = min(mpb, M - m0);
+    const TS *src = samples + (w * (int64_t)hop) * M;
+
+    // load + window + bit-reversed placement
+    for (int idx = threadIdx.x; idx < H * nm; idx += blockDim.x) {
+        const int ml = idx % nm;
+        const int j = idx / nm;
+        const double x0 = (double)src[(int64_t)(2 * j) * M + m0 + ml] * window[2 * j];
+        const double x1 = (double)src[(int64_t)(2 * j + 1) * M + m0 + ml] * window[2 * j + 1];
+        const int jr = (int)(__brev((unsigned)j) >> (32 - logH));
+        zs[ml * H + (logH ? jr : 0)] = make_double2(x0, x1);
+    }
+    __syncthreads();
+
+    // radix-2 DIT butterflies
+    for (int len = 2; len <= H; len <<= 1) {
+        const int half = len >> 1;
+        const int stride = N / len;  // twiddle index step in the N-point table
+        for (int idx = threadIdx.x; idx < nm * (H >> 1); idx += blockDim.x) {
+            const int ml = idx / (H >> 1);
+            const int p = idx % (H >> 1);
+            const int grp = p / half, pos = p % half;
+            double2 *z = zs + ml * H;
+            const int i0 = grp * len + pos, i1 = i0 + half;
+            const double2 t = tw[pos * stride];
+            const double2 b = z[i1];
+            const double br = b.x * t.x - b.y * t.y;
+            const double bi = b.x * t.y + b.y * t.x;
+            const double2 a = z[i0];
+            z[i0] = make_double2(a.x + br, a.y + bi);
+            z[i1] = make_double2(a.x - br, a.y - bi);
+        }
+        __syncthreads();
+    }
+
+    // real-input split: X[k] = E + W^k O,  E = (Z[k] + conj(Z[H-k]))/2,  O = -i (Z[k] - conj(Z[H-k]))/2
+    for (int idx = threadIdx.x; idx < nbins * nm; idx += blockDim.x) {
+        const int ml = idx % nm;
+        const int k = bin_lo + idx / nm;
+        const double2 *z = zs + ml * H;
+        const double2 zk = z[k % H];
+        const double2 zc = z[(H - k % H) % H];
+        const double er = 0.5 * (zk.x + zc.x), ei = 0.5 * (zk.y - zc.y);
+        const double orr = 0.5 * (zk.y + zc.y), oi = -0.5 * (zk.x - zc.x);
+        double2 wk;
+        if (k < H) wk = tw[k];
+        else wk = make_double2(-1.0, 0.0);
+        const double xr = er + (wk.x * orr - wk.y * oi);
+        const double xi = ei + (wk.x * oi + wk.y * orr);
+        const int64_t o = ((int64_t)(k - bin_lo) * nw + blockIdx.y) * M + m0 + ml;
+        if (C64) reinterpret_cast<float2 *>(out)[o] = make_float2(__double2float_rn(xr), __double2float_rn(xi));
+        else reinterpret_cast<double2 *>(out)[o] = make_double2(xr, xi);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Welch Gram accumulation, upper-triangular 64x64 tiles; thread (tx, ty) owns rows ty+16i and
+// columns tx+16j of the tile (conflict-free shared-memory reads, coalesced stores).
+// ------------------------------------------------------------------------------------------------
+template <bool C64>
+struct GramT {
+    using V = typename std::conditional<C64, float2, double2>::type;
+    using S = typename std::conditional<C64, float, double>::type;
+};
+
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+constexpr int GT = 64;   // tile edge
+constexpr int GKC = 16;  // windows per shared-memory stage
+
+template <bool C64>
+__global__ void __launch_bounds__(256) gram_kernel(const void *__restrict__ spec_, int M, int64_t nw,
+                                                   void *__restrict__ csm_)
+{
+    using V = typename GramT<C64>::V;
+    using S = typename GramT<C64>::S;
+    __shared__ V xr_s[GKC][GT];
+    __shared__ V xc_s[GKC][GT];
+    const V *spec = reinterpret_cast<const V *>(spec_);
+    V *csm = reinterpret_cast<V *>(csm_);
+
+    // upper-triangular tile index -> (ti, tj), ti <= tj
+    const int T = (M + GT - 1) / GT;
+    int t = blockIdx.x, ti = 0;
+    while (t >= T - ti) {
+        t -= T - ti;
+        ++ti;
+    }
+    const int tj = ti + t;
+    const int f = blockIdx.y;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int r0 = ti * GT, c0 = tj * GT;
+
+    S acc_re[4][4], acc_im[4][4];
+    V *base = csm + (int64_t)f * M * M;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = r0 + ty + 16 * i, c = c0 + tx + 16 * j;
+            V v = {0, 0};
+            if (r < M && c < M && r <= c) v = base[(int64_t)r * M + c];
+            acc_re[i][j] = v.x;
+            acc_im[i][j] = v.y;
+        }
+
+    const V *sp = spec + (int64_t)f * nw * M;
+    for (int64_t k0 = 0; k0 < nw; k0 += GKC) {
+        const int kc = (int)((nw - k0) < GKC ? (nw - k0) : GKC);
+        for (int idx = threadIdx.x; idx < GKC * GT; idx += blockDim.x) {
+            const int kk = idx / GT, m = idx % GT;
+            V a = {0, 0}, b = {0, 0};
+            if (kk < kc) {
+                if (r0 + m < M) a = sp[(k0 + kk) * M + r0 + m];
+                if (c0 + m < M) b = sp[(k0 + kk) * M + c0 + m];
+            }
+            xr_s[kk][m] = a;
+            xc_s[kk][m] = b;
+        }
+        __syncthreads();
+        for (int kk = 0; kk < kc; ++kk) {
+            V xr[4], xc[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) xr[i] = xr_s[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) xc[j] = xc_s[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    // temp = conj(X[c]) = (tr, ti); csm += temp * X[r]
+                    const S tr = xc[j].x, tim = -xc[j].y;
+                    acc_re[i][j] = fma_rn(-tim, xr[i].y, fma_rn(tr, xr[i].x, acc_re[i][j]));
+                    acc_im[i][j] = fma_rn(tr, xr[i].y, fma_rn(tim, xr[i].x, acc_im[i][j]));
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = r0 + ty + 16 * i, c = c0 + tx + 16 * j;
+            if (r < M && c < M && r <= c) {
+                V v;
+                v.x = acc_re[i][j];
+                v.y = acc_im[i][j];
+                base[(int64_t)r * M + c] = v;
+            }
+        }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Hermitian completion + scale, 32x32 tiles through shared memory for the transposed half.
+// ------------------------------------------------------------------------------------------------
+template <bool C64>
+__global__ void __launch_bounds__(256) finalize_kernel(const void *__restrict__ up_, int M, double scale,
+                                                       double2 *__restrict__ out)
+{
+    using V = typename GramT<C64>::V;
+    __shared__ double2 tile[32][33];
+    const V *up = reinterpret_cast<const V *>(up_);
+    const int f = blockIdx.z;
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const V *ub = up + (int64_t)f * M * M;
+    double2 *ob = out + (int64_t)f * M * M;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (r0 <= c0 + 31) {
+        // tile touches the upper triangle: direct read (lower part of a diagonal tile handled below)
+        for (int i = ty; i < 32; i += 8) {
+            const int r = r0 + i, c = c0 + tx;
+            if (r < M && c < M && r <= c) {
+                const V v = ub[(int64_t)r * M + c];
+                ob[(int64_t)r * M + c] = make_double2((double)v.x * scale, (double)v.y * scale);
+            }
+        }
+    }
+    if (c0 <= r0 + 31) {
+        // lower elements (r > c) read transposed from upper[c][r]
+        for (int i = ty; i < 32; i += 8) {
+            const int c = c0 + i, r = r0 + tx;  // coalesced read along r of upper[c][*]
+            double2 v = make_double2(0.0, 0.0);
+            if (r < M && c < M && c < r) {
+                const V u = ub[(int64_t)c * M + r];
+                v = make_double2((double)u.x, (double)u.y);
+            }
+            tile[i][tx] = v;
+        }
+        __syncthreads();
+        for (int i = ty; i < 32; i += 8) {
+            const int r = r0 + i, c = c0 + tx;
+            if (r < M && c < M && r > c) {
+                const double2 u = tile[tx][i];
+                ob[(int64_t)r * M + c] = make_double2(u.x * scale, -u.y * scale);
+            }
+        }
+    }
+}
+
+static int fft_mics_per_block(int N)
+{
+    const int cap = 16384 / N;  // 128 KB of complex doubles per CTA
+    return cap >= 16 ? 16 : (cap < 1 ? 1 : cap);
+}
+
+}  // namespace acb
+
+using namespace acb;
+
+extern "C" {
+
+const char *acb_status_string(int s)
+{
+    switch (s) {
+    case ACB_OK: return "ok";
+    case ACB_ERR_SHAPE: return "size or shape out of range";
+    case ACB_ERR_ARG: return "invalid argument";
+    case ACB_ERR_CUDA: return "CUDA error";
+    case ACB_ERR_UNSUPPORTED: return "unsupported by this build";
+    case ACB_ERR_WORKSPACE: return "workspace missing or too small";
+    case ACB_ERR_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+    }
+}
+
+int acb_abi_version(void) { return 1; }
+
+const char *acb_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
+
+int acb_calc_csm_c128(void *csm, const void *spec, int num_freqs, int num_mics, void *stream)
+{
+    if (!csm || !spec) return ACB_ERR_ARG;
+    if (num_freqs <= 0 || num_mics <= 0) return ACB_ERR_SHAPE;
+    const int T = (num_mics + GT - 1) / GT;
+    gram_kernel<false><<<dim3(T * (T + 1) / 2, num_freqs), 256, 0, as_stream(stream)>>>(spec, num_mics, 1, csm);
+    return check_launch();
+}
+
+int acb_calc_csm_c64(void *csm, const void *spec, int num_freqs, int num_mics, void *stream)
+{
+    if (!csm || !spec) return ACB_ERR_ARG;
+    if (num_freqs <= 0 || num_mics <= 0) return ACB_ERR_SHAPE;
+    const int T = (num_mics + GT - 1) / GT;
+    gram_kernel<true><<<dim3(T * (T + 1) / 2, num_freqs), 256, 0, as_stream(stream)>>>(spec, num_mics, 1, csm);
+    return check_launch();
+}
+
+size_t acb_csm_workspace_bytes(int num_mics, int num_bins, int64_t num_windows, int precision)
+{
+    if (num_mics <= 0 || num_bins <= 0 || num_windows <= 0) return 0;
+    const size_t es = precision == ACB_C64 ? 8 : 16;
+    return (size_t)num_mics * (size_t)num_bins * (size_t)num_windows * es;
+}
+
+int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_samples, int num_mics, int block_size,
+                       int hop, int64_t first_window, int64_t num_windows, const double *window,
+                       const void *twiddle, int bin_lo, int num_bins, int precision, void *csm_upper,
+                       void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!samples || !window || !twiddle || !csm_upper) return ACB_ERR_ARG;
+    if (sample_dtype != ACB_F32 && sample_dtype != ACB_F64) return ACB_ERR_ARG;
+    if (precision != ACB_C128 && precision != ACB_C64) return ACB_ERR_ARG;
+    if (num_mics <= 0 || num_windows < 0 || first_window < 0 || hop <= 0) return ACB_ERR_SHAPE;
+    if (block_size < 16 || (block_size & (block_size - 1))) return ACB_ERR_SHAPE;
+    if (block_size > 16384) return ACB_ERR_UNSUPPORTED;
+    if (bin_lo < 0 || num_bins <= 0 || bin_lo + num_bins > block_size / 2 + 1) return ACB_ERR_SHAPE;
+    if (num_windows == 0) return ACB_OK;
+    if ((first_window + num_windows - 1) * (int64_t)hop + block_size > num_samples) return ACB_ERR_SHAPE;
+    if (num_windows > 65535) return ACB_ERR_SHAPE;  // one grid row per window
+    const size_t need = acb_csm_workspace_bytes(num_mics, num_bins, num_windows, precision);
+    if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
+    cudaStream_t s = as_stream(stream);
+    const int mpb = fft_mics_per_block(block_size);
+    const dim3 g1((num_mics + mpb - 1) / mpb, (unsigned)num_windows);
+    const size_t smem = (size_t)mpb * (block_size / 2) * sizeof(double2);
+    const double2 *tw = reinterpret_cast<const double2 *>(twiddle);
+#define ACB_FFT_LAUNCH(TS, C64)                                                                              \
+    do {                                                                                                     \
+        auto kern = fft_window_kernel<TS, C64>;                                                              \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                  \
+        kern<<<g1, 256, smem, s>>>(reinterpret_cast<const TS *>(samples), num_mics, block_size, hop,         \
+                                   first_window, num_windows, mpb, window, tw, bin_lo, num_bins, workspace); \
+    } while (0)
+    if (sample_dtype == ACB_F32) {
+        if (precision == ACB_C64) ACB_FFT_LAUNCH(float, true);
+        else ACB_FFT_LAUNCH(float, false);
+    } else {
+        if (precision == ACB_C64) ACB_FFT_LAUNCH(double, true);
+        else ACB_FFT_LAUNCH(double, false);
+    }
+#undef ACB_FFT_LAUNCH
+    int st = check_launch();
+    if (st) return st;
+    const int T = (num_mics + GT - 1) / GT;
+    const dim3 g2(T * (T + 1) / 2, num_bins);
+    if (precision == ACB_C64) gram_kernel<true><<<g2, 256, 0, s>>>(workspace, num_mics, num_windows, csm_upper);
+    else gram_kernel<false><<<g2, 256, 0, s>>>(workspace, num_mics, num_windows, csm_upper);
+    return check_launch();
+}
+
+int acb_csm_finalize(const void *csm_upper, int num_bins, int num_mics, int precision, double scale, void *csm_out,
+                     void *stream)
+{
+    if (!csm_upper || !csm_out) return ACB_ERR_ARG;
+    if (precision != ACB_C128 && precision != ACB_C64) return ACB_ERR_ARG;
+    if (num_bins <= 0 || num_mics <= 0 || num_bins > 65535) return ACB_ERR_SHAPE;
+    const int T = (num_mics + 31) / 32;
+    const dim3 g(T, T, num_bins);
+    if (precision == ACB_C64)
+        finalize_kernel<true><<<g, 256, 0, as_stream(stream)>>>(csm_upper, num_mics, scale, (double2 *)csm_out);
+    else
+        finalize_kernel<false><<<g, 256, 0, as_stream(stream)>>>(csm_upper, num_mics, scale, (double2 *)csm_out);
+    return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,306 @@
+// Stage B, plain FP64 form: h^H C h per (grid point, bin) as in _freqBeamformer_FullCSM
+// (acoular/fastFuncs.py:217-311), batched over bins.
+//
+// CTA = 32 grid points (one per lane) x one bin, 8 warps.
+//   1. distances |g - m| in FP64 (same contraction as the reference's dist_mat), phase
+//      fl32(k*r), float32 cos/sin (correctly rounded, optionally corrected to the C library's
+//      cosf/sinf by the exception table), steering h = cos - i sin, scaled by r (inverse) or 1/r
+//      (true level / true location); h lives only in shared memory, chunk by chunk.
+//   2. B = 2 Re sum_{a<b} conj(h_a) C_ab h_b (+ sum_a C_aa |h_a|^2 without diagonal removal):
+//      warps take 8-row blocks of C (snake order for balance), each lane accumulates
+//      y_r = sum_b C_{a_r b} h_b for its grid point with C_ab broadcast from L1/L2 and h_b from
+//      shared memory, then conj(h_a) y.
+//   3. cross-warp sum, normalisation of the steering type, optional clipping of negatives.
+// Mic chunks: M <= 256 is one chunk; larger arrays use 128-mic chunks and loop over chunk pairs.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace acb {
+
+constexpr int kLanes = 32;
+constexpr int kWarps = 8;
+constexpr int kRowBlock = 8;
+
+struct MapArgs {
+    int M;
+    int64_t G;
+    int steer_type;
+    int r_diag;
+    int clip;
+    double norm;
+    int ref_mode;
+    double ref0, ref1, ref2, ref_dist;
+    int faithful;
+    const uint64_t *table;
+    uint64_t table_mask;
+};
+
+template <bool USE_RM>
+__device__ __forceinline__ double grid_mic_dist(const MapArgs &a, const double *__restrict__ rm, int64_t g, int m,
+                                                double g0, double g1, double g2, const double *mp)
+{
+    if (USE_RM) return rm[g * a.M + m];
+    return dist3(g0, g1, g2, mp[m], mp[a.M + m], mp[2 * a.M + m]);
+}
+
+// Synthesise h for mics [m0, m0+n) of this CTA's 32 grid points into hs[m - m0][lane].
+template <bool USE_RM>
+__device__ __forceinline__ void synth_chunk(const MapArgs &a, const double *__restrict__ rm, double k, int64_t g,
+                                           bool gvalid, double g0, double g1, double g2, const double *mp, int m0,
+                                           int n, double2 *hs)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = warp; i < n; i += kWarps) {
+        double2 h = make_double2(0.0, 0.0);
+        if (gvalid) {
+            const double r = grid_mic_dist<USE_RM>(a, rm, g, m0 + i, g0, g1, g2, mp);
+            const float arg = __double2float_rn(__dmul_rn(k, r));
+            float c, s;
+            sincos_f32_arg(arg, a.table, a.table_mask, a.faithful != 0, c, s);
+            h = make_double2((double)c, -(double)s);
+            if (a.steer_type == 2) {
+                h.x = __dmul_rn(h.x, r);
+                h.y = __dmul_rn(h.y, r);
+            } else if (a.steer_type >= 3) {
+                h.x = __ddiv_rn(h.x, r);
+                h.y = __ddiv_rn(h.y, r);
+            }
+        }
+        hs[i * kLanes + lane] = h;
+    }
+}
+
+// Quadratic-form contribution of rows [ra0, ra0+na) x cols [cb0, cb0+nb) of C for this lane.
+// If `diag_block` the block pair is the same chunk: only b > a counts (plus the diagonal when
+// requested).  Returns (off-diagonal sum, diagonal sum).
+__device__ __forceinline__ void quad_block(const double2 *__restrict__ C, int M, const double2 *ha, int ra0, int na,
+                                           const double2 *hb, int cb0, int nb, bool diag_block, bool with_diag,
+                                           double &off, double &dsum)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nrb = (na + kRowBlock - 1) / kRowBlock;
+    for (int j = 0; j < nrb; ++j) {
+        // snake assignment of row blocks to warps: 0..7, 7..0, 0..7, ...
+        const int owner = ((j / kWarps) & 1) ? (kWarps - 1 - (j % kWarps)) : (j % kWarps);
+        if (owner != warp) continue;
+        const int a0 = j * kRowBlock;  // local row index in chunk A
+        double yr[kRowBlock], yi[kRowBlock];
+        const double2 *crow[kRowBlock];
+#pragma unroll
+        for (int r = 0; r < kRowBlock; ++r) {
+            yr[r] = 0.0;
+            yi[r] = 0.0;
+            const int ar = min(a0 + r, na - 1);
+            crow[r] = C + (int64_t)(ra0 + ar) * M + cb0;
+        }
+        const int bstart = diag_block ? a0 + 1 : 0;
+        for (int b = bstart; b < nb; ++b) {
+            const double2 h = hb[b * kLanes + lane];
+#pragma unroll
+            for (int r = 0; r < kRowBlock; ++r) {
+                const bool use = (a0 + r < na) && (!diag_block || b > a0 + r);
+                double2 c = __ldg(crow[r] + b);
+                if (!use) c = make_double2(0.0, 0.0);
+                yr[r] = fma(c.x, h.x, fma(-c.y, h.y, yr[r]));
+                yi[r] = fma(c.x, h.y, fma(c.y, h.x, yi[r]));
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kRowBlock; ++r) {
+            if (a0 + r < na) {
+                const double2 h = ha[(a0 + r) * kLanes + lane];
+                off = fma(h.x, yr[r], fma(h.y, yi[r], off));  // Re(conj(h) y)
+                if (with_diag) {
+                    const double2 c = __ldg(C + (int64_t)(ra0 + a0 + r) * M + (ra0 + a0 + r));
+                    // (C_aa * conj(h)) * h, real part
+                    const double pr = c.x * h.x + c.y * h.y;
+                    const double pi = -c.x * h.y + c.y * h.x;
+                    dsum += pr * h.x - pi * h.y;
+                }
+            }
+        }
+    }
+}
+
+template <bool USE_RM>
+__global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2 *__restrict__ csm,
+                                                        const double *__restrict__ wavenumber, double k_scalar,
+                                                        const double *__restrict__ mpos,
+                                                        const double *__restrict__ gpos,
+                                                        const double *__restrict__ r0_in,
+                                                        const double *__restrict__ rm, int mc,
+                                                        double *__restrict__ out_map,
+                                                        double *__restrict__ out_norm)
+{
+    extern __shared__ double smem[];
+    const int M = a.M;
+    double *mp = smem;                                          // [3][M]
+    double2 *ha = reinterpret_cast<double2 *>(smem + ((3 * M + 1) & ~1));  // [mc][32]
+    double2 *hb = ha + (size_t)mc * kLanes;                      // [mc][32] (only if M > mc)
+    __shared__ double red_off[kWarps][kLanes], red_diag[kWarps][kLanes], red_s[kWarps][kLanes];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int bin = blockIdx.y;
+    const int64_t g = (int64_t)blockIdx.x * kLanes + lane;
+    const bool gvalid = g < a.G;
+    const double k = wavenumber ? wavenumber[bin] : k_scalar;
+    const double2 *C = csm + (int64_t)bin * M * M;
+
+    if (!USE_RM)
+        for (int i = threadIdx.x; i < 3 * M; i += blockDim.x) mp[i] = mpos[i];
+    double g0 = 0, g1 = 0, g2 = 0;
+    if (gvalid && !USE_RM) {
+        g0 = gpos[g];
+        g1 = gpos[a.G + g];
+        g2 = gpos[2 * a.G + g];
+    }
+    __syncthreads();
+
+    // steering normalisation sum S (inverse: sum r^2; true level / location: sum 1/r^2)
+    double s_part = 0.0;
+    if (gvalid && a.steer_type >= 2) {
+        for (int m = warp; m < M; m += kWarps) {
+            const double r = grid_mic_dist<USE_RM>(a, rm, g, m, g0, g1, g2, mp);
+            s_part += (a.steer_type == 2) ? r * r : 1.0 / (r * r);
+        }
+    }
+
+    double off = 0.0, dsum = 0.0;
+    const int nchunks = (M + mc - 1) / mc;
+    for (int ca = 0; ca < nchunks; ++ca) {
+        const int ma0 = ca * mc, na = min(mc, M - ma0);
+        synth_chunk<USE_RM>(a, rm, k, g, gvalid, g0, g1, g2, mp, ma0, na, ha);
+        __syncthreads();
+        quad_block(C, M, ha, ma0, na, ha, ma0, na, true, a.r_diag == 0, off, dsum);
+        for (int cb = ca + 1; cb < nchunks; ++cb) {
+            const int mb0 = cb * mc, nb = min(mc, M - mb0);
+            __syncthreads();
+            synth_chunk<USE_RM>(a, rm, k, g, gvalid, g0, g1, g2, mp, mb0, nb, hb);
+            __syncthreads();
+            quad_block(C, M, ha, ma0, na, hb, mb0, nb, false, false, off, dsum);
+        }
+        __syncthreads();
+    }
+
+    red_off[warp][lane] = off;
+    red_diag[warp][lane] = dsum;
+    red_s[warp][lane] = s_part;
+    __syncthreads();
+    if (warp == 0 && gvalid) {
+        double o = 0.0, d = 0.0, S = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            o += red_off[w][lane];
+            d += red_diag[w][lane];
+            S += red_s[w][lane];
+        }
+        const double scalar = 2.0 * o + d;
+        double r0;
+        if (a.ref_mode == 1) r0 = a.ref_dist;
+        else if (USE_RM) r0 = r0_in[g];
+        else r0 = dist3(g0, g1, g2, a.ref0, a.ref1, a.ref2);
+        const double Md = (double)M;
+        double res, ns;
+        if (a.steer_type == 1) {
+            ns = 1.0 / Md;
+            res = scalar / (Md * Md) * a.norm;
+        } else if (a.steer_type == 2) {
+            const double nf = Md * r0;
+            const double nf2 = nf * nf;
+            ns = S / nf2;
+            res = scalar / nf2 * a.norm;
+        } else if (a.steer_type == 3) {
+            const double nf = r0 * S;
+            ns = 1.0 / (r0 * r0) / S;
+            res = scalar / (nf * nf) * a.norm;
+        } else {
+            const double nf = Md * S;
+            ns = 1.0 / Md;
+            res = scalar / nf * a.norm;
+        }
+        if (a.clip && res < 0.0) res = 0.0;
+        out_map[(int64_t)bin * a.G + g] = res;
+        if (out_norm) out_norm[(int64_t)bin * a.G + g] = ns;
+    }
+}
+
+static int make_args(const acb_map_params *p, MapArgs &a)
+{
+    if (!p) return ACB_ERR_ARG;
+    if (p->num_mics < 2 || p->num_mics > 2048 || p->num_grid <= 0 || p->num_bins <= 0 || p->num_bins > 65535)
+        return ACB_ERR_SHAPE;
+    if (p->steer_type < 1 || p->steer_type > 4) return ACB_ERR_ARG;
+    if (p->glibc_faithful && (!p->sincos_table || p->sincos_table_slots <= 0 ||
+                              (p->sincos_table_slots & (p->sincos_table_slots - 1))))
+        return ACB_ERR_ARG;
+    a.M = p->num_mics;
+    a.G = p->num_grid;
+    a.steer_type = p->steer_type;
+    a.r_diag = p->r_diag;
+    a.clip = p->clip_negative;
+    a.norm = p->norm;
+    a.ref_mode = p->ref_mode;
+    a.ref0 = p->ref_point[0];
+    a.ref1 = p->ref_point[1];
+    a.ref2 = p->ref_point[2];
+    a.ref_dist = p->ref_distance;
+    a.faithful = p->glibc_faithful;
+    a.table = p->sincos_table;
+    a.table_mask = p->glibc_faithful ? (uint64_t)p->sincos_table_slots - 1 : 0;
+    return ACB_OK;
+}
+
+template <bool USE_RM>
+static int launch_plain(const MapArgs &a, int nbins, const void *csm, const double *k, double k_scalar,
+                        const double *mpos,
+                        const double *gpos, const double *r0, const double *rm, double *out_map, double *out_norm,
+                        cudaStream_t s)
+{
+    const int mc = a.M <= 256 ? a.M : 128;
+    const int nbuf = a.M <= mc ? 1 : 2;
+    const size_t smem = (size_t)(((3 * a.M + 1) & ~1) * sizeof(double)) + (size_t)nbuf * mc * kLanes * sizeof(double2);
+    auto kern = map_plain_kernel<USE_RM>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const dim3 grid((unsigned)((a.G + kLanes - 1) / kLanes), nbins);
+    kern<<<grid, kLanes * kWarps, smem, s>>>(a, reinterpret_cast<const double2 *>(csm), k, k_scalar, mpos, gpos, r0,
+                                            rm, mc,
+                                            out_map, out_norm);
+    return check_launch();
+}
+
+}  // namespace acb
+
+using namespace acb;
+
+extern "C" {
+
+int acb_map_f64(const acb_map_params *p, const void *csm, const double *wavenumber, const double *mpos,
+                const double *gpos, double *out_map, double *out_steer_norm, int *error_word, void *stream)
+{
+    (void)error_word;
+    MapArgs a;
+    int st = make_args(p, a);
+    if (st) return st;
+    if (!csm || !wavenumber || !mpos || !gpos || !out_map) return ACB_ERR_ARG;
+    if ((a.G + kLanes - 1) / kLanes > 0x7fffffffLL) return ACB_ERR_SHAPE;
+    return launch_plain<false>(a, p->num_bins, csm, wavenumber, 0.0, mpos, gpos, nullptr, nullptr, out_map,
+                               out_steer_norm, as_stream(stream));
+}
+
+int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wavenumber, const double *r0,
+                            const double *rm, double *out_map, double *out_steer_norm, void *stream)
+{
+    MapArgs a;
+    int st = make_args(p, a);
+    if (st) return st;
+    if (p->num_bins != 1) return ACB_ERR_SHAPE;
+    if (!csm || !r0 || !rm || !out_map) return ACB_ERR_ARG;
+    a.ref_mode = 0;
+    st = launch_plain<true>(a, 1, csm, nullptr, wavenumber, nullptr, nullptr, r0, rm, out_map, out_steer_norm,
+                            as_stream(stream));
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,248 @@
+"""Device-level entry points: resident buffers, CSM and map launches on the current torch stream.
+
+Everything here takes and returns torch CUDA tensors; the Acoular-compatible classes in
+:mod:`acoular_b200.spectra` and :mod:`acoular_b200.fbeamform` wrap these for numpy users.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import os
+import threading
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+WINDOWS = {
+    'Rectangular': np.ones,
+    'Hanning': np.hanning,
+    'Hamming': np.hamming,
+    'Bartlett': np.bartlett,
+    'Blackman': np.blackman,
+}
+OVERLAPS = {'None': 1, '50%': 2, '75%': 4, '87.5%': 8}
+
+DEFAULT_WORKSPACE_BYTES = 2 << 30
+
+
+def require_cuda(device=None) -> torch.device:
+    if not torch.cuda.is_available():
+        msg = 'acoular_b200 needs a CUDA device (B200, sm_100a); no CPU fallback exists'
+        raise RuntimeError(msg)
+    N.lib()
+    return torch.device('cuda', torch.cuda.current_device() if device is None else torch.device(device).index or 0)
+
+
+def num_windows(num_samples: int, block_size: int, overlap: int) -> int:
+    """Windows yielded by ``_get_source_data`` (acoular/spectra.py:171-184): starts j*hop with
+    j*hop + block_size <= num_samples."""
+    hop = block_size // overlap
+    if num_samples < block_size:
+        return 0
+    return (num_samples - block_size) // hop + 1
+
+
+def num_blocks(num_samples: int, block_size: int, overlap: int) -> float:
+    """The reference's averaging divisor (acoular/spectra.py:281-283), a float formula."""
+    return overlap * num_samples / block_size - overlap + 1
+
+
+_tw_cache: dict = {}
+_win_cache: dict = {}
+
+
+def twiddles(block_size: int, device) -> torch.Tensor:
+    key = (block_size, str(device))
+    t = _tw_cache.get(key)
+    if t is None:
+        k = np.arange(block_size // 2)
+        w = np.exp(-2j * np.pi * k / block_size)
+        t = torch.as_tensor(w.astype(np.complex128), device=device)
+        _tw_cache[key] = t
+    return t
+
+
+def window_vector(window: str, block_size: int, device) -> tuple[torch.Tensor, float]:
+    key = (window, block_size, str(device))
+    v = _win_cache.get(key)
+    if v is None:
+        w = WINDOWS[window](block_size).astype(np.float64)
+        v = (torch.as_tensor(w, device=device), float(np.dot(w, w)))
+        _win_cache[key] = v
+    return v
+
+
+def csm_upper_accumulate(samples: torch.Tensor, block_size: int, window: str, overlap: str,
+                         precision: str = 'complex128', bin_lo: int = 0, num_bins: int | None = None,
+                         csm_upper: torch.Tensor | None = None, workspace: torch.Tensor | None = None,
+                         max_workspace_bytes: int = DEFAULT_WORKSPACE_BYTES, first_window: int = 0,
+                         windows: int | None = None):
+    """Welch sum (upper triangle) of all windows of ``samples`` (device, (S, M) f32/f64).
+
+    Returns ``(csm_upper, n_windows)``; ``csm_upper`` is (num_bins, M, M) complex128/complex64.
+    """
+    dev = samples.device
+    if samples.dim() != 2 or not samples.is_contiguous():
+        msg = 'samples must be a contiguous (num_samples, num_mics) tensor'
+        raise ValueError(msg)
+    S, M = samples.shape
+    ov = OVERLAPS[overlap]
+    hop = block_size // ov
+    F = block_size // 2 + 1
+    nb = F - bin_lo if num_bins is None else num_bins
+    prec = N.C64 if precision == 'complex64' else N.C128
+    cdt = torch.complex64 if prec == N.C64 else torch.complex128
+    if csm_upper is None:
+        csm_upper = torch.zeros((nb, M, M), dtype=cdt, device=dev)
+    K = num_windows(S, block_size, ov) if windows is None else windows
+    sd = N.F32 if samples.dtype == torch.float32 else N.F64
+    if samples.dtype not in (torch.float32, torch.float64):
+        samples = samples.to(torch.float64)
+        sd = N.F64
+    wv, _ = window_vector(window, block_size, dev)
+    tw = twiddles(block_size, dev)
+    per_win = N.lib().acb_csm_workspace_bytes(M, nb, 1, prec)
+    chunk = int(max(1, min(65535, max_workspace_bytes // max(per_win, 1), K if K > 0 else 1)))
+    if workspace is None or workspace.numel() < per_win * chunk:
+        workspace = torch.empty(per_win * chunk, dtype=torch.uint8, device=dev)
+    st = N.stream_handle()
+    L = N.lib()
+    w = first_window
+    end = first_window + K
+    while w < end:
+        nw = min(chunk, end - w)
+        N.check(L.acb_csm_accumulate(samples.data_ptr(), sd, S, M, block_size, hop, w, nw, wv.data_ptr(),
+                                     tw.data_ptr(), bin_lo, nb, prec, csm_upper.data_ptr(), workspace.data_ptr(),
+                                     workspace.numel(), st), 'acb_csm_accumulate')
+        w += nw
+    return csm_upper, K
+
+
+def csm_finalize(csm_upper: torch.Tensor, scale: float, out: torch.Tensor | None = None) -> torch.Tensor:
+    nb, M, _ = csm_upper.shape
+    prec = N.C64 if csm_upper.dtype == torch.complex64 else N.C128
+    if out is None:
+        out = torch.empty((nb, M, M), dtype=torch.complex128, device=csm_upper.device)
+    N.check(N.lib().acb_csm_finalize(csm_upper.data_ptr(), nb, M, prec, float(scale), out.data_ptr(),
+                                     N.stream_handle()), 'acb_csm_finalize')
+    return out
+
+
+def calc_csm(samples: torch.Tensor, block_size: int = 1024, window: str = 'Rectangular', overlap: str = 'None',
+             precision: str = 'complex128', bin_lo: int = 0, num_bins: int | None = None,
+             max_workspace_bytes: int = DEFAULT_WORKSPACE_BYTES) -> torch.Tensor:
+    """Full CSM (num_bins, M, M) complex128 on the device, as ``PowerSpectra.calc_csm`` returns it."""
+    ov = OVERLAPS[overlap]
+    up, _ = csm_upper_accumulate(samples, block_size, window, overlap, precision, bin_lo, num_bins,
+                                 max_workspace_bytes=max_workspace_bytes)
+    _, weight = window_vector(window, block_size, samples.device)
+    nblk = num_blocks(samples.shape[0], block_size, ov)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        scale = np.float64(2.0 / block_size) / np.float64(weight) / np.float64(nblk)
+    return csm_finalize(up, float(scale))
+
+
+# ------------------------------------------------------------------------------------------------
+# sincos exception table (glibc-faithful plain form)
+# ------------------------------------------------------------------------------------------------
+SINCOS_MAX_ARG = 2048.0
+SINCOS_SLOTS = 1 << 23
+_table_lock = threading.Lock()
+_table_host = None
+_table_dev: dict = {}
+
+
+def _cache_dir() -> Path:
+    d = Path(os.environ.get('ACOULAR_B200_CACHE', Path.home() / '.cache' / 'acoular_b200'))
+    d.mkdir(parents=True, exist_ok=True)
+    return d
+
+
+def sincos_table_host() -> np.ndarray:
+    """Exception table of the host C library's float32 cosf/sinf over [0, 2048) (built once, cached)."""
+    global _table_host
+    with _table_lock:
+        if _table_host is not None:
+            return _table_host
+        libc_ver = os.confstr('CS_GNU_LIBC_VERSION') if hasattr(os, 'confstr') else 'unknown'
+        tag = hashlib.blake2b(f'{libc_ver}|{SINCOS_MAX_ARG}|{SINCOS_SLOTS}|v1'.encode(), digest_size=8).hexdigest()
+        path = _cache_dir() / f'sincos_exc_{tag}.npy'
+        if path.exists():
+            try:
+                _table_host = np.load(path)
+                return _table_host
+            except Exception:  # noqa: BLE001 - rebuild a corrupt cache file
+                pass
+        tab = np.empty(SINCOS_SLOTS, dtype=np.uint64)
+        n = N.lib().acb_sincos_table_build_host(tab.ctypes.data_as(ctypes.c_void_p), SINCOS_SLOTS,
+                                                ctypes.c_float(SINCOS_MAX_ARG), N.nproc())
+        if n < 0:
+            raise N.AcbError(int(-n), 'acb_sincos_table_build_host')
+        tmp = path.with_suffix(f'.{os.getpid()}.tmp.npy')
+        np.save(tmp, tab)
+        os.replace(tmp, path)
+        _table_host = tab
+        return tab
+
+
+def sincos_table_device(device) -> torch.Tensor:
+    key = str(device)
+    t = _table_dev.get(key)
+    if t is None:
+        t = torch.as_tensor(sincos_table_host().view(np.int64), device=device)
+        _table_dev[key] = t
+    return t
+
+
+# ------------------------------------------------------------------------------------------------
+# map
+# ------------------------------------------------------------------------------------------------
+def map_params(num_mics, num_grid, num_bins, steer_type, r_diag, norm, clip_negative=None, ref=None,
+               glibc_faithful=False, device=None) -> N.MapParams:
+    p = N.MapParams()
+    p.num_mics = int(num_mics)
+    p.num_grid = int(num_grid)
+    p.num_bins = int(num_bins)
+    p.steer_type = N.STEER_CODES[steer_type]
+    p.r_diag = int(bool(r_diag))
+    p.clip_negative = int(bool(r_diag) if clip_negative is None else bool(clip_negative))
+    p.norm = float(norm)
+    if ref is None:
+        p.ref_mode = 0
+        p.ref_point[:] = (0.0, 0.0, 0.0)
+    elif np.isscalar(ref):
+        if float(ref) > 0:
+            p.ref_mode = 1
+            p.ref_distance = float(ref)
+        else:
+            p.ref_mode = 0
+            p.ref_point[:] = (0.0, 0.0, 0.0)
+    else:
+        p.ref_mode = 0
+        p.ref_point[:] = tuple(float(x) for x in np.asarray(ref, dtype=float).reshape(3))
+    if glibc_faithful:
+        t = sincos_table_device(device)
+        p.glibc_faithful = 1
+        p.sincos_table = t.data_ptr()
+        p.sincos_table_slots = t.numel()
+    return p
+
+
+def map_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, mpos: torch.Tensor, gpos: torch.Tensor, steer_type: str,
+            r_diag: bool, norm: float, ref=None, clip_negative=None, glibc_faithful=True,
+            out: torch.Tensor | None = None, steer_norm: torch.Tensor | None = None) -> torch.Tensor:
+    """Plain FP64 map for B bins: csm (B, M, M) complex128, wavenumbers (B,) -> (B, G) float64."""
+    B, M, _ = csm.shape
+    G = gpos.shape[1]
+    dev = csm.device
+    p = map_params(M, G, B, steer_type, r_diag, norm, clip_negative, ref, glibc_faithful, dev)
+    if out is None:
+        out = torch.empty((B, G), dtype=torch.float64, device=dev)
+    N.check(N.lib().acb_map_f64(ctypes.byref(p), csm.data_ptr(), wavenumbers.data_ptr(), mpos.data_ptr(),
+                                gpos.data_ptr(), out.data_ptr(), N.ptr(steer_norm), None, N.stream_handle()),
+            'acb_map_f64')
+    return out

@@ -1,0 +1,80 @@
+"""Drop-ins for the reference's numba kernel entry points (acoular/fastFuncs.py), on the GPU.
+
+* :func:`calcCSM`        -- fastFuncs.py:19-58; ``csm`` (F, M, M) c128/c64 C-contiguous is updated
+  in place with ``conj(spec[f, c]) * spec[f, r]`` for r <= c; returns ``csm``.
+* :func:`beamformerFreq` -- fastFuncs.py:61-214 for the predefined steering types and a full CSM:
+  ``(steerVecType, boolRemovedDiagOfCSM, normFactor, (r0, rm, k), csm) -> (map, steerNorm)``.
+  The 'custom' steering and eigenvalue forms are not implemented by this build
+  (``NotImplementedError``).
+
+Wrong dtypes or non-contiguous arrays raise ``TypeError`` where the reference's explicit numba
+signatures raise a typing error.  Every call uploads its inputs, runs the kernel and downloads the
+result (these are the per-call ABI; the batched path in :mod:`acoular_b200.device` keeps data
+resident).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import device as D
+
+
+def _check_contig(a, dtype, name):
+    if not isinstance(a, np.ndarray) or a.dtype != dtype or not a.flags.c_contiguous:
+        msg = f'{name} must be a C-contiguous {np.dtype(dtype).name} array'
+        raise TypeError(msg)
+
+
+def calcCSM(csm: np.ndarray, SpecAllMics: np.ndarray) -> np.ndarray:  # noqa: N802, N803
+    if not isinstance(csm, np.ndarray) or csm.dtype not in (np.complex128, np.complex64):
+        msg = 'csm must be complex128 or complex64'
+        raise TypeError(msg)
+    _check_contig(csm, csm.dtype, 'csm')
+    _check_contig(SpecAllMics, csm.dtype, 'SpecAllMics')
+    if csm.ndim != 3 or SpecAllMics.ndim != 2 or csm.shape[0] != SpecAllMics.shape[0] or \
+            csm.shape[1] != csm.shape[2] or csm.shape[1] != SpecAllMics.shape[1]:
+        msg = 'csm must be (F, M, M) and SpecAllMics (F, M)'
+        raise ValueError(msg)
+    dev = D.require_cuda()
+    c = torch.from_numpy(csm).to(dev)
+    s = torch.from_numpy(SpecAllMics).to(dev)
+    fn = N.lib().acb_calc_csm_c64 if csm.dtype == np.complex64 else N.lib().acb_calc_csm_c128
+    N.check(fn(c.data_ptr(), s.data_ptr(), csm.shape[0], csm.shape[1], N.stream_handle()), 'calcCSM')
+    csm[...] = c.cpu().numpy()
+    return csm
+
+
+def beamformerFreq(steerVecType, boolRemovedDiagOfCSM, normFactor, inputTupleSteer, inputTupleCsm,  # noqa: N802, N803
+                   glibc_faithful: bool = True):
+    if steerVecType == 'custom' or isinstance(inputTupleCsm, tuple):
+        msg = "custom steering vectors and the eigenvalue form of beamformerFreq are not implemented"
+        raise NotImplementedError(msg)
+    if steerVecType not in N.STEER_CODES:
+        raise KeyError(steerVecType)
+    r0, rm, k = inputTupleSteer
+    if isinstance(k, np.ndarray):
+        k = k.reshape(-1)[0]
+    _check_contig(r0, np.float64, 'distGridToArrayCenter')
+    _check_contig(rm, np.float64, 'distGridToAllMics')
+    _check_contig(inputTupleCsm, np.complex128, 'csm')
+    G, M = rm.shape
+    if r0.shape != (G,) or inputTupleCsm.shape != (M, M):
+        msg = 'shape mismatch between r0 (G,), rm (G, M) and csm (M, M)'
+        raise ValueError(msg)
+    dev = D.require_cuda()
+    csm_d = torch.from_numpy(inputTupleCsm).to(dev)
+    r0_d = torch.from_numpy(r0).to(dev)
+    rm_d = torch.from_numpy(rm).to(dev)
+    out = torch.empty(G, dtype=torch.float64, device=dev)
+    nrm = torch.empty(G, dtype=torch.float64, device=dev)
+    p = D.map_params(M, G, 1, steerVecType, boolRemovedDiagOfCSM, normFactor, clip_negative=False, ref=None,
+                     glibc_faithful=glibc_faithful, device=dev)
+    N.check(N.lib().acb_beamformer_freq_f64(ctypes.byref(p), csm_d.data_ptr(), float(k), r0_d.data_ptr(),
+                                            rm_d.data_ptr(), out.data_ptr(), nrm.data_ptr(), N.stream_handle()),
+            'beamformerFreq')
+    return out.cpu().numpy(), nrm.cpu().numpy()

@@ -41,7 +41,10 @@ class TimeSamples(SamplesGenerator):
     """Multichannel time data held in memory, shape ``(num_samples, num_channels)``."""
 
     def __init__(self, data=None, sample_freq: float = 1.0):
-        self.data = None if data is None else np.asarray(data)
+        if data is None or hasattr(data, 'data_ptr'):
+            self.data = data  # None or a torch tensor (kept as is, e.g. pinned host memory)
+        else:
+            self.data = np.asarray(data)
         self.sample_freq = float(sample_freq)
 
     @property
@@ -54,13 +57,24 @@ class TimeSamples(SamplesGenerator):
 
     @property
     def digest(self) -> str:
-        h = hashlib.blake2b(digest_size=16)
-        if self.data is not None:
-            a = np.ascontiguousarray(self.data)
-            h.update(str((a.shape, a.dtype.str, self.sample_freq)).encode())
-            h.update(a.view(np.uint8).reshape(-1)[:: max(1, a.nbytes // (1 << 20))].tobytes())
-            h.update(np.float64(a.sum(dtype=np.float64)).tobytes())
-        return '_' + h.hexdigest()
+        """Identifier of the data: content hash of a strided sample, computed once per array object.
+
+        Replace ``data`` (assign a new array) after changing samples in place."""
+        key = (id(self.data), None if self.data is None else (tuple(self.data.shape), str(self.data.dtype)),
+               self.sample_freq)
+        if getattr(self, '_digest_key', None) != key:
+            h = hashlib.blake2b(digest_size=16)
+            if self.data is not None:
+                a = self.data
+                if not isinstance(a, np.ndarray):
+                    a = a.detach().cpu().numpy() if hasattr(a, 'detach') else np.asarray(a)
+                a = np.ascontiguousarray(a)
+                h.update(str((a.shape, a.dtype.str, self.sample_freq)).encode())
+                flat = a.view(np.uint8).reshape(-1)
+                h.update(flat[:: max(1, a.nbytes // (1 << 20))].tobytes())
+            self._digest = '_' + h.hexdigest()
+            self._digest_key = key
+        return self._digest
 
     def result(self, num=128):
         if self.num_samples == 0:

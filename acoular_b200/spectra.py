@@ -1,0 +1,265 @@
+"""``PowerSpectra`` with the CSM computed on the B200 (acoular/spectra.py:52-588).
+
+Same attributes and semantics as the reference: ``block_size`` (128 ... 65536; this build's FFT
+kernel covers up to 16384), ``window``, ``overlap``, ``precision`` ('complex128' | 'complex64'),
+``fftfreq()``, ``num_blocks`` (the reference's float formula), ``csm`` (lazy, recomputed when
+the source or a setting changes), ``indices`` / ``ind_low`` / ``ind_high`` / ``freq_range``,
+``eigvals`` / ``eigvecs``.  ``calc_csm()`` returns the complex128 (F, M, M) numpy array the
+reference returns; ``csm_device`` keeps the same matrix resident on the GPU for the beamformer.
+HDF5 result caching (``cached`` / ``config.global_caching``) is not implemented: every setting
+behaves like ``global_caching='none'``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+from scipy import fft
+
+from . import device as D
+
+BLOCK_SIZES = (1024, 128, 256, 512, 2048, 4096, 8192, 16384, 32768, 65536)
+
+
+class PowerSpectra:
+    def __init__(self, source=None, block_size: int = 1024, window: str = 'Rectangular', overlap: str = 'None',
+                 precision: str = 'complex128', cached: bool = False, ind_low: int | None = None,
+                 ind_high: int | None = None, device=None):
+        self.source = source
+        self.block_size = block_size
+        self.window = window
+        self.overlap = overlap
+        self.precision = precision
+        self.cached = cached
+        self._ind_low = 1 if ind_low is None else ind_low
+        self._ind_high = -1 if ind_high is None else ind_high
+        self._freqlc, self._freqhc = 0.0, 0.0
+        self._index_set_last = True
+        self.device = device
+        self._cache_key = None
+        self._csm_dev = None
+        self._csm_host = None
+        self._evd = None
+
+    # --- validated settings (traits Enum / Map semantics) -------------------------------------
+    def __setattr__(self, name, value):
+        if name == 'block_size' and value not in BLOCK_SIZES:
+            msg = f'block_size must be one of {BLOCK_SIZES}, got {value!r}'
+            raise ValueError(msg)
+        if name == 'window' and value not in D.WINDOWS:
+            msg = f'window must be one of {tuple(D.WINDOWS)}, got {value!r}'
+            raise ValueError(msg)
+        if name == 'overlap' and value not in D.OVERLAPS:
+            msg = f'overlap must be one of {tuple(D.OVERLAPS)}, got {value!r}'
+            raise ValueError(msg)
+        if name == 'precision' and value not in ('complex128', 'complex64'):
+            msg = f"precision must be 'complex128' or 'complex64', got {value!r}"
+            raise ValueError(msg)
+        object.__setattr__(self, name, value)
+
+    @property
+    def overlap_(self) -> int:
+        return D.OVERLAPS[self.overlap]
+
+    @property
+    def window_(self):
+        return D.WINDOWS[self.window]
+
+    @property
+    def sample_freq(self):
+        return self.source.sample_freq
+
+    @property
+    def num_channels(self):
+        return self.source.num_channels
+
+    @property
+    def num_blocks(self) -> float:
+        return D.num_blocks(self.source.num_samples, self.block_size, self.overlap_)
+
+    @property
+    def digest(self) -> str:
+        src = getattr(self.source, 'digest', id(self.source))
+        return f'{src}|{self.block_size}|{self.window}|{self.overlap}|{self.precision}'
+
+    def fftfreq(self):
+        if self.source is not None:
+            return abs(fft.fftfreq(self.block_size, 1.0 / self.source.sample_freq)[: int(self.block_size / 2 + 1)])
+        return None
+
+    # --- frequency range (acoular/spectra.py:285-341) ------------------------------------------
+    @property
+    def ind_low(self):
+        f = self.fftfreq()
+        if f is None:
+            return 0
+        if self._index_set_last:
+            return min(self._ind_low, f.shape[0] - 1)
+        return int(np.searchsorted(f[:-1], self._freqlc))
+
+    @ind_low.setter
+    def ind_low(self, v):
+        self._index_set_last = True
+        self._ind_low = v
+
+    @property
+    def ind_high(self):
+        f = self.fftfreq()
+        if f is None:
+            return None
+        if self._index_set_last:
+            if self._ind_high is None:
+                return None
+            return min(self._ind_high, f.shape[0] - 1)
+        if self._freqhc is None:
+            return None
+        return int(np.searchsorted(f[:-1], self._freqhc))
+
+    @ind_high.setter
+    def ind_high(self, v):
+        self._index_set_last = True
+        self._ind_high = v
+
+    @property
+    def freq_range(self):
+        f = self.fftfreq()
+        if f is None:
+            return None
+        if self.ind_high is None:
+            return np.array([f[self.ind_low], None])
+        return f[[self.ind_low, self.ind_high]]
+
+    @freq_range.setter
+    def freq_range(self, fr):
+        if fr is not None:
+            self._index_set_last = False
+            self._freqlc, self._freqhc = fr[0], fr[1]
+
+    @property
+    def indices(self):
+        f = self.fftfreq()
+        if f is None:
+            return None
+        idx = np.arange(f.shape[0], dtype=int)
+        if self.ind_high is None:
+            return idx[self.ind_low:]
+        return idx[self.ind_low:self.ind_high]
+
+    # --- CSM ------------------------------------------------------------------------------------
+    def _device(self):
+        return D.require_cuda(self.device)
+
+    def _samples_device(self) -> torch.Tensor:
+        t = self.source
+        dev = self._device()
+        data = getattr(t, 'data', None)
+        if data is None:
+            data = t.as_array()
+        if isinstance(data, torch.Tensor):
+            x = data
+        else:
+            arr = np.ascontiguousarray(data)
+            if arr.dtype not in (np.float32, np.float64):
+                arr = arr.astype(np.float64)
+            x = torch.from_numpy(arr)
+        if x.dtype not in (torch.float32, torch.float64):
+            x = x.to(torch.float64)
+        if x.device.type == 'cpu':
+            x = x.to(dev, non_blocking=x.is_pinned())
+        return x.contiguous()
+
+    def calc_csm_device(self) -> torch.Tensor:
+        """The CSM (F, M, M) complex128 as a device tensor (see :meth:`calc_csm`)."""
+        t = self.source
+        if t.num_samples == -1:
+            msg = 'PowerSpectra requires a finite source'
+            raise ValueError(msg)
+        x = self._samples_device()
+        return D.calc_csm(x, self.block_size, self.window, self.overlap, self.precision)
+
+    def calc_csm(self) -> np.ndarray:
+        """CSM of the source for all ``block_size/2 + 1`` bins, (F, M, M) complex128."""
+        return self.calc_csm_device().cpu().numpy()
+
+    def _refresh(self):
+        key = self.digest
+        if key != self._cache_key:
+            self._cache_key = key
+            self._csm_dev = None
+            self._csm_host = None
+            self._evd = None
+
+    @property
+    def csm_device(self) -> torch.Tensor:
+        self._refresh()
+        if self._csm_dev is None:
+            self._csm_dev = self.calc_csm_device()
+        return self._csm_dev
+
+    @property
+    def csm(self) -> np.ndarray:
+        self._refresh()
+        if self._csm_host is None:
+            self._csm_host = self.csm_device.cpu().numpy()
+        return self._csm_host
+
+    # --- eigen-decomposition (acoular/spectra.py:351-364), host LAPACK ---------------------------
+    def _get_evd(self):
+        self._refresh()
+        if self._evd is None:
+            dt = 'float64' if self.precision == 'complex128' else 'float32'
+            csm = self.csm
+            ev = np.empty(csm.shape[0:2], dtype=dt)
+            evec = np.empty(csm.shape, dtype=self.precision)
+            for i in range(csm.shape[0]):
+                ev[i], evec[i] = np.linalg.eigh(csm[i])
+            self._evd = (ev, evec)
+        return self._evd
+
+    @property
+    def eigvals(self):
+        return self._get_evd()[0]
+
+    @property
+    def eigvecs(self):
+        return self._get_evd()[1]
+
+
+class PowerSpectraImport(PowerSpectra):
+    """A given CSM (F, M, M) with its frequencies (acoular/spectra.py:591-697)."""
+
+    def __init__(self, csm=None, frequencies=None, device=None):
+        object.__setattr__(self, 'block_size', 1024)
+        super().__init__(source=None, device=device)
+        self._import_csm = None
+        self._frequencies = None
+        self.set_csm(csm, frequencies)
+
+    def set_csm(self, csm, frequencies):
+        if csm is None:
+            return
+        csm = np.asarray(csm)
+        if csm.ndim != 3 or csm.shape[1] != csm.shape[2]:
+            msg = 'The cross spectral matrix must have the following shape: (number of frequencies, num_channels, num_channels)!'
+            raise ValueError(msg)
+        self._import_csm = csm
+        self._frequencies = np.atleast_1d(np.asarray(frequencies, dtype=float))
+        self._cache_key = None
+
+    @property
+    def num_channels(self):
+        return self._import_csm.shape[1]
+
+    @property
+    def digest(self) -> str:
+        c = self._import_csm
+        return f'import|{id(c)}|{c.shape if c is not None else None}'
+
+    def fftfreq(self):
+        return self._frequencies
+
+    def calc_csm_device(self) -> torch.Tensor:
+        return torch.as_tensor(np.ascontiguousarray(self._import_csm, dtype=np.complex128), device=self._device())
+
+    def calc_csm(self) -> np.ndarray:
+        return self._import_csm

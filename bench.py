@@ -1,0 +1,362 @@
+"""Benchmark: CSM + steered-response map throughput (grid-pts x bins / s) on B200.
+
+Workload (one step): the 256-mic precision workload -- 10 s of float32 samples at 51.2 kHz
+(512,000 x 256, resident in HBM), CSM with block 1024 / Hanning / 50 % for all 513 bins (999
+windows), then the map of every bin on a 401 x 401 grid ('true level', diagonal removed):
+160,801 x 513 = 8.25e7 grid-pts x bins per step.
+
+``value``  = grid-pts x bins per second of the whole step (CSM + map), inputs resident on the GPU,
+             timed with CUDA events between barriers; max over ranks; each rank runs one full
+             instance (weak scaling, no collective on the data path).
+``e2e``    = same metric through the public API (``PowerSpectra`` + ``BeamformerBase.result[:]``)
+             from pinned host samples to the host result array, copies included.
+``--impl reference`` times the CPU oracle (a C/OpenMP port of the reference's numba kernels) on a
+bounded sample of the same workload on all host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'map grid-pts*bins/s (CSM + map, 256 mics, 401x401 grid, 513 bins)'
+UNIT = 'grid-pts*bins/s'
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--form', default=None, choices=['tc', 'f64'])
+    ap.add_argument('--steer', default='true level')
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--bins', type=int, default=0, help='limit the number of map bins (profiling only)')
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(['nvidia-smi', f'--id={self.gpu}', f'--query-gpu={self.FIELDS}',
+                                      '--format=csv,noheader,nounits'], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(',')])
+            except Exception:  # noqa: BLE001 - clocks are advisory
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unavailable']}
+        sm = [float(r[1]) for r in self.rows if r[1].replace('.', '').isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == 'Active'})
+        pw = [float(r[3]) for r in self.rows if r[3].replace('.', '').isdigit()]
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(smax) if smax else None,
+                'reasons': reasons, 'power_w_max': max(pw) if pw else None, 'samples': len(self.rows)}
+
+
+def dist_setup(args):
+    import torch
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'ours':
+        torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = 'nccl' if args.impl == 'ours' else 'gloo'
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda' if dist.get_backend() == 'nccl' else 'cpu')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def peaks():
+    p = ROOT / 'MEASURED_PEAKS.json'
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {'hbm_gbs': d.get('hbm_gbs', 6650.0), 'bf16_tflops': d.get('bf16_tflops', 1590.0),
+                'bf16_tflops_sustained': d.get('bf16_tflops_sustained', 1400.0), 'source': 'measured'}
+    return {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0, 'bf16_tflops_sustained': 1400.0, 'source': 'fallback'}
+
+
+def run_reference(args, wl):
+    """CPU oracle (C/OpenMP port of the reference's numba kernels), bounded sample per step."""
+    from acoular_b200 import device as D
+    from oracle import oracle as O
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    ncores = len(os.sched_getaffinity(0))
+    O.set_num_threads(ncores)
+    G = wl.grid.size
+    M = wl.mics.num_mics
+    N = wl.block_size
+    F = N // 2 + 1
+    K = D.num_windows(wl.num_samples, N, 2)
+    kw = max(1, round(K / F))  # one bin's share of the CSM work: K/F windows for all bins
+    hop = N // 2
+    gpos = wl.grid.pos
+    r0 = O.apparent_r(gpos)
+    rm = O.apparent_r(gpos, wl.mics.pos)
+    rng = np.random.RandomState(0)
+    data = rng.randn((kw - 1) * hop + N, M)  # sample values do not change the CPU cost
+    X = rng.randn(2 * M, M) + 1j * rng.randn(2 * M, M)
+    csm_bin = (X.conj().T @ X) / (2 * M)
+    freqs = O.fftfreq(N, wl.fs)
+    b = F // 2
+    norm = O.sig_loss_norm(True, M)
+
+    def step():
+        seg = data[: (kw - 1) * hop + N]
+        O.calc_csm(seg, N, 'Hanning', '50%', 'complex128')
+        res, _ = O.beamformer_freq(args.steer, True, norm, r0, rm, 2 * np.pi * freqs[b] / wl.c, csm_bin)
+        return res
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = G / dt
+    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': ws, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': dt * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded monopoles)',
+            'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': F, 'block_size': N,
+                       'steer_type': args.steer, 'r_diag': True},
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': ncores, 'kind': 'port',
+                             'sample': f'per step: CSM of {kw} windows x all {F} bins (1/{F} of the CSM) + map of '
+                                       f'1 bin over {G} grid points (C/OpenMP port of calcCSM and '
+                                       f'_freqBeamformer_FullCSM, {ncores} threads)'},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(wl, steer):
+    """Oracle timing on the host cores for the bench line's cpu_baseline (rank 0, N=1)."""
+    from acoular_b200 import device as D
+    from oracle import oracle as O
+    ncores = len(os.sched_getaffinity(0))
+    O.set_num_threads(ncores)
+    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
+    F = N // 2 + 1
+    K = D.num_windows(wl.num_samples, N, 2)
+    gpos = wl.grid.pos
+    r0 = O.apparent_r(gpos)
+    rm = O.apparent_r(gpos, wl.mics.pos)
+    rng = np.random.RandomState(1)
+    X = rng.randn(2 * M, M) + 1j * rng.randn(2 * M, M)
+    csm_bin = (X.conj().T @ X) / (2 * M)
+    freqs = O.fftfreq(N, wl.fs)
+    data = rng.randn(64 * (N // 2) + N, M)
+    O.beamformer_freq(steer, True, 1.0, r0[:64], rm[:64], 1.0, csm_bin)  # warm
+    t0 = time.perf_counter()
+    nb = 0
+    while nb < 3 and (nb == 0 or time.perf_counter() - t0 < 20):
+        O.beamformer_freq(steer, True, 1.0, r0, rm, 2 * np.pi * freqs[100 + 50 * nb] / wl.c, csm_bin)
+        nb += 1
+    t_map = (time.perf_counter() - t0) / nb
+    t1 = time.perf_counter()
+    O.calc_csm(data, N, 'Hanning', '50%', 'complex128')
+    t_csm_64 = time.perf_counter() - t1
+    t_csm_bin = t_csm_64 * (K / 65.0) / F  # per-bin share of the full CSM
+    value = G / (t_map + t_csm_bin)
+    return {'value': value, 'unit': UNIT, 'cores': ncores, 'kind': 'port',
+            'sample': f'map of {nb} bins x {G} grid points + CSM of 65 windows x {F} bins, scaled to one bin '
+                      f'(C/OpenMP port of the reference numba kernels, {ncores} threads)'}
+
+
+def main():
+    args = parse()
+    from acoular_b200 import workloads
+    wl = workloads.precision_256()
+    if args.impl == 'reference':
+        return run_reference(args, wl)
+
+    import torch
+
+    from acoular_b200 import _native as NAT
+    from acoular_b200 import device as D
+    ws, rank, local = dist_setup(args)
+    dev = torch.device('cuda', local)
+    form = args.form or ('tc' if hasattr(D, 'map_tc') else 'f64')
+    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
+    F = N // 2 + 1
+    nbins = args.bins or F
+    bins = np.arange(F)[:nbins]
+
+    # resident inputs
+    samples = workloads.monopole_time_data_torch(wl, device=dev)
+    mpos = torch.as_tensor(wl.mics.pos, device=dev)
+    gpos = torch.as_tensor(wl.grid.pos, device=dev)
+    freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[:F])
+    kvec = torch.as_tensor(2 * np.pi * freqs[bins] / wl.c, device=dev)
+    norm = M / (M - 1.0)
+    out = torch.empty((nbins, G), dtype=torch.float64, device=dev)
+    K = D.num_windows(wl.num_samples, N, 2)
+    ws_bytes = NAT.lib().acb_csm_workspace_bytes(M, F, K, NAT.C128)
+    workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    csm_up = torch.zeros((F, M, M), dtype=torch.complex128, device=dev)
+    csm_full = torch.empty((F, M, M), dtype=torch.complex128, device=dev)
+    _, weight = D.window_vector('Hanning', N, dev)
+    scale = 2.0 / N / weight / D.num_blocks(wl.num_samples, N, 2)
+    ev_map = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    map_ms = []
+
+    def step(record=False):
+        csm_up.zero_()
+        D.csm_upper_accumulate(samples, N, 'Hanning', '50%', csm_upper=csm_up, workspace=workspace,
+                               max_workspace_bytes=ws_bytes)
+        D.csm_finalize(csm_up, scale, out=csm_full)
+        c = csm_full if nbins == F else csm_full[:nbins]
+        if record:
+            ev_map[0].record()
+        if form == 'f64':
+            D.map_f64(c, kvec, mpos, gpos, args.steer, True, norm, out=out)
+        else:
+            D.map_tc(c, kvec, mpos, gpos, args.steer, True, norm, out=out)
+        if record:
+            ev_map[1].record()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step(record=True)
+            ev_map[1].synchronize()
+            map_ms.append(ev_map[0].elapsed_time(ev_map[1]))
+        e1.record()
+        torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms, ws)
+    units = float(G) * nbins
+    value = units * ws / (ms / 1e3)
+
+    # map kernel roofline: algorithmic flops 8 M^2 + 8 M per grid-pt x bin
+    pk = peaks()
+    flops = (8.0 * M * M + 8.0 * M) * units
+    map_avg = float(np.mean(map_ms))
+    achieved_tf = flops / (map_avg / 1e3) / 1e12
+    if form == 'f64':
+        roof = {'bound': 'fp64', 'achieved': achieved_tf, 'peak': None, 'unit': 'TFLOP/s', 'frac': None,
+                'traffic': None, 'kernel': 'map_plain_kernel', 'note': 'FP64 CUDA-core form; fp64 peak not measured'}
+    else:
+        roof = {'bound': 'tensor', 'achieved': achieved_tf, 'peak': pk['bf16_tflops_sustained'], 'unit': 'TFLOP/s',
+                'frac': achieved_tf / pk['bf16_tflops_sustained'], 'traffic': None, 'kernel': 'map_tc_kernel',
+                'peak_kind': f"bf16 sustained ({pk['source']})"}
+
+    # end to end through the public API (pinned host samples -> host result)
+    e2e = None
+    if not args.no_e2e:
+        import acoular_b200 as ac
+        host = torch.empty((wl.num_samples, M), dtype=torch.float32, pin_memory=True)
+        host.copy_(samples.cpu())
+        ts = ac.TimeSamples(data=host, sample_freq=wl.fs)
+        times = []
+        for i in range(2 + max(1, min(args.steps, 3))):
+            ps = ac.PowerSpectra(source=ts, block_size=N, window='Hanning', overlap='50%')
+            st = ac.SteeringVector(grid=wl.grid, mics=wl.mics, steer_type=args.steer)
+            bb = ac.BeamformerBase(freq_data=ps, steer=st, r_diag=True, form=form)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = bb.result[0:nbins]
+            t = time.perf_counter() - t0
+            if i >= 2:
+                times.append(t)
+        e2e_s = max_over_ranks(float(np.median(times)), ws)
+        e2e = {'value': units * ws / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': int(host.numel() * 4),
+               'd2h_bytes_per_step': int(res.nbytes), 'ms_per_step': e2e_s * 1e3}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(wl, args.steer)
+
+    if rank == 0:
+        line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': ws, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+                'vs_baseline': None, 'dtype': 'f64' if form == 'f64' else 'bf16x3 (split) / f32 accum',
+                'data': 'synthetic (seeded monopoles, GPU-generated)',
+                'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': nbins, 'block_size': N,
+                           'windows': K, 'steer_type': args.steer, 'r_diag': True, 'form': form,
+                           'l2': 'inputs larger than L2 (samples 524 MB, CSM 538 MB, map 660 MB)',
+                           'parallelism': f'{ws} independent instances (one per GPU)'},
+                'map_ms_per_step': map_avg, 'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e,
+                'gpu_launches': None, 'clocks': clk.summary()}
+        line['gpu_launches'] = launches_per_step(F, nbins, K, M) * args.steps
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def launches_per_step(F, nbins, K, M):
+    # csm_up.zero_ is a torch fill (not counted); ours: fft + gram per workspace chunk, finalize, map
+    chunks = -(-K // 65535)
+    return 2 * chunks + 1 + 1
+
+
+if __name__ == '__main__':
+    main()

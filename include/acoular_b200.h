@@ -1,0 +1,136 @@
+/*
+ * acoular_b200 -- C ABI of the B200 (sm_100a) frequency-domain beamforming path.
+ *
+ * Two stages of Acoular's path are exported:
+ *   Stage A  cross-spectral matrix (CSM) estimation       PowerSpectra.calc_csm / calcCSM
+ *   Stage B  steered-response map h^H C h per grid point  BeamformerBase._calc / beamformerFreq
+ *
+ * Conventions
+ *   - Every pointer argument is DEVICE memory unless its name ends in _host.
+ *   - Complex values are interleaved (re, im): complex128 = 2 doubles, complex64 = 2 floats.
+ *   - Matrices are row-major and C-contiguous exactly like the numpy arrays of the reference.
+ *   - Every call is asynchronous on `stream` (a cudaStream_t passed as void*; NULL = legacy
+ *     default stream) and returns an acb_status code; argument errors are reported before any
+ *     work is enqueued.  Kernel-side faults surface at the next synchronising call.
+ *   - No call allocates device memory unless its comment says so; scratch space is passed in
+ *     by the caller (workspace pointer + size).
+ */
+#ifndef ACOULAR_B200_H
+#define ACOULAR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum acb_status {
+    ACB_OK = 0,
+    ACB_ERR_SHAPE = 1,        /* a size or shape argument is out of range                */
+    ACB_ERR_ARG = 2,          /* an enum / flag / pointer argument is invalid            */
+    ACB_ERR_CUDA = 3,         /* a CUDA launch or runtime call failed                    */
+    ACB_ERR_UNSUPPORTED = 4,  /* valid request this build does not implement             */
+    ACB_ERR_WORKSPACE = 5,    /* workspace pointer missing or too small                  */
+    ACB_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up (error word set)     */
+};
+
+enum acb_steer { ACB_STEER_CLASSIC = 1, ACB_STEER_INVERSE = 2, ACB_STEER_TRUE_LEVEL = 3, ACB_STEER_TRUE_LOCATION = 4 };
+enum acb_precision { ACB_C128 = 0, ACB_C64 = 1 };
+enum acb_sample_dtype { ACB_F32 = 0, ACB_F64 = 1 };
+
+/* Human-readable text of a status code (static storage). */
+const char *acb_status_string(int status);
+/* ABI version of this library (bumped on any signature change). */
+int acb_abi_version(void);
+/* Last CUDA error text seen by the library on this host thread (static storage). */
+const char *acb_last_cuda_error(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Stage A: cross-spectral matrix
+ * ------------------------------------------------------------------------------------------- */
+
+/* calcCSM drop-in (acoular/fastFuncs.py:19-58): adds one ensemble spectrum to the upper triangle
+ * of the CSM, csm[f, r, c] += conj(spec[f, c]) * spec[f, r] for r <= c.
+ * csm: complex128 [num_freqs][num_mics][num_mics] (updated in place); spec: complex128 [num_freqs][num_mics]. */
+int acb_calc_csm_c128(void *csm, const void *spec, int num_freqs, int num_mics, void *stream);
+/* Same for complex64 CSM and spectra. */
+int acb_calc_csm_c64(void *csm, const void *spec, int num_freqs, int num_mics, void *stream);
+
+/* Bytes of workspace acb_csm_accumulate needs for `num_windows` windows of `num_bins` bins. */
+size_t acb_csm_workspace_bytes(int num_mics, int num_bins, int64_t num_windows, int precision);
+
+/* Welch accumulation of PowerSpectra.calc_csm (acoular/spectra.py:366-416, windows as yielded by
+ * BaseSpectra._get_source_data, acoular/spectra.py:171-184):
+ *   for every window w in [first_window, first_window + num_windows):
+ *     x   = samples[w*hop : w*hop + block_size, :] * window[:, None]    (FP64)
+ *     X   = rfft(x, axis=0)[bin_lo : bin_lo + num_bins]                  (FP64 FFT, then rounded
+ *                                                                         to `precision`)
+ *     csm_upper[f, r, c] += conj(X[f, c]) * X[f, r]     for r <= c       (in `precision`)
+ * samples: [num_samples][num_mics], float32 or float64 (sample_dtype).
+ * window: float64 [block_size].  twiddle: complex128 [block_size/2], exp(-2*pi*i*k/block_size).
+ * csm_upper: [num_bins][num_mics][num_mics] in `precision`; only r <= c is written.
+ * block_size: power of two, 16 <= block_size <= 16384.  workspace: >= acb_csm_workspace_bytes. */
+int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_samples, int num_mics,
+                       int block_size, int hop, int64_t first_window, int64_t num_windows,
+                       const double *window, const void *twiddle, int bin_lo, int num_bins,
+                       int precision, void *csm_upper, void *workspace, size_t workspace_bytes,
+                       void *stream);
+
+/* Hermitian completion and scaling (acoular/spectra.py:411-416):
+ *   csm_out[f, r, c] = scale * (r <= c ? upper[f, r, c] : conj(upper[f, c, r]))
+ * upper in `precision`; csm_out always complex128 (as the reference returns). */
+int acb_csm_finalize(const void *csm_upper, int num_bins, int num_mics, int precision, double scale,
+                     void *csm_out, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Stage B: steered-response map (full CSM, predefined steering vectors)
+ * ------------------------------------------------------------------------------------------- */
+
+/* Map parameters shared by the map entry points. */
+typedef struct acb_map_params {
+    int num_mics;            /* M                                                            */
+    int64_t num_grid;        /* G                                                            */
+    int num_bins;            /* B: bins computed in this call                                */
+    int steer_type;          /* acb_steer                                                    */
+    int r_diag;              /* 1: remove the CSM diagonal (fastFuncs.py:277-291)            */
+    int clip_negative;       /* 1: set negative map values to 0 (fbeamform.py:506-508)       */
+    double norm;             /* signal-loss normalisation (BeamformerBase.sig_loss_norm)     */
+    int ref_mode;            /* 0: r0 = |g - ref_point|; 1: r0 = ref_distance (scalar ref)   */
+    double ref_point[3];     /* SteeringVector.ref as a position (default origin)            */
+    double ref_distance;     /* SteeringVector.ref as a distance (> 0)                       */
+    int glibc_faithful;      /* 1: apply the sincos exception table (plain form only)        */
+    const uint64_t *sincos_table; /* device hash table from acb_sincos_table_build_host      */
+    int64_t sincos_table_slots;   /* power of two                                           */
+} acb_map_params;
+
+/* Plain FP64 form of _freqBeamformer_FullCSM (acoular/fastFuncs.py:217-311), batched over bins:
+ *   csm:       complex128 [num_bins][M][M]   (full Hermitian CSM per bin)
+ *   wavenumber: float64 [num_bins]           (k = 2*pi*f/c)
+ *   mpos:      float64 [3][M];  gpos: float64 [3][G]
+ *   out_map:   float64 [num_bins][G];  out_steer_norm: float64 [num_bins][G] or NULL
+ * Distances and steering vectors are synthesised on the device from the positions.
+ * error_word: int32 on the device or NULL (set nonzero on a device-detected fault). */
+int acb_map_f64(const acb_map_params *p, const void *csm, const double *wavenumber, const double *mpos,
+                const double *gpos, double *out_map, double *out_steer_norm, int *error_word, void *stream);
+
+/* beamformerFreq drop-in (acoular/fastFuncs.py:61-214) for one bin with precomputed distances:
+ *   r0: float64 [G] (distGridToArrayCenter), rm: float64 [G][M] (distGridToAllMics). */
+int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wavenumber, const double *r0,
+                            const double *rm, double *out_map, double *out_steer_norm, void *stream);
+
+/* Host-side construction of the sincos exception table used by glibc_faithful=1.
+ * The reference evaluates float32 cos/sin of the float32 phase through the C library (numba
+ * lowers np.cos/np.sin on float32 to cosf/sinf).  The device computes the correctly rounded
+ * float32 value of cos/sin of the same float32 argument; this table lists every float32 argument
+ * x in [0, max_arg) where the host C library's cosf/sinf differ from that value, with the
+ * difference in units of the last place.  It is built by CALLING the host cosf/sinf on every
+ * float32 in the range (no knowledge of their implementation is used).
+ * table_host: uint64 [slots] (slots a power of two, >= 2^22 recommended), filled here.
+ * Returns the number of exception entries, or a negative acb_status on error. */
+int64_t acb_sincos_table_build_host(uint64_t *table_host, int64_t slots, float max_arg, int num_threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ACOULAR_B200_H */

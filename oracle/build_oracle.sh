@@ -4,6 +4,6 @@
 set -euo pipefail
 here="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 mkdir -p "$here/lib"
-gcc -O2 -fopenmp -fPIC -shared -ffp-contract=off -fno-fast-math -std=c11 \
+gcc -O3 -march=x86-64-v3 -fopenmp -fPIC -shared -ffp-contract=off -fno-fast-math -std=c11 \
     -o "$here/lib/liboracle_acoular.so.tmp" "$here/oracle_core.c" -lm
 mv "$here/lib/liboracle_acoular.so.tmp" "$here/lib/liboracle_acoular.so"

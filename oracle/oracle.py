@@ -270,4 +270,4 @@ def synthetic(result: np.ndarray, freq: np.ndarray, f: float, num=0, shape=None)
 
 def L_p(x):
     """acoular/fbeamform.py:2412-2429."""
-    return 10 * np.log10(np.clip(x / 4e-10, 1e-35, None))
+    return 10 * np.log10(np.maximum(x / 4e-10, np.finfo(x.dtype).eps))
