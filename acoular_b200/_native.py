@@ -19,6 +19,7 @@ STATUS_NAMES = {0: 'ok', 1: 'ACB_ERR_SHAPE', 2: 'ACB_ERR_ARG', 3: 'ACB_ERR_CUDA'
                 5: 'ACB_ERR_WORKSPACE', 6: 'ACB_ERR_TIMEOUT'}
 STEER_CODES = {'classic': 1, 'inverse': 2, 'true level': 3, 'true location': 4}
 C128, C64 = 0, 1
+TC_PRECISIONS = {'bf16x3': 0}
 F32, F64 = 0, 1
 
 
@@ -71,6 +72,8 @@ SIGNATURES = {
     'acb_map_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     'acb_beamformer_freq_f64': (_I, [ctypes.POINTER(MapParams), _VP, _D, _VP, _VP, _VP, _VP, _VP]),
     'acb_sincos_table_build_host': (_I64, [_VP, _I64, ctypes.c_float, _I]),
+    'acb_map_tc_workspace_bytes': (_SZ, [_I, _I, _I]),
+    'acb_map_tc': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _SZ, _VP, _VP]),
 }
 
 

@@ -246,3 +246,35 @@ def map_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, mpos: torch.Tensor, gp
                                 gpos.data_ptr(), out.data_ptr(), N.ptr(steer_norm), None, N.stream_handle()),
             'acb_map_f64')
     return out
+
+
+_tc_ws: dict = {}
+
+
+def map_tc_workspace(num_mics: int, num_bins: int, precision: str, device) -> torch.Tensor:
+    """Cached scratch buffer for the split-BF16 copy of the real-embedded CSM."""
+    need = N.lib().acb_map_tc_workspace_bytes(num_mics, num_bins, N.TC_PRECISIONS[precision])
+    key = str(device)
+    ws = _tc_ws.get(key)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(need, dtype=torch.uint8, device=device)
+        _tc_ws[key] = ws
+    return ws
+
+
+def map_tc(csm: torch.Tensor, wavenumbers: torch.Tensor, mpos: torch.Tensor, gpos: torch.Tensor, steer_type: str,
+           r_diag: bool, norm: float, ref=None, clip_negative=None, precision: str = 'bf16x3',
+           out: torch.Tensor | None = None, steer_norm: torch.Tensor | None = None,
+           error_word: torch.Tensor | None = None) -> torch.Tensor:
+    """Tensor-core map for B bins (same contract as :func:`map_f64`)."""
+    B, M, _ = csm.shape
+    G = gpos.shape[1]
+    dev = csm.device
+    p = map_params(M, G, B, steer_type, r_diag, norm, clip_negative, ref, False, dev)
+    if out is None:
+        out = torch.empty((B, G), dtype=torch.float64, device=dev)
+    ws = map_tc_workspace(M, B, precision, dev)
+    N.check(N.lib().acb_map_tc(ctypes.byref(p), N.TC_PRECISIONS[precision], csm.data_ptr(), wavenumbers.data_ptr(),
+                               mpos.data_ptr(), gpos.data_ptr(), out.data_ptr(), N.ptr(steer_norm), ws.data_ptr(),
+                               ws.numel(), N.ptr(error_word), N.stream_handle()), 'acb_map_tc')
+    return out

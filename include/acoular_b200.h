@@ -119,6 +119,25 @@ int acb_map_f64(const acb_map_params *p, const void *csm, const double *wavenumb
 int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wavenumber, const double *r0,
                             const double *rm, double *out_map, double *out_steer_norm, void *stream);
 
+/* Tensor-core operand precisions. */
+enum acb_tc_precision { ACB_TC_BF16X3 = 0 /* split-BF16 hi/lo, 3 products, FP32 accumulation */ };
+
+/* Bytes of workspace acb_map_tc needs (the per-bin split-BF16 copy of the real-embedded CSM). */
+size_t acb_map_tc_workspace_bytes(int num_mics, int num_bins, int precision);
+
+/* Tensor-core form of the same map (acoular/fastFuncs.py:217-311 semantics, same arguments and
+ * outputs as acb_map_f64): the quadratic form h^H C h is evaluated as the real quadratic form
+ * v^T R v of the 2M-dimensional real embedding, R = [[Re C, -Im C], [Im C, Re C]], on tcgen05
+ * tensor cores with split-BF16 operands (hi*hi + hi*lo + lo*hi) and FP32 accumulation in TMEM.
+ * Steering vectors are synthesised per 128-grid-point tile in shared memory (float32 phase k*r as
+ * the reference rounds it, FP64 range reduction); distances, the normalisation sums and the final
+ * normalisation are FP64.  num_mics <= 256 in this build.  glibc_faithful is ignored.
+ * workspace: >= acb_map_tc_workspace_bytes(num_mics, num_bins, precision) bytes.
+ * error_word: int32 on the device or NULL; bit 0 is set if a bounded device-side wait gave up. */
+int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const double *wavenumber,
+               const double *mpos, const double *gpos, double *out_map, double *out_steer_norm,
+               void *workspace, size_t workspace_bytes, int *error_word, void *stream);
+
 /* Host-side construction of the sincos exception table used by glibc_faithful=1.
  * The reference evaluates float32 cos/sin of the float32 phase through the C library (numba
  * lowers np.cos/np.sin on float32 to cosf/sinf).  The device computes the correctly rounded

@@ -1,0 +1,103 @@
+"""Tensor-core (split-BF16, tcgen05) map against the FP64 oracle.
+
+Error measure (the one the benchmark reports): max |map - ref| / max |ref| over the map, per call,
+and the peak level error in dB.  Bar: <= 1e-3 relative and <= 0.05 dB at the peak.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+STEERS = ['classic', 'inverse', 'true level', 'true location']
+TOL = 1e-3
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _case(M, G, seed, nb=3, z=-0.6):
+    rng = np.random.RandomState(seed)
+    mpos = np.vstack([rng.uniform(-0.5, 0.5, (2, M)), np.zeros((1, M))])
+    gpos = np.vstack([rng.uniform(-0.4, 0.4, (2, G)), np.full((1, G), z)])
+    # CSM of a few coherent sources plus noise (peaked maps, like the benchmark data)
+    src = np.vstack([rng.uniform(-0.3, 0.3, (2, 3)), np.full((1, 3), z)])
+    freqs = np.array([1500.0, 4000.0, 9100.0, 12000.0])[:nb]
+    csm = np.zeros((nb, M, M), complex)
+    for f_i, f in enumerate(freqs):
+        k = 2 * np.pi * f / 343.0
+        for s in range(3):
+            r = O.apparent_r(src[:, s:s + 1], mpos).reshape(-1)
+            a = np.exp(-1j * k * r) / r
+            csm[f_i] += (1.0 + s) * np.outer(a, a.conj())
+        X = rng.randn(2 * M, M) + 1j * rng.randn(2 * M, M)
+        csm[f_i] += 0.05 * np.abs(csm[f_i]).max() * (X.conj().T @ X) / (2 * M)
+    return mpos, gpos, freqs, csm
+
+
+def _tc(csm, freqs, mpos, gpos, steer, r_diag, ref=None):
+    from acoular_b200 import device as D
+    dev = torch.device('cuda')
+    M = mpos.shape[1]
+    out = D.map_tc(torch.as_tensor(csm, device=dev), torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
+                   torch.as_tensor(mpos, device=dev), torch.as_tensor(np.ascontiguousarray(gpos), device=dev), steer,
+                   r_diag, O.sig_loss_norm(r_diag, M), ref=ref, clip_negative=r_diag)
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize('M,G', [(2, 1), (16, 128), (37, 300), (64, 257), (128, 129), (256, 200)])
+@pytest.mark.parametrize('steer', STEERS)
+def test_tc_vs_oracle(M, G, steer):
+    mpos, gpos, freqs, csm = _case(M, G, seed=M + G)
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    for r_diag in (False, True):
+        ref = O.beamformer_calc(csm, freqs, range(len(freqs)), r0, rm, 343.0, steer, r_diag)
+        got = _tc(csm, freqs, mpos, gpos, steer, r_diag)
+        for b in range(len(freqs)):
+            assert rel(got[b], ref[b]) <= TOL, (b, rel(got[b], ref[b]))
+
+
+def test_tc_config1_golden_and_peak_level(golden):
+    from acoular_b200 import workloads
+    d = golden('config1_band.npz')
+    wl = workloads.three_sources_64()
+    for steer in STEERS:
+        for r_diag in (False, True):
+            key = f'map_{steer.replace(" ", "_")}_{int(r_diag)}'
+            got = _tc(d['csm_band'], d['freqs'][18:23], wl.mics.pos, wl.grid.pos, steer, r_diag)
+            assert rel(got, d[key]) <= TOL
+            syn, ref = got.sum(0), d['syn_' + key].reshape(-1)
+            assert rel(syn, ref) <= TOL
+            assert abs(O.L_p(syn.max()) - O.L_p(ref.max())) <= 0.05
+
+
+def test_tc_reference_position_and_workspace_errors():
+    from acoular_b200 import _native as N
+    from acoular_b200 import device as D
+    mpos, gpos, freqs, csm = _case(24, 150, seed=3)
+    ref_pt = np.array([0.05, 0.1, -0.02])
+    r0, rm = O.apparent_r(gpos, ref_pt[:, None]), O.apparent_r(gpos, mpos)
+    ref = O.beamformer_calc(csm, freqs, range(3), r0, rm, 343.0, 'true level', True)
+    got = _tc(csm, freqs, mpos, gpos, 'true level', True, ref=ref_pt)
+    assert rel(got, ref) <= TOL
+    p = D.map_params(300, 10, 1, 'classic', True, 1.0)
+    import ctypes
+    assert N.lib().acb_map_tc(ctypes.byref(p), 0, 1, 1, 1, 1, 1, None, 1, 1 << 30, None, None) == 4  # > 256 mics
+    p = D.map_params(64, 10, 1, 'classic', True, 1.0)
+    assert N.lib().acb_map_tc(ctypes.byref(p), 0, 1, 1, 1, 1, 1, None, 1, 10, None, None) == 5  # workspace
+
+
+def test_tc_error_word_stays_clear():
+    from acoular_b200 import device as D
+    dev = torch.device('cuda')
+    mpos, gpos, freqs, csm = _case(64, 1000, seed=9)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    D.map_tc(torch.as_tensor(csm, device=dev), torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
+             torch.as_tensor(mpos, device=dev), torch.as_tensor(gpos, device=dev), 'classic', True, 1.0,
+             error_word=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
