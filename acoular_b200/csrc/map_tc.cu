@@ -16,9 +16,11 @@
 //                 core-matrix order by tc_prep_kernel) into a 2-stage ring
 //   warp 1      : TMEM allocation; one thread issues tcgen05.mma (A = steering chunk, B = R'
 //                 tiles; products hi*hi + hi*lo + lo*hi) and commits to the stage's mbarrier
-//   warps 2..5  : steering synthesis of chunk i for their grid point (FP64 distance, FP32-rounded
-//                 phase k*r as in the reference, FP64 range reduction, fast sincos), bf16 hi/lo
-//                 split into the A stage, then the epilogue of chunk i-1 from TMEM.
+//   warps 2..9  : steering synthesis of chunk i (two warps per grid point, one per half chunk):
+//                 FP32 distance (Newton rsqrt), the phase k*r as an exact float-float product,
+//                 Cody-Waite reduction by a three-term 2*pi, hardware sincos, bf16 hi/lo split
+//                 into the A stage; then the epilogue of chunk i-1 from TMEM.  No FP64<->FP32
+//                 conversion sits in the per-element path (the conversion pipe is the scarce one).
 // Every mbarrier wait is bounded (globaltimer); on timeout the CTA raises an error word and exits
 // its loops without further work.
 #include <cuda_bf16.h>
@@ -38,7 +40,15 @@ constexpr int TC_TILE_ELEMS = TC_CHUNK * TC_CHUNK;
 constexpr int TC_TILE_BYTES = TC_TILE_ELEMS * 2;          // bf16
 constexpr int TC_A_BYTES = TC_ROWS * TC_CHUNK * 2;        // 8 KB per (stage, hi|lo)
 constexpr int TC_STAGES = 2;
-constexpr int TC_THREADS = 192;
+constexpr int TC_SYNTH_WARPS = 8;           // two warps per TMEM lane quarter, one per half chunk
+constexpr int TC_SYNTH_THREADS = 32 * TC_SYNTH_WARPS;
+constexpr int TC_THREADS = 64 + TC_SYNTH_THREADS;
+
+// 2*pi = P2A + P2B + P2C (Cody-Waite split; P2A has 8 significant bits so n*P2A is exact)
+__device__ constexpr float TC_P2A = 0x1.92p+2f;
+__device__ constexpr float TC_P2B = 0x1.fb5444p-10f;
+__device__ constexpr float TC_P2C = 0x1.68c234p-37f;
+__device__ constexpr float TC_INV2PI = 0.15915493667125702f;
 
 struct TcArgs {
     int M, Mp, C;
@@ -108,7 +118,8 @@ struct TcSmem {
         return b_base() + (stage * 2 + lo) * C * TC_TILE_BYTES;
     }
     __host__ __device__ static constexpr int mic_off(int C) { return b_base() + TC_STAGES * 2 * C * TC_TILE_BYTES; }
-    __host__ __device__ static constexpr int bar_off(int C, int Mp) { return mic_off(C) + 3 * Mp * 8; }
+    __host__ __device__ static constexpr int red_off(int C, int Mp) { return mic_off(C) + 3 * Mp * 4; }
+    __host__ __device__ static constexpr int bar_off(int C, int Mp) { return red_off(C, Mp) + 2 * TC_ROWS * 8; }
     __host__ __device__ static constexpr int total(int C, int Mp) { return bar_off(C, Mp) + 128; }
 };
 
@@ -129,7 +140,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     // operand tiles start on a 1 KB boundary (the launch reserves 1 KB of slack for this)
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     const int C = a.C, Mp = a.Mp;
-    double *mp = reinterpret_cast<double *>(smem + TcSmem::mic_off(C));
+    float *mp = reinterpret_cast<float *>(smem + TcSmem::mic_off(C));            // [3][Mp]
+    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(C, Mp));     // [2][128]
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(C, Mp));
     uint64_t *full_a = bars;        // [2]
     uint64_t *full_b = bars + 2;    // [2]
@@ -144,11 +156,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
 
     for (int i = threadIdx.x; i < 3 * Mp; i += blockDim.x) {
         const int d = i / Mp, m = i % Mp;
-        mp[i] = m < a.M ? mpos[d * a.M + m] : 0.0;
+        mp[i] = m < a.M ? (float)mpos[d * a.M + m] : 0.f;
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
-            tc::mbar_init(&full_a[s], 128);
+            tc::mbar_init(&full_a[s], TC_SYNTH_THREADS);
             tc::mbar_init(&full_b[s], 1);
             tc::mbar_init(&done[s], 1);
         }
@@ -212,8 +224,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             if (last >= 0) tc::mbar_wait(&done[last & 1], (last >> 1) & 1, abort_flag, a.wait_limit_ns);
         }
     } else {
-        // ---------------- steering synthesis + epilogue (warps 2..5) ----------------
-        const int q = warp & 3;            // TMEM lane quarter of this warp
+        // ---------------- steering synthesis + epilogue (warps 2..9) ----------------
+        // Warp w serves TMEM lane quarter q = w % 4 (grid points 32q..32q+31 of the tile) and half
+        // h of every chunk (mics 8h..8h+7 of the chunk's 16, components 16h..16h+15).
+        const int q = warp & 3;
+        const int h = (warp - 2) >> 2;
         const int row = q * 32 + lane;     // A row == TMEM lane == grid point in the tile
         const int64_t g = tile0 + row;
         const bool gvalid = g < a.G;
@@ -223,62 +238,74 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             gy = gpos[a.G + g];
             gz = gpos[2 * a.G + g];
         }
+        const float gxf = (float)gx, gyf = (float)gy, gzf = (float)gz;
         const double k = wavenumber[bin];
+        const float khi = (float)k, klo = (float)(k - (double)khi);
         const uint32_t lane_addr = taddr + ((uint32_t)(q * 32) << 16);
+        const float *mx = mp, *my = mp + Mp, *mz = mp + 2 * Mp;
+        constexpr int HC = TC_CHUNK / 2;   // components per half chunk
         double S = 0.0, acc = 0.0;
-        float va[TC_CHUNK], vb[TC_CHUNK];
+        float va[HC], vb[HC];
 
-        auto synth = [&](int t, float (&v)[TC_CHUNK]) {
+        auto synth = [&](int t, float (&v)[HC]) {
             const int s = t & 1;
             uint8_t *ahi = smem + TcSmem::a_off(s, 0);
             uint8_t *alo = smem + TcSmem::a_off(s, 1);
+            float s_part = 0.f;
 #pragma unroll
-            for (int grp = 0; grp < 4; ++grp) {
+            for (int gl = 0; gl < 2; ++gl) {
                 uint32_t hw[4], lw[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    const int mm = grp * 4 + e;
-                    const int m = t * TC_MPC + mm;
+                    const int mm = gl * 4 + e;                 // mic within the half chunk
+                    const int m = t * TC_MPC + h * 8 + mm;
                     float vr = 0.f, vi = 0.f;
                     if (gvalid && m < a.M) {
-                        const double d0 = gx - mp[m], d1 = gy - mp[Mp + m], d2 = gz - mp[2 * Mp + m];
-                        const double r2 = fma(d2, d2, fma(d1, d1, d0 * d0));
-                        // r = sqrt(r2): float rsqrt seed + one FP64 Newton step (~1e-14 relative)
-                        const double y = (double)rsqrtf((float)r2);
-                        const double r0 = r2 * y;
-                        const double r = fma(0.5 * y, fma(-r0, r0, r2), r0);
-                        const float ph = __double2float_rn(k * r);   // the reference's float32 phase
-                        const float nq = rintf(ph * 0.15915494309189535f);
-                        const float x = (float)fma(-(double)nq, 6.283185307179586, (double)ph);
+                        const float dx = gxf - mx[m], dy = gyf - my[m], dz = gzf - mz[m];
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        // 1/sqrt(r2): integer seed + three Newton steps; r by one more correction
+                        float y = __int_as_float(0x5f375a86 - (__float_as_int(r2) >> 1));
+                        const float hr2 = 0.5f * r2;
+                        y = y * fmaf(-hr2 * y, y, 1.5f);
+                        y = y * fmaf(-hr2 * y, y, 1.5f);
+                        y = y * fmaf(-hr2 * y, y, 1.5f);
+                        float r = r2 * y;
+                        r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);
+                        // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
+                        const float ph = khi * r;
+                        const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
+                        const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
+                        float x = fmaf(-nq, TC_P2A, ph);
+                        x = fmaf(-nq, TC_P2B, x);
+                        x = fmaf(-nq, TC_P2C, x);
+                        x += pl;
                         float sn, cs;
                         __sincosf(x, &sn, &cs);
                         vr = cs;
                         vi = -sn;
                         if (a.steer_type == 2) {
-                            const float rf = (float)r;
-                            vr *= rf;
-                            vi *= rf;
-                            S = fma(r, r, S);
+                            vr *= r;
+                            vi *= r;
+                            s_part += r2;
                         } else if (a.steer_type >= 3) {
-                            const double yd = y * fma(-0.5 * r2 * y, y, 1.5);  // 1/r, one Newton step
-                            const float irf = (float)yd;
-                            vr *= irf;
-                            vi *= irf;
-                            S = fma(yd, yd, S);
+                            vr *= y;
+                            vi *= y;
+                            s_part = fmaf(y, y, s_part);
                         }
                     }
                     v[2 * mm] = vr;
                     v[2 * mm + 1] = vi;
-                    const __nv_bfloat16 hr = __float2bfloat16_rn(vr), hi_ = __float2bfloat16_rn(vi);
-                    const __nv_bfloat16 lr = __float2bfloat16_rn(vr - __bfloat162float(hr));
-                    const __nv_bfloat16 li = __float2bfloat16_rn(vi - __bfloat162float(hi_));
-                    hw[e] = pack_bf16x2(hr, hi_);
-                    lw[e] = pack_bf16x2(lr, li);
+                    const __nv_bfloat162 hi2 = __floats2bfloat162_rn(vr, vi);
+                    const __nv_bfloat162 lo2 = __floats2bfloat162_rn(vr - __low2float(hi2), vi - __high2float(hi2));
+                    hw[e] = *reinterpret_cast<const uint32_t *>(&hi2);
+                    lw[e] = *reinterpret_cast<const uint32_t *>(&lo2);
                 }
+                const int grp = 2 * h + gl;   // 16-byte core-matrix column of this row
                 const int off = (((row >> 3) * 4 + grp) << 7) + ((row & 7) << 4);
                 *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
                 *reinterpret_cast<uint4 *>(alo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
             }
+            S += (double)s_part;
             tc::fence_proxy_async_smem();
             tc::mbar_arrive(&full_a[s]);
         };
@@ -288,19 +315,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             return __all_sync(0xffffffffu, ok);
         };
         auto warp_abort = [&]() -> bool { return __any_sync(0xffffffffu, *abort_flag != 0); };
-        auto epilogue = [&](int t, const float (&v)[TC_CHUNK]) {
+        auto epilogue = [&](int t, const float (&v)[HC]) {
             const int s = t & 1, u = t >> 1;
             if (!warp_wait(&done[s], u & 1)) return;
             tc::tc_fence_after();
-            float d[TC_CHUNK];
-            tc::tmem_ld_x32(lane_addr + (uint32_t)(TC_CHUNK * t), d);
+            float d[HC];
+            tc::tmem_ld_x16(lane_addr + (uint32_t)(TC_CHUNK * t + HC * h), d);
             float part = 0.f;
 #pragma unroll
-            for (int e = 0; e < TC_CHUNK; ++e) part = fmaf(d[e], v[e], part);
+            for (int e = 0; e < HC; ++e) part = fmaf(d[e], v[e], part);
             acc += (double)part;
         };
-        // S = 2 stages: synthesis of chunk t+1 overlaps the MMAs of chunk t; chunk t-1's columns
-        // are read while chunk t's MMAs run.
+        // 2 stages: synthesis of chunk t+1 overlaps the MMAs of chunk t; chunk t-1's columns are
+        // read while chunk t's MMAs run.
         for (int t = 0; t < C && !warp_abort(); t += 2) {
             if (t >= 2 && !warp_wait(&done[0], ((t >> 1) - 1) & 1)) break;
             synth(t, va);
@@ -316,8 +343,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             else epilogue(C - 1, va);
         }
         tc::tc_fence_before();
-        if (gvalid && !*abort_flag) {
-            const double scalar = acc;
+        // combine the two half-chunk partial sums of each grid point (named barrier: synth warps)
+        if (h == 1) {
+            red[row] = acc;
+            red[TC_ROWS + row] = S;
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
+        if (h == 0 && gvalid && !*abort_flag) {
+            const double scalar = acc + red[row];
+            S += red[TC_ROWS + row];
             double r0;
             if (a.ref_mode == 1) r0 = a.ref_dist;
             else r0 = dist3(gx, gy, gz, a.ref0, a.ref1, a.ref2);
