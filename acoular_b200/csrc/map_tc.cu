@@ -118,15 +118,10 @@ struct TcSmem {
         return b_base() + (stage * 2 + lo) * C * TC_TILE_BYTES;
     }
     __host__ __device__ static constexpr int mic_off(int C) { return b_base() + TC_STAGES * 2 * C * TC_TILE_BYTES; }
-    __host__ __device__ static constexpr int red_off(int C, int Mp) { return mic_off(C) + 3 * Mp * 4; }
+    __host__ __device__ static constexpr int red_off(int C, int Mp) { return mic_off(C) + Mp * 16; }
     __host__ __device__ static constexpr int bar_off(int C, int Mp) { return red_off(C, Mp) + 2 * TC_ROWS * 8; }
     __host__ __device__ static constexpr int total(int C, int Mp) { return bar_off(C, Mp) + 128; }
 };
-
-__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi)
-{
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
 
 __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const double *__restrict__ wavenumber,
                                                                const double *__restrict__ mpos,
@@ -140,7 +135,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     // operand tiles start on a 1 KB boundary (the launch reserves 1 KB of slack for this)
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     const int C = a.C, Mp = a.Mp;
-    float *mp = reinterpret_cast<float *>(smem + TcSmem::mic_off(C));            // [3][Mp]
+    float4 *mp4 = reinterpret_cast<float4 *>(smem + TcSmem::mic_off(C));        // [Mp] (x, y, z, 0)
     double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(C, Mp));     // [2][128]
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(C, Mp));
     uint64_t *full_a = bars;        // [2]
@@ -154,9 +149,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     const int64_t tile0 = (int64_t)blockIdx.x * TC_ROWS;
     const uint32_t ncols = (uint32_t)(C <= 1 ? 32 : (C <= 2 ? 64 : (C <= 4 ? 128 : (C <= 8 ? 256 : 512))));
 
-    for (int i = threadIdx.x; i < 3 * Mp; i += blockDim.x) {
-        const int d = i / Mp, m = i % Mp;
-        mp[i] = m < a.M ? (float)mpos[d * a.M + m] : 0.f;
+    for (int m = threadIdx.x; m < Mp; m += blockDim.x) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (m < a.M) v = make_float4((float)mpos[m], (float)mpos[a.M + m], (float)mpos[2 * a.M + m], 0.f);
+        mp4[m] = v;
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
@@ -242,7 +238,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         const double k = wavenumber[bin];
         const float khi = (float)k, klo = (float)(k - (double)khi);
         const uint32_t lane_addr = taddr + ((uint32_t)(q * 32) << 16);
-        const float *mx = mp, *my = mp + Mp, *mz = mp + 2 * Mp;
         constexpr int HC = TC_CHUNK / 2;   // components per half chunk
         double S = 0.0, acc = 0.0;
         float va[HC], vb[HC];
@@ -261,16 +256,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                     const int m = t * TC_MPC + h * 8 + mm;
                     float vr = 0.f, vi = 0.f;
                     if (gvalid && m < a.M) {
-                        const float dx = gxf - mx[m], dy = gyf - my[m], dz = gzf - mz[m];
+                        const float4 mv = mp4[m];
+                        const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
                         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        // 1/sqrt(r2): integer seed + three Newton steps; r by one more correction
-                        float y = __int_as_float(0x5f375a86 - (__float_as_int(r2) >> 1));
-                        const float hr2 = 0.5f * r2;
-                        y = y * fmaf(-hr2 * y, y, 1.5f);
-                        y = y * fmaf(-hr2 * y, y, 1.5f);
-                        y = y * fmaf(-hr2 * y, y, 1.5f);
+                        const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
                         float r = r2 * y;
-                        r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);
+                        r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
                         // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
                         const float ph = khi * r;
                         const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
@@ -280,25 +271,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                         x = fmaf(-nq, TC_P2C, x);
                         x += pl;
                         float sn, cs;
-                        __sincosf(x, &sn, &cs);
-                        vr = cs;
-                        vi = -sn;
+                        tc::sincos_approx(x, sn, cs);
+                        float w = 1.f;
                         if (a.steer_type == 2) {
-                            vr *= r;
-                            vi *= r;
+                            w = r;
                             s_part += r2;
                         } else if (a.steer_type >= 3) {
-                            vr *= y;
-                            vi *= y;
+                            w = y;
                             s_part = fmaf(y, y, s_part);
                         }
+                        vr = cs * w;
+                        vi = -sn * w;
                     }
                     v[2 * mm] = vr;
                     v[2 * mm + 1] = vi;
-                    const __nv_bfloat162 hi2 = __floats2bfloat162_rn(vr, vi);
-                    const __nv_bfloat162 lo2 = __floats2bfloat162_rn(vr - __low2float(hi2), vi - __high2float(hi2));
-                    hw[e] = *reinterpret_cast<const uint32_t *>(&hi2);
-                    lw[e] = *reinterpret_cast<const uint32_t *>(&lo2);
+                    // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
+                    // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
+                    const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
+                    hw[e] = __byte_perm(rr, ri, 0x7632);
+                    const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
+                    const float li = vi - __uint_as_float(ri & 0xFFFF0000u);
+                    lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li) + 0x8000u, 0x7632);
                 }
                 const int grp = 2 * h + gl;   // 16-byte core-matrix column of this row
                 const int off = (((row >> 3) * 4 + grp) << 7) + ((row & 7) << 4);

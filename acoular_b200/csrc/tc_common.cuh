@@ -154,6 +154,20 @@ __device__ __forceinline__ void tmem_ld_x32(uint32_t taddr, float (&v)[32])
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Hardware approximations (MUFU): rsqrt ~2^-22 relative; sin/cos ~2^-21 absolute on [-pi, pi].
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ void sincos_approx(float x, float &s, float &c)
+{
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
+}
+
 __device__ __forceinline__ void tmem_ld_x16(uint32_t taddr, float (&v)[16])
 {
     uint32_t r[16];

@@ -295,6 +295,24 @@ def main():
     units = float(G) * nbins
     value = units * ws / (ms / 1e3)
 
+    # accuracy of the timed form against the plain FP64 form on a spread of bins
+    acc_bins = np.unique(np.linspace(2, nbins - 1, 6).round().astype(int))
+    accuracy = None
+    if form != 'f64':
+        ref_map = D.map_f64(csm_full[torch.as_tensor(acc_bins, device=dev)].contiguous(),
+                            kvec[torch.as_tensor(acc_bins, device=dev)].contiguous(), mpos, gpos, args.steer, True,
+                            norm).cpu().numpy()
+        got = out[torch.as_tensor(acc_bins, device=dev)].cpu().numpy()
+        scale = np.abs(ref_map).max(axis=1, keepdims=True)
+        err = np.abs(got - ref_map) / scale
+        peak = ref_map.argmax(axis=1)
+        lp = lambda x: 10 * np.log10(np.maximum(x / 4e-10, np.finfo(np.float64).eps))
+        db = np.abs(lp(got[np.arange(len(acc_bins)), peak]) - lp(ref_map[np.arange(len(acc_bins)), peak]))
+        accuracy = {'vs': 'plain FP64 form (reference method on the GPU)', 'bins': acc_bins.tolist(),
+                    'max_rel_err': float(err.max()), 'rms_rel_err': float(np.sqrt((err ** 2).mean())),
+                    'peak_level_err_db': float(db.max()),
+                    'definition': '|map - ref| / max|ref| per bin; L_p difference at the reference peak'}
+
     # map kernel roofline: algorithmic flops 8 M^2 + 8 M per grid-pt x bin
     pk = peaks()
     flops = (8.0 * M * M + 8.0 * M) * units
@@ -343,7 +361,7 @@ def main():
                            'windows': K, 'steer_type': args.steer, 'r_diag': True, 'form': form,
                            'l2': 'inputs larger than L2 (samples 524 MB, CSM 538 MB, map 660 MB)',
                            'parallelism': f'{ws} independent instances (one per GPU)'},
-                'map_ms_per_step': map_avg, 'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e,
+                'map_ms_per_step': map_avg, 'roofline': roof, 'accuracy': accuracy, 'cpu_baseline': cpu, 'e2e': e2e,
                 'gpu_launches': None, 'clocks': clk.summary()}
         line['gpu_launches'] = launches_per_step(F, nbins, K, M) * args.steps
         print(json.dumps(line), flush=True)
