@@ -16,7 +16,7 @@
 //                 core-matrix order by tc_prep_kernel) into a 2-stage ring
 //   warp 1      : TMEM allocation; one thread issues tcgen05.mma (A = steering chunk, B = R'
 //                 tiles; products hi*hi + hi*lo + lo*hi) and commits to the stage's mbarrier
-//   warps 2..9  : steering synthesis of chunk i (two warps per grid point, one per half chunk):
+//   warps 2..17 : steering synthesis of chunk i (four threads per grid point, 4 mics each):
 //                 FP32 distance (Newton rsqrt), the phase k*r as an exact float-float product,
 //                 Cody-Waite reduction by a three-term 2*pi, hardware sincos, bf16 hi/lo split
 //                 into the A stage; then the epilogue of chunk i-1 from TMEM.  No FP64<->FP32
@@ -39,8 +39,10 @@ constexpr int TC_MAX_CHUNKS = 16;          // 2M <= 512 TMEM columns in one pass
 constexpr int TC_TILE_ELEMS = TC_CHUNK * TC_CHUNK;
 constexpr int TC_TILE_BYTES = TC_TILE_ELEMS * 2;          // bf16
 constexpr int TC_A_BYTES = TC_ROWS * TC_CHUNK * 2;        // 8 KB per (stage, hi|lo)
-constexpr int TC_STAGES = 2;
-constexpr int TC_SYNTH_WARPS = 8;           // two warps per TMEM lane quarter, one per half chunk
+constexpr int TC_ASTAGES = 3;              // steering (A) ring: synthesis runs up to 2 chunks ahead
+constexpr int TC_BSTAGES = 2;              // R' tile (B) ring
+constexpr int TC_PARTS = 4;                 // synthesis threads per grid point (one per 4 mics of a chunk)
+constexpr int TC_SYNTH_WARPS = 4 * TC_PARTS;  // TC_PARTS warps per TMEM lane quarter
 constexpr int TC_SYNTH_THREADS = 32 * TC_SYNTH_WARPS;
 constexpr int TC_THREADS = 64 + TC_SYNTH_THREADS;
 
@@ -112,17 +114,18 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const double2 *__restrict_
 struct TcSmem {
     // offsets in bytes from the 1024-aligned dynamic shared-memory base
     __host__ __device__ static constexpr int a_off(int stage, int lo) { return (stage * 2 + lo) * TC_A_BYTES; }
-    __host__ __device__ static constexpr int b_base() { return TC_STAGES * 2 * TC_A_BYTES; }
+    __host__ __device__ static constexpr int b_base() { return TC_ASTAGES * 2 * TC_A_BYTES; }
     __host__ __device__ static constexpr int b_off(int C, int stage, int lo)
     {
         return b_base() + (stage * 2 + lo) * C * TC_TILE_BYTES;
     }
-    __host__ __device__ static constexpr int mic_off(int C) { return b_base() + TC_STAGES * 2 * C * TC_TILE_BYTES; }
+    __host__ __device__ static constexpr int mic_off(int C) { return b_base() + TC_BSTAGES * 2 * C * TC_TILE_BYTES; }
     __host__ __device__ static constexpr int red_off(int C, int Mp) { return mic_off(C) + Mp * 16; }
-    __host__ __device__ static constexpr int bar_off(int C, int Mp) { return red_off(C, Mp) + 2 * TC_ROWS * 8; }
+    __host__ __device__ static constexpr int bar_off(int C, int Mp) { return red_off(C, Mp) + 2 * TC_PARTS * TC_ROWS * 8; }
     __host__ __device__ static constexpr int total(int C, int Mp) { return bar_off(C, Mp) + 128; }
 };
 
+template <int ST>
 __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const double *__restrict__ wavenumber,
                                                                const double *__restrict__ mpos,
                                                                const double *__restrict__ gpos,
@@ -136,13 +139,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     const int C = a.C, Mp = a.Mp;
     float4 *mp4 = reinterpret_cast<float4 *>(smem + TcSmem::mic_off(C));        // [Mp] (x, y, z, 0)
-    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(C, Mp));     // [2][128]
+    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(C, Mp));     // [2][parts][128]
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(C, Mp));
-    uint64_t *full_a = bars;        // [2]
-    uint64_t *full_b = bars + 2;    // [2]
-    uint64_t *done = bars + 4;      // [2]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 6);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 7);
+    uint64_t *full_a = bars;        // [3] steering chunk t in A stage t % 3
+    uint64_t *full_b = bars + 3;    // [2] R' tiles of chunk t in B stage t % 2
+    uint64_t *done = bars + 5;      // [3] MMAs of chunk t complete (committed to done[t % 3])
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 9);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int bin = blockIdx.y;
@@ -155,11 +158,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         mp4[m] = v;
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_STAGES; ++s) {
+        for (int s = 0; s < TC_ASTAGES; ++s) {
             tc::mbar_init(&full_a[s], TC_SYNTH_THREADS);
-            tc::mbar_init(&full_b[s], 1);
             tc::mbar_init(&done[s], 1);
         }
+        for (int s = 0; s < TC_BSTAGES; ++s) tc::mbar_init(&full_b[s], 1);
         *abort_flag = 0;
         tc::fence_mbar_init();
     }
@@ -175,8 +178,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         if (lane == 0) {
             int last = -1;
             for (int t = 0; t < C && !*abort_flag; ++t) {
-                const int s = t & 1, u = t >> 1;
-                if (t >= TC_STAGES && !tc::mbar_wait(&done[s], (u - 1) & 1, abort_flag, a.wait_limit_ns)) break;
+                const int s = t & 1;
+                // B stage t % 2 was last read by the MMAs of chunk t - 2
+                if (t >= TC_BSTAGES &&
+                    !tc::mbar_wait(&done[(t - 2) % 3], ((t - 2) / 3) & 1, abort_flag, a.wait_limit_ns))
+                    break;
                 const uint32_t bytes = (uint32_t)(C - t) * TC_TILE_BYTES;
                 tc::mbar_arrive_expect_tx(&full_b[s], 2 * bytes);
                 const int64_t src = bin_off + (int64_t)tile_index(C, t, t) * TC_TILE_ELEMS;
@@ -186,16 +192,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             }
             // on an abort, let the last copies land before the CTA releases its shared memory
             if (*abort_flag && last >= 0)
-                tc::mbar_wait(&full_b[last & 1], (last >> 1) & 1, abort_flag, a.wait_limit_ns);
+                tc::mbar_wait(&full_b[last & 1], (last >> 1) & 1, abort_flag, 4 * a.wait_limit_ns);
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             int last = -1;
             for (int t = 0; t < C && !*abort_flag; ++t) {
-                const int s = t & 1, u = t >> 1;
-                if (!tc::mbar_wait(&full_a[s], u & 1, abort_flag, a.wait_limit_ns)) break;
-                if (!tc::mbar_wait(&full_b[s], u & 1, abort_flag, a.wait_limit_ns)) break;
+                const int sa = t % 3, sb = t & 1;
+                if (!tc::mbar_wait(&full_a[sa], (t / 3) & 1, abort_flag, a.wait_limit_ns)) break;
+                if (!tc::mbar_wait(&full_b[sb], (t >> 1) & 1, abort_flag, a.wait_limit_ns)) break;
                 tc::tc_fence_after();
                 const int ntot = TC_CHUNK * (C - t);
                 const uint32_t c0 = (uint32_t)(TC_CHUNK * t);
@@ -203,8 +209,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                 for (int ks = 0; ks < 2; ++ks) {
 #pragma unroll
                     for (int prod = 0; prod < 3; ++prod) {
-                        const uint32_t a_addr = tc::smem_u32(smem + TcSmem::a_off(s, prod == 2)) + ks * 256;
-                        const uint32_t b_addr = tc::smem_u32(smem + TcSmem::b_off(C, s, prod == 1)) + ks * 256;
+                        const uint32_t a_addr = tc::smem_u32(smem + TcSmem::a_off(sa, prod == 2)) + ks * 256;
+                        const uint32_t b_addr = tc::smem_u32(smem + TcSmem::b_off(C, sb, prod == 1)) + ks * 256;
                         const uint64_t ad = tc::sdesc_noswizzle(a_addr, 128, 512);
                         for (int n0 = 0; n0 < ntot; n0 += 256) {
                             const int np = min(256, ntot - n0);
@@ -214,17 +220,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                         }
                     }
                 }
-                tc::mma_commit(&done[s]);
+                tc::mma_commit(&done[sa]);
                 last = t;
             }
-            if (last >= 0) tc::mbar_wait(&done[last & 1], (last >> 1) & 1, abort_flag, a.wait_limit_ns);
+            if (last >= 0) tc::mbar_wait(&done[last % 3], (last / 3) & 1, abort_flag, 4 * a.wait_limit_ns);
         }
     } else {
-        // ---------------- steering synthesis + epilogue (warps 2..9) ----------------
-        // Warp w serves TMEM lane quarter q = w % 4 (grid points 32q..32q+31 of the tile) and half
-        // h of every chunk (mics 8h..8h+7 of the chunk's 16, components 16h..16h+15).
+        // ---------------- steering synthesis + epilogue (warps 2..17) ----------------
+        // Warp w serves TMEM lane quarter q = w % 4 (grid points 32q..32q+31 of the tile) and
+        // part p of every chunk: mics 4p..4p+3 of the chunk's 16, components 8p..8p+7, which is
+        // exactly one 16-byte core-matrix column of the A tile.
         const int q = warp & 3;
-        const int h = (warp - 2) >> 2;
+        const int p = (warp - 2) >> 2;
         const int row = q * 32 + lane;     // A row == TMEM lane == grid point in the tile
         const int64_t g = tile0 + row;
         const bool gvalid = g < a.G;
@@ -238,66 +245,57 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         const double k = wavenumber[bin];
         const float khi = (float)k, klo = (float)(k - (double)khi);
         const uint32_t lane_addr = taddr + ((uint32_t)(q * 32) << 16);
-        constexpr int HC = TC_CHUNK / 2;   // components per half chunk
+        constexpr int PC = TC_CHUNK / TC_PARTS;   // components per part
         double S = 0.0, acc = 0.0;
-        float va[HC], vb[HC];
+        float va[PC], vb[PC];
+        const int a_off_row = (((row >> 3) * 4 + p) << 7) + ((row & 7) << 4);
 
-        auto synth = [&](int t, float (&v)[HC]) {
-            const int s = t & 1;
-            uint8_t *ahi = smem + TcSmem::a_off(s, 0);
-            uint8_t *alo = smem + TcSmem::a_off(s, 1);
+        auto synth = [&](int t, float (&v)[PC]) {
+            const int s = t % 3;
             float s_part = 0.f;
+            uint32_t hw[4], lw[4];
 #pragma unroll
-            for (int gl = 0; gl < 2; ++gl) {
-                uint32_t hw[4], lw[4];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int mm = gl * 4 + e;                 // mic within the half chunk
-                    const int m = t * TC_MPC + h * 8 + mm;
-                    float vr = 0.f, vi = 0.f;
-                    if (gvalid && m < a.M) {
-                        const float4 mv = mp4[m];
-                        const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
-                        float r = r2 * y;
-                        r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
-                        // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
-                        const float ph = khi * r;
-                        const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
-                        const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
-                        float x = fmaf(-nq, TC_P2A, ph);
-                        x = fmaf(-nq, TC_P2B, x);
-                        x = fmaf(-nq, TC_P2C, x);
-                        x += pl;
-                        float sn, cs;
-                        tc::sincos_approx(x, sn, cs);
-                        float w = 1.f;
-                        if (a.steer_type == 2) {
-                            w = r;
-                            s_part += r2;
-                        } else if (a.steer_type >= 3) {
-                            w = y;
-                            s_part = fmaf(y, y, s_part);
-                        }
-                        vr = cs * w;
-                        vi = -sn * w;
-                    }
-                    v[2 * mm] = vr;
-                    v[2 * mm + 1] = vi;
-                    // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
-                    // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
-                    const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
-                    hw[e] = __byte_perm(rr, ri, 0x7632);
-                    const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
-                    const float li = vi - __uint_as_float(ri & 0xFFFF0000u);
-                    lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li) + 0x8000u, 0x7632);
+            for (int e = 0; e < 4; ++e) {
+                const int m = t * TC_MPC + p * 4 + e;
+                const bool valid = gvalid && m < a.M;
+                const float4 mv = mp4[m];
+                const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
+                float r = r2 * y;
+                r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
+                // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
+                const float ph = khi * r;
+                const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
+                const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
+                float x = fmaf(-nq, TC_P2A, ph);
+                x = fmaf(-nq, TC_P2B, x);
+                x = fmaf(-nq, TC_P2C, x);
+                x += pl;
+                float sn, cs;
+                tc::sincos_approx(x, sn, cs);
+                float w = 1.f;
+                if (ST == 2) {
+                    w = r;
+                    s_part += valid ? r2 : 0.f;
+                } else if (ST >= 3) {
+                    w = y;
+                    s_part += valid ? y * y : 0.f;
                 }
-                const int grp = 2 * h + gl;   // 16-byte core-matrix column of this row
-                const int off = (((row >> 3) * 4 + grp) << 7) + ((row & 7) << 4);
-                *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                *reinterpret_cast<uint4 *>(alo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                const float vr = valid ? cs * w : 0.f;
+                const float vi = valid ? -sn * w : 0.f;
+                v[2 * e] = vr;
+                v[2 * e + 1] = vi;
+                // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
+                // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
+                const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
+                hw[e] = __byte_perm(rr, ri, 0x7632);
+                const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
+                const float li = vi - __uint_as_float(ri & 0xFFFF0000u);
+                lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li) + 0x8000u, 0x7632);
             }
+            *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 0) + a_off_row) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 1) + a_off_row) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
             S += (double)s_part;
             tc::fence_proxy_async_smem();
             tc::mbar_arrive(&full_a[s]);
@@ -308,57 +306,67 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             return __all_sync(0xffffffffu, ok);
         };
         auto warp_abort = [&]() -> bool { return __any_sync(0xffffffffu, *abort_flag != 0); };
-        auto epilogue = [&](int t, const float (&v)[HC]) {
-            const int s = t & 1, u = t >> 1;
-            if (!warp_wait(&done[s], u & 1)) return;
+        auto epilogue = [&](int t, const float (&v)[PC]) {
+            if (!warp_wait(&done[t % 3], (t / 3) & 1)) return;
             tc::tc_fence_after();
-            float d[HC];
-            tc::tmem_ld_x16(lane_addr + (uint32_t)(TC_CHUNK * t + HC * h), d);
+            float d[PC];
+            tc::tmem_ld_x8(lane_addr + (uint32_t)(TC_CHUNK * t + PC * p), d);
             float part = 0.f;
 #pragma unroll
-            for (int e = 0; e < HC; ++e) part = fmaf(d[e], v[e], part);
+            for (int e = 0; e < PC; ++e) part = fmaf(d[e], v[e], part);
             acc += (double)part;
         };
-        // 2 stages: synthesis of chunk t+1 overlaps the MMAs of chunk t; chunk t-1's columns are
-        // read while chunk t's MMAs run.
-        for (int t = 0; t < C && !warp_abort(); t += 2) {
-            if (t >= 2 && !warp_wait(&done[0], ((t >> 1) - 1) & 1)) break;
-            synth(t, va);
-            if (t >= 1) epilogue(t - 1, vb);
-            if (t + 1 < C && !warp_abort()) {
-                if (t + 1 >= 2 && !warp_wait(&done[1], (((t + 1) >> 1) - 1) & 1)) break;
-                synth(t + 1, vb);
-                epilogue(t, va);
-            }
+        // Synthesis runs two chunks ahead of the epilogue: chunk t is written to A stage t % 3 while
+        // the MMAs of chunks t-1 and t-2 may still run; the columns of chunk t-2 are read after.
+        // Stage t % 3 was last used by chunk t-3, whose epilogue (and hence MMA completion) was
+        // awaited one iteration earlier.
+        float vc[PC];
+        auto step = [&](int t, float (&cur)[PC], const float (&old)[PC]) {
+            synth(t, cur);
+            if (t >= 2) epilogue(t - 2, old);
+        };
+        int t = 0;
+        for (; t + 3 <= C && !warp_abort(); t += 3) {
+            step(t, va, vb);       // va: chunk t % 3 == 0; vb: chunk (t - 2) % 3 == 1
+            step(t + 1, vb, vc);   // vb: 1; vc: (t - 1) % 3 == 2
+            step(t + 2, vc, va);   // vc: 2; va: t % 3 == 0
         }
-        if (!warp_abort()) {
-            if ((C - 1) & 1) epilogue(C - 1, vb);
-            else epilogue(C - 1, va);
+        if (t < C && !warp_abort()) step(t, va, vb);
+        if (t + 1 < C && !warp_abort()) step(t + 1, vb, vc);
+        // drain: the last two chunks (slots follow chunk % 3: 0 -> va, 1 -> vb, 2 -> vc)
+        for (int tt = (C >= 2 ? C - 2 : 0); tt < C && !warp_abort(); ++tt) {
+            if (tt % 3 == 0) epilogue(tt, va);
+            else if (tt % 3 == 1) epilogue(tt, vb);
+            else epilogue(tt, vc);
         }
         tc::tc_fence_before();
-        // combine the two half-chunk partial sums of each grid point (named barrier: synth warps)
-        if (h == 1) {
-            red[row] = acc;
-            red[TC_ROWS + row] = S;
+        // combine the per-part partial sums of each grid point (named barrier over the synth warps)
+        if (p > 0) {
+            red[p * TC_ROWS + row] = acc;
+            red[(TC_PARTS + p) * TC_ROWS + row] = S;
         }
         asm volatile("bar.sync 1, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
-        if (h == 0 && gvalid && !*abort_flag) {
-            const double scalar = acc + red[row];
-            S += red[TC_ROWS + row];
+        if (p == 0 && gvalid && !*abort_flag) {
+            double scalar = acc;
+#pragma unroll
+            for (int pp = 1; pp < TC_PARTS; ++pp) {
+                scalar += red[pp * TC_ROWS + row];
+                S += red[(TC_PARTS + pp) * TC_ROWS + row];
+            }
             double r0;
             if (a.ref_mode == 1) r0 = a.ref_dist;
             else r0 = dist3(gx, gy, gz, a.ref0, a.ref1, a.ref2);
             const double Md = (double)a.M;
             double res, ns;
-            if (a.steer_type == 1) {
+            if (ST == 1) {
                 ns = 1.0 / Md;
                 res = scalar / (Md * Md) * a.norm;
-            } else if (a.steer_type == 2) {
+            } else if (ST == 2) {
                 const double nf = Md * r0;
                 const double nf2 = nf * nf;
                 ns = S / nf2;
                 res = scalar / nf2 * a.norm;
-            } else if (a.steer_type == 3) {
+            } else if (ST == 3) {
                 const double nf = r0 * S;
                 ns = 1.0 / (r0 * r0) / S;
                 res = scalar / (nf * nf) * a.norm;
@@ -437,10 +445,13 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
     // a CTA that takes all 512 TMEM columns must be alone on its SM: size the shared memory so
     // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)
     if (C > 8 && smem < 116 * 1024) smem = 116 * 1024;
-    cudaFuncSetAttribute(map_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const dim3 grid((unsigned)((p->num_grid + TC_ROWS - 1) / TC_ROWS), p->num_bins);
-    map_tc_kernel<<<grid, TC_THREADS, smem, s>>>(a, wavenumber, mpos, gpos, rh, rl, out_map, out_steer_norm,
-                                                 error_word);
+    auto kern = p->steer_type == 1 ? map_tc_kernel<1>
+                : p->steer_type == 2 ? map_tc_kernel<2>
+                : p->steer_type == 3 ? map_tc_kernel<3>
+                                     : map_tc_kernel<4>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    kern<<<grid, TC_THREADS, smem, s>>>(a, wavenumber, mpos, gpos, rh, rl, out_map, out_steer_norm, error_word);
     return check_launch();
 }
 
