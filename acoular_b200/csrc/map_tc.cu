@@ -13,14 +13,16 @@
 //
 // Per CTA: 128 grid points (UMMA M = 128, one TMEM lane each) x one frequency bin.
 //   warp 0      : bulk copies of the R' tiles of chunk i (pre-laid in HBM in the shared-memory
-//                 core-matrix order by tc_prep_kernel) into a 2-stage ring
+//                 core-matrix order by tc_prep_kernel) into a 32-tile ring, running ahead of the MMAs
 //   warp 1      : TMEM allocation; one thread issues tcgen05.mma (A = steering chunk, B = R'
 //                 tiles; products hi*hi + hi*lo + lo*hi) and commits to the stage's mbarrier
-//   warps 2..17 : steering synthesis of chunk i (four threads per grid point, 4 mics each):
+//   warps 2..5  : epilogue: after the MMAs of chunk i, read its accumulator columns from TMEM and
+//                 dot them with the steering chunk read back from the A stage (hi + lo)
+//   warps 6..21 : steering synthesis of chunk i (four threads per grid point, 4 mics each):
 //                 FP32 distance (Newton rsqrt), the phase k*r as an exact float-float product,
 //                 Cody-Waite reduction by a three-term 2*pi, hardware sincos, bf16 hi/lo split
-//                 into the A stage; then the epilogue of chunk i-1 from TMEM.  No FP64<->FP32
-//                 conversion sits in the per-element path (the conversion pipe is the scarce one).
+//                 into the A stage.  No FP64<->FP32 conversion and no TMEM access sits in the
+//                 per-element path.
 // Every mbarrier wait is bounded (globaltimer); on timeout the CTA raises an error word and exits
 // its loops without further work.
 #include <cuda_bf16.h>
@@ -40,11 +42,14 @@ constexpr int TC_TILE_ELEMS = TC_CHUNK * TC_CHUNK;
 constexpr int TC_TILE_BYTES = TC_TILE_ELEMS * 2;          // bf16
 constexpr int TC_A_BYTES = TC_ROWS * TC_CHUNK * 2;        // 8 KB per (stage, hi|lo)
 constexpr int TC_ASTAGES = 3;              // steering (A) ring: synthesis runs up to 2 chunks ahead
-constexpr int TC_BSTAGES = 2;              // R' tile (B) ring
+constexpr int TC_RING = 32;                // R' tile (B) ring: 32 tiles of hi + lo (128 KB)
 constexpr int TC_PARTS = 4;                 // synthesis threads per grid point (one per 4 mics of a chunk)
 constexpr int TC_SYNTH_WARPS = 4 * TC_PARTS;  // TC_PARTS warps per TMEM lane quarter
 constexpr int TC_SYNTH_THREADS = 32 * TC_SYNTH_WARPS;
-constexpr int TC_THREADS = 64 + TC_SYNTH_THREADS;
+constexpr int TC_EPI_WARPS = 4;             // one per TMEM lane quarter
+constexpr int TC_EPI_THREADS = 32 * TC_EPI_WARPS;
+constexpr int TC_SYNTH_WARP0 = 2 + TC_EPI_WARPS;
+constexpr int TC_THREADS = 64 + TC_EPI_THREADS + TC_SYNTH_THREADS;
 
 // 2*pi = P2A + P2B + P2C (Cody-Waite split; P2A has 8 significant bits so n*P2A is exact)
 __device__ constexpr float TC_P2A = 0x1.92p+2f;
@@ -62,7 +67,11 @@ struct TcArgs {
     double ref0, ref1, ref2, ref_dist;
     uint64_t wait_limit_ns;
     int64_t bin_stride_elems;  // R' elements per bin (hi and lo separately)
+    int64_t ntiles;            // 128-point grid tiles per bin
+    int64_t nitems;            // work items = bins x tiles (bin-major: CTAs in flight share a bin)
 };
+
+constexpr int TC_NB = 8;       // chunk barrier ring (full_b / done); the producer runs <= 7 chunks ahead
 
 __host__ __device__ constexpr int tri_tiles(int C) { return C * (C + 1) / 2; }
 // index of tile (i, j >= i) in the row-major upper-triangular tile order
@@ -115,16 +124,53 @@ struct TcSmem {
     // offsets in bytes from the 1024-aligned dynamic shared-memory base
     __host__ __device__ static constexpr int a_off(int stage, int lo) { return (stage * 2 + lo) * TC_A_BYTES; }
     __host__ __device__ static constexpr int b_base() { return TC_ASTAGES * 2 * TC_A_BYTES; }
-    __host__ __device__ static constexpr int b_off(int C, int stage, int lo)
+    // ring slot of R' tile pair: hi at b_off(slot, 0), lo at b_off(slot, 1)
+    __host__ __device__ static constexpr int b_off(int slot, int lo)
     {
-        return b_base() + (stage * 2 + lo) * C * TC_TILE_BYTES;
+        return b_base() + (lo * TC_RING + slot) * TC_TILE_BYTES;
     }
-    __host__ __device__ static constexpr int mic_off(int C) { return b_base() + TC_BSTAGES * 2 * C * TC_TILE_BYTES; }
+    __host__ __device__ static constexpr int mic_off(int C) { return b_base() + 2 * TC_RING * TC_TILE_BYTES; }
     __host__ __device__ static constexpr int red_off(int C, int Mp) { return mic_off(C) + Mp * 16; }
+    // per-item normalisation partial sums, double-buffered by item parity: [2][parts][128]
     __host__ __device__ static constexpr int bar_off(int C, int Mp) { return red_off(C, Mp) + 2 * TC_PARTS * TC_ROWS * 8; }
-    __host__ __device__ static constexpr int total(int C, int Mp) { return bar_off(C, Mp) + 128; }
+    __host__ __device__ static constexpr int nbars() { return 2 * TC_ASTAGES + 2 * TC_NB + 1 + 2 + 2; }
+    __host__ __device__ static constexpr int total(int C, int Mp) { return bar_off(C, Mp) + nbars() * 8 + 16; }
 };
 
+// Normalisation of the steering type (acoular/fastFuncs.py:293-310) and clipping.
+template <int ST>
+__device__ __forceinline__ void finish_point(const TcArgs &a, double scalar, double S, double gx, double gy, double gz,
+                                             int bin, int64_t g, double *out_map, double *out_norm)
+{
+    double r0;
+    if (a.ref_mode == 1) r0 = a.ref_dist;
+    else r0 = dist3(gx, gy, gz, a.ref0, a.ref1, a.ref2);
+    const double Md = (double)a.M;
+    double res, ns;
+    if (ST == 1) {
+        ns = 1.0 / Md;
+        res = scalar / (Md * Md) * a.norm;
+    } else if (ST == 2) {
+        const double nf = Md * r0;
+        const double nf2 = nf * nf;
+        ns = S / nf2;
+        res = scalar / nf2 * a.norm;
+    } else if (ST == 3) {
+        const double nf = r0 * S;
+        ns = 1.0 / (r0 * r0) / S;
+        res = scalar / (nf * nf) * a.norm;
+    } else {
+        const double nf = Md * S;
+        ns = 1.0 / Md;
+        res = scalar / nf * a.norm;
+    }
+    if (a.clip && res < 0.0) res = 0.0;
+    out_map[(int64_t)bin * a.G + g] = res;
+    if (out_norm) out_norm[(int64_t)bin * a.G + g] = ns;
+}
+
+// Persistent kernel: one CTA per SM walks the work items (bin, tile) blockIdx.x, +gridDim.x, ...;
+// the chunk pipeline runs on across item boundaries.  Global chunk counter T = local item * C + t.
 template <int ST>
 __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const double *__restrict__ wavenumber,
                                                                const double *__restrict__ mpos,
@@ -139,18 +185,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     const int C = a.C, Mp = a.Mp;
     float4 *mp4 = reinterpret_cast<float4 *>(smem + TcSmem::mic_off(C));        // [Mp] (x, y, z, 0)
-    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(C, Mp));     // [2][parts][128]
+    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(C, Mp));     // [2][parts][128] sums S
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(C, Mp));
-    uint64_t *full_a = bars;        // [3] steering chunk t in A stage t % 3
-    uint64_t *full_b = bars + 3;    // [2] R' tiles of chunk t in B stage t % 2
-    uint64_t *done = bars + 5;      // [3] MMAs of chunk t complete (committed to done[t % 3])
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 9);
+    uint64_t *full_a = bars;                          // [3]  chunk T written to A stage T % 3
+    uint64_t *afree = bars + TC_ASTAGES;              // [3]  epilogue of chunk T has read A stage T % 3
+    uint64_t *full_b = bars + 2 * TC_ASTAGES;         // [8]  R' tiles of chunk T landed
+    uint64_t *done = full_b + TC_NB;                  // [8]  MMAs of chunk T complete
+    uint64_t *tmem_free = done + TC_NB;               // [1]  epilogue has read all columns of an item
+    uint64_t *s_ready = tmem_free + 1;                // [2]  synthesis sums S of item parity written
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(s_ready + 2 + 2);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(s_ready + 2 + 3);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bin = blockIdx.y;
-    const int64_t tile0 = (int64_t)blockIdx.x * TC_ROWS;
     const uint32_t ncols = (uint32_t)(C <= 1 ? 32 : (C <= 2 ? 64 : (C <= 4 ? 128 : (C <= 8 ? 256 : 512))));
+    const int64_t nmine = a.nitems > blockIdx.x ? (a.nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     for (int m = threadIdx.x; m < Mp; m += blockDim.x) {
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -160,9 +208,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_ASTAGES; ++s) {
             tc::mbar_init(&full_a[s], TC_SYNTH_THREADS);
+            tc::mbar_init(&afree[s], TC_EPI_THREADS);
+        }
+        for (int s = 0; s < TC_NB; ++s) {
+            tc::mbar_init(&full_b[s], 1);
             tc::mbar_init(&done[s], 1);
         }
-        for (int s = 0; s < TC_BSTAGES; ++s) tc::mbar_init(&full_b[s], 1);
+        tc::mbar_init(tmem_free, TC_EPI_THREADS);
+        tc::mbar_init(&s_ready[0], TC_SYNTH_THREADS);
+        tc::mbar_init(&s_ready[1], TC_SYNTH_THREADS);
         *abort_flag = 0;
         tc::fence_mbar_init();
     }
@@ -171,213 +225,251 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t taddr = *tmem_slot;
-    const int64_t bin_off = (int64_t)bin * a.bin_stride_elems;
 
     if (warp == 0) {
-        // ---------------- producer: R' tiles of chunk t ----------------
+        // ---------------- producer: R' tiles of every chunk into the tile ring ----------------
+        // Chunk T takes C - t consecutive ring tiles starting at the running tile counter U; tile U
+        // reuses slot U % TC_RING, free once the chunk that held tile U - TC_RING is complete.
         if (lane == 0) {
-            int last = -1;
-            for (int t = 0; t < C && !*abort_flag; ++t) {
-                const int s = t & 1;
-                // B stage t % 2 was last read by the MMAs of chunk t - 2
-                if (t >= TC_BSTAGES &&
-                    !tc::mbar_wait(&done[(t - 2) % 3], ((t - 2) / 3) & 1, abort_flag, a.wait_limit_ns))
-                    break;
-                const uint32_t bytes = (uint32_t)(C - t) * TC_TILE_BYTES;
-                tc::mbar_arrive_expect_tx(&full_b[s], 2 * bytes);
-                const int64_t src = bin_off + (int64_t)tile_index(C, t, t) * TC_TILE_ELEMS;
-                tc::bulk_g2s(smem + TcSmem::b_off(C, s, 0), rh + src, bytes, &full_b[s]);
-                tc::bulk_g2s(smem + TcSmem::b_off(C, s, 1), rl + src, bytes, &full_b[s]);
-                last = t;
+            uint32_t ustart[TC_NB];   // first ring tile of the last TC_NB chunks
+            uint32_t U = 0;
+            int T = 0, freed = -1, lastT = -1;
+            bool ok = true;
+            for (int64_t li = 0; li < nmine && ok; ++li) {
+                const int64_t item = blockIdx.x + li * gridDim.x;
+                const __nv_bfloat16 *bh = rh + (item / a.ntiles) * a.bin_stride_elems;
+                const __nv_bfloat16 *bl = rl + (item / a.ntiles) * a.bin_stride_elems;
+                for (int t = 0; t < C && ok; ++t, ++T) {
+                    const int n = C - t;
+                    // chunk barriers form a ring of TC_NB: chunk T - TC_NB must be complete; ring
+                    // slots: every chunk holding a tile <= U + n - 1 - TC_RING must be complete
+                    while (ok && (freed < T - TC_NB ||
+                                  (freed + 1 < T && (int)(ustart[(freed + 1) & (TC_NB - 1)] - (U + n - 1 - TC_RING)) <= 0))) {
+                        ok = tc::mbar_wait(&done[(freed + 1) & (TC_NB - 1)], (uint32_t)(((freed + 1) / TC_NB) & 1),
+                                           abort_flag, a.wait_limit_ns);
+                        if (ok) ++freed;
+                    }
+                    if (!ok) break;
+                    ustart[T & (TC_NB - 1)] = U;
+                    uint64_t *fb = &full_b[T & (TC_NB - 1)];
+                    tc::mbar_arrive_expect_tx(fb, 2u * n * TC_TILE_BYTES);
+                    const int64_t src = (int64_t)tile_index(C, t, t) * TC_TILE_ELEMS;
+                    int j = 0;
+                    while (j < n) {   // contiguous runs of ring slots
+                        const int slot = (int)((U + j) & (TC_RING - 1));
+                        const int run = min(n - j, TC_RING - slot);
+                        const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
+                        tc::bulk_g2s(smem + TcSmem::b_off(slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                        tc::bulk_g2s(smem + TcSmem::b_off(slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                        j += run;
+                    }
+                    U += (uint32_t)n;
+                    lastT = T;
+                }
             }
             // on an abort, let the last copies land before the CTA releases its shared memory
-            if (*abort_flag && last >= 0)
-                tc::mbar_wait(&full_b[last & 1], (last >> 1) & 1, abort_flag, 4 * a.wait_limit_ns);
+            if (*abort_flag && lastT >= 0)
+                tc::mbar_wait(&full_b[lastT & (TC_NB - 1)], (uint32_t)((lastT / TC_NB) & 1), abort_flag,
+                              4 * a.wait_limit_ns);
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
+        // Kept lean: it sits on every chunk's critical path.  Descriptors are built once and
+        // advanced by adding byte offsets >> 4 to their 14-bit start-address field; ring and
+        // stage indices are 32-bit counters advanced incrementally.
         if (lane == 0) {
-            int last = -1;
-            for (int t = 0; t < C && !*abort_flag; ++t) {
-                const int sa = t % 3, sb = t & 1;
-                if (!tc::mbar_wait(&full_a[sa], (t / 3) & 1, abort_flag, a.wait_limit_ns)) break;
-                if (!tc::mbar_wait(&full_b[sb], (t >> 1) & 1, abort_flag, a.wait_limit_ns)) break;
-                tc::tc_fence_after();
-                const int ntot = TC_CHUNK * (C - t);
-                const uint32_t c0 = (uint32_t)(TC_CHUNK * t);
+            const uint64_t a_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::a_off(0, 0)), 128, 512);
+            const uint64_t b_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::b_off(0, 0)), 128, 512);
+            constexpr uint32_t A_STEP = TC_A_BYTES >> 4;          // next (stage, hi|lo) block
+            constexpr uint32_t T_STEP = TC_TILE_BYTES >> 4;       // next ring tile
+            constexpr uint32_t LO_B = (TC_RING * TC_TILE_BYTES) >> 4;
+            const uint32_t idesc0 = tc::idesc_m128(1, 0);
+            int sa = 0, ua = 0;     // A stage and its phase parity
+            int sb = 0, ub = 0;     // chunk barrier slot and parity
+            uint32_t slot0 = 0;     // ring slot of the chunk's first tile
+            int lastb = -1, lastu = 0;
+            bool ok = true;
+            for (int64_t li = 0; li < nmine && ok; ++li) {
+                // the previous item's epilogue must have read every accumulator column
+                if (li > 0) ok = tc::mbar_wait(tmem_free, (uint32_t)((li - 1) & 1), abort_flag, a.wait_limit_ns);
+                for (int t = 0; t < C && ok; ++t) {
+                    ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, a.wait_limit_ns) &&
+                         tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, a.wait_limit_ns);
+                    if (!ok) break;
+                    tc::tc_fence_after();
+                    const int n = C - t;
+                    const uint32_t dcol = taddr + (uint32_t)(TC_CHUNK * t);
+                    // split the chunk's n tiles into runs of <= 8 (N <= 256) that do not wrap
+                    int run0 = min(min(n, 8), (int)(TC_RING - slot0));
+                    const uint32_t slot1 = (slot0 + run0) & (TC_RING - 1);
+                    const int rest = n - run0;
+                    int run1 = min(min(rest, 8), (int)(TC_RING - slot1));
+                    const uint32_t slot2 = (slot1 + run1) & (TC_RING - 1);
+                    const int run2 = rest - run1;   // at most one more run (n <= 16)
 #pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
+                    for (int ks = 0; ks < 2; ++ks) {
 #pragma unroll
-                    for (int prod = 0; prod < 3; ++prod) {
-                        const uint32_t a_addr = tc::smem_u32(smem + TcSmem::a_off(sa, prod == 2)) + ks * 256;
-                        const uint32_t b_addr = tc::smem_u32(smem + TcSmem::b_off(C, sb, prod == 1)) + ks * 256;
-                        const uint64_t ad = tc::sdesc_noswizzle(a_addr, 128, 512);
-                        for (int n0 = 0; n0 < ntot; n0 += 256) {
-                            const int np = min(256, ntot - n0);
-                            const uint64_t bd = tc::sdesc_noswizzle(b_addr + (n0 / TC_CHUNK) * TC_TILE_BYTES, 128, 512);
+                        for (int prod = 0; prod < 3; ++prod) {
+                            const uint64_t ad = a_base + (uint64_t)((sa * 2 + (prod == 2)) * A_STEP + ks * 16);
+                            const uint64_t bd = b_base + (uint64_t)((prod == 1 ? LO_B : 0u) + ks * 16);
                             const uint32_t accum = (t == 0 && ks == 0 && prod == 0) ? 0u : 1u;
-                            tc::mma_bf16(taddr + c0 + (uint32_t)n0, ad, bd, tc::idesc_m128(1, (uint32_t)np), accum);
+                            tc::mma_bf16(dcol, ad, bd + slot0 * T_STEP, idesc0 | ((uint32_t)(run0 * 4) << 17), accum);
+                            if (run1 > 0)
+                                tc::mma_bf16(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP,
+                                             idesc0 | ((uint32_t)(run1 * 4) << 17), accum);
+                            if (run2 > 0)
+                                tc::mma_bf16(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
+                                             idesc0 | ((uint32_t)(run2 * 4) << 17), accum);
                         }
                     }
+                    tc::mma_commit(&done[sb]);
+                    lastb = sb;
+                    lastu = ub;
+                    slot0 = (slot0 + (uint32_t)n) & (TC_RING - 1);
+                    if (++sa == TC_ASTAGES) { sa = 0; ua ^= 1; }
+                    if (++sb == TC_NB) { sb = 0; ub ^= 1; }
                 }
-                tc::mma_commit(&done[sa]);
-                last = t;
             }
-            if (last >= 0) tc::mbar_wait(&done[last % 3], (last / 3) & 1, abort_flag, 4 * a.wait_limit_ns);
+            if (lastb >= 0) tc::mbar_wait(&done[lastb], (uint32_t)lastu, abort_flag, 4 * a.wait_limit_ns);
+        }
+    } else if (warp < TC_SYNTH_WARP0) {
+        // ---------------- epilogue (warps 2..5): one thread per grid point ----------------
+        // After the MMAs of chunk t the accumulator columns of chunk t are final; dot them with the
+        // steering chunk as the MMA saw it (hi + lo from A stage T % 3), then release the stage.
+        const int q = warp & 3;
+        const int row = q * 32 + lane;
+        const uint32_t lane_addr = taddr + ((uint32_t)(q * 32) << 16);
+        const int a_row = ((row >> 3) << 9) + ((row & 7) << 4);   // byte offset of the row's first chunk
+        int T = 0;
+        bool ok = true;
+        for (int64_t li = 0; li < nmine && ok; ++li) {
+            const int64_t item = blockIdx.x + li * gridDim.x;
+            const int bin = (int)(item / a.ntiles);
+            const int64_t g = (item % a.ntiles) * TC_ROWS + row;
+            double acc = 0.0;
+            for (int t = 0; t < C; ++t, ++T) {
+                ok = __all_sync(0xffffffffu, tc::mbar_wait(&done[T & (TC_NB - 1)], (uint32_t)((T / TC_NB) & 1),
+                                                           abort_flag, a.wait_limit_ns));
+                if (!ok) break;
+                tc::tc_fence_after();
+                float d[TC_CHUNK];
+                tc::tmem_ld_x32(lane_addr + (uint32_t)(TC_CHUNK * t), d);
+                const int sa = (int)(T % TC_ASTAGES);
+                const uint8_t *ahi = smem + TcSmem::a_off(sa, 0) + a_row;
+                const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;
+                float part = 0.f;
+#pragma unroll
+                for (int grp = 0; grp < 4; ++grp) {
+                    const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
+                    const uint4 lw = *reinterpret_cast<const uint4 *>(alo + grp * 128);
+                    const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w}, lv[4] = {lw.x, lw.y, lw.z, lw.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float vr = __uint_as_float(hv[e] << 16) + __uint_as_float(lv[e] << 16);
+                        const float vi = __uint_as_float(hv[e] & 0xFFFF0000u) + __uint_as_float(lv[e] & 0xFFFF0000u);
+                        part = fmaf(d[grp * 8 + 2 * e], vr, part);
+                        part = fmaf(d[grp * 8 + 2 * e + 1], vi, part);
+                    }
+                }
+                acc += (double)part;
+                tc::tc_fence_before();
+                tc::mbar_arrive(&afree[sa]);
+            }
+            if (!ok) break;
+            tc::mbar_arrive(tmem_free);
+            // normalisation sums of this item from the synthesis warps
+            ok = __all_sync(0xffffffffu, tc::mbar_wait(&s_ready[li & 1], (uint32_t)((li >> 1) & 1), abort_flag,
+                                                       a.wait_limit_ns));
+            if (!ok) break;
+            if (g < a.G) {
+                const double *rs = red + (li & 1) * TC_PARTS * TC_ROWS;
+                double S = 0.0;
+#pragma unroll
+                for (int pp = 0; pp < TC_PARTS; ++pp) S += rs[pp * TC_ROWS + row];
+                finish_point<ST>(a, acc, S, gpos[g], gpos[a.G + g], gpos[2 * a.G + g], bin, g, out_map, out_norm);
+            }
         }
     } else {
-        // ---------------- steering synthesis + epilogue (warps 2..17) ----------------
-        // Warp w serves TMEM lane quarter q = w % 4 (grid points 32q..32q+31 of the tile) and
-        // part p of every chunk: mics 4p..4p+3 of the chunk's 16, components 8p..8p+7, which is
-        // exactly one 16-byte core-matrix column of the A tile.
+        // ---------------- steering synthesis (warps 6..21) ----------------
+        // Warp w serves grid points 32q..32q+31 (q = w % 4) and part p of every chunk: mics
+        // 4p..4p+3 of the chunk's 16, i.e. one 16-byte core-matrix column of the A tile.
         const int q = warp & 3;
-        const int p = (warp - 2) >> 2;
-        const int row = q * 32 + lane;     // A row == TMEM lane == grid point in the tile
-        const int64_t g = tile0 + row;
-        const bool gvalid = g < a.G;
-        double gx = 0, gy = 0, gz = 0;
-        if (gvalid) {
-            gx = gpos[g];
-            gy = gpos[a.G + g];
-            gz = gpos[2 * a.G + g];
-        }
-        const float gxf = (float)gx, gyf = (float)gy, gzf = (float)gz;
-        const double k = wavenumber[bin];
-        const float khi = (float)k, klo = (float)(k - (double)khi);
-        const uint32_t lane_addr = taddr + ((uint32_t)(q * 32) << 16);
-        constexpr int PC = TC_CHUNK / TC_PARTS;   // components per part
-        double S = 0.0, acc = 0.0;
-        float va[PC], vb[PC];
+        const int p = (warp - TC_SYNTH_WARP0) >> 2;
+        const int row = q * 32 + lane;
         const int a_off_row = (((row >> 3) * 4 + p) << 7) + ((row & 7) << 4);
-
-        auto synth = [&](int t, float (&v)[PC]) {
-            const int s = t % 3;
-            float s_part = 0.f;
-            uint32_t hw[4], lw[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int m = t * TC_MPC + p * 4 + e;
-                const bool valid = gvalid && m < a.M;
-                const float4 mv = mp4[m];
-                const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
-                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
-                float r = r2 * y;
-                r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
-                // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
-                const float ph = khi * r;
-                const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
-                const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
-                float x = fmaf(-nq, TC_P2A, ph);
-                x = fmaf(-nq, TC_P2B, x);
-                x = fmaf(-nq, TC_P2C, x);
-                x += pl;
-                float sn, cs;
-                tc::sincos_approx(x, sn, cs);
-                float w = 1.f;
-                if (ST == 2) {
-                    w = r;
-                    s_part += valid ? r2 : 0.f;
-                } else if (ST >= 3) {
-                    w = y;
-                    s_part += valid ? y * y : 0.f;
+        int T = 0;
+        bool ok = true;
+        for (int64_t li = 0; li < nmine && ok; ++li) {
+            const int64_t item = blockIdx.x + li * gridDim.x;
+            const int bin = (int)(item / a.ntiles);
+            const int64_t g = (item % a.ntiles) * TC_ROWS + row;
+            const bool gvalid = g < a.G;
+            float gxf = 0.f, gyf = 0.f, gzf = 0.f;
+            if (gvalid) {
+                gxf = (float)gpos[g];
+                gyf = (float)gpos[a.G + g];
+                gzf = (float)gpos[2 * a.G + g];
+            }
+            const double k = wavenumber[bin];
+            const float khi = (float)k, klo = (float)(k - (double)khi);
+            double S = 0.0;
+            for (int t = 0; t < C; ++t, ++T) {
+                const int s = (int)(T % TC_ASTAGES);
+                if (T >= TC_ASTAGES) {
+                    // A stage T % 3 is free once the epilogue of chunk T - 3 has read it
+                    ok = __all_sync(0xffffffffu, tc::mbar_wait(&afree[s], (uint32_t)(((T - 3) / 3) & 1), abort_flag,
+                                                               a.wait_limit_ns));
+                    if (!ok) break;
                 }
-                const float vr = valid ? cs * w : 0.f;
-                const float vi = valid ? -sn * w : 0.f;
-                v[2 * e] = vr;
-                v[2 * e + 1] = vi;
-                // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
-                // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
-                const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
-                hw[e] = __byte_perm(rr, ri, 0x7632);
-                const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
-                const float li = vi - __uint_as_float(ri & 0xFFFF0000u);
-                lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li) + 0x8000u, 0x7632);
-            }
-            *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 0) + a_off_row) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-            *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 1) + a_off_row) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
-            S += (double)s_part;
-            tc::fence_proxy_async_smem();
-            tc::mbar_arrive(&full_a[s]);
-        };
-        // warp-uniform waits: tcgen05.ld is .sync.aligned, all 32 lanes must take the same path
-        auto warp_wait = [&](uint64_t *bar, uint32_t parity) -> bool {
-            const bool ok = tc::mbar_wait(bar, parity, abort_flag, a.wait_limit_ns);
-            return __all_sync(0xffffffffu, ok);
-        };
-        auto warp_abort = [&]() -> bool { return __any_sync(0xffffffffu, *abort_flag != 0); };
-        auto epilogue = [&](int t, const float (&v)[PC]) {
-            if (!warp_wait(&done[t % 3], (t / 3) & 1)) return;
-            tc::tc_fence_after();
-            float d[PC];
-            tc::tmem_ld_x8(lane_addr + (uint32_t)(TC_CHUNK * t + PC * p), d);
-            float part = 0.f;
+                float s_part = 0.f;
+                uint32_t hw[4], lw[4];
 #pragma unroll
-            for (int e = 0; e < PC; ++e) part = fmaf(d[e], v[e], part);
-            acc += (double)part;
-        };
-        // Synthesis runs two chunks ahead of the epilogue: chunk t is written to A stage t % 3 while
-        // the MMAs of chunks t-1 and t-2 may still run; the columns of chunk t-2 are read after.
-        // Stage t % 3 was last used by chunk t-3, whose epilogue (and hence MMA completion) was
-        // awaited one iteration earlier.
-        float vc[PC];
-        auto step = [&](int t, float (&cur)[PC], const float (&old)[PC]) {
-            synth(t, cur);
-            if (t >= 2) epilogue(t - 2, old);
-        };
-        int t = 0;
-        for (; t + 3 <= C && !warp_abort(); t += 3) {
-            step(t, va, vb);       // va: chunk t % 3 == 0; vb: chunk (t - 2) % 3 == 1
-            step(t + 1, vb, vc);   // vb: 1; vc: (t - 1) % 3 == 2
-            step(t + 2, vc, va);   // vc: 2; va: t % 3 == 0
-        }
-        if (t < C && !warp_abort()) step(t, va, vb);
-        if (t + 1 < C && !warp_abort()) step(t + 1, vb, vc);
-        // drain: the last two chunks (slots follow chunk % 3: 0 -> va, 1 -> vb, 2 -> vc)
-        for (int tt = (C >= 2 ? C - 2 : 0); tt < C && !warp_abort(); ++tt) {
-            if (tt % 3 == 0) epilogue(tt, va);
-            else if (tt % 3 == 1) epilogue(tt, vb);
-            else epilogue(tt, vc);
-        }
-        tc::tc_fence_before();
-        // combine the per-part partial sums of each grid point (named barrier over the synth warps)
-        if (p > 0) {
-            red[p * TC_ROWS + row] = acc;
-            red[(TC_PARTS + p) * TC_ROWS + row] = S;
-        }
-        asm volatile("bar.sync 1, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
-        if (p == 0 && gvalid && !*abort_flag) {
-            double scalar = acc;
-#pragma unroll
-            for (int pp = 1; pp < TC_PARTS; ++pp) {
-                scalar += red[pp * TC_ROWS + row];
-                S += red[(TC_PARTS + pp) * TC_ROWS + row];
+                for (int e = 0; e < 4; ++e) {
+                    const int m = t * TC_MPC + p * 4 + e;
+                    const bool valid = gvalid && m < a.M;
+                    const float4 mv = mp4[m];
+                    const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
+                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                    const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
+                    float r = r2 * y;
+                    r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
+                    // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
+                    const float ph = khi * r;
+                    const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
+                    const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
+                    float x = fmaf(-nq, TC_P2A, ph);
+                    x = fmaf(-nq, TC_P2B, x);
+                    x = fmaf(-nq, TC_P2C, x);
+                    x += pl;
+                    float sn, cs;
+                    tc::sincos_approx(x, sn, cs);
+                    float w = 1.f;
+                    if (ST == 2) {
+                        w = r;
+                        s_part += valid ? r2 : 0.f;
+                    } else if (ST >= 3) {
+                        w = y;
+                        s_part += valid ? y * y : 0.f;
+                    }
+                    const float vr = valid ? cs * w : 0.f;
+                    const float vi = valid ? -sn * w : 0.f;
+                    // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
+                    // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
+                    const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
+                    hw[e] = __byte_perm(rr, ri, 0x7632);
+                    const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
+                    const float li_ = vi - __uint_as_float(ri & 0xFFFF0000u);
+                    lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li_) + 0x8000u, 0x7632);
+                }
+                *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 0) + a_off_row) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 1) + a_off_row) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                S += (double)s_part;
+                tc::fence_proxy_async_smem();
+                tc::mbar_arrive(&full_a[s]);
             }
-            double r0;
-            if (a.ref_mode == 1) r0 = a.ref_dist;
-            else r0 = dist3(gx, gy, gz, a.ref0, a.ref1, a.ref2);
-            const double Md = (double)a.M;
-            double res, ns;
-            if (ST == 1) {
-                ns = 1.0 / Md;
-                res = scalar / (Md * Md) * a.norm;
-            } else if (ST == 2) {
-                const double nf = Md * r0;
-                const double nf2 = nf * nf;
-                ns = S / nf2;
-                res = scalar / nf2 * a.norm;
-            } else if (ST == 3) {
-                const double nf = r0 * S;
-                ns = 1.0 / (r0 * r0) / S;
-                res = scalar / (nf * nf) * a.norm;
-            } else {
-                const double nf = Md * S;
-                ns = 1.0 / Md;
-                res = scalar / nf * a.norm;
-            }
-            if (a.clip && res < 0.0) res = 0.0;
-            out_map[(int64_t)bin * a.G + g] = res;
-            if (out_norm) out_norm[(int64_t)bin * a.G + g] = ns;
+            if (!ok) break;
+            red[((li & 1) * TC_PARTS + p) * TC_ROWS + row] = S;
+            tc::mbar_arrive(&s_ready[li & 1]);
         }
     }
     __syncthreads();
@@ -435,6 +527,8 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
     a.ref_dist = p->ref_distance;
     a.wait_limit_ns = 500ull * 1000 * 1000;
     a.bin_stride_elems = (int64_t)tri_tiles(C) * TC_TILE_ELEMS;
+    a.ntiles = (p->num_grid + TC_ROWS - 1) / TC_ROWS;
+    a.nitems = a.ntiles * p->num_bins;
     __nv_bfloat16 *rh = reinterpret_cast<__nv_bfloat16 *>(workspace);
     __nv_bfloat16 *rl = rh + (size_t)p->num_bins * a.bin_stride_elems;
     tc_prep_kernel<<<dim3(tri_tiles(C), p->num_bins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csm), M, C,
@@ -445,7 +539,9 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
     // a CTA that takes all 512 TMEM columns must be alone on its SM: size the shared memory so
     // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)
     if (C > 8 && smem < 116 * 1024) smem = 116 * 1024;
-    const dim3 grid((unsigned)((p->num_grid + TC_ROWS - 1) / TC_ROWS), p->num_bins);
+    int dev = 0, nsm = kNumSMs;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const dim3 grid((unsigned)(a.nitems < nsm ? a.nitems : nsm));
     auto kern = p->steer_type == 1 ? map_tc_kernel<1>
                 : p->steer_type == 2 ? map_tc_kernel<2>
                 : p->steer_type == 3 ? map_tc_kernel<3>

@@ -101,3 +101,14 @@ def test_tc_error_word_stays_clear():
              error_word=err)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
+
+
+@pytest.mark.parametrize('M,G,nb', [(64, 20000, 4), (256, 12000, 3), (40, 50000, 2)])
+def test_tc_persistent_many_items_per_cta(M, G, nb):
+    """More work items (bin x 128-point tile) than CTAs: the pipeline runs across item boundaries."""
+    mpos, gpos, freqs, csm = _case(M, G, seed=M * 3 + nb, nb=nb)
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    ref = O.beamformer_calc(csm, freqs, range(nb), r0, rm, 343.0, 'true location', True)
+    got = _tc(csm, freqs, mpos, gpos, 'true location', True)
+    for b in range(nb):
+        assert rel(got[b], ref[b]) <= TOL
