@@ -74,6 +74,7 @@ SIGNATURES = {
     'acb_sincos_table_build_host': (_I64, [_VP, _I64, ctypes.c_float, _I]),
     'acb_map_tc_workspace_bytes': (_SZ, [_I, _I, _I]),
     'acb_map_tc': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _SZ, _VP, _VP]),
+    'acb_map_tc_noalloc': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
 }
 
 

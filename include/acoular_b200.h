@@ -138,6 +138,25 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
                const double *mpos, const double *gpos, double *out_map, double *out_steer_norm,
                void *workspace, size_t workspace_bytes, int *error_word, void *stream);
 
+/* Size of the fixed device array behind acb_map_tc_noalloc (32 MiB per GPU, held until exit). */
+#define ACB_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+
+/* No counterpart in the reference.  Same computation and arguments as acb_map_tc, but it allocates
+ * nothing and takes no workspace: the scratch lives in a fixed array of ACB_NOALLOC_SCRATCH_BYTES
+ * that the library keeps on every GPU that loads it.  Meant for callers that cannot allocate device
+ * memory when they call, such as a real-time acquisition loop that must not risk cudaMalloc's
+ * implicit device synchronisation, or a host program with no device allocator of its own.
+ * Limit: acb_map_tc_workspace_bytes(num_mics, num_bins, precision) must not exceed
+ * ACB_NOALLOC_SCRATCH_BYTES (e.g. 60 bins at 256 mics); larger requests return ACB_ERR_SHAPE before
+ * any work is enqueued -- split the bins over several calls.
+ * The first call on a device looks up the array's device address (once per device, with that
+ * device current); make that first call before capturing a stream.
+ * All calls share the one array: calls whose GPU work overlaps (different streams, or different
+ * host threads on one device) race on it; order them on one stream. */
+int acb_map_tc_noalloc(const acb_map_params *p, int precision, const void *csm, const double *wavenumber,
+                       const double *mpos, const double *gpos, double *out_map, double *out_steer_norm,
+                       int *error_word, void *stream);
+
 /* Host-side construction of the sincos exception table used by glibc_faithful=1.
  * The reference evaluates float32 cos/sin of the float32 phase through the C library (numba
  * lowers np.cos/np.sin on float32 to cosf/sinf).  The device computes the correctly rounded
