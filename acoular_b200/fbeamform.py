@@ -24,6 +24,25 @@ from . import device as D
 from .environments import Environment
 
 
+def _zeros_pinned(shape, dtype):
+    """Zero-filled result array in page-locked host memory when a GPU is present (fast copies)."""
+    if torch.cuda.is_available():
+        t = torch.zeros(shape, dtype=getattr(torch, np.dtype(dtype).name), pin_memory=True)
+        return t.numpy()
+    return np.zeros(shape, dtype=dtype)
+
+
+_copy_streams: dict = {}
+
+
+def _copy_stream(dev):
+    s = _copy_streams.get(str(dev))
+    if s is None:
+        s = torch.cuda.Stream(device=dev)
+        _copy_streams[str(dev)] = s
+    return s
+
+
 class SteeringVector:
     STEER_TYPES = ('true level', 'true location', 'classic', 'inverse')
 
@@ -154,7 +173,7 @@ class BeamformerBase:
             self._f = self.freq_data.fftfreq()
             self._numfreq = self._f.shape[0]
             self._assert_equal_channels()
-            self._ac = np.zeros((self._numfreq, self.steer.grid.size), dtype=self.precision)
+            self._ac = _zeros_pinned((self._numfreq, self.steer.grid.size), self.precision)
             self._fr = np.zeros(self._numfreq, dtype='int8')
             self._key = key
         return LazyBfResult(self)
@@ -177,7 +196,12 @@ class BeamformerBase:
         return self._mpos_d, self._gpos_d
 
     def _calc(self, ind):
-        """Compute bins ``ind`` (array of int) on the device; writes ``_ac[ind]`` and ``_fr[ind] = 1``."""
+        """Compute bins ``ind`` (array of int) on the device; writes ``_ac[ind]`` and ``_fr[ind] = 1``.
+
+        All requested bins go to the device in a few large launches; contiguous runs of bins are
+        passed as views (no copy of the CSM), and each launch's map is copied into ``_ac`` on a side
+        stream while the next launch computes.
+        """
         ind = np.asarray(ind, dtype=np.int64)
         if ind.size == 0:
             return
@@ -187,12 +211,22 @@ class BeamformerBase:
         G = gpos.shape[1]
         M = mpos.shape[1]
         cap = self.max_bins_per_launch or max(1, int((1 << 30) // max(1, G * 8 + M * M * 16)))
+        # a few launches so that the copy of one overlaps the next one's computation
+        cap = min(cap, max(1, -(-ind.size // 4)))
         norm = self.sig_loss_norm()
         ref = self.steer.ref
+        ac_t = torch.from_numpy(self._ac)
+        pinned = ac_t.is_pinned()
+        compute = torch.cuda.current_stream(dev)
+        copy = _copy_stream(dev)
+        pending = []
         for s0 in range(0, ind.size, cap):
             sub = ind[s0:s0 + cap]
-            idx = torch.as_tensor(sub, device=dev)
-            csm = csm_all.index_select(0, idx).contiguous()
+            contiguous = bool(np.all(np.diff(sub) == 1))
+            if contiguous:
+                csm = csm_all[int(sub[0]):int(sub[-1]) + 1]
+            else:
+                csm = csm_all.index_select(0, torch.as_tensor(sub, device=dev)).contiguous()
             k = torch.as_tensor(2 * np.pi * self._f[sub] / self.steer.env.c, dtype=torch.float64, device=dev)
             if self.form == 'f64':
                 out = D.map_f64(csm, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm, ref=ref,
@@ -200,8 +234,25 @@ class BeamformerBase:
             else:
                 out = D.map_tc(csm, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm, ref=ref,
                                clip_negative=self.r_diag, precision=self.tc_precision)
-            self._ac[sub] = out.cpu().numpy().astype(self.precision, copy=False)
-            self._fr[sub] = 1
+            if self.precision == 'float32':
+                out = out.float()
+            done = torch.cuda.Event()
+            done.record(compute)
+            copy.wait_event(done)
+            with torch.cuda.stream(copy):
+                if contiguous and pinned:
+                    ac_t[int(sub[0]):int(sub[-1]) + 1].copy_(out, non_blocking=True)
+                    pending.append((None, out))
+                else:
+                    host = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+                    host.copy_(out, non_blocking=True)
+                    pending.append((sub, host))
+            out.record_stream(copy)
+        copy.synchronize()
+        for sub, host in pending:
+            if sub is not None:
+                self._ac[sub] = host.numpy()
+        self._fr[ind] = 1
 
     # --- band synthesis and integration (acoular/fbeamform.py:512-685) -----------------------
     def synthetic(self, f, num=0):

@@ -75,6 +75,11 @@ class RectGrid(Grid):
         return (self.x_min, self.x_max, self.y_min, self.y_max)
 
     @property
+    def digest(self) -> str:
+        """Identifier from the defining parameters (positions follow from them)."""
+        return f'_rect|{self.x_min!r}|{self.x_max!r}|{self.y_min!r}|{self.y_max!r}|{self.z!r}|{self.increment!r}'
+
+    @property
     def pos(self) -> np.ndarray:
         key = (self.x_min, self.x_max, self.y_min, self.y_max, self.z, self.increment)
         if self._pos is None or self._pos[0] != key:
@@ -131,6 +136,11 @@ class RectGrid3D(RectGrid):
         super().__init__(x_min, x_max, y_min, y_max, 0.0, 0.1)
         self.z_min, self.z_max = float(z_min), float(z_max)
         self.increment = increment
+
+    @property
+    def digest(self) -> str:
+        return (f'_rect3d|{self.x_min!r}|{self.x_max!r}|{self.y_min!r}|{self.y_max!r}|{self.z_min!r}|{self.z_max!r}|'
+                f'{self.increment!r}')
 
     def _inc(self, axis):
         return abs(self.increment) if np.isscalar(self.increment) else abs(self.increment[axis])
