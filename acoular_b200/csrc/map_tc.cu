@@ -37,7 +37,8 @@ namespace acb {
 constexpr int TC_ROWS = 128;
 constexpr int TC_CHUNK = 32;               // real components per chunk
 constexpr int TC_MPC = TC_CHUNK / 2;       // mics per chunk
-constexpr int TC_MAX_CHUNKS = 16;          // 2M <= 512 TMEM columns in one pass
+constexpr int TC_PASS_CHUNKS = 16;         // accumulator chunks per column pass (512 TMEM columns)
+constexpr int TC_MAX_MICS = 2048;          // mic positions live in shared memory
 constexpr int TC_TILE_ELEMS = TC_CHUNK * TC_CHUNK;
 constexpr int TC_TILE_BYTES = TC_TILE_ELEMS * 2;          // bf16
 constexpr int TC_A_BYTES = TC_ROWS * TC_CHUNK * 2;        // 8 KB per (stage, hi|lo)
@@ -226,12 +227,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     tc::tc_fence_after();
     const uint32_t taddr = *tmem_slot;
 
+    // Step sequence of one item: column passes p = 0 .. P-1, each covering accumulator chunks
+    // [16p, je) with je = min(C, 16p + 16); in pass p the K chunks i = 0 .. je-1 run, chunk i feeding
+    // the columns of chunks j in [max(i, 16p), je).  Chunk i's columns are final after step (p, i)
+    // when i >= 16p; those steps also carry chunk i's dot product and normalisation sum.
+    const int P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+
     if (warp == 0) {
-        // ---------------- producer: R' tiles of every chunk into the tile ring ----------------
-        // Chunk T takes C - t consecutive ring tiles starting at the running tile counter U; tile U
-        // reuses slot U % TC_RING, free once the chunk that held tile U - TC_RING is complete.
+        // ---------------- producer: R' tiles of every step into the tile ring ----------------
+        // Step T takes n consecutive ring tiles starting at the running tile counter U; tile U
+        // reuses slot U % TC_RING, free once the step that held tile U - TC_RING is complete.
         if (lane == 0) {
-            uint32_t ustart[TC_NB];   // first ring tile of the last TC_NB chunks
+            uint32_t ustart[TC_NB];   // first ring tile of the last TC_NB steps
             uint32_t U = 0;
             int T = 0, freed = -1, lastT = -1;
             bool ok = true;
@@ -239,32 +246,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                 const int64_t item = blockIdx.x + li * gridDim.x;
                 const __nv_bfloat16 *bh = rh + (item / a.ntiles) * a.bin_stride_elems;
                 const __nv_bfloat16 *bl = rl + (item / a.ntiles) * a.bin_stride_elems;
-                for (int t = 0; t < C && ok; ++t, ++T) {
-                    const int n = C - t;
-                    // chunk barriers form a ring of TC_NB: chunk T - TC_NB must be complete; ring
-                    // slots: every chunk holding a tile <= U + n - 1 - TC_RING must be complete
-                    while (ok && (freed < T - TC_NB ||
-                                  (freed + 1 < T && (int)(ustart[(freed + 1) & (TC_NB - 1)] - (U + n - 1 - TC_RING)) <= 0))) {
-                        ok = tc::mbar_wait(&done[(freed + 1) & (TC_NB - 1)], (uint32_t)(((freed + 1) / TC_NB) & 1),
-                                           abort_flag, a.wait_limit_ns);
-                        if (ok) ++freed;
+                for (int pp = 0; pp < P && ok; ++pp) {
+                    const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+                    for (int i = 0; i < je && ok; ++i, ++T) {
+                        const int j0 = max(i, jb), n = je - j0;
+                        // step barriers form a ring of TC_NB: step T - TC_NB must be complete; ring
+                        // slots: every step holding a tile <= U + n - 1 - TC_RING must be complete
+                        while (ok && (freed < T - TC_NB ||
+                                      (freed + 1 < T &&
+                                       (int)(ustart[(freed + 1) & (TC_NB - 1)] - (U + n - 1 - TC_RING)) <= 0))) {
+                            ok = tc::mbar_wait(&done[(freed + 1) & (TC_NB - 1)], (uint32_t)(((freed + 1) / TC_NB) & 1),
+                                               abort_flag, a.wait_limit_ns);
+                            if (ok) ++freed;
+                        }
+                        if (!ok) break;
+                        ustart[T & (TC_NB - 1)] = U;
+                        uint64_t *fb = &full_b[T & (TC_NB - 1)];
+                        tc::mbar_arrive_expect_tx(fb, 2u * n * TC_TILE_BYTES);
+                        const int64_t src = (int64_t)tile_index(C, i, j0) * TC_TILE_ELEMS;
+                        int j = 0;
+                        while (j < n) {   // contiguous runs of ring slots
+                            const int slot = (int)((U + j) & (TC_RING - 1));
+                            const int run = min(n - j, TC_RING - slot);
+                            const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
+                            tc::bulk_g2s(smem + TcSmem::b_off(slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                            tc::bulk_g2s(smem + TcSmem::b_off(slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                            j += run;
+                        }
+                        U += (uint32_t)n;
+                        lastT = T;
                     }
-                    if (!ok) break;
-                    ustart[T & (TC_NB - 1)] = U;
-                    uint64_t *fb = &full_b[T & (TC_NB - 1)];
-                    tc::mbar_arrive_expect_tx(fb, 2u * n * TC_TILE_BYTES);
-                    const int64_t src = (int64_t)tile_index(C, t, t) * TC_TILE_ELEMS;
-                    int j = 0;
-                    while (j < n) {   // contiguous runs of ring slots
-                        const int slot = (int)((U + j) & (TC_RING - 1));
-                        const int run = min(n - j, TC_RING - slot);
-                        const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
-                        tc::bulk_g2s(smem + TcSmem::b_off(slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
-                        tc::bulk_g2s(smem + TcSmem::b_off(slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
-                        j += run;
-                    }
-                    U += (uint32_t)n;
-                    lastT = T;
                 }
             }
             // on an abort, let the last copies land before the CTA releases its shared memory
@@ -274,7 +285,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
-        // Kept lean: it sits on every chunk's critical path.  Descriptors are built once and
+        // Kept lean: it sits on every step's critical path.  Descriptors are built once and
         // advanced by adding byte offsets >> 4 to their 14-bit start-address field; ring and
         // stage indices are 32-bit counters advanced incrementally.
         if (lane == 0) {
@@ -285,98 +296,112 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             constexpr uint32_t LO_B = (TC_RING * TC_TILE_BYTES) >> 4;
             const uint32_t idesc0 = tc::idesc_m128(1, 0);
             int sa = 0, ua = 0;     // A stage and its phase parity
-            int sb = 0, ub = 0;     // chunk barrier slot and parity
-            uint32_t slot0 = 0;     // ring slot of the chunk's first tile
+            int sb = 0, ub = 0;     // step barrier slot and parity
+            uint32_t slot0 = 0;     // ring slot of the step's first tile
             int lastb = -1, lastu = 0;
+            int npass = 0;          // passes started (tmem_free phases to wait for)
             bool ok = true;
             for (int64_t li = 0; li < nmine && ok; ++li) {
-                // the previous item's epilogue must have read every accumulator column
-                if (li > 0) ok = tc::mbar_wait(tmem_free, (uint32_t)((li - 1) & 1), abort_flag, a.wait_limit_ns);
-                for (int t = 0; t < C && ok; ++t) {
-                    ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, a.wait_limit_ns) &&
-                         tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, a.wait_limit_ns);
-                    if (!ok) break;
-                    tc::tc_fence_after();
-                    const int n = C - t;
-                    const uint32_t dcol = taddr + (uint32_t)(TC_CHUNK * t);
-                    // split the chunk's n tiles into runs of <= 8 (N <= 256) that do not wrap
-                    int run0 = min(min(n, 8), (int)(TC_RING - slot0));
-                    const uint32_t slot1 = (slot0 + run0) & (TC_RING - 1);
-                    const int rest = n - run0;
-                    int run1 = min(min(rest, 8), (int)(TC_RING - slot1));
-                    const uint32_t slot2 = (slot1 + run1) & (TC_RING - 1);
-                    const int run2 = rest - run1;   // at most one more run (n <= 16)
+                for (int pp = 0; pp < P && ok; ++pp) {
+                    const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+                    // the previous pass's epilogue must have read every accumulator column
+                    if (npass > 0)
+                        ok = tc::mbar_wait(tmem_free, (uint32_t)((npass - 1) & 1), abort_flag, a.wait_limit_ns);
+                    ++npass;
+                    for (int i = 0; i < je && ok; ++i) {
+                        ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, a.wait_limit_ns) &&
+                             tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, a.wait_limit_ns);
+                        if (!ok) break;
+                        tc::tc_fence_after();
+                        const int j0 = max(i, jb), n = je - j0;
+                        const uint32_t dcol = taddr + (uint32_t)(TC_CHUNK * (j0 - jb));
+                        // split the step's n tiles into runs of <= 8 (N <= 256) that do not wrap
+                        const int run0 = min(min(n, 8), (int)(TC_RING - slot0));
+                        const uint32_t slot1 = (slot0 + run0) & (TC_RING - 1);
+                        const int rest = n - run0;
+                        const int run1 = min(min(rest, 8), (int)(TC_RING - slot1));
+                        const uint32_t slot2 = (slot1 + run1) & (TC_RING - 1);
+                        const int run2 = rest - run1;   // at most one more run (n <= 16)
 #pragma unroll
-                    for (int ks = 0; ks < 2; ++ks) {
+                        for (int ks = 0; ks < 2; ++ks) {
 #pragma unroll
-                        for (int prod = 0; prod < 3; ++prod) {
-                            const uint64_t ad = a_base + (uint64_t)((sa * 2 + (prod == 2)) * A_STEP + ks * 16);
-                            const uint64_t bd = b_base + (uint64_t)((prod == 1 ? LO_B : 0u) + ks * 16);
-                            const uint32_t accum = (t == 0 && ks == 0 && prod == 0) ? 0u : 1u;
-                            tc::mma_bf16(dcol, ad, bd + slot0 * T_STEP, idesc0 | ((uint32_t)(run0 * 4) << 17), accum);
-                            if (run1 > 0)
-                                tc::mma_bf16(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP,
-                                             idesc0 | ((uint32_t)(run1 * 4) << 17), accum);
-                            if (run2 > 0)
-                                tc::mma_bf16(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
-                                             idesc0 | ((uint32_t)(run2 * 4) << 17), accum);
+                            for (int prod = 0; prod < 3; ++prod) {
+                                const uint64_t ad = a_base + (uint64_t)((sa * 2 + (prod == 2)) * A_STEP + ks * 16);
+                                const uint64_t bd = b_base + (uint64_t)((prod == 1 ? LO_B : 0u) + ks * 16);
+                                const uint32_t accum = (i == 0 && ks == 0 && prod == 0) ? 0u : 1u;
+                                tc::mma_bf16(dcol, ad, bd + slot0 * T_STEP, idesc0 | ((uint32_t)(run0 * 4) << 17), accum);
+                                if (run1 > 0)
+                                    tc::mma_bf16(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP,
+                                                 idesc0 | ((uint32_t)(run1 * 4) << 17), accum);
+                                if (run2 > 0)
+                                    tc::mma_bf16(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
+                                                 idesc0 | ((uint32_t)(run2 * 4) << 17), accum);
+                            }
                         }
+                        tc::mma_commit(&done[sb]);
+                        lastb = sb;
+                        lastu = ub;
+                        slot0 = (slot0 + (uint32_t)n) & (TC_RING - 1);
+                        if (++sa == TC_ASTAGES) { sa = 0; ua ^= 1; }
+                        if (++sb == TC_NB) { sb = 0; ub ^= 1; }
                     }
-                    tc::mma_commit(&done[sb]);
-                    lastb = sb;
-                    lastu = ub;
-                    slot0 = (slot0 + (uint32_t)n) & (TC_RING - 1);
-                    if (++sa == TC_ASTAGES) { sa = 0; ua ^= 1; }
-                    if (++sb == TC_NB) { sb = 0; ub ^= 1; }
                 }
             }
             if (lastb >= 0) tc::mbar_wait(&done[lastb], (uint32_t)lastu, abort_flag, 4 * a.wait_limit_ns);
         }
     } else if (warp < TC_SYNTH_WARP0) {
         // ---------------- epilogue (warps 2..5): one thread per grid point ----------------
-        // After the MMAs of chunk t the accumulator columns of chunk t are final; dot them with the
-        // steering chunk as the MMA saw it (hi + lo from A stage T % 3), then release the stage.
+        // After step (p, i) with i >= 16p the accumulator columns of chunk i are final; dot them
+        // with the steering chunk as the MMA saw it (hi + lo from the A stage).  Every step then
+        // releases its A stage.
         const int q = warp & 3;
         const int row = q * 32 + lane;
         const uint32_t lane_addr = taddr + ((uint32_t)(q * 32) << 16);
         const int a_row = ((row >> 3) << 9) + ((row & 7) << 4);   // byte offset of the row's first chunk
-        int T = 0;
+        int T = 0, sa = 0;
         bool ok = true;
         for (int64_t li = 0; li < nmine && ok; ++li) {
             const int64_t item = blockIdx.x + li * gridDim.x;
             const int bin = (int)(item / a.ntiles);
             const int64_t g = (item % a.ntiles) * TC_ROWS + row;
             double acc = 0.0;
-            for (int t = 0; t < C; ++t, ++T) {
-                ok = __all_sync(0xffffffffu, tc::mbar_wait(&done[T & (TC_NB - 1)], (uint32_t)((T / TC_NB) & 1),
-                                                           abort_flag, a.wait_limit_ns));
-                if (!ok) break;
-                tc::tc_fence_after();
-                float d[TC_CHUNK];
-                tc::tmem_ld_x32(lane_addr + (uint32_t)(TC_CHUNK * t), d);
-                const int sa = (int)(T % TC_ASTAGES);
-                const uint8_t *ahi = smem + TcSmem::a_off(sa, 0) + a_row;
-                const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;
-                float part = 0.f;
+            for (int pp = 0; pp < P && ok; ++pp) {
+                const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+                for (int i = 0; i < je; ++i, ++T) {
+                    ok = __all_sync(0xffffffffu, tc::mbar_wait(&done[T & (TC_NB - 1)], (uint32_t)((T / TC_NB) & 1),
+                                                               abort_flag, a.wait_limit_ns));
+                    if (!ok) break;
+                    if (i >= jb) {
+                        tc::tc_fence_after();
+                        float d[TC_CHUNK];
+                        tc::tmem_ld_x32(lane_addr + (uint32_t)(TC_CHUNK * (i - jb)), d);
+                        const uint8_t *ahi = smem + TcSmem::a_off(sa, 0) + a_row;
+                        const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;
+                        float part = 0.f;
 #pragma unroll
-                for (int grp = 0; grp < 4; ++grp) {
-                    const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
-                    const uint4 lw = *reinterpret_cast<const uint4 *>(alo + grp * 128);
-                    const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w}, lv[4] = {lw.x, lw.y, lw.z, lw.w};
+                        for (int grp = 0; grp < 4; ++grp) {
+                            const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
+                            const uint4 lw = *reinterpret_cast<const uint4 *>(alo + grp * 128);
+                            const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w}, lv[4] = {lw.x, lw.y, lw.z, lw.w};
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float vr = __uint_as_float(hv[e] << 16) + __uint_as_float(lv[e] << 16);
-                        const float vi = __uint_as_float(hv[e] & 0xFFFF0000u) + __uint_as_float(lv[e] & 0xFFFF0000u);
-                        part = fmaf(d[grp * 8 + 2 * e], vr, part);
-                        part = fmaf(d[grp * 8 + 2 * e + 1], vi, part);
+                            for (int e = 0; e < 4; ++e) {
+                                const float vr = __uint_as_float(hv[e] << 16) + __uint_as_float(lv[e] << 16);
+                                const float vi =
+                                    __uint_as_float(hv[e] & 0xFFFF0000u) + __uint_as_float(lv[e] & 0xFFFF0000u);
+                                part = fmaf(d[grp * 8 + 2 * e], vr, part);
+                                part = fmaf(d[grp * 8 + 2 * e + 1], vi, part);
+                            }
+                        }
+                        acc += (double)part;
+                        tc::tc_fence_before();
                     }
+                    tc::mbar_arrive(&afree[sa]);
+                    if (++sa == TC_ASTAGES) sa = 0;
                 }
-                acc += (double)part;
-                tc::tc_fence_before();
-                tc::mbar_arrive(&afree[sa]);
+                if (!ok) break;
+                tc::mbar_arrive(tmem_free);
             }
             if (!ok) break;
-            tc::mbar_arrive(tmem_free);
             // normalisation sums of this item from the synthesis warps
             ok = __all_sync(0xffffffffu, tc::mbar_wait(&s_ready[li & 1], (uint32_t)((li >> 1) & 1), abort_flag,
                                                        a.wait_limit_ns));
@@ -397,7 +422,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         const int p = (warp - TC_SYNTH_WARP0) >> 2;
         const int row = q * 32 + lane;
         const int a_off_row = (((row >> 3) * 4 + p) << 7) + ((row & 7) << 4);
-        int T = 0;
+        int T = 0, sa = 0, ua = 0;
         bool ok = true;
         for (int64_t li = 0; li < nmine && ok; ++li) {
             const int64_t item = blockIdx.x + li * gridDim.x;
@@ -413,59 +438,64 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             const double k = wavenumber[bin];
             const float khi = (float)k, klo = (float)(k - (double)khi);
             double S = 0.0;
-            for (int t = 0; t < C; ++t, ++T) {
-                const int s = (int)(T % TC_ASTAGES);
-                if (T >= TC_ASTAGES) {
-                    // A stage T % 3 is free once the epilogue of chunk T - 3 has read it
-                    ok = __all_sync(0xffffffffu, tc::mbar_wait(&afree[s], (uint32_t)(((T - 3) / 3) & 1), abort_flag,
-                                                               a.wait_limit_ns));
-                    if (!ok) break;
-                }
-                float s_part = 0.f;
-                uint32_t hw[4], lw[4];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int m = t * TC_MPC + p * 4 + e;
-                    const bool valid = gvalid && m < a.M;
-                    const float4 mv = mp4[m];
-                    const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
-                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                    const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
-                    float r = r2 * y;
-                    r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
-                    // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
-                    const float ph = khi * r;
-                    const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
-                    const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
-                    float x = fmaf(-nq, TC_P2A, ph);
-                    x = fmaf(-nq, TC_P2B, x);
-                    x = fmaf(-nq, TC_P2C, x);
-                    x += pl;
-                    float sn, cs;
-                    tc::sincos_approx(x, sn, cs);
-                    float w = 1.f;
-                    if (ST == 2) {
-                        w = r;
-                        s_part += valid ? r2 : 0.f;
-                    } else if (ST >= 3) {
-                        w = y;
-                        s_part += valid ? y * y : 0.f;
+            for (int pp = 0; pp < P && ok; ++pp) {
+                const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+                for (int t = 0; t < je; ++t, ++T) {
+                    if (T >= TC_ASTAGES) {
+                        // the A stage is free once the epilogue of step T - 3 has released it
+                        ok = __all_sync(0xffffffffu, tc::mbar_wait(&afree[sa], (uint32_t)(ua ^ 1), abort_flag,
+                                                                   a.wait_limit_ns));
+                        if (!ok) break;
                     }
-                    const float vr = valid ? cs * w : 0.f;
-                    const float vi = valid ? -sn * w : 0.f;
-                    // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
-                    // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
-                    const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
-                    hw[e] = __byte_perm(rr, ri, 0x7632);
-                    const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
-                    const float li_ = vi - __uint_as_float(ri & 0xFFFF0000u);
-                    lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li_) + 0x8000u, 0x7632);
+                    float s_part = 0.f;
+                    uint32_t hw[4], lw[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int m = t * TC_MPC + p * 4 + e;
+                        const bool valid = gvalid && m < a.M;
+                        const float4 mv = mp4[m];
+                        const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
+                        float r = r2 * y;
+                        r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
+                        // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
+                        const float ph = khi * r;
+                        const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
+                        const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
+                        float x = fmaf(-nq, TC_P2A, ph);
+                        x = fmaf(-nq, TC_P2B, x);
+                        x = fmaf(-nq, TC_P2C, x);
+                        x += pl;
+                        float sn, cs;
+                        tc::sincos_approx(x, sn, cs);
+                        float w = 1.f;
+                        if (ST == 2) {
+                            w = r;
+                            s_part += valid ? r2 : 0.f;
+                        } else if (ST >= 3) {
+                            w = y;
+                            s_part += valid ? y * y : 0.f;
+                        }
+                        const float vr = valid ? cs * w : 0.f;
+                        const float vi = valid ? -sn * w : 0.f;
+                        // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
+                        // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
+                        const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
+                        hw[e] = __byte_perm(rr, ri, 0x7632);
+                        const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
+                        const float li_ = vi - __uint_as_float(ri & 0xFFFF0000u);
+                        lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li_) + 0x8000u, 0x7632);
+                    }
+                    *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 0) + a_off_row) =
+                        make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
+                        make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    if (t >= jb) S += (double)s_part;   // each mic's term once, in its own pass
+                    tc::fence_proxy_async_smem();
+                    tc::mbar_arrive(&full_a[sa]);
+                    if (++sa == TC_ASTAGES) { sa = 0; ua ^= 1; }
                 }
-                *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 0) + a_off_row) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(s, 1) + a_off_row) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
-                S += (double)s_part;
-                tc::fence_proxy_async_smem();
-                tc::mbar_arrive(&full_a[s]);
             }
             if (!ok) break;
             red[((li & 1) * TC_PARTS + p) * TC_ROWS + row] = S;
@@ -507,7 +537,7 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
     const int M = p->num_mics;
     const int Mp = (M + TC_MPC - 1) / TC_MPC * TC_MPC;
     const int C = Mp / TC_MPC;
-    if (C > TC_MAX_CHUNKS) return ACB_ERR_UNSUPPORTED;
+    if (M > TC_MAX_MICS) return ACB_ERR_UNSUPPORTED;
     const size_t need = acb_map_tc_workspace_bytes(M, p->num_bins, precision);
     if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
     if ((p->num_grid + TC_ROWS - 1) / TC_ROWS > 0x7fffffffLL) return ACB_ERR_SHAPE;

@@ -131,7 +131,8 @@ size_t acb_map_tc_workspace_bytes(int num_mics, int num_bins, int precision);
  * tensor cores with split-BF16 operands (hi*hi + hi*lo + lo*hi) and FP32 accumulation in TMEM.
  * Steering vectors are synthesised per 128-grid-point tile in shared memory (float32 phase k*r as
  * the reference rounds it, FP64 range reduction); distances, the normalisation sums and the final
- * normalisation are FP64.  num_mics <= 256 in this build.  glibc_faithful is ignored.
+ * normalisation are FP64.  num_mics <= 2048; above 256 mics the accumulator is computed in column
+ * passes of 512 (steering chunks before a pass are synthesised again).  glibc_faithful is ignored.
  * workspace: >= acb_map_tc_workspace_bytes(num_mics, num_bins, precision) bytes.
  * error_word: int32 on the device or NULL; bit 0 is set if a bounded device-side wait gave up. */
 int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const double *wavenumber,

@@ -49,7 +49,8 @@ def _tc(csm, freqs, mpos, gpos, steer, r_diag, ref=None):
     return out.cpu().numpy()
 
 
-@pytest.mark.parametrize('M,G', [(2, 1), (16, 128), (37, 300), (64, 257), (128, 129), (256, 200)])
+@pytest.mark.parametrize('M,G', [(2, 1), (16, 128), (37, 300), (64, 257), (128, 129), (256, 200), (300, 150),
+                                 (513, 140)])
 @pytest.mark.parametrize('steer', STEERS)
 def test_tc_vs_oracle(M, G, steer):
     mpos, gpos, freqs, csm = _case(M, G, seed=M + G)
@@ -84,9 +85,9 @@ def test_tc_reference_position_and_workspace_errors():
     ref = O.beamformer_calc(csm, freqs, range(3), r0, rm, 343.0, 'true level', True)
     got = _tc(csm, freqs, mpos, gpos, 'true level', True, ref=ref_pt)
     assert rel(got, ref) <= TOL
-    p = D.map_params(300, 10, 1, 'classic', True, 1.0)
+    p = D.map_params(3000, 10, 1, 'classic', True, 1.0)
     import ctypes
-    assert N.lib().acb_map_tc(ctypes.byref(p), 0, 1, 1, 1, 1, 1, None, 1, 1 << 30, None, None) == 4  # > 256 mics
+    assert N.lib().acb_map_tc(ctypes.byref(p), 0, 1, 1, 1, 1, 1, None, 1, 1 << 40, None, None) == 4  # > 2048 mics
     p = D.map_params(64, 10, 1, 'classic', True, 1.0)
     assert N.lib().acb_map_tc(ctypes.byref(p), 0, 1, 1, 1, 1, 1, None, 1, 10, None, None) == 5  # workspace
 
@@ -103,7 +104,7 @@ def test_tc_error_word_stays_clear():
     assert int(err.item()) == 0
 
 
-@pytest.mark.parametrize('M,G,nb', [(64, 20000, 4), (256, 12000, 3), (40, 50000, 2)])
+@pytest.mark.parametrize('M,G,nb', [(64, 20000, 4), (256, 12000, 3), (40, 50000, 2), (700, 2000, 2)])
 def test_tc_persistent_many_items_per_cta(M, G, nb):
     """More work items (bin x 128-point tile) than CTAs: the pipeline runs across item boundaries."""
     mpos, gpos, freqs, csm = _case(M, G, seed=M * 3 + nb, nb=nb)
