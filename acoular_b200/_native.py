@@ -51,6 +51,17 @@ class MapParams(ctypes.Structure):
     ]
 
 
+class MapIO(ctypes.Structure):
+    _fields_ = [
+        ('csm', ctypes.c_void_p),
+        ('wavenumber', ctypes.c_void_p),
+        ('mpos', ctypes.c_void_p),
+        ('gpos', ctypes.c_void_p),
+        ('out_map', ctypes.c_void_p),
+        ('out_steer_norm', ctypes.c_void_p),
+    ]
+
+
 _lib = None
 
 _VP = ctypes.c_void_p
@@ -75,6 +86,8 @@ SIGNATURES = {
     'acb_map_tc_workspace_bytes': (_SZ, [_I, _I, _I]),
     'acb_map_tc': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _SZ, _VP, _VP]),
     'acb_map_tc_noalloc': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    'acb_map_tc_batch_workspace_bytes': (_SZ, [ctypes.POINTER(MapParams), _I, _I]),
+    'acb_map_tc_batch': (_I, [ctypes.POINTER(MapParams), ctypes.POINTER(MapIO), _I, _I, _VP, _SZ, _VP, _VP]),
 }
 
 

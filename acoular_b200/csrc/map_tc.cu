@@ -58,19 +58,45 @@ __device__ constexpr float TC_P2B = 0x1.fb5444p-10f;
 __device__ constexpr float TC_P2C = 0x1.68c234p-37f;
 __device__ constexpr float TC_INV2PI = 0.15915493667125702f;
 
-struct TcArgs {
-    int M, Mp, C;
+// One beamforming instance of a batch: its geometry, CSM operand and outputs.  The batch's
+// instances travel in the kernel parameters (grid constant), so a launch needs no device-side
+// descriptor upload and can be captured in a CUDA graph as it is.
+struct TcInst {
+    int64_t item_off;          // first global work item of this instance
+    int64_t ntiles;            // 128-point grid tiles
     int64_t G;
-    int steer_type;
-    int clip;
-    double norm;
-    int ref_mode;
-    double ref0, ref1, ref2, ref_dist;
-    uint64_t wait_limit_ns;
-    int64_t bin_stride_elems;  // R' elements per bin (hi and lo separately)
-    int64_t ntiles;            // 128-point grid tiles per bin
-    int64_t nitems;            // work items = bins x tiles (bin-major: CTAs in flight share a bin)
+    int M, Mp, C, nbins;
+    int clip, ref_mode;
+    double norm, ref0, ref1, ref2, ref_dist;
+    const double *k;           // [nbins] wave numbers
+    const double *mpos;        // [3][M]
+    const double *gpos;        // [3][G]
+    double *out;               // [nbins][G]
+    double *out_norm;          // [nbins][G] or null
+    const __nv_bfloat16 *rh, *rl;   // split-BF16 R' tiles, bin_stride elements per bin
+    int64_t bin_stride;
 };
+
+constexpr int TC_MAX_INST = 64;
+
+struct TcBatch {
+    int n_inst;
+    int mp_max;                // largest padded mic count (shared-memory mic table size)
+    int64_t nitems;
+    uint64_t wait_limit_ns;
+    TcInst inst[TC_MAX_INST];
+};
+
+__device__ __forceinline__ int find_inst(const TcBatch &b, int64_t item)
+{
+    int lo = 0, hi = b.n_inst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (b.inst[mid].item_off <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 constexpr int TC_NB = 8;       // chunk barrier ring (full_b / done); the producer runs <= 7 chunks ahead
 
@@ -140,7 +166,7 @@ struct TcSmem {
 
 // Normalisation of the steering type (acoular/fastFuncs.py:293-310) and clipping.
 template <int ST>
-__device__ __forceinline__ void finish_point(const TcArgs &a, double scalar, double S, double gx, double gy, double gz,
+__device__ __forceinline__ void finish_point(const TcInst &a, double scalar, double S, double gx, double gy, double gz,
                                              int bin, int64_t g, double *out_map, double *out_norm)
 {
     double r0;
@@ -170,42 +196,33 @@ __device__ __forceinline__ void finish_point(const TcArgs &a, double scalar, dou
     if (out_norm) out_norm[(int64_t)bin * a.G + g] = ns;
 }
 
-// Persistent kernel: one CTA per SM walks the work items (bin, tile) blockIdx.x, +gridDim.x, ...;
-// the chunk pipeline runs on across item boundaries.  Global chunk counter T = local item * C + t.
+// Persistent kernel: one CTA per SM walks the batch's work items (instance, bin, 128-point tile)
+// blockIdx.x, +gridDim.x, ...; the step pipeline runs on across item and instance boundaries.
 template <int ST>
-__global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const double *__restrict__ wavenumber,
-                                                               const double *__restrict__ mpos,
-                                                               const double *__restrict__ gpos,
-                                                               const __nv_bfloat16 *__restrict__ rh,
-                                                               const __nv_bfloat16 *__restrict__ rl,
-                                                               double *__restrict__ out_map,
-                                                               double *__restrict__ out_norm, int *err)
+__global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_constant__ TcBatch b, int *err)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // operand tiles start on a 1 KB boundary (the launch reserves 1 KB of slack for this)
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
-    const int C = a.C, Mp = a.Mp;
-    float4 *mp4 = reinterpret_cast<float4 *>(smem + TcSmem::mic_off(C));        // [Mp] (x, y, z, 0)
-    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(C, Mp));     // [2][parts][128] sums S
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(C, Mp));
-    uint64_t *full_a = bars;                          // [3]  chunk T written to A stage T % 3
-    uint64_t *afree = bars + TC_ASTAGES;              // [3]  epilogue of chunk T has read A stage T % 3
-    uint64_t *full_b = bars + 2 * TC_ASTAGES;         // [8]  R' tiles of chunk T landed
-    uint64_t *done = full_b + TC_NB;                  // [8]  MMAs of chunk T complete
-    uint64_t *tmem_free = done + TC_NB;               // [1]  epilogue has read all columns of an item
+    const int MPX = b.mp_max;
+    float4 *mp4 = reinterpret_cast<float4 *>(smem + TcSmem::mic_off(0));          // [MPX] (x, y, z, 0)
+    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(0, MPX));     // [2][parts][128] sums S
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(0, MPX));
+    uint64_t *full_a = bars;                          // [3]  step T written to A stage T % 3
+    uint64_t *afree = bars + TC_ASTAGES;              // [3]  epilogue of step T has released A stage T % 3
+    uint64_t *full_b = bars + 2 * TC_ASTAGES;         // [8]  R' tiles of step T landed
+    uint64_t *done = full_b + TC_NB;                  // [8]  MMAs of step T complete
+    uint64_t *tmem_free = done + TC_NB;               // [1]  epilogue has read all columns of a pass
     uint64_t *s_ready = tmem_free + 1;                // [2]  synthesis sums S of item parity written
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(s_ready + 2 + 2);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(s_ready + 2 + 3);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t ncols = (uint32_t)(C <= 1 ? 32 : (C <= 2 ? 64 : (C <= 4 ? 128 : (C <= 8 ? 256 : 512))));
-    const int64_t nmine = a.nitems > blockIdx.x ? (a.nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t nmine = b.nitems > blockIdx.x ? (b.nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    int cmax = 1;
+    for (int i = 0; i < b.n_inst; ++i) cmax = max(cmax, b.inst[i].C);
+    const uint32_t ncols = (uint32_t)(cmax <= 1 ? 32 : (cmax <= 2 ? 64 : (cmax <= 4 ? 128 : (cmax <= 8 ? 256 : 512))));
 
-    for (int m = threadIdx.x; m < Mp; m += blockDim.x) {
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (m < a.M) v = make_float4((float)mpos[m], (float)mpos[a.M + m], (float)mpos[2 * a.M + m], 0.f);
-        mp4[m] = v;
-    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_ASTAGES; ++s) {
             tc::mbar_init(&full_a[s], TC_SYNTH_THREADS);
@@ -231,8 +248,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     // [16p, je) with je = min(C, 16p + 16); in pass p the K chunks i = 0 .. je-1 run, chunk i feeding
     // the columns of chunks j in [max(i, 16p), je).  Chunk i's columns are final after step (p, i)
     // when i >= 16p; those steps also carry chunk i's dot product and normalisation sum.
-    const int P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
-
     if (warp == 0) {
         // ---------------- producer: R' tiles of every step into the tile ring ----------------
         // Step T takes n consecutive ring tiles starting at the running tile counter U; tile U
@@ -244,8 +259,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             bool ok = true;
             for (int64_t li = 0; li < nmine && ok; ++li) {
                 const int64_t item = blockIdx.x + li * gridDim.x;
-                const __nv_bfloat16 *bh = rh + (item / a.ntiles) * a.bin_stride_elems;
-                const __nv_bfloat16 *bl = rl + (item / a.ntiles) * a.bin_stride_elems;
+                const TcInst &in = b.inst[find_inst(b, item)];
+                const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+                const int64_t bin = (item - in.item_off) / in.ntiles;
+                const __nv_bfloat16 *bh = in.rh + bin * in.bin_stride;
+                const __nv_bfloat16 *bl = in.rl + bin * in.bin_stride;
                 for (int pp = 0; pp < P && ok; ++pp) {
                     const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
                     for (int i = 0; i < je && ok; ++i, ++T) {
@@ -256,7 +274,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                                       (freed + 1 < T &&
                                        (int)(ustart[(freed + 1) & (TC_NB - 1)] - (U + n - 1 - TC_RING)) <= 0))) {
                             ok = tc::mbar_wait(&done[(freed + 1) & (TC_NB - 1)], (uint32_t)(((freed + 1) / TC_NB) & 1),
-                                               abort_flag, a.wait_limit_ns);
+                                               abort_flag, b.wait_limit_ns);
                             if (ok) ++freed;
                         }
                         if (!ok) break;
@@ -281,7 +299,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             // on an abort, let the last copies land before the CTA releases its shared memory
             if (*abort_flag && lastT >= 0)
                 tc::mbar_wait(&full_b[lastT & (TC_NB - 1)], (uint32_t)((lastT / TC_NB) & 1), abort_flag,
-                              4 * a.wait_limit_ns);
+                              4 * b.wait_limit_ns);
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
@@ -302,15 +320,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             int npass = 0;          // passes started (tmem_free phases to wait for)
             bool ok = true;
             for (int64_t li = 0; li < nmine && ok; ++li) {
+                const int64_t item = blockIdx.x + li * gridDim.x;
+                const int C = b.inst[find_inst(b, item)].C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
                 for (int pp = 0; pp < P && ok; ++pp) {
                     const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
                     // the previous pass's epilogue must have read every accumulator column
                     if (npass > 0)
-                        ok = tc::mbar_wait(tmem_free, (uint32_t)((npass - 1) & 1), abort_flag, a.wait_limit_ns);
+                        ok = tc::mbar_wait(tmem_free, (uint32_t)((npass - 1) & 1), abort_flag, b.wait_limit_ns);
                     ++npass;
                     for (int i = 0; i < je && ok; ++i) {
-                        ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, a.wait_limit_ns) &&
-                             tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, a.wait_limit_ns);
+                        ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, b.wait_limit_ns) &&
+                             tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, b.wait_limit_ns);
                         if (!ok) break;
                         tc::tc_fence_after();
                         const int j0 = max(i, jb), n = je - j0;
@@ -347,7 +367,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                     }
                 }
             }
-            if (lastb >= 0) tc::mbar_wait(&done[lastb], (uint32_t)lastu, abort_flag, 4 * a.wait_limit_ns);
+            if (lastb >= 0) tc::mbar_wait(&done[lastb], (uint32_t)lastu, abort_flag, 4 * b.wait_limit_ns);
         }
     } else if (warp < TC_SYNTH_WARP0) {
         // ---------------- epilogue (warps 2..5): one thread per grid point ----------------
@@ -362,14 +382,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         bool ok = true;
         for (int64_t li = 0; li < nmine && ok; ++li) {
             const int64_t item = blockIdx.x + li * gridDim.x;
-            const int bin = (int)(item / a.ntiles);
-            const int64_t g = (item % a.ntiles) * TC_ROWS + row;
+            const TcInst &in = b.inst[find_inst(b, item)];
+            const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+            const int bin = (int)((item - in.item_off) / in.ntiles);
+            const int64_t g = ((item - in.item_off) % in.ntiles) * TC_ROWS + row;
             double acc = 0.0;
             for (int pp = 0; pp < P && ok; ++pp) {
                 const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
                 for (int i = 0; i < je; ++i, ++T) {
                     ok = __all_sync(0xffffffffu, tc::mbar_wait(&done[T & (TC_NB - 1)], (uint32_t)((T / TC_NB) & 1),
-                                                               abort_flag, a.wait_limit_ns));
+                                                               abort_flag, b.wait_limit_ns));
                     if (!ok) break;
                     if (i >= jb) {
                         tc::tc_fence_after();
@@ -404,14 +426,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
             if (!ok) break;
             // normalisation sums of this item from the synthesis warps
             ok = __all_sync(0xffffffffu, tc::mbar_wait(&s_ready[li & 1], (uint32_t)((li >> 1) & 1), abort_flag,
-                                                       a.wait_limit_ns));
+                                                       b.wait_limit_ns));
             if (!ok) break;
-            if (g < a.G) {
+            if (g < in.G) {
                 const double *rs = red + (li & 1) * TC_PARTS * TC_ROWS;
                 double S = 0.0;
 #pragma unroll
                 for (int pp = 0; pp < TC_PARTS; ++pp) S += rs[pp * TC_ROWS + row];
-                finish_point<ST>(a, acc, S, gpos[g], gpos[a.G + g], gpos[2 * a.G + g], bin, g, out_map, out_norm);
+                finish_point<ST>(in, acc, S, in.gpos[g], in.gpos[in.G + g], in.gpos[2 * in.G + g], bin, g, in.out,
+                                 in.out_norm);
             }
         }
     } else {
@@ -422,20 +445,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
         const int p = (warp - TC_SYNTH_WARP0) >> 2;
         const int row = q * 32 + lane;
         const int a_off_row = (((row >> 3) * 4 + p) << 7) + ((row & 7) << 4);
-        int T = 0, sa = 0, ua = 0;
+        const int sid = threadIdx.x - TC_SYNTH_WARP0 * 32;   // 0 .. TC_SYNTH_THREADS-1
+        int T = 0, sa = 0, ua = 0, cur_inst = -1;
         bool ok = true;
         for (int64_t li = 0; li < nmine && ok; ++li) {
             const int64_t item = blockIdx.x + li * gridDim.x;
-            const int bin = (int)(item / a.ntiles);
-            const int64_t g = (item % a.ntiles) * TC_ROWS + row;
-            const bool gvalid = g < a.G;
+            const int ii = find_inst(b, item);
+            const TcInst &in = b.inst[ii];
+            if (ii != cur_inst) {
+                // new instance: every synthesis thread is past the previous item, reload the mics
+                asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
+                for (int m = sid; m < in.Mp; m += TC_SYNTH_THREADS) {
+                    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (m < in.M)
+                        v = make_float4((float)in.mpos[m], (float)in.mpos[in.M + m], (float)in.mpos[2 * in.M + m], 0.f);
+                    mp4[m] = v;
+                }
+                asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
+                cur_inst = ii;
+            }
+            const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+            const int bin = (int)((item - in.item_off) / in.ntiles);
+            const int64_t g = ((item - in.item_off) % in.ntiles) * TC_ROWS + row;
+            const bool gvalid = g < in.G;
             float gxf = 0.f, gyf = 0.f, gzf = 0.f;
             if (gvalid) {
-                gxf = (float)gpos[g];
-                gyf = (float)gpos[a.G + g];
-                gzf = (float)gpos[2 * a.G + g];
+                gxf = (float)in.gpos[g];
+                gyf = (float)in.gpos[in.G + g];
+                gzf = (float)in.gpos[2 * in.G + g];
             }
-            const double k = wavenumber[bin];
+            const double k = in.k[bin];
             const float khi = (float)k, klo = (float)(k - (double)khi);
             double S = 0.0;
             for (int pp = 0; pp < P && ok; ++pp) {
@@ -444,7 +483,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
                     if (T >= TC_ASTAGES) {
                         // the A stage is free once the epilogue of step T - 3 has released it
                         ok = __all_sync(0xffffffffu, tc::mbar_wait(&afree[sa], (uint32_t)(ua ^ 1), abort_flag,
-                                                                   a.wait_limit_ns));
+                                                                   b.wait_limit_ns));
                         if (!ok) break;
                     }
                     float s_part = 0.f;
@@ -452,7 +491,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
                         const int m = t * TC_MPC + p * 4 + e;
-                        const bool valid = gvalid && m < a.M;
+                        const bool valid = gvalid && m < in.M;
                         const float4 mv = mp4[m];
                         const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
                         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
@@ -511,6 +550,76 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(TcArgs a, const d
     if (threadIdx.x == 0 && *abort_flag && err) atomicOr(err, 1);
 }
 
+// Host side: validate and lay out one instance; the R' region of the instance starts at `ws`.
+static int tc_fill_inst(const acb_map_params *p, const void *csm, const double *wavenumber, const double *mpos,
+                        const double *gpos, double *out_map, double *out_steer_norm, __nv_bfloat16 *ws,
+                        int64_t item_off, TcInst &in)
+{
+    if (!p || !csm || !wavenumber || !mpos || !gpos || !out_map) return ACB_ERR_ARG;
+    if (p->steer_type < 1 || p->steer_type > 4) return ACB_ERR_ARG;
+    if (p->num_mics < 2 || p->num_grid <= 0 || p->num_bins <= 0 || p->num_bins > 65535) return ACB_ERR_SHAPE;
+    if (p->num_mics > TC_MAX_MICS) return ACB_ERR_UNSUPPORTED;
+    const int M = p->num_mics;
+    in.M = M;
+    in.Mp = (M + TC_MPC - 1) / TC_MPC * TC_MPC;
+    in.C = in.Mp / TC_MPC;
+    in.G = p->num_grid;
+    in.nbins = p->num_bins;
+    in.ntiles = (p->num_grid + TC_ROWS - 1) / TC_ROWS;
+    in.item_off = item_off;
+    in.clip = p->clip_negative;
+    in.norm = p->norm;
+    in.ref_mode = p->ref_mode;
+    in.ref0 = p->ref_point[0];
+    in.ref1 = p->ref_point[1];
+    in.ref2 = p->ref_point[2];
+    in.ref_dist = p->ref_distance;
+    in.k = wavenumber;
+    in.mpos = mpos;
+    in.gpos = gpos;
+    in.out = out_map;
+    in.out_norm = out_steer_norm;
+    in.bin_stride = (int64_t)tri_tiles(in.C) * TC_TILE_ELEMS;
+    in.rh = ws;
+    in.rl = ws + (size_t)p->num_bins * in.bin_stride;
+    return ACB_OK;
+}
+
+// Launch the R' preparation of every instance and the persistent map kernel over the batch.
+static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const void *const *csms, int steer_type,
+                     int *error_word, cudaStream_t s)
+{
+    int mp_max = 16;
+    int cmax = 1;
+    for (int i = 0; i < bt.n_inst; ++i) {
+        const TcInst &in = bt.inst[i];
+        tc_prep_kernel<<<dim3(tri_tiles(in.C), in.nbins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csms[i]), in.M,
+                                                                      in.C, params[i]->r_diag, in.bin_stride,
+                                                                      const_cast<__nv_bfloat16 *>(in.rh),
+                                                                      const_cast<__nv_bfloat16 *>(in.rl));
+        const int st = check_launch();
+        if (st) return st;
+        mp_max = max(mp_max, in.Mp);
+        cmax = max(cmax, in.C);
+    }
+    bt.mp_max = mp_max;
+    bt.wait_limit_ns = 500ull * 1000 * 1000;
+    int smem = TcSmem::total(0, mp_max) + 1024;
+    // a CTA that takes all 512 TMEM columns must be alone on its SM: size the shared memory so
+    // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)
+    if (cmax > 8 && smem < 116 * 1024) smem = 116 * 1024;
+    int dev = 0, nsm = kNumSMs;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const dim3 grid((unsigned)(bt.nitems < nsm ? bt.nitems : nsm));
+    auto kern = steer_type == 1 ? map_tc_kernel<1>
+                : steer_type == 2 ? map_tc_kernel<2>
+                : steer_type == 3 ? map_tc_kernel<3>
+                                  : map_tc_kernel<4>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    kern<<<grid, TC_THREADS, smem, s>>>(bt, error_word);
+    return check_launch();
+}
+
 }  // namespace acb
 
 using namespace acb;
@@ -530,55 +639,61 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
                const double *gpos, double *out_map, double *out_steer_norm, void *workspace, size_t workspace_bytes,
                int *error_word, void *stream)
 {
-    if (!p || !csm || !wavenumber || !mpos || !gpos || !out_map) return ACB_ERR_ARG;
+    if (!p) return ACB_ERR_ARG;
     if (precision != ACB_TC_BF16X3) return ACB_ERR_UNSUPPORTED;
-    if (p->steer_type < 1 || p->steer_type > 4) return ACB_ERR_ARG;
-    if (p->num_mics < 2 || p->num_grid <= 0 || p->num_bins <= 0 || p->num_bins > 65535) return ACB_ERR_SHAPE;
-    const int M = p->num_mics;
-    const int Mp = (M + TC_MPC - 1) / TC_MPC * TC_MPC;
-    const int C = Mp / TC_MPC;
-    if (M > TC_MAX_MICS) return ACB_ERR_UNSUPPORTED;
-    const size_t need = acb_map_tc_workspace_bytes(M, p->num_bins, precision);
-    if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
-    if ((p->num_grid + TC_ROWS - 1) / TC_ROWS > 0x7fffffffLL) return ACB_ERR_SHAPE;
-    cudaStream_t s = as_stream(stream);
-    TcArgs a;
-    a.M = M;
-    a.Mp = Mp;
-    a.C = C;
-    a.G = p->num_grid;
-    a.steer_type = p->steer_type;
-    a.clip = p->clip_negative;
-    a.norm = p->norm;
-    a.ref_mode = p->ref_mode;
-    a.ref0 = p->ref_point[0];
-    a.ref1 = p->ref_point[1];
-    a.ref2 = p->ref_point[2];
-    a.ref_dist = p->ref_distance;
-    a.wait_limit_ns = 500ull * 1000 * 1000;
-    a.bin_stride_elems = (int64_t)tri_tiles(C) * TC_TILE_ELEMS;
-    a.ntiles = (p->num_grid + TC_ROWS - 1) / TC_ROWS;
-    a.nitems = a.ntiles * p->num_bins;
-    __nv_bfloat16 *rh = reinterpret_cast<__nv_bfloat16 *>(workspace);
-    __nv_bfloat16 *rl = rh + (size_t)p->num_bins * a.bin_stride_elems;
-    tc_prep_kernel<<<dim3(tri_tiles(C), p->num_bins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csm), M, C,
-                                                                   p->r_diag, a.bin_stride_elems, rh, rl);
-    int st = check_launch();
+    TcBatch bt;
+    bt.n_inst = 1;
+    int st = tc_fill_inst(p, csm, wavenumber, mpos, gpos, out_map, out_steer_norm,
+                          reinterpret_cast<__nv_bfloat16 *>(workspace), 0, bt.inst[0]);
     if (st) return st;
-    int smem = TcSmem::total(C, Mp) + 1024;
-    // a CTA that takes all 512 TMEM columns must be alone on its SM: size the shared memory so
-    // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)
-    if (C > 8 && smem < 116 * 1024) smem = 116 * 1024;
-    int dev = 0, nsm = kNumSMs;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const dim3 grid((unsigned)(a.nitems < nsm ? a.nitems : nsm));
-    auto kern = p->steer_type == 1 ? map_tc_kernel<1>
-                : p->steer_type == 2 ? map_tc_kernel<2>
-                : p->steer_type == 3 ? map_tc_kernel<3>
-                                     : map_tc_kernel<4>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    kern<<<grid, TC_THREADS, smem, s>>>(a, wavenumber, mpos, gpos, rh, rl, out_map, out_steer_norm, error_word);
-    return check_launch();
+    const size_t need = acb_map_tc_workspace_bytes(p->num_mics, p->num_bins, precision);
+    if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
+    bt.nitems = bt.inst[0].ntiles * bt.inst[0].nbins;
+    const acb_map_params *pp[1] = {p};
+    const void *cc[1] = {csm};
+    return tc_launch(bt, pp, cc, p->steer_type, error_word, as_stream(stream));
+}
+
+size_t acb_map_tc_batch_workspace_bytes(const acb_map_params *params, int num_instances, int precision)
+{
+    if (!params || num_instances <= 0) return 0;
+    size_t tot = 0;
+    for (int i = 0; i < num_instances; ++i) {
+        const size_t b = acb_map_tc_workspace_bytes(params[i].num_mics, params[i].num_bins, precision);
+        if (b == 0) return 0;
+        tot += (b + 255) / 256 * 256;
+    }
+    return tot;
+}
+
+int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num_instances, int precision,
+                     void *workspace, size_t workspace_bytes, int *error_word, void *stream)
+{
+    if (!params || !io) return ACB_ERR_ARG;
+    if (num_instances <= 0 || num_instances > TC_MAX_INST) return ACB_ERR_SHAPE;
+    if (precision != ACB_TC_BF16X3) return ACB_ERR_UNSUPPORTED;
+    const size_t need = acb_map_tc_batch_workspace_bytes(params, num_instances, precision);
+    if (need == 0) return ACB_ERR_SHAPE;
+    if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
+    const int steer = params[0].steer_type;
+    TcBatch bt;
+    bt.n_inst = num_instances;
+    int64_t items = 0;
+    uint8_t *w = reinterpret_cast<uint8_t *>(workspace);
+    const acb_map_params *pp[TC_MAX_INST];
+    const void *cc[TC_MAX_INST];
+    for (int i = 0; i < num_instances; ++i) {
+        if (params[i].steer_type != steer) return ACB_ERR_ARG;   // one steering type per launch
+        const int st = tc_fill_inst(&params[i], io[i].csm, io[i].wavenumber, io[i].mpos, io[i].gpos, io[i].out_map,
+                                    io[i].out_steer_norm, reinterpret_cast<__nv_bfloat16 *>(w), items, bt.inst[i]);
+        if (st) return st;
+        items += bt.inst[i].ntiles * bt.inst[i].nbins;
+        w += (acb_map_tc_workspace_bytes(params[i].num_mics, params[i].num_bins, precision) + 255) / 256 * 256;
+        pp[i] = &params[i];
+        cc[i] = io[i].csm;
+    }
+    bt.nitems = items;
+    return tc_launch(bt, pp, cc, steer, error_word, as_stream(stream));
 }
 
 }  // extern "C"

@@ -278,3 +278,47 @@ def map_tc(csm: torch.Tensor, wavenumbers: torch.Tensor, mpos: torch.Tensor, gpo
                                mpos.data_ptr(), gpos.data_ptr(), out.data_ptr(), N.ptr(steer_norm), ws.data_ptr(),
                                ws.numel(), N.ptr(error_word), N.stream_handle()), 'acb_map_tc')
     return out
+
+
+class MapInstance:
+    """One map of a batch: device tensors of its CSM (B, M, M) c128, wave numbers (B,), positions,
+    the output (B, G) and the beamformer settings."""
+
+    def __init__(self, csm, wavenumbers, mpos, gpos, steer_type='true level', r_diag=True, norm=1.0, ref=None,
+                 clip_negative=None, out=None, steer_norm=None):
+        self.csm, self.wavenumbers, self.mpos, self.gpos = csm, wavenumbers, mpos, gpos
+        self.steer_type, self.r_diag, self.norm, self.ref = steer_type, r_diag, norm, ref
+        self.clip_negative = clip_negative
+        B, M, _ = csm.shape
+        self.out = out if out is not None else torch.empty((B, gpos.shape[1]), dtype=torch.float64,
+                                                           device=csm.device)
+        self.steer_norm = steer_norm
+
+
+_batch_ws: dict = {}
+
+
+def map_tc_batch(instances, precision: str = 'bf16x3', error_word: torch.Tensor | None = None):
+    """Many maps of uneven shape in one persistent tensor-core launch (<= 64 per call, one steer type)."""
+    if not instances:
+        return []
+    dev = instances[0].csm.device
+    n = len(instances)
+    params = (N.MapParams * n)()
+    io = (N.MapIO * n)()
+    for i, it in enumerate(instances):
+        B, M, _ = it.csm.shape
+        params[i] = map_params(M, it.gpos.shape[1], B, it.steer_type, it.r_diag, it.norm, it.clip_negative, it.ref,
+                               False, dev)
+        io[i].csm, io[i].wavenumber = it.csm.data_ptr(), it.wavenumbers.data_ptr()
+        io[i].mpos, io[i].gpos = it.mpos.data_ptr(), it.gpos.data_ptr()
+        io[i].out_map, io[i].out_steer_norm = it.out.data_ptr(), N.ptr(it.steer_norm)
+    prec = N.TC_PRECISIONS[precision]
+    need = N.lib().acb_map_tc_batch_workspace_bytes(params, n, prec)
+    ws = _batch_ws.get(str(dev))
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(need, dtype=torch.uint8, device=dev)
+        _batch_ws[str(dev)] = ws
+    N.check(N.lib().acb_map_tc_batch(params, io, n, prec, ws.data_ptr(), ws.numel(), N.ptr(error_word),
+                                     N.stream_handle()), 'acb_map_tc_batch')
+    return [it.out for it in instances]

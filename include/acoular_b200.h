@@ -139,6 +139,29 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
                const double *mpos, const double *gpos, double *out_map, double *out_steer_norm,
                void *workspace, size_t workspace_bytes, int *error_word, void *stream);
 
+/* Device buffers of one instance of a batched map (sizes given by its acb_map_params). */
+typedef struct acb_map_io {
+    const void *csm;            /* complex128 [num_bins][M][M]                              */
+    const double *wavenumber;   /* float64 [num_bins]                                       */
+    const double *mpos;         /* float64 [3][M]                                           */
+    const double *gpos;         /* float64 [3][G]                                           */
+    double *out_map;            /* float64 [num_bins][G]                                    */
+    double *out_steer_norm;     /* float64 [num_bins][G] or NULL                            */
+} acb_map_io;
+
+/* Bytes of workspace acb_map_tc_batch needs for these instances. */
+size_t acb_map_tc_batch_workspace_bytes(const acb_map_params *params, int num_instances, int precision);
+
+/* Many independent maps of uneven size (mic counts, grids, bin counts) in ONE persistent launch of
+ * the tensor-core kernel: the work items (instance, bin, 128-point tile) of all instances share the
+ * GPU, so small instances fill the SMs that large ones leave idle.  Each instance's result is the
+ * one acb_map_tc gives for it alone.  params/io: host arrays of num_instances (<= 64) entries; all
+ * instances use params[0].steer_type.  The instance table travels in the kernel parameters, so the
+ * call can be captured in a CUDA graph.  The batched counterpart of BeamformerBase._calc
+ * (acoular/fbeamform.py:475-510) over many beamformers. */
+int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num_instances, int precision,
+                     void *workspace, size_t workspace_bytes, int *error_word, void *stream);
+
 /* Size of the fixed device array behind acb_map_tc_noalloc (32 MiB per GPU, held until exit). */
 #define ACB_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 

@@ -113,3 +113,54 @@ def test_tc_persistent_many_items_per_cta(M, G, nb):
     got = _tc(csm, freqs, mpos, gpos, 'true location', True)
     for b in range(nb):
         assert rel(got[b], ref[b]) <= TOL
+
+
+def _instances(specs, seed=0):
+    """Uneven instances (M, G, bins) with random geometry and CSMs, as device tensors."""
+    from acoular_b200 import device as D
+    dev = torch.device('cuda')
+    out = []
+    for idx, (M, G, nb) in enumerate(specs):
+        mpos, gpos, freqs, csm = _case(M, G, seed=seed + 17 * idx, nb=nb, z=-0.5 - 0.1 * idx)
+        out.append((D.MapInstance(torch.as_tensor(csm, device=dev),
+                                  torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
+                                  torch.as_tensor(mpos, device=dev), torch.as_tensor(gpos, device=dev),
+                                  'true level', True, O.sig_loss_norm(True, M)), (mpos, gpos, freqs, csm)))
+    return out
+
+
+def test_tc_batch_uneven_instances_equal_alone():
+    """Each instance's map is the same in the batched launch as alone, and matches the oracle."""
+    from acoular_b200 import device as D
+    specs = [(32, 441, 3), (64, 2000, 2), (128, 700, 4), (256, 300, 2), (300, 150, 2), (37, 90001, 1)]
+    inst = _instances(specs)
+    D.map_tc_batch([i for i, _ in inst])
+    torch.cuda.synchronize()
+    for it, (mpos, gpos, freqs, csm) in inst:
+        alone = D.map_tc(it.csm, it.wavenumbers, it.mpos, it.gpos, 'true level', True, it.norm).cpu().numpy()
+        got = it.out.cpu().numpy()
+        assert np.array_equal(got, alone)
+        nb = len(freqs)
+        if gpos.shape[1] <= 2000:
+            ref = O.beamformer_calc(csm, freqs, range(nb), O.apparent_r(gpos), O.apparent_r(gpos, mpos), 343.0,
+                                    'true level', True)
+            assert rel(got, ref) <= TOL
+
+
+def test_tc_batch_graph_capture_replay():
+    from acoular_b200 import device as D
+    inst = _instances([(64, 3000, 3), (128, 1000, 2)], seed=5)
+    its = [i for i, _ in inst]
+    D.map_tc_batch(its)  # warm-up outside capture (workspace allocation, kernel attributes)
+    torch.cuda.synchronize()
+    ref = [it.out.clone() for it in its]
+    for it in its:
+        it.out.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        D.map_tc_batch(its)
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    for it, r in zip(its, ref):
+        assert torch.equal(it.out, r)
