@@ -160,7 +160,7 @@ struct TcSmem {
     __host__ __device__ static constexpr int red_off(int C, int Mp) { return mic_off(C) + Mp * 16; }
     // per-item normalisation partial sums, double-buffered by item parity: [2][parts][128]
     __host__ __device__ static constexpr int bar_off(int C, int Mp) { return red_off(C, Mp) + 2 * TC_PARTS * TC_ROWS * 8; }
-    __host__ __device__ static constexpr int nbars() { return 2 * TC_ASTAGES + 2 * TC_NB + 1 + 2 + 2; }
+    __host__ __device__ static constexpr int nbars() { return 2 * TC_ASTAGES + 3 * TC_NB + 2 + 2; }
     __host__ __device__ static constexpr int total(int C, int Mp) { return bar_off(C, Mp) + nbars() * 8 + 16; }
 };
 
@@ -212,16 +212,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     uint64_t *afree = bars + TC_ASTAGES;              // [3]  epilogue of step T has released A stage T % 3
     uint64_t *full_b = bars + 2 * TC_ASTAGES;         // [8]  R' tiles of step T landed
     uint64_t *done = full_b + TC_NB;                  // [8]  MMAs of step T complete
-    uint64_t *tmem_free = done + TC_NB;               // [1]  epilogue has read all columns of a pass
-    uint64_t *s_ready = tmem_free + 1;                // [2]  synthesis sums S of item parity written
+    uint64_t *tfree = done + TC_NB;                   // [8]  epilogue has read all columns of window W
+    uint64_t *s_ready = tfree + TC_NB;                // [2]  synthesis sums S of item parity written
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(s_ready + 2 + 2);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(s_ready + 2 + 3);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t nmine = b.nitems > blockIdx.x ? (b.nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    int cmax = 1;
-    for (int i = 0; i < b.n_inst; ++i) cmax = max(cmax, b.inst[i].C);
-    const uint32_t ncols = (uint32_t)(cmax <= 1 ? 32 : (cmax <= 2 ? 64 : (cmax <= 4 ? 128 : (cmax <= 8 ? 256 : 512))));
+    const uint32_t ncols = 512;   // the whole TMEM: accumulator windows rotate through it
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_ASTAGES; ++s) {
@@ -232,7 +230,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             tc::mbar_init(&full_b[s], 1);
             tc::mbar_init(&done[s], 1);
         }
-        tc::mbar_init(tmem_free, TC_EPI_THREADS);
+        for (int s = 0; s < TC_NB; ++s) tc::mbar_init(&tfree[s], TC_EPI_THREADS);
         tc::mbar_init(&s_ready[0], TC_SYNTH_THREADS);
         tc::mbar_init(&s_ready[1], TC_SYNTH_THREADS);
         *abort_flag = 0;
@@ -317,24 +315,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             int sb = 0, ub = 0;     // step barrier slot and parity
             uint32_t slot0 = 0;     // ring slot of the step's first tile
             int lastb = -1, lastu = 0;
-            int npass = 0;          // passes started (tmem_free phases to wait for)
+            // accumulator windows (one per column pass) rotate through TMEM in slots of the
+            // instance's width; a slot is reused once the epilogue has released the window that
+            // last held it.  An instance change drains all windows and restarts the rotation.
+            int W = 0, w_start = 0, wpt = 1, width = 512, cur_inst = -1;
             bool ok = true;
             for (int64_t li = 0; li < nmine && ok; ++li) {
                 const int64_t item = blockIdx.x + li * gridDim.x;
-                const int C = b.inst[find_inst(b, item)].C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
-                for (int pp = 0; pp < P && ok; ++pp) {
+                const int ii = find_inst(b, item);
+                const int C = b.inst[ii].C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+                if (ii != cur_inst) {
+                    if (W > 0)
+                        ok = tc::mbar_wait(&tfree[(W - 1) & (TC_NB - 1)], (uint32_t)(((W - 1) / TC_NB) & 1), abort_flag,
+                                           b.wait_limit_ns);
+                    width = TC_CHUNK * min(C, TC_PASS_CHUNKS);
+                    wpt = min(TC_NB, 512 / width);
+                    w_start = W;
+                    cur_inst = ii;
+                }
+                for (int pp = 0; pp < P && ok; ++pp, ++W) {
                     const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
-                    // the previous pass's epilogue must have read every accumulator column
-                    if (npass > 0)
-                        ok = tc::mbar_wait(tmem_free, (uint32_t)((npass - 1) & 1), abort_flag, b.wait_limit_ns);
-                    ++npass;
+                    if (W - w_start >= wpt)
+                        ok = tc::mbar_wait(&tfree[(W - wpt) & (TC_NB - 1)], (uint32_t)(((W - wpt) / TC_NB) & 1),
+                                           abort_flag, b.wait_limit_ns);
+                    const uint32_t wcol = taddr + (uint32_t)(((W - w_start) % wpt) * width);
                     for (int i = 0; i < je && ok; ++i) {
                         ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, b.wait_limit_ns) &&
                              tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, b.wait_limit_ns);
                         if (!ok) break;
                         tc::tc_fence_after();
                         const int j0 = max(i, jb), n = je - j0;
-                        const uint32_t dcol = taddr + (uint32_t)(TC_CHUNK * (j0 - jb));
+                        const uint32_t dcol = wcol + (uint32_t)(TC_CHUNK * (j0 - jb));
                         // split the step's n tiles into runs of <= 8 (N <= 256) that do not wrap
                         const int run0 = min(min(n, 8), (int)(TC_RING - slot0));
                         const uint32_t slot1 = (slot0 + run0) & (TC_RING - 1);
@@ -379,16 +390,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
         const uint32_t lane_addr = taddr + ((uint32_t)(q * 32) << 16);
         const int a_row = ((row >> 3) << 9) + ((row & 7) << 4);   // byte offset of the row's first chunk
         int T = 0, sa = 0;
+        int W = 0, w_start = 0, wpt = 1, width = 512, cur_inst = -1;   // same window rotation as the MMAs
         bool ok = true;
         for (int64_t li = 0; li < nmine && ok; ++li) {
             const int64_t item = blockIdx.x + li * gridDim.x;
-            const TcInst &in = b.inst[find_inst(b, item)];
+            const int ii = find_inst(b, item);
+            const TcInst &in = b.inst[ii];
             const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+            if (ii != cur_inst) {
+                width = TC_CHUNK * min(C, TC_PASS_CHUNKS);
+                wpt = min(TC_NB, 512 / width);
+                w_start = W;
+                cur_inst = ii;
+            }
             const int bin = (int)((item - in.item_off) / in.ntiles);
             const int64_t g = ((item - in.item_off) % in.ntiles) * TC_ROWS + row;
             double acc = 0.0;
-            for (int pp = 0; pp < P && ok; ++pp) {
+            for (int pp = 0; pp < P && ok; ++pp, ++W) {
                 const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+                const uint32_t wcol = lane_addr + (uint32_t)(((W - w_start) % wpt) * width);
                 for (int i = 0; i < je; ++i, ++T) {
                     ok = __all_sync(0xffffffffu, tc::mbar_wait(&done[T & (TC_NB - 1)], (uint32_t)((T / TC_NB) & 1),
                                                                abort_flag, b.wait_limit_ns));
@@ -396,7 +416,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                     if (i >= jb) {
                         tc::tc_fence_after();
                         float d[TC_CHUNK];
-                        tc::tmem_ld_x32(lane_addr + (uint32_t)(TC_CHUNK * (i - jb)), d);
+                        tc::tmem_ld_x32(wcol + (uint32_t)(TC_CHUNK * (i - jb)), d);
                         const uint8_t *ahi = smem + TcSmem::a_off(sa, 0) + a_row;
                         const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;
                         float part = 0.f;
@@ -421,7 +441,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                     if (++sa == TC_ASTAGES) sa = 0;
                 }
                 if (!ok) break;
-                tc::mbar_arrive(tmem_free);
+                tc::mbar_arrive(&tfree[W & (TC_NB - 1)]);
             }
             if (!ok) break;
             // normalisation sums of this item from the synthesis warps
@@ -590,7 +610,6 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
                      int *error_word, cudaStream_t s)
 {
     int mp_max = 16;
-    int cmax = 1;
     for (int i = 0; i < bt.n_inst; ++i) {
         const TcInst &in = bt.inst[i];
         tc_prep_kernel<<<dim3(tri_tiles(in.C), in.nbins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csms[i]), in.M,
@@ -600,14 +619,13 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
         const int st = check_launch();
         if (st) return st;
         mp_max = max(mp_max, in.Mp);
-        cmax = max(cmax, in.C);
     }
     bt.mp_max = mp_max;
     bt.wait_limit_ns = 500ull * 1000 * 1000;
     int smem = TcSmem::total(0, mp_max) + 1024;
-    // a CTA that takes all 512 TMEM columns must be alone on its SM: size the shared memory so
+    // each CTA takes all 512 TMEM columns and must be alone on its SM: size the shared memory so
     // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)
-    if (cmax > 8 && smem < 116 * 1024) smem = 116 * 1024;
+    if (smem < 116 * 1024) smem = 116 * 1024;
     int dev = 0, nsm = kNumSMs;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const dim3 grid((unsigned)(bt.nitems < nsm ? bt.nitems : nsm));
