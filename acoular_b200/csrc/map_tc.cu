@@ -475,10 +475,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             if (ii != cur_inst) {
                 // new instance: every synthesis thread is past the previous item, reload the mics
                 asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
+                // (x, y, z, weight): padding mics beyond M get weight 0 and a position off the grid
                 for (int m = sid; m < in.Mp; m += TC_SYNTH_THREADS) {
-                    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                    float4 v = make_float4(1.f, 1.f, 1.f, 0.f);
                     if (m < in.M)
-                        v = make_float4((float)in.mpos[m], (float)in.mpos[in.M + m], (float)in.mpos[2 * in.M + m], 0.f);
+                        v = make_float4((float)in.mpos[m], (float)in.mpos[in.M + m], (float)in.mpos[2 * in.M + m], 1.f);
                     mp4[m] = v;
                 }
                 asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
@@ -511,7 +512,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
                         const int m = t * TC_MPC + p * 4 + e;
-                        const bool valid = gvalid && m < in.M;
                         const float4 mv = mp4[m];
                         const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
                         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
@@ -528,23 +528,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         x += pl;
                         float sn, cs;
                         tc::sincos_approx(x, sn, cs);
-                        float w = 1.f;
-                        if (ST == 2) {
-                            w = r;
-                            s_part += valid ? r2 : 0.f;
-                        } else if (ST >= 3) {
-                            w = y;
-                            s_part += valid ? y * y : 0.f;
-                        }
-                        const float vr = valid ? cs * w : 0.f;
-                        const float vi = valid ? -sn * w : 0.f;
-                        // split-BF16 by integer rounding (half away from zero) of the upper 16 bits:
-                        // hi = round16(x), lo = round16(x - hi); byte permutes pack (re, im) pairs
-                        const uint32_t rr = __float_as_uint(vr) + 0x8000u, ri = __float_as_uint(vi) + 0x8000u;
-                        hw[e] = __byte_perm(rr, ri, 0x7632);
-                        const float lr = vr - __uint_as_float(rr & 0xFFFF0000u);
-                        const float li_ = vi - __uint_as_float(ri & 0xFFFF0000u);
-                        lw[e] = __byte_perm(__float_as_uint(lr) + 0x8000u, __float_as_uint(li_) + 0x8000u, 0x7632);
+                        // steering weight: 1, r (inverse) or 1/r (true level / location), times the
+                        // mic's table weight (0 for padding mics)
+                        const float w = (ST == 2 ? r : (ST >= 3 ? y : 1.f)) * mv.w;
+                        if (ST == 2) s_part = fmaf(r2, mv.w, s_part);
+                        else if (ST >= 3) s_part = fmaf(y * y, mv.w, s_part);
+                        const float vr = cs * w, vi = -sn * w;
+                        // split-BF16: hi = bf16(x) (packed pair conversion), lo = bf16(x - hi)
+                        const __nv_bfloat162 h2 = __floats2bfloat162_rn(vr, vi);
+                        hw[e] = *reinterpret_cast<const uint32_t *>(&h2);
+                        const float lr = vr - __uint_as_float(hw[e] << 16);
+                        const float li_ = vi - __uint_as_float(hw[e] & 0xFFFF0000u);
+                        const __nv_bfloat162 l2 = __floats2bfloat162_rn(lr, li_);
+                        lw[e] = *reinterpret_cast<const uint32_t *>(&l2);
+                    }
+                    if (!gvalid) {   // grid points past the end of the grid contribute nothing
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) hw[e] = lw[e] = 0u;
                     }
                     *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 0) + a_off_row) =
                         make_uint4(hw[0], hw[1], hw[2], hw[3]);
