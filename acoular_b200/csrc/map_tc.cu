@@ -113,6 +113,16 @@ __device__ __forceinline__ int tile_off(int row, int col)
 // ------------------------------------------------------------------------------------------------
 // R' in split-BF16, per bin: tiles (i, j >= i) of 32 x 32, stored row = n (column of D), col = k.
 // ------------------------------------------------------------------------------------------------
+// TF32 operand layout of a 32x32 tile: core matrices of 8 rows x 4 fp32 (16 bytes), 8 per row group.
+__device__ __forceinline__ int tile_off_tf32(int row, int col)
+{
+    return (((row >> 3) * 8 + (col >> 2)) << 5) + ((row & 7) << 2) + (col & 3);
+}
+
+// Round an FP32 value to TF32 (nearest, ties away from zero), as the MMA reads only 19 bits.
+__device__ __forceinline__ uint32_t tf32_bits(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
+
+template <bool TF32>
 __global__ void __launch_bounds__(256) tc_prep_kernel(const double2 *__restrict__ csm, int M, int C, int r_diag,
                                                       int64_t bin_stride, __nv_bfloat16 *__restrict__ rh,
                                                       __nv_bfloat16 *__restrict__ rl)
@@ -139,11 +149,19 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const double2 *__restrict_
             val *= factor;
         }
         const float vf = (float)val;
-        const __nv_bfloat16 h = __float2bfloat16_rn(vf);
-        const __nv_bfloat16 l = __float2bfloat16_rn(vf - __bfloat162float(h));
-        const int o = tile_off(rr, kk);
-        th[o] = h;
-        tl[o] = l;
+        if (TF32) {
+            // FP32 tiles of 4 KB: the whole workspace (hi and lo halves) holds them, 2 x bin_stride
+            // bf16 elements per bin
+            uint32_t *t32 = reinterpret_cast<uint32_t *>(rh + 2 * (int64_t)bin * bin_stride) +
+                            (int64_t)tile_index(C, i, j) * TC_TILE_ELEMS;
+            t32[tile_off_tf32(rr, kk)] = tf32_bits(vf);
+        } else {
+            const __nv_bfloat16 h = __float2bfloat16_rn(vf);
+            const __nv_bfloat16 l = __float2bfloat16_rn(vf - __bfloat162float(h));
+            const int o = tile_off(rr, kk);
+            th[o] = h;
+            tl[o] = l;
+        }
     }
 }
 
@@ -198,7 +216,7 @@ __device__ __forceinline__ void finish_point(const TcInst &a, double scalar, dou
 
 // Persistent kernel: one CTA per SM walks the batch's work items (instance, bin, 128-point tile)
 // blockIdx.x, +gridDim.x, ...; the step pipeline runs on across item and instance boundaries.
-template <int ST>
+template <int ST, bool TF32>
 __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_constant__ TcBatch b, int *err)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -260,7 +278,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 const TcInst &in = b.inst[find_inst(b, item)];
                 const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
                 const int64_t bin = (item - in.item_off) / in.ntiles;
-                const __nv_bfloat16 *bh = in.rh + bin * in.bin_stride;
+                const __nv_bfloat16 *bh = in.rh + (TF32 ? 2 : 1) * bin * in.bin_stride;
                 const __nv_bfloat16 *bl = in.rl + bin * in.bin_stride;
                 for (int pp = 0; pp < P && ok; ++pp) {
                     const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
@@ -278,15 +296,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         if (!ok) break;
                         ustart[T & (TC_NB - 1)] = U;
                         uint64_t *fb = &full_b[T & (TC_NB - 1)];
-                        tc::mbar_arrive_expect_tx(fb, 2u * n * TC_TILE_BYTES);
+                        tc::mbar_arrive_expect_tx(fb, 2u * n * TC_TILE_BYTES);   // hi + lo, or one FP32 tile
                         const int64_t src = (int64_t)tile_index(C, i, j0) * TC_TILE_ELEMS;
                         int j = 0;
                         while (j < n) {   // contiguous runs of ring slots
                             const int slot = (int)((U + j) & (TC_RING - 1));
                             const int run = min(n - j, TC_RING - slot);
                             const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
-                            tc::bulk_g2s(smem + TcSmem::b_off(slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
-                            tc::bulk_g2s(smem + TcSmem::b_off(slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                            if (TF32) {   // FP32 tiles of 4 KB, ring slot s at b_base + s * 4 KB
+                                tc::bulk_g2s(smem + TcSmem::b_base() + slot * 2 * TC_TILE_BYTES,
+                                             reinterpret_cast<const uint32_t *>(bh) + src + (int64_t)j * TC_TILE_ELEMS,
+                                             2 * bytes, fb);
+                            } else {
+                                tc::bulk_g2s(smem + TcSmem::b_off(slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                                tc::bulk_g2s(smem + TcSmem::b_off(slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                            }
                             j += run;
                         }
                         U += (uint32_t)n;
@@ -305,12 +329,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
         // advanced by adding byte offsets >> 4 to their 14-bit start-address field; ring and
         // stage indices are 32-bit counters advanced incrementally.
         if (lane == 0) {
-            const uint64_t a_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::a_off(0, 0)), 128, 512);
-            const uint64_t b_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::b_off(0, 0)), 128, 512);
+            // BF16: 8-row x 8-element core matrices, 4 per 32-component row group (SBO 512);
+            // TF32: 8-row x 4-element core matrices, 8 per row group (SBO 1024)
+            constexpr uint32_t SBO = TF32 ? 1024 : 512;
+            const uint64_t a_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::a_off(0, 0)), 128, SBO);
+            const uint64_t b_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::b_off(0, 0)), 128, SBO);
             constexpr uint32_t A_STEP = TC_A_BYTES >> 4;          // next (stage, hi|lo) block
-            constexpr uint32_t T_STEP = TC_TILE_BYTES >> 4;       // next ring tile
+            constexpr uint32_t T_STEP = (TF32 ? 2 : 1) * (TC_TILE_BYTES >> 4);   // next ring tile
             constexpr uint32_t LO_B = (TC_RING * TC_TILE_BYTES) >> 4;
-            const uint32_t idesc0 = tc::idesc_m128(1, 0);
+            const uint32_t idesc0 = tc::idesc_m128(TF32 ? 2 : 1, 0);
             int sa = 0, ua = 0;     // A stage and its phase parity
             int sb = 0, ub = 0;     // step barrier slot and parity
             uint32_t slot0 = 0;     // ring slot of the step's first tile
@@ -353,20 +380,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         const int run1 = min(min(rest, 8), (int)(TC_RING - slot1));
                         const uint32_t slot2 = (slot1 + run1) & (TC_RING - 1);
                         const int run2 = rest - run1;   // at most one more run (n <= 16)
+                        // BF16: K steps of 16 (2) x products hi*hi, hi*lo, lo*hi; TF32: K steps of 8 (4) x 1
+                        constexpr int KS = TF32 ? 4 : 2, NPROD = TF32 ? 1 : 3;
 #pragma unroll
-                        for (int ks = 0; ks < 2; ++ks) {
+                        for (int ks = 0; ks < KS; ++ks) {
 #pragma unroll
-                            for (int prod = 0; prod < 3; ++prod) {
+                            for (int prod = 0; prod < NPROD; ++prod) {
                                 const uint64_t ad = a_base + (uint64_t)((sa * 2 + (prod == 2)) * A_STEP + ks * 16);
                                 const uint64_t bd = b_base + (uint64_t)((prod == 1 ? LO_B : 0u) + ks * 16);
                                 const uint32_t accum = (i == 0 && ks == 0 && prod == 0) ? 0u : 1u;
-                                tc::mma_bf16(dcol, ad, bd + slot0 * T_STEP, idesc0 | ((uint32_t)(run0 * 4) << 17), accum);
-                                if (run1 > 0)
-                                    tc::mma_bf16(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP,
-                                                 idesc0 | ((uint32_t)(run1 * 4) << 17), accum);
-                                if (run2 > 0)
-                                    tc::mma_bf16(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
-                                                 idesc0 | ((uint32_t)(run2 * 4) << 17), accum);
+                                const uint32_t n0 = idesc0 | ((uint32_t)(run0 * 4) << 17);
+                                const uint32_t n1 = idesc0 | ((uint32_t)(run1 * 4) << 17);
+                                const uint32_t n2 = idesc0 | ((uint32_t)(run2 * 4) << 17);
+                                if (TF32) {
+                                    tc::mma_tf32(dcol, ad, bd + slot0 * T_STEP, n0, accum);
+                                    if (run1 > 0)
+                                        tc::mma_tf32(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP, n1, accum);
+                                    if (run2 > 0)
+                                        tc::mma_tf32(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
+                                                     n2, accum);
+                                } else {
+                                    tc::mma_bf16(dcol, ad, bd + slot0 * T_STEP, n0, accum);
+                                    if (run1 > 0)
+                                        tc::mma_bf16(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP, n1, accum);
+                                    if (run2 > 0)
+                                        tc::mma_bf16(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
+                                                     n2, accum);
+                                }
                             }
                         }
                         tc::mma_commit(&done[sb]);
@@ -420,8 +460,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         const uint8_t *ahi = smem + TcSmem::a_off(sa, 0) + a_row;
                         const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;
                         float part = 0.f;
+                        if (TF32) {
+                            // FP32 row: 8 core-matrix columns of 4 values, 128 bytes apart
+                            const uint8_t *a32 = smem + TcSmem::a_off(sa, 0) + ((row >> 3) << 10) + ((row & 7) << 4);
 #pragma unroll
-                        for (int grp = 0; grp < 4; ++grp) {
+                            for (int c4 = 0; c4 < 8; ++c4) {
+                                const float4 v = *reinterpret_cast<const float4 *>(a32 + c4 * 128);
+                                part = fmaf(d[c4 * 4 + 0], v.x, part);
+                                part = fmaf(d[c4 * 4 + 1], v.y, part);
+                                part = fmaf(d[c4 * 4 + 2], v.z, part);
+                                part = fmaf(d[c4 * 4 + 3], v.w, part);
+                            }
+                        }
+#pragma unroll
+                        for (int grp = 0; grp < (TF32 ? 0 : 4); ++grp) {
                             const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
                             const uint4 lw = *reinterpret_cast<const uint4 *>(alo + grp * 128);
                             const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w}, lv[4] = {lw.x, lw.y, lw.z, lw.w};
@@ -534,6 +586,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         if (ST == 2) s_part = fmaf(r2, mv.w, s_part);
                         else if (ST >= 3) s_part = fmaf(y * y, mv.w, s_part);
                         const float vr = cs * w, vi = -sn * w;
+                        if (TF32) {   // FP32 operand rounded to TF32: (re, im) of mic e in hw[e], lw[e]
+                            hw[e] = tf32_bits(vr);
+                            lw[e] = tf32_bits(vi);
+                            continue;
+                        }
                         // split-BF16: hi = bf16(x) (packed pair conversion), lo = bf16(x - hi)
                         const __nv_bfloat162 h2 = __floats2bfloat162_rn(vr, vi);
                         hw[e] = *reinterpret_cast<const uint32_t *>(&h2);
@@ -546,10 +603,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
 #pragma unroll
                         for (int e = 0; e < 4; ++e) hw[e] = lw[e] = 0u;
                     }
-                    *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 0) + a_off_row) =
-                        make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                    *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
-                        make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    if (TF32) {
+                        // components 8p..8p+7 = core-matrix columns 2p, 2p+1 of the FP32 row
+                        uint8_t *a32 = smem + TcSmem::a_off(sa, 0) + ((row >> 3) << 10) + ((row & 7) << 4) + p * 256;
+                        *reinterpret_cast<uint4 *>(a32) = make_uint4(hw[0], lw[0], hw[1], lw[1]);
+                        *reinterpret_cast<uint4 *>(a32 + 128) = make_uint4(hw[2], lw[2], hw[3], lw[3]);
+                    } else {
+                        *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 0) + a_off_row) =
+                            make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                        *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
+                            make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    }
                     if (t >= jb) S += (double)s_part;   // each mic's term once, in its own pass
                     tc::fence_proxy_async_smem();
                     tc::mbar_arrive(&full_a[sa]);
@@ -607,15 +671,16 @@ static int tc_fill_inst(const acb_map_params *p, const void *csm, const double *
 
 // Launch the R' preparation of every instance and the persistent map kernel over the batch.
 static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const void *const *csms, int steer_type,
-                     int *error_word, cudaStream_t s)
+                     int precision, int *error_word, cudaStream_t s)
 {
     int mp_max = 16;
     for (int i = 0; i < bt.n_inst; ++i) {
         const TcInst &in = bt.inst[i];
-        tc_prep_kernel<<<dim3(tri_tiles(in.C), in.nbins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csms[i]), in.M,
-                                                                      in.C, params[i]->r_diag, in.bin_stride,
-                                                                      const_cast<__nv_bfloat16 *>(in.rh),
-                                                                      const_cast<__nv_bfloat16 *>(in.rl));
+        auto prep = precision == ACB_TC_TF32 ? tc_prep_kernel<true> : tc_prep_kernel<false>;
+        prep<<<dim3(tri_tiles(in.C), in.nbins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csms[i]), in.M, in.C,
+                                                            params[i]->r_diag, in.bin_stride,
+                                                            const_cast<__nv_bfloat16 *>(in.rh),
+                                                            const_cast<__nv_bfloat16 *>(in.rl));
         const int st = check_launch();
         if (st) return st;
         mp_max = max(mp_max, in.Mp);
@@ -629,10 +694,11 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
     int dev = 0, nsm = kNumSMs;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const dim3 grid((unsigned)(bt.nitems < nsm ? bt.nitems : nsm));
-    auto kern = steer_type == 1 ? map_tc_kernel<1>
-                : steer_type == 2 ? map_tc_kernel<2>
-                : steer_type == 3 ? map_tc_kernel<3>
-                                  : map_tc_kernel<4>;
+    const bool tf = precision == ACB_TC_TF32;
+    auto kern = steer_type == 1 ? (tf ? map_tc_kernel<1, true> : map_tc_kernel<1, false>)
+                : steer_type == 2 ? (tf ? map_tc_kernel<2, true> : map_tc_kernel<2, false>)
+                : steer_type == 3 ? (tf ? map_tc_kernel<3, true> : map_tc_kernel<3, false>)
+                                  : (tf ? map_tc_kernel<4, true> : map_tc_kernel<4, false>);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     kern<<<grid, TC_THREADS, smem, s>>>(bt, error_word);
     return check_launch();
@@ -658,7 +724,7 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
                int *error_word, void *stream)
 {
     if (!p) return ACB_ERR_ARG;
-    if (precision != ACB_TC_BF16X3) return ACB_ERR_UNSUPPORTED;
+    if (precision != ACB_TC_BF16X3 && precision != ACB_TC_TF32) return ACB_ERR_UNSUPPORTED;
     TcBatch bt;
     bt.n_inst = 1;
     int st = tc_fill_inst(p, csm, wavenumber, mpos, gpos, out_map, out_steer_norm,
@@ -669,7 +735,7 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
     bt.nitems = bt.inst[0].ntiles * bt.inst[0].nbins;
     const acb_map_params *pp[1] = {p};
     const void *cc[1] = {csm};
-    return tc_launch(bt, pp, cc, p->steer_type, error_word, as_stream(stream));
+    return tc_launch(bt, pp, cc, p->steer_type, precision, error_word, as_stream(stream));
 }
 
 size_t acb_map_tc_batch_workspace_bytes(const acb_map_params *params, int num_instances, int precision)
@@ -689,7 +755,7 @@ int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num
 {
     if (!params || !io) return ACB_ERR_ARG;
     if (num_instances <= 0 || num_instances > TC_MAX_INST) return ACB_ERR_SHAPE;
-    if (precision != ACB_TC_BF16X3) return ACB_ERR_UNSUPPORTED;
+    if (precision != ACB_TC_BF16X3 && precision != ACB_TC_TF32) return ACB_ERR_UNSUPPORTED;
     const size_t need = acb_map_tc_batch_workspace_bytes(params, num_instances, precision);
     if (need == 0) return ACB_ERR_SHAPE;
     if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
@@ -711,7 +777,7 @@ int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num
         cc[i] = io[i].csm;
     }
     bt.nitems = items;
-    return tc_launch(bt, pp, cc, steer, error_word, as_stream(stream));
+    return tc_launch(bt, pp, cc, steer, precision, error_word, as_stream(stream));
 }
 
 }  // extern "C"

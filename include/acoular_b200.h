@@ -120,7 +120,10 @@ int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wav
                             const double *rm, double *out_map, double *out_steer_norm, void *stream);
 
 /* Tensor-core operand precisions. */
-enum acb_tc_precision { ACB_TC_BF16X3 = 0 /* split-BF16 hi/lo, 3 products, FP32 accumulation */ };
+enum acb_tc_precision {
+    ACB_TC_BF16X3 = 0,  /* split-BF16 hi/lo operands, 3 products, FP32 accumulation (~1e-5)      */
+    ACB_TC_TF32 = 1     /* FP32 operands rounded to TF32, 1 product, FP32 accumulation (~1e-4)  */
+};
 
 /* Bytes of workspace acb_map_tc needs (the per-bin split-BF16 copy of the real-embedded CSM). */
 size_t acb_map_tc_workspace_bytes(int num_mics, int num_bins, int precision);

@@ -39,13 +39,13 @@ def _case(M, G, seed, nb=3, z=-0.6):
     return mpos, gpos, freqs, csm
 
 
-def _tc(csm, freqs, mpos, gpos, steer, r_diag, ref=None):
+def _tc(csm, freqs, mpos, gpos, steer, r_diag, ref=None, precision='bf16x3'):
     from acoular_b200 import device as D
     dev = torch.device('cuda')
     M = mpos.shape[1]
     out = D.map_tc(torch.as_tensor(csm, device=dev), torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
                    torch.as_tensor(mpos, device=dev), torch.as_tensor(np.ascontiguousarray(gpos), device=dev), steer,
-                   r_diag, O.sig_loss_norm(r_diag, M), ref=ref, clip_negative=r_diag)
+                   r_diag, O.sig_loss_norm(r_diag, M), ref=ref, clip_negative=r_diag, precision=precision)
     return out.cpu().numpy()
 
 
@@ -164,3 +164,16 @@ def test_tc_batch_graph_capture_replay():
     torch.cuda.synchronize()
     for it, r in zip(its, ref):
         assert torch.equal(it.out, r)
+
+
+@pytest.mark.parametrize('M,G', [(16, 128), (64, 257), (256, 200), (300, 150)])
+@pytest.mark.parametrize('steer', STEERS)
+def test_tf32_form_vs_oracle(M, G, steer):
+    """The FP32/TF32 operand form: one TF32 product, FP32 accumulation; <= 1e-3 of max."""
+    mpos, gpos, freqs, csm = _case(M, G, seed=M + 3 * G)
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    for r_diag in (False, True):
+        ref = O.beamformer_calc(csm, freqs, range(len(freqs)), r0, rm, 343.0, steer, r_diag)
+        got = _tc(csm, freqs, mpos, gpos, steer, r_diag, precision='tf32')
+        for b in range(len(freqs)):
+            assert rel(got[b], ref[b]) <= TOL, (b, rel(got[b], ref[b]))
