@@ -62,8 +62,10 @@ class BatchPlan:
         ws_bytes = 0
         for it in self.inst:
             S, M = np.shape(it.samples)
-            dtype = torch.float32 if np.dtype(getattr(it.samples, 'dtype', np.float64)) == np.float32 or \
-                (isinstance(it.samples, torch.Tensor) and it.samples.dtype == torch.float32) else torch.float64
+            if isinstance(it.samples, torch.Tensor):
+                dtype = torch.float32 if it.samples.dtype == torch.float32 else torch.float64
+            else:
+                dtype = torch.float32 if np.asarray(it.samples).dtype == np.float32 else torch.float64
             self.samples.append(torch.empty((S, M), dtype=dtype, device=dev))
             cdt = torch.complex64 if it.precision == 'complex64' else torch.complex128
             self.upper.append(torch.zeros((it.num_bins, M, M), dtype=cdt, device=dev))

@@ -6,7 +6,10 @@ geometry, grid, FFT block size and frequency band.  The server keeps, per stream
 * the running Welch sum of the CSM (upper triangle) over everything the stream has sent, for the
   band's bins only, plus the samples of the not yet complete window (so windows span request
   boundaries exactly as ``PowerSpectra`` windows a continuous recording, acoular/spectra.py:171-184);
-* its geometry and grid (shared by streams that use the same ones).
+* its geometry and grid (shared by streams that use the same ones);
+* its finished CSM, map and band-map buffers, and pinned host buffers for the samples coming in and
+  the band map going out -- so serving a request allocates no pinned host memory (a pinned
+  allocation on the request path stalled the worker for 100-250 ms at a time).
 
 A worker thread takes every request that is pending when the GPU becomes free (continuous
 batching: requests that arrive during a batch join the next one), updates each stream's CSM with
@@ -52,6 +55,11 @@ class StreamState:
     r_diag: bool
     upper: torch.Tensor                 # running Welch sum, (num_bins, M, M) complex128
     tail: torch.Tensor                  # samples of the incomplete window
+    csm: torch.Tensor = None            # finished CSM of the band's bins (num_bins, M, M) complex128
+    out: torch.Tensor = None            # map of the band's bins (num_bins, G) float64
+    band: torch.Tensor = None           # band map (G,) float64
+    h_band: torch.Tensor = None         # pinned host copy of ``band``
+    h_in: torch.Tensor = None           # pinned host staging of a request's samples (capacity, M) float32
     total_samples: int = 0
     bytes: int = 0
     gkey: object = None
@@ -82,6 +90,10 @@ class BeamformingServer:
         self._used = 0
         self._stop = False
         self.batches: list[int] = []        # batch sizes served (for inspection)
+        # per batch: (requests, t_taken, t_csm_issued, t_maps_issued, t_done), perf_counter seconds
+        self.batch_times: list[tuple] = []
+        self._err = torch.zeros(1, dtype=torch.int32, device=self.dev)     # kernel wait-timeout flag
+        self._h_err = torch.zeros(1, dtype=torch.int32, pin_memory=True)
         self._worker = threading.Thread(target=self._run, name='acb-serving', daemon=True)
         self._worker.start()
 
@@ -119,7 +131,7 @@ class BeamformingServer:
         G = gpos.shape[1]
         nb = i2 - i1
         gkey = (mpos.tobytes(), gpos.tobytes())
-        state_bytes = nb * M * M * 16 + block_size * M * 8
+        state_bytes = 2 * nb * M * M * 16 + block_size * M * 8 + nb * G * 8 + G * 8
         geo_bytes = 0 if gkey in self._geom else (mpos.size + gpos.size) * 8
         self._reserve(state_bytes + geo_bytes, block=False)
         if gkey not in self._geom:
@@ -134,7 +146,12 @@ class BeamformingServer:
                          steer_type=steer_type, r_diag=r_diag,
                          upper=torch.zeros((nb, M, M), dtype=torch.complex128, device=self.dev),
                          tail=torch.zeros((0, M), dtype=torch.float32, device=self.dev), bytes=state_bytes,
-                         gkey=gkey)
+                         gkey=gkey,
+                         csm=torch.empty((nb, M, M), dtype=torch.complex128, device=self.dev),
+                         out=torch.empty((nb, G), dtype=torch.float64, device=self.dev),
+                         band=torch.empty(G, dtype=torch.float64, device=self.dev),
+                         h_band=torch.empty(G, dtype=torch.float64, pin_memory=True),
+                         h_in=torch.empty((int(sample_freq * 0.25), M), dtype=torch.float32, pin_memory=True))
         self.streams[sid] = st
         return st
 
@@ -186,10 +203,15 @@ class BeamformingServer:
 
     def _process(self, batch):
         dev = self.dev
+        t_taken = time.perf_counter()
         insts = []
         for r in batch:
             st = r.stream
-            x = torch.from_numpy(r.samples).pin_memory().to(dev, non_blocking=True)
+            S = r.samples.shape[0]
+            if S > st.h_in.shape[0]:        # a request longer than any before on this stream
+                st.h_in = torch.empty((S, st.h_in.shape[1]), dtype=torch.float32, pin_memory=True)
+            st.h_in[:S].numpy()[...] = r.samples
+            x = st.h_in[:S].to(dev, non_blocking=True)
             buf = torch.cat([st.tail, x], 0) if st.tail.shape[0] else x
             ov = D.OVERLAPS[st.overlap]
             hop = st.block_size // ov
@@ -203,24 +225,35 @@ class BeamformingServer:
             with np.errstate(divide='ignore', invalid='ignore'):
                 scale = float(np.float64(2.0 / st.block_size) / np.float64(weight) /
                               np.float64(D.num_blocks(st.total_samples, st.block_size, ov)))
-            csm = D.csm_finalize(st.upper, scale)
+            D.csm_finalize(st.upper, scale, out=st.csm)
             M = st.mpos.shape[1]
             norm = (M / (M - 1.0)) if st.r_diag else 1.0
-            insts.append(D.MapInstance(csm, st.k, st.mpos, st.gpos, st.steer_type, st.r_diag, norm,
-                                       clip_negative=st.r_diag))
+            insts.append(D.MapInstance(st.csm, st.k, st.mpos, st.gpos, st.steer_type, st.r_diag, norm,
+                                       clip_negative=st.r_diag, out=st.out))
+        t_csm = time.perf_counter()
         groups = {}
         for mi in insts:
             groups.setdefault(mi.steer_type, []).append(mi)
         for g in groups.values():
             for s0 in range(0, len(g), 64):
-                D.map_tc_batch(g[s0:s0 + 64], precision=self.tc_precision)
-        bands = [mi.out.sum(0) for mi in insts]
-        host = [b.to('cpu', non_blocking=True) for b in bands]
+                D.map_tc_batch(g[s0:s0 + 64], precision=self.tc_precision, error_word=self._err)
+        for r in batch:
+            st = r.stream
+            torch.sum(st.out, 0, out=st.band)
+            st.h_band.copy_(st.band, non_blocking=True)
+        self._h_err.copy_(self._err, non_blocking=True)
+        t_maps = time.perf_counter()
         torch.cuda.current_stream(dev).synchronize()
         now = time.perf_counter()
-        for r, h in zip(batch, host):
+        self.batch_times.append((len(batch), t_taken, t_csm, t_maps, now))
+        if int(self._h_err[0]):
+            self._err.zero_()
+            msg = 'acb_map_tc_batch: a tensor-core pipeline wait timed out'
+            raise RuntimeError(msg)
+        for r in batch:
             r.t_done = now
-            r.future.set_result(h.numpy().reshape(r.stream.gshape))
+            r.future.latency = now - r.t_submit     # submit -> result ready, seconds
+            r.future.set_result(r.stream.h_band.numpy().reshape(r.stream.gshape).copy())
         self.batches.append(len(batch))
 
     def _run(self):

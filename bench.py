@@ -45,6 +45,10 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--bins', type=int, default=0, help='limit the number of map bins (profiling only)')
+    ap.add_argument('--workload', default='precision256',
+                    choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed'])
+    ap.add_argument('--tc-precision', default='bf16x3', choices=['bf16x3', 'tf32'])
+    ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     return ap.parse_args()
 
 
@@ -222,9 +226,213 @@ def cpu_baseline_sample(wl, steer):
                       f'(C/OpenMP port of the reference numba kernels, {ncores} threads)'}
 
 
+def _line(metric, value, unit, ms, args, config, **extra):
+    d = {'metric': metric, 'value': value, 'unit': unit, 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+         'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+         'data': 'synthetic (seeded monopoles)', 'config': config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def run_batched(args):
+    """64 uneven instances: per-instance CSM of 30 bins (complex64) + one batched tensor-core map."""
+    import torch
+
+    from acoular_b200 import workloads
+    from acoular_b200.batch import BatchPlan, Instance
+    dev = torch.device('cuda', 0)
+    wls = workloads.batched_instances()
+    insts = []
+    for wl in wls:
+        x = workloads.monopole_time_data_torch(wl, device=dev)
+        insts.append(Instance(samples=x, mpos=wl.mics.pos, gpos=wl.grid.pos, sample_freq=wl.fs,
+                              block_size=wl.block_size, bin_lo=int(wl.bins[0]), num_bins=len(wl.bins),
+                              precision='complex64'))
+    plan = BatchPlan(insts, tc_precision=args.tc_precision).capture()
+    for _ in range(args.warmup):
+        plan.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            plan.run()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    units = plan.units()
+    mics = sorted({int(w.mics.num_mics) for w in wls})
+    _line('batched maps grid-pts*bins/s (64 uneven instances, CSM + map, one CUDA graph)', units / (ms / 1e3),
+          UNIT, ms, args, {'workload': 'batched64', 'instances': len(wls), 'mics': mics,
+                           'grid_points': [int(w.grid.size) for w in wls][:8] + ['...'],
+                           'block_sizes': sorted({int(w.block_size) for w in wls}), 'bins_per_instance': 30,
+                           'csm': 'complex64', 'form': f'tc {args.tc_precision}'},
+          units_per_step=units, gpu_launches_per_step='1 graph', clocks=clk.summary(),
+          dtype=f'{args.tc_precision} / f32 accum')
+
+
+def run_large3d(args):
+    """1024-mic log spiral, 101x101x41 grid, 200 bins in 1-16 kHz, true location, r_diag.
+
+    The CSM of the 200 bins is computed once (in contiguous bin chunks, then gathered); the timed step
+    is the tensor-core map over all 200 bins and 418,241 grid points.
+    """
+    import torch
+
+    from acoular_b200 import device as D
+    from acoular_b200 import workloads
+    dev = torch.device('cuda', 0)
+    wl = workloads.large_3d()
+    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
+    bins = np.asarray(wl.bins)
+    nb = len(bins)
+    x = workloads.monopole_time_data_torch(wl, device=dev)
+    freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[: N // 2 + 1])
+    mpos, gpos = torch.as_tensor(wl.mics.pos, device=dev), torch.as_tensor(wl.grid.pos, device=dev)
+    k = torch.as_tensor(2 * np.pi * freqs[bins] / wl.c, device=dev)
+    c = torch.empty((nb, M, M), dtype=torch.complex128, device=dev)
+    t0 = time.perf_counter()
+    for j0 in range(0, nb, 40):
+        sel = bins[j0:j0 + 40]
+        part = D.calc_csm(x, N, wl.window, wl.overlap, 'complex128', bin_lo=int(sel[0]),
+                          num_bins=int(sel[-1] - sel[0] + 1))
+        c[j0:j0 + len(sel)] = part[torch.as_tensor(sel - sel[0], device=dev)]
+        del part
+    torch.cuda.synchronize()
+    csm_s = time.perf_counter() - t0
+    del x
+    out = torch.empty((nb, G), dtype=torch.float64, device=dev)
+    norm = M / (M - 1.0)
+
+    def step():
+        D.map_tc(c, k, mpos, gpos, 'true location', True, norm, out=out, precision=args.tc_precision)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # accuracy against the plain FP64 form on 3 bins (timed too: the TC/FP64 rate ratio on this shape)
+    sel = torch.as_tensor([0, nb // 2, nb - 1], device=dev)
+    cs, ks = c[sel].contiguous(), k[sel].contiguous()
+    D.map_f64(cs, ks, mpos, gpos, 'true location', True, norm)
+    torch.cuda.synchronize()
+    e0.record()
+    ref = D.map_f64(cs, ks, mpos, gpos, 'true location', True, norm)
+    e1.record()
+    torch.cuda.synchronize()
+    f64_rate = 3 * G / (e0.elapsed_time(e1) / 1e3)
+    ref = ref.cpu().numpy()
+    got = out[sel].cpu().numpy()
+    err = float((np.abs(got - ref) / np.abs(ref).max(axis=1, keepdims=True)).max())
+    rate = G * nb / (ms / 1e3)
+    _line('map grid-pts*bins/s (1024 mics, 101x101x41 grid, 200 bins)', rate, UNIT, ms, args,
+          {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': nb, 'block_size': N,
+           'steer_type': 'true location', 'r_diag': True, 'form': f'tc {args.tc_precision}',
+           'csm': 'complex128, computed once outside the timed map steps'},
+          accuracy={'max_rel_err_vs_f64': err, 'bins_checked': 3}, f64_form_rate=f64_rate,
+          tc_over_f64=rate / f64_rate, csm_seconds_once=csm_s, clocks=clk.summary(),
+          dtype=f'{args.tc_precision} / f32 accum')
+
+
+def run_serving(args, mixed: bool):
+    """Poisson arrivals from 32 streams, 0.1 s of 51.2 kHz samples per request, one third-octave band."""
+    import torch
+
+    from acoular_b200.microphones import disk_mics
+    from acoular_b200.serving import BeamformingServer
+    rng = np.random.RandomState(7)
+    n_streams = 32
+    srv = BeamformingServer(hbm_budget_bytes=120 << 30, tc_precision=args.tc_precision)
+    specs = []
+    for i in range(n_streams):
+        M = int(rng.choice([64, 128, 256, 512])) if mixed else 64
+        side = int(rng.randint(41, 202))
+        z = float(rng.uniform(-2.0, -0.3))
+        g = np.linspace(-1.0, 1.0, side)
+        gx, gy = np.meshgrid(g, g, indexing='ij')
+        gpos = np.vstack([gx.ravel(), gy.ravel(), np.full(side * side, z)])
+        N = int(rng.choice([256, 512, 1024]))
+        while True:   # a third-octave band in 0.5-16 kHz that holds at least one FFT line
+            fc = float(np.exp(rng.uniform(np.log(500.0), np.log(16000.0))))
+            fr = np.abs(np.fft.fftfreq(N, 1 / 51200.0)[: N // 2 + 1])
+            if np.searchsorted(fr, fc * 2 ** (-1 / 6)) < np.searchsorted(fr, fc * 2 ** (1 / 6)):
+                break
+        mpos = disk_mics(M, 0.5, seed=1000 + i).pos
+        srv.open_stream(i, mpos, gpos, 51200.0, N, (fc, 3), gshape=(side, side))
+        specs.append((M, side, N, fc))
+    blocks = {i: rng.randn(5120, specs[i][0]).astype(np.float32) for i in range(n_streams)}
+    # warm-up: one request per stream
+    for f in [srv.submit(i, blocks[i]) for i in range(n_streams)]:
+        f.result(timeout=120)
+    torch.cuda.synchronize()
+    import gc
+    gc_pauses = []
+
+    def _gc_cb(phase, info, _t=[0.0]):
+        if phase == 'start':
+            _t[0] = time.perf_counter()
+        else:
+            gc_pauses.append((info['generation'], (time.perf_counter() - _t[0]) * 1e3))
+    gc.callbacks.append(_gc_cb)
+    if os.environ.get('ACB_BENCH_GC_FREEZE') == '1':
+        gc.freeze()
+    rate = 10.0 * n_streams            # real time: each stream sends 0.1 s of data every 0.1 s
+    t_end = time.perf_counter() + args.duration
+    futs = []
+    t_next = time.perf_counter()
+    with ClockSampler(0) as clk:
+        while t_next < t_end:
+            t_next += rng.exponential(1.0 / rate)
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            sid = int(rng.randint(n_streams))
+            t0 = time.perf_counter()
+            futs.append((t0, srv.submit(sid, blocks[sid])))
+        for _, f in futs:
+            f.result(timeout=120)
+    srv.close()
+    lat = np.array([f.latency for _, f in futs]) * 1e3
+    bt = np.array([b for b in srv.batch_times if b[1] >= futs[0][0]]) if futs else np.zeros((0, 5))
+    if len(bt):
+        dur = (bt[:, 4] - bt[:, 1]) * 1e3
+        top = np.argsort(dur)[-5:][::-1]
+        print('slowest batches (n, inputs+csm issue ms, map issue ms, gpu wait ms):',
+              [(int(bt[i, 0]), round((bt[i, 2] - bt[i, 1]) * 1e3, 2), round((bt[i, 3] - bt[i, 2]) * 1e3, 2),
+                round((bt[i, 4] - bt[i, 3]) * 1e3, 2)) for i in top], file=sys.stderr)
+        gaps = np.diff(bt[:, 1]) * 1e3
+        g2 = [ms for g, ms in gc_pauses if g == 2]
+        print(f'gc: {len(gc_pauses)} collections, gen2 {len(g2)} totalling {sum(g2):.1f} ms (max '
+              f'{max(g2) if g2 else 0:.1f} ms); max any {max((m for _, m in gc_pauses), default=0):.1f} ms',
+              file=sys.stderr)
+        print('largest gaps between batch starts (ms):', np.sort(gaps)[-5:].round(2).tolist(), file=sys.stderr)
+    n = len(futs)
+    _line('serving latency p50/p99 ms (Poisson arrivals, 32 streams, 0.1 s requests, one third-octave band)',
+          float(np.percentile(lat, 99)), 'ms (p99)', float(np.percentile(lat, 50)), args,
+          {'workload': 'serving-mixed' if mixed else 'serving-64mic', 'streams': n_streams,
+           'mics': sorted({s[0] for s in specs}), 'grid_sides': [min(s[1] for s in specs), max(s[1] for s in specs)],
+           'block_sizes': sorted({s[2] for s in specs}), 'offered_rate_req_s': rate, 'duration_s': args.duration},
+          higher_is_better=False, p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
+          max_ms=float(lat.max()), requests=n, mean_batch=float(np.mean(srv.batches)) if srv.batches else None,
+          clocks=clk.summary(), dtype=f'{args.tc_precision} / f32 accum')
+
+
 def main():
     args = parse()
     from acoular_b200 import workloads
+    if args.workload == 'batched64':
+        return run_batched(args)
+    if args.workload == 'large3d':
+        return run_large3d(args)
+    if args.workload in ('serving', 'serving-mixed'):
+        return run_serving(args, args.workload == 'serving-mixed')
     wl = workloads.precision_256()
     if args.impl == 'reference':
         return run_reference(args, wl)
