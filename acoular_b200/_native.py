@@ -48,6 +48,8 @@ class MapParams(ctypes.Structure):
         ('glibc_faithful', ctypes.c_int),
         ('sincos_table', ctypes.c_void_p),
         ('sincos_table_slots', ctypes.c_int64),
+        ('tc_pass_chunks', ctypes.c_int),
+        ('tc_splits', ctypes.c_int),
     ]
 
 

@@ -11,7 +11,12 @@
 // the epilogue dots them with v_i while v_i is still in the synthesising thread's registers.
 // Steering vectors are never re-synthesised and about half of the dense GEMM is skipped.
 //
-// Per CTA: 128 grid points (UMMA M = 128, one TMEM lane each) x one frequency bin.
+// Work item: 128 grid points (UMMA M = 128, one TMEM lane each) x one frequency bin x one group of
+// column passes.  The accumulator columns of an item are covered in passes of `pw` chunks (a
+// runtime tile width: 4, 8 or 16 chunks = 128, 256 or 512 TMEM columns); with `splits` > 1 the
+// passes of one (bin, tile) are shared among several items whose partial sums (B and the
+// normalisation sum S are both additive over chunks) are combined by the last item to finish, in
+// split order, before the steering-type normalisation.
 //   warp 0      : bulk copies of the R' tiles of chunk i (pre-laid in HBM in the shared-memory
 //                 core-matrix order by tc_prep_kernel) into a 32-tile ring, running ahead of the MMAs
 //   warp 1      : TMEM allocation; one thread issues tcgen05.mma (A = steering chunk, B = R'
@@ -37,7 +42,8 @@ namespace acb {
 constexpr int TC_ROWS = 128;
 constexpr int TC_CHUNK = 32;               // real components per chunk
 constexpr int TC_MPC = TC_CHUNK / 2;       // mics per chunk
-constexpr int TC_PASS_CHUNKS = 16;         // accumulator chunks per column pass (512 TMEM columns)
+constexpr int TC_PASS_CHUNKS = 16;         // widest column pass (512 TMEM columns), the default
+constexpr int TC_MAX_SPLIT = 8;            // pass groups per (bin, tile)
 constexpr int TC_MAX_MICS = 2048;          // mic positions live in shared memory
 constexpr int TC_TILE_ELEMS = TC_CHUNK * TC_CHUNK;
 constexpr int TC_TILE_BYTES = TC_TILE_ELEMS * 2;          // bf16
@@ -75,7 +81,31 @@ struct TcInst {
     double *out_norm;          // [nbins][G] or null
     const __nv_bfloat16 *rh, *rl;   // split-BF16 R' tiles, bin_stride elements per bin
     int64_t bin_stride;
+    int pw, P, splits;         // pass width (chunks), passes per (bin, tile), pass groups
+    uint8_t sp0[TC_MAX_SPLIT + 1];  // pass group s covers passes [sp0[s], sp0[s+1])
+    double2 *part;             // [nbins * ntiles][splits][128] partial (B, S) when splits > 1
+    int *cnt;                  // [nbins * ntiles][4] finished groups per epilogue warp (zeroed per launch)
 };
+
+// Position of a work item inside its instance: items run (bin, tile, group) with the group fastest.
+struct TcItem {
+    int64_t base;              // bin * ntiles + tile
+    int bin, split, pa, pz;    // passes [pa, pz)
+    int64_t tile;
+};
+
+__device__ __forceinline__ TcItem decode_item(const TcInst &in, int64_t item)
+{
+    TcItem t;
+    const int64_t local = item - in.item_off;
+    t.split = (int)(local % in.splits);
+    t.base = local / in.splits;
+    t.bin = (int)(t.base / in.ntiles);
+    t.tile = t.base % in.ntiles;
+    t.pa = in.sp0[t.split];
+    t.pz = in.sp0[t.split + 1];
+    return t;
+}
 
 constexpr int TC_MAX_INST = 64;
 
@@ -276,12 +306,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             for (int64_t li = 0; li < nmine && ok; ++li) {
                 const int64_t item = blockIdx.x + li * gridDim.x;
                 const TcInst &in = b.inst[find_inst(b, item)];
-                const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
-                const int64_t bin = (item - in.item_off) / in.ntiles;
+                const TcItem it = decode_item(in, item);
+                const int C = in.C, pw = in.pw;
+                const int64_t bin = it.bin;
                 const __nv_bfloat16 *bh = in.rh + (TF32 ? 2 : 1) * bin * in.bin_stride;
                 const __nv_bfloat16 *bl = in.rl + bin * in.bin_stride;
-                for (int pp = 0; pp < P && ok; ++pp) {
-                    const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+                for (int pp = it.pa; pp < it.pz && ok; ++pp) {
+                    const int jb = pp * pw, je = min(C, jb + pw);
                     for (int i = 0; i < je && ok; ++i, ++T) {
                         const int j0 = max(i, jb), n = je - j0;
                         // step barriers form a ring of TC_NB: step T - TC_NB must be complete; ring
@@ -350,18 +381,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             for (int64_t li = 0; li < nmine && ok; ++li) {
                 const int64_t item = blockIdx.x + li * gridDim.x;
                 const int ii = find_inst(b, item);
-                const int C = b.inst[ii].C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+                const TcItem it = decode_item(b.inst[ii], item);
+                const int C = b.inst[ii].C, pw = b.inst[ii].pw;
                 if (ii != cur_inst) {
                     if (W > 0)
                         ok = tc::mbar_wait(&tfree[(W - 1) & (TC_NB - 1)], (uint32_t)(((W - 1) / TC_NB) & 1), abort_flag,
                                            b.wait_limit_ns);
-                    width = TC_CHUNK * min(C, TC_PASS_CHUNKS);
+                    width = TC_CHUNK * min(C, pw);
                     wpt = min(TC_NB, 512 / width);
                     w_start = W;
                     cur_inst = ii;
                 }
-                for (int pp = 0; pp < P && ok; ++pp, ++W) {
-                    const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+                for (int pp = it.pa; pp < it.pz && ok; ++pp, ++W) {
+                    const int jb = pp * pw, je = min(C, jb + pw);
                     if (W - w_start >= wpt)
                         ok = tc::mbar_wait(&tfree[(W - wpt) & (TC_NB - 1)], (uint32_t)(((W - wpt) / TC_NB) & 1),
                                            abort_flag, b.wait_limit_ns);
@@ -436,18 +468,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             const int64_t item = blockIdx.x + li * gridDim.x;
             const int ii = find_inst(b, item);
             const TcInst &in = b.inst[ii];
-            const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
+            const TcItem it = decode_item(in, item);
+            const int C = in.C, pw = in.pw;
             if (ii != cur_inst) {
-                width = TC_CHUNK * min(C, TC_PASS_CHUNKS);
+                width = TC_CHUNK * min(C, pw);
                 wpt = min(TC_NB, 512 / width);
                 w_start = W;
                 cur_inst = ii;
             }
-            const int bin = (int)((item - in.item_off) / in.ntiles);
-            const int64_t g = ((item - in.item_off) % in.ntiles) * TC_ROWS + row;
+            const int bin = it.bin;
+            const int64_t g = it.tile * TC_ROWS + row;
             double acc = 0.0;
-            for (int pp = 0; pp < P && ok; ++pp, ++W) {
-                const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+            for (int pp = it.pa; pp < it.pz && ok; ++pp, ++W) {
+                const int jb = pp * pw, je = min(C, jb + pw);
                 const uint32_t wcol = lane_addr + (uint32_t)(((W - w_start) % wpt) * width);
                 for (int i = 0; i < je; ++i, ++T) {
                     ok = __all_sync(0xffffffffu, tc::mbar_wait(&done[T & (TC_NB - 1)], (uint32_t)((T / TC_NB) & 1),
@@ -500,14 +533,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             ok = __all_sync(0xffffffffu, tc::mbar_wait(&s_ready[li & 1], (uint32_t)((li >> 1) & 1), abort_flag,
                                                        b.wait_limit_ns));
             if (!ok) break;
-            if (g < in.G) {
-                const double *rs = red + (li & 1) * TC_PARTS * TC_ROWS;
-                double S = 0.0;
+            const double *rs = red + (li & 1) * TC_PARTS * TC_ROWS;
+            double S = 0.0;
 #pragma unroll
-                for (int pp = 0; pp < TC_PARTS; ++pp) S += rs[pp * TC_ROWS + row];
+            for (int pp = 0; pp < TC_PARTS; ++pp) S += rs[pp * TC_ROWS + row];
+            if (in.splits > 1) {
+                // publish this group's partial sums; the last group of the (bin, tile) to finish
+                // adds all groups' partials in group order and writes the map
+                // (per warp: a warp's 32 rows are counted on their own, so no barrier spans warps)
+                double2 *pb = in.part + it.base * in.splits * TC_ROWS;
+                pb[it.split * TC_ROWS + row] = make_double2(acc, S);
+                __threadfence();
+                __syncwarp();
+                int last = 0;
+                if (lane == 0) last = atomicAdd(&in.cnt[it.base * 4 + q], 1) == in.splits - 1;
+                last = __shfl_sync(0xffffffffu, last, 0);
+                if (!last) continue;
+                __threadfence();
+                acc = 0.0;
+                S = 0.0;
+                for (int s = 0; s < in.splits; ++s) {
+                    const double2 v = __ldcg(pb + s * TC_ROWS + row);
+                    acc += v.x;
+                    S += v.y;
+                }
+            }
+            if (g < in.G)
                 finish_point<ST>(in, acc, S, in.gpos[g], in.gpos[in.G + g], in.gpos[2 * in.G + g], bin, g, in.out,
                                  in.out_norm);
-            }
         }
     } else {
         // ---------------- steering synthesis (warps 6..21) ----------------
@@ -537,9 +590,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
                 cur_inst = ii;
             }
-            const int C = in.C, P = (C + TC_PASS_CHUNKS - 1) / TC_PASS_CHUNKS;
-            const int bin = (int)((item - in.item_off) / in.ntiles);
-            const int64_t g = ((item - in.item_off) % in.ntiles) * TC_ROWS + row;
+            const TcItem it = decode_item(in, item);
+            const int C = in.C, pw = in.pw;
+            const int bin = it.bin;
+            const int64_t g = it.tile * TC_ROWS + row;
             const bool gvalid = g < in.G;
             float gxf = 0.f, gyf = 0.f, gzf = 0.f;
             if (gvalid) {
@@ -550,8 +604,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             const double k = in.k[bin];
             const float khi = (float)k, klo = (float)(k - (double)khi);
             double S = 0.0;
-            for (int pp = 0; pp < P && ok; ++pp) {
-                const int jb = pp * TC_PASS_CHUNKS, je = min(C, jb + TC_PASS_CHUNKS);
+            for (int pp = it.pa; pp < it.pz && ok; ++pp) {
+                const int jb = pp * pw, je = min(C, jb + pw);
                 for (int t = 0; t < je; ++t, ++T) {
                     if (T >= TC_ASTAGES) {
                         // the A stage is free once the epilogue of step T - 3 has released it
@@ -666,7 +720,77 @@ static int tc_fill_inst(const acb_map_params *p, const void *csm, const double *
     in.bin_stride = (int64_t)tri_tiles(in.C) * TC_TILE_ELEMS;
     in.rh = ws;
     in.rl = ws + (size_t)p->num_bins * in.bin_stride;
+    const int pw = p->tc_pass_chunks;
+    if (pw != 0 && pw != 4 && pw != 8 && pw != 16) return ACB_ERR_ARG;
+    if (p->tc_splits < 0) return ACB_ERR_ARG;
+    in.pw = pw ? pw : TC_PASS_CHUNKS;
+    in.P = (in.C + in.pw - 1) / in.pw;
+    in.splits = 1;
+    in.sp0[0] = 0;
+    in.sp0[1] = (uint8_t)in.P;
+    in.part = nullptr;
+    in.cnt = nullptr;
     return ACB_OK;
+}
+
+// Split the passes [0, P) of an instance into `splits` contiguous groups of balanced cost.  Cost of
+// pass p in units of one R' tile step: its MMA tiles sum_{j in pass} (j + 1) plus its steering
+// synthesis (chunks 0 .. je-1), weighted 2 tiles per chunk.
+static void tc_split_passes(TcInst &in, int splits)
+{
+    const int P = in.P;
+    if (splits > P) splits = P;
+    if (splits > TC_MAX_SPLIT) splits = TC_MAX_SPLIT;
+    if (splits < 1) splits = 1;
+    double cost[TC_MAX_MICS / TC_MPC + 1];
+    for (int pp = 0; pp < P; ++pp) {
+        const int jb = pp * in.pw, je = in.C < jb + in.pw ? in.C : jb + in.pw;
+        double c = 2.0 * je;
+        for (int j = jb; j < je; ++j) c += j + 1;
+        cost[pp] = c;
+    }
+    // minimise the largest group cost: dp[s][e] = best max over the first e passes in s groups
+    static thread_local double dp[TC_MAX_SPLIT + 1][TC_MAX_MICS / TC_MPC + 1];
+    static thread_local int cut[TC_MAX_SPLIT + 1][TC_MAX_MICS / TC_MPC + 1];
+    double pre[TC_MAX_MICS / TC_MPC + 2];
+    pre[0] = 0.0;
+    for (int pp = 0; pp < P; ++pp) pre[pp + 1] = pre[pp] + cost[pp];
+    for (int e = 0; e <= P; ++e) dp[1][e] = pre[e];
+    for (int sgrp = 2; sgrp <= splits; ++sgrp)
+        for (int e = sgrp; e <= P; ++e) {
+            dp[sgrp][e] = 1e300;
+            for (int c = sgrp - 1; c < e; ++c) {
+                const double v = dp[sgrp - 1][c] > pre[e] - pre[c] ? dp[sgrp - 1][c] : pre[e] - pre[c];
+                if (v < dp[sgrp][e]) {
+                    dp[sgrp][e] = v;
+                    cut[sgrp][e] = c;
+                }
+            }
+        }
+    in.splits = splits;
+    int e = P;
+    in.sp0[splits] = (uint8_t)P;
+    for (int sgrp = splits; sgrp >= 2; --sgrp) {
+        e = cut[sgrp][e];
+        in.sp0[sgrp - 1] = (uint8_t)e;
+    }
+    in.sp0[0] = 0;
+}
+
+static inline size_t round256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Workspace of one batch instance: R' tiles, then (when split) the partial sums and group counters.
+static size_t tc_inst_ws_bytes(const acb_map_params &p, int precision)
+{
+    const size_t r = acb_map_tc_workspace_bytes(p.num_mics, p.num_bins, precision);
+    if (r == 0) return 0;
+    size_t tot = round256(r);
+    if (p.tc_splits > 1) {
+        const int64_t nbase = (int64_t)p.num_bins * ((p.num_grid + TC_ROWS - 1) / TC_ROWS);
+        tot += round256((size_t)nbase * TC_MAX_SPLIT * TC_ROWS * sizeof(double2));
+        tot += round256((size_t)nbase * 4 * sizeof(int));
+    }
+    return tot;
 }
 
 // Launch the R' preparation of every instance and the persistent map kernel over the batch.
@@ -676,6 +800,13 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
     int mp_max = 16;
     for (int i = 0; i < bt.n_inst; ++i) {
         const TcInst &in = bt.inst[i];
+        if (in.splits > 1) {
+            const cudaError_t e = cudaMemsetAsync(in.cnt, 0, (size_t)in.nbins * in.ntiles * 4 * sizeof(int), s);
+            if (e != cudaSuccess) {
+                set_cuda_error(e);
+                return ACB_ERR_CUDA;
+            }
+        }
         auto prep = precision == ACB_TC_TF32 ? tc_prep_kernel<true> : tc_prep_kernel<false>;
         prep<<<dim3(tri_tiles(in.C), in.nbins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csms[i]), in.M, in.C,
                                                             params[i]->r_diag, in.bin_stride,
@@ -743,9 +874,9 @@ size_t acb_map_tc_batch_workspace_bytes(const acb_map_params *params, int num_in
     if (!params || num_instances <= 0) return 0;
     size_t tot = 0;
     for (int i = 0; i < num_instances; ++i) {
-        const size_t b = acb_map_tc_workspace_bytes(params[i].num_mics, params[i].num_bins, precision);
+        const size_t b = tc_inst_ws_bytes(params[i], precision);
         if (b == 0) return 0;
-        tot += (b + 255) / 256 * 256;
+        tot += b;
     }
     return tot;
 }
@@ -768,11 +899,19 @@ int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num
     const void *cc[TC_MAX_INST];
     for (int i = 0; i < num_instances; ++i) {
         if (params[i].steer_type != steer) return ACB_ERR_ARG;   // one steering type per launch
+        TcInst &in = bt.inst[i];
         const int st = tc_fill_inst(&params[i], io[i].csm, io[i].wavenumber, io[i].mpos, io[i].gpos, io[i].out_map,
-                                    io[i].out_steer_norm, reinterpret_cast<__nv_bfloat16 *>(w), items, bt.inst[i]);
+                                    io[i].out_steer_norm, reinterpret_cast<__nv_bfloat16 *>(w), items, in);
         if (st) return st;
-        items += bt.inst[i].ntiles * bt.inst[i].nbins;
-        w += (acb_map_tc_workspace_bytes(params[i].num_mics, params[i].num_bins, precision) + 255) / 256 * 256;
+        if (params[i].tc_splits > 1) {
+            tc_split_passes(in, params[i].tc_splits);
+            const size_t r = round256(acb_map_tc_workspace_bytes(params[i].num_mics, params[i].num_bins, precision));
+            const int64_t nbase = (int64_t)in.nbins * in.ntiles;
+            in.part = reinterpret_cast<double2 *>(w + r);
+            in.cnt = reinterpret_cast<int *>(w + r + round256((size_t)nbase * TC_MAX_SPLIT * TC_ROWS * sizeof(double2)));
+        }
+        items += in.ntiles * in.nbins * in.splits;
+        w += tc_inst_ws_bytes(params[i], precision);
         pp[i] = &params[i];
         cc[i] = io[i].csm;
     }

@@ -202,8 +202,10 @@ def sincos_table_device(device) -> torch.Tensor:
 # map
 # ------------------------------------------------------------------------------------------------
 def map_params(num_mics, num_grid, num_bins, steer_type, r_diag, norm, clip_negative=None, ref=None,
-               glibc_faithful=False, device=None) -> N.MapParams:
+               glibc_faithful=False, device=None, tc_pass_chunks: int = 0, tc_splits: int = 0) -> N.MapParams:
     p = N.MapParams()
+    p.tc_pass_chunks = int(tc_pass_chunks)
+    p.tc_splits = int(tc_splits)
     p.num_mics = int(num_mics)
     p.num_grid = int(num_grid)
     p.num_bins = int(num_bins)
@@ -265,8 +267,18 @@ def map_tc_workspace(num_mics: int, num_bins: int, precision: str, device) -> to
 def map_tc(csm: torch.Tensor, wavenumbers: torch.Tensor, mpos: torch.Tensor, gpos: torch.Tensor, steer_type: str,
            r_diag: bool, norm: float, ref=None, clip_negative=None, precision: str = 'bf16x3',
            out: torch.Tensor | None = None, steer_norm: torch.Tensor | None = None,
-           error_word: torch.Tensor | None = None) -> torch.Tensor:
-    """Tensor-core map for B bins (same contract as :func:`map_f64`)."""
+           error_word: torch.Tensor | None = None, tuning='auto') -> torch.Tensor:
+    """Tensor-core map for B bins (same contract as :func:`map_f64`).
+
+    ``tuning``: ``'auto'`` (the autotuned (pass width, split) of this shape class, through the batch
+    entry, so the result equals the one the same instance gets inside any batch), ``None`` (the
+    single-instance entry ``acb_map_tc`` with the default tile and no split), or an explicit
+    ``(pass_chunks, splits)``.
+    """
+    if tuning is not None:
+        mi = MapInstance(csm, wavenumbers, mpos, gpos, steer_type, r_diag, norm, ref=ref, clip_negative=clip_negative,
+                         out=out, steer_norm=steer_norm, tuning=None if tuning == 'auto' else tuning)
+        return map_tc_batch([mi], precision=precision, error_word=error_word)[0]
     B, M, _ = csm.shape
     G = gpos.shape[1]
     dev = csm.device
@@ -285,7 +297,8 @@ class MapInstance:
     the output (B, G) and the beamformer settings."""
 
     def __init__(self, csm, wavenumbers, mpos, gpos, steer_type='true level', r_diag=True, norm=1.0, ref=None,
-                 clip_negative=None, out=None, steer_norm=None):
+                 clip_negative=None, out=None, steer_norm=None, tuning=None):
+        self.tuning = tuning            # (pass_chunks, splits) or None: the autotuned value
         self.csm, self.wavenumbers, self.mpos, self.gpos = csm, wavenumbers, mpos, gpos
         self.steer_type, self.r_diag, self.norm, self.ref = steer_type, r_diag, norm, ref
         self.clip_negative = clip_negative
@@ -306,10 +319,13 @@ def map_tc_batch(instances, precision: str = 'bf16x3', error_word: torch.Tensor 
     n = len(instances)
     params = (N.MapParams * n)()
     io = (N.MapIO * n)()
+    from . import autotune
     for i, it in enumerate(instances):
         B, M, _ = it.csm.shape
-        params[i] = map_params(M, it.gpos.shape[1], B, it.steer_type, it.r_diag, it.norm, it.clip_negative, it.ref,
-                               False, dev)
+        G = it.gpos.shape[1]
+        pw, sp = it.tuning if it.tuning is not None else autotune.lookup(M, G, B, precision)
+        params[i] = map_params(M, G, B, it.steer_type, it.r_diag, it.norm, it.clip_negative, it.ref,
+                               False, dev, tc_pass_chunks=pw, tc_splits=sp)
         io[i].csm, io[i].wavenumber = it.csm.data_ptr(), it.wavenumbers.data_ptr()
         io[i].mpos, io[i].gpos = it.mpos.data_ptr(), it.gpos.data_ptr()
         io[i].out_map, io[i].out_steer_norm = it.out.data_ptr(), N.ptr(it.steer_norm)

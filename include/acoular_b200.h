@@ -102,6 +102,11 @@ typedef struct acb_map_params {
     int glibc_faithful;      /* 1: apply the sincos exception table (plain form only)        */
     const uint64_t *sincos_table; /* device hash table from acb_sincos_table_build_host      */
     int64_t sincos_table_slots;   /* power of two                                           */
+    /* tensor-core form only (0 = default); no counterpart in the reference:                    */
+    int tc_pass_chunks;      /* accumulator width per column pass, in 16-mic chunks: 4, 8 or 16 */
+    int tc_splits;           /* CTAs sharing one (bin, 128-point tile): its column passes are   *
+                              * split into this many groups whose partial sums are combined in  *
+                              * a fixed order (batch entry only; acb_map_tc runs unsplit)       */
 } acb_map_params;
 
 /* Plain FP64 form of _freqBeamformer_FullCSM (acoular/fastFuncs.py:217-311), batched over bins:

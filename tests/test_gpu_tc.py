@@ -177,3 +177,54 @@ def test_tf32_form_vs_oracle(M, G, steer):
         got = _tc(csm, freqs, mpos, gpos, steer, r_diag, precision='tf32')
         for b in range(len(freqs)):
             assert rel(got[b], ref[b]) <= TOL, (b, rel(got[b], ref[b]))
+
+
+@pytest.mark.parametrize('M,G,steer', [(40, 700, 'true level'), (256, 300, 'true location'), (600, 260, 'inverse'),
+                                       (1100, 130, 'classic')])
+def test_tc_tile_width_and_split_agree(M, G, steer):
+    """Every (pass width, split) candidate gives the default schedule's map (FP64 partial-sum order
+    differs only), and the single-instance entry (acb_map_tc) gives it too."""
+    from acoular_b200 import autotune
+    from acoular_b200 import device as D
+    dev = torch.device('cuda')
+    mpos, gpos, freqs, csm = _case(M, G, seed=M + 5 * G)
+    args = (torch.as_tensor(csm, device=dev), torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
+            torch.as_tensor(mpos, device=dev), torch.as_tensor(np.ascontiguousarray(gpos), device=dev), steer, True,
+            O.sig_loss_norm(True, M))
+    base = D.map_tc(*args, clip_negative=True, tuning=(16, 1)).cpu().numpy()
+    single = D.map_tc(*args, clip_negative=True, tuning=None).cpu().numpy()
+    assert np.array_equal(single, base)
+    cands = autotune.candidates(M)
+    assert len(cands) >= (3 if M > 64 else 1)
+    for pw, sp in cands:
+        got = D.map_tc(*args, clip_negative=True, tuning=(pw, sp)).cpu().numpy()
+        assert rel(got, base) <= 1e-12, (pw, sp)
+    ref = O.beamformer_calc(csm, freqs, range(len(freqs)), O.apparent_r(gpos), O.apparent_r(gpos, mpos), 343.0, steer,
+                            True)
+    assert rel(base, ref) <= TOL
+
+
+def test_tc_split_graph_replay_and_mix():
+    """Split instances replay in a CUDA graph (group counters are reset by every launch) and give the
+    same map inside a batch with unsplit instances."""
+    from acoular_b200 import device as D
+    inst = _instances([(600, 700, 2), (64, 3000, 3), (300, 500, 2)], seed=11)
+    its = [i for i, _ in inst]
+    its[0].tuning, its[1].tuning, its[2].tuning = (4, 8), (16, 1), (8, 2)
+    alone = []
+    for it in its:
+        D.map_tc_batch([it])
+        alone.append(it.out.clone())
+    D.map_tc_batch(its)
+    torch.cuda.synchronize()
+    for it, a in zip(its, alone):
+        assert torch.equal(it.out, a)
+        it.out.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        D.map_tc_batch(its)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    for it, a in zip(its, alone):
+        assert torch.equal(it.out, a)

@@ -1,6 +1,7 @@
 """CPU tests: the C-ABI library loads and exports its header, and the host-side mirror logic."""
 
 import ctypes
+import json
 
 import numpy as np
 import pytest
@@ -156,3 +157,44 @@ def test_l_p_and_integrate():
     assert ac.integrate(data, g, (-1, -1, 0, 0)) == data.reshape(3, 3)[0:2, 0:2].sum()
     h = ac.integrate(np.vstack([data, 2 * data]), g, (0, 0, 1, 1))
     assert np.array_equal(h, [data.reshape(3, 3)[1:, 1:].sum(), 2 * data.reshape(3, 3)[1:, 1:].sum()])
+
+
+def test_autotune_classes_and_lookup(tmp_path):
+    from acoular_b200 import autotune as A
+    assert A.mic_bucket(2) == 32 and A.mic_bucket(33) == 64 and A.mic_bucket(1024) == 1024
+    assert A.mic_bucket(5000) == 2048
+    assert A.item_bucket(128 * 37, 1) == 'tiny' and A.item_bucket(128 * 38, 1) == 'few'
+    assert A.item_bucket(128 * 148, 1) == 'few' and A.item_bucket(128 * 149, 1) == 'mid'
+    assert A.item_bucket(160801, 513) == 'many'
+    # candidates: distinct schedules only, splits never above the pass count
+    for M in (2, 40, 256, 600, 2048):
+        C = (M + 15) // 16
+        cands = A.candidates(M)
+        assert (16, 1) in cands or (C <= 4 and cands[0][1] == 1)
+        for pw, sp in cands:
+            assert pw in A.PASS_CHUNKS and 1 <= sp <= -(-C // pw)
+    assert A.candidates(32) == [(4, 1)]
+    # missing table -> default; a table entry is honoured; an invalid one falls back
+    missing = tmp_path / 'none.json'
+    assert A.lookup(256, 160801, 513, 'bf16x3', path=missing) == A.DEFAULT
+    t = tmp_path / 't.json'
+    key = A.shape_class(600, 1000, 2, 'tf32')
+    t.write_text(json.dumps({'classes': {key: {'pass_chunks': 8, 'splits': 4}}}))
+    assert A.lookup(600, 1000, 2, 'tf32', path=t) == (8, 4)
+    t2 = tmp_path / 't2.json'
+    t2.write_text(json.dumps({'classes': {key: {'pass_chunks': 8, 'splits': 8}}}))   # 5 passes < 8
+    assert A.lookup(600, 1000, 2, 'tf32', path=t2) == A.DEFAULT
+
+
+def test_committed_tuning_table_is_valid():
+    from acoular_b200 import autotune as A
+    if not A.TABLE_PATH.exists():
+        pytest.skip('no tuning table')
+    tab = json.loads(A.TABLE_PATH.read_text())
+    assert tab['classes']
+    for key, ent in tab['classes'].items():
+        prec, mb, ib = key.split(':')
+        M = int(mb[1:])
+        assert prec in ('bf16x3', 'tf32') and ib in ('tiny', 'few', 'mid', 'many')
+        assert (ent['pass_chunks'], ent['splits']) in A.candidates(M)
+        assert ent['ms'] == min(ent['candidates_ms'].values())
