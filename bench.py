@@ -32,6 +32,9 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = 'map grid-pts*bins/s (CSM + map, 256 mics, 401x401 grid, 513 bins)'
 UNIT = 'grid-pts*bins/s'
+# DRAM bytes of one tensor-core map launch per bin of the 256-mic workload (ncu capture of 4 bins:
+# dram__bytes_read.sum + dram__bytes_write.sum, divided by 4)
+TC_TRAFFIC_PER_BIN = 1.54e6
 
 
 def parse():
@@ -47,7 +50,7 @@ def parse():
     ap.add_argument('--bins', type=int, default=0, help='limit the number of map bins (profiling only)')
     ap.add_argument('--workload', default='precision256',
                     choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed'])
-    ap.add_argument('--tc-precision', default='bf16x3', choices=['bf16x3', 'tf32'])
+    ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     return ap.parse_args()
 
@@ -136,6 +139,32 @@ def peaks():
         return {'hbm_gbs': d.get('hbm_gbs', 6650.0), 'bf16_tflops': d.get('bf16_tflops', 1590.0),
                 'bf16_tflops_sustained': d.get('bf16_tflops_sustained', 1400.0), 'source': 'measured'}
     return {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0, 'bf16_tflops_sustained': 1400.0, 'source': 'fallback'}
+
+
+def gemm_peaks(dev, n: int = 8192) -> dict:
+    """FP64 (DGEMM) and TF32 (FP32 GEMM with TF32 math) cuBLAS throughput measured here over about half a
+    second each (the map launches it is compared with run ~0.1 s): the denominators of the plain form's and
+    of the TF32 form's roofline (the peak file holds HBM and BF16 only)."""
+    import torch
+    out = {}
+    for name, dt, tf32, reps in (('fp64_tflops', torch.float64, False, 16), ('tf32_tflops', torch.float32, True, 400)):
+        prev = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn((n, n), dtype=dt, device=dev)
+        b = torch.randn((n, n), dtype=dt, device=dev)
+        c = a @ b
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = 2.0 * n ** 3 * reps / (e0.elapsed_time(e1) / 1e3) / 1e12
+        torch.backends.cuda.matmul.allow_tf32 = prev
+        del a, b, c
+    out['how'] = f'torch.matmul {n}x{n}x{n}, 16 (FP64) / 400 (TF32) back-to-back reps, CUDA events, this run'
+    return out
 
 
 def run_reference(args, wl):
@@ -465,9 +494,13 @@ def main():
     _, weight = D.window_vector('Hanning', N, dev)
     scale = 2.0 / N / weight / D.num_blocks(wl.num_samples, N, 2)
     ev_map = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    map_ms = []
+    ev_csm = torch.cuda.Event(enable_timing=True)
+    map_ms, csm_ms = [], []
+    prec = args.tc_precision
 
     def step(record=False):
+        if record:
+            ev_csm.record()
         csm_up.zero_()
         D.csm_upper_accumulate(samples, N, 'Hanning', '50%', csm_upper=csm_up, workspace=workspace,
                                max_workspace_bytes=ws_bytes)
@@ -478,7 +511,7 @@ def main():
         if form == 'f64':
             D.map_f64(c, kvec, mpos, gpos, args.steer, True, norm, out=out)
         else:
-            D.map_tc(c, kvec, mpos, gpos, args.steer, True, norm, out=out)
+            D.map_tc(c, kvec, mpos, gpos, args.steer, True, norm, out=out, precision=prec)
         if record:
             ev_map[1].record()
 
@@ -494,6 +527,7 @@ def main():
             step(record=True)
             ev_map[1].synchronize()
             map_ms.append(ev_map[0].elapsed_time(ev_map[1]))
+            csm_ms.append(ev_csm.elapsed_time(ev_map[0]))
         e1.record()
         torch.cuda.synchronize()
     barrier(ws)
@@ -503,36 +537,73 @@ def main():
     units = float(G) * nbins
     value = units * ws / (ms / 1e3)
 
-    # accuracy of the timed form against the plain FP64 form on a spread of bins
+    # the forms side by side on the same CSM: both tensor-core precisions over all bins, and the plain
+    # FP64 form on a spread of 6 bins (its rate per grid-pt x bin does not depend on the bin)
     acc_bins = np.unique(np.linspace(2, nbins - 1, 6).round().astype(int))
-    accuracy = None
-    if form != 'f64':
-        ref_map = D.map_f64(csm_full[torch.as_tensor(acc_bins, device=dev)].contiguous(),
-                            kvec[torch.as_tensor(acc_bins, device=dev)].contiguous(), mpos, gpos, args.steer, True,
-                            norm).cpu().numpy()
-        got = out[torch.as_tensor(acc_bins, device=dev)].cpu().numpy()
-        scale = np.abs(ref_map).max(axis=1, keepdims=True)
-        err = np.abs(got - ref_map) / scale
+    sel = torch.as_tensor(acc_bins, device=dev)
+    accuracy, forms = None, {}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            r = fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / reps, r
+
+    c_all = csm_full if nbins == F else csm_full[:nbins]
+    cs, ks = c_all[sel].contiguous(), kvec[sel].contiguous()
+    f64_ms, ref_t = timed(lambda: D.map_f64(cs, ks, mpos, gpos, args.steer, True, norm), reps=1)
+    ref_map = ref_t.cpu().numpy()
+    forms['f64'] = {'rate': len(acc_bins) * G / (f64_ms / 1e3), 'bins_timed': len(acc_bins)}
+    lp = lambda x: 10 * np.log10(np.maximum(x / 4e-10, np.finfo(np.float64).eps))  # noqa: E731
+
+    def acc_of(m):
+        got = m[sel].cpu().numpy()
+        err = np.abs(got - ref_map) / np.abs(ref_map).max(axis=1, keepdims=True)
         peak = ref_map.argmax(axis=1)
-        lp = lambda x: 10 * np.log10(np.maximum(x / 4e-10, np.finfo(np.float64).eps))
         db = np.abs(lp(got[np.arange(len(acc_bins)), peak]) - lp(ref_map[np.arange(len(acc_bins)), peak]))
+        return {'max_rel_err': float(err.max()), 'rms_rel_err': float(np.sqrt((err ** 2).mean())),
+                'peak_level_err_db': float(db.max())}
+
+    if form != 'f64':
+        out2 = torch.empty_like(out)
+        for pr in ('bf16x3', 'tf32'):
+            o = out if pr == prec else out2
+            t_ms, _ = timed(lambda: D.map_tc(c_all, kvec, mpos, gpos, args.steer, True, norm, out=o, precision=pr))
+            forms[f'tc_{pr}'] = {'rate': units / (t_ms / 1e3), 'map_ms': t_ms, **acc_of(o),
+                                 'tc_over_f64': units / (t_ms / 1e3) / forms['f64']['rate']}
         accuracy = {'vs': 'plain FP64 form (reference method on the GPU)', 'bins': acc_bins.tolist(),
-                    'max_rel_err': float(err.max()), 'rms_rel_err': float(np.sqrt((err ** 2).mean())),
-                    'peak_level_err_db': float(db.max()),
+                    **acc_of(out),
                     'definition': '|map - ref| / max|ref| per bin; L_p difference at the reference peak'}
 
     # map kernel roofline: algorithmic flops 8 M^2 + 8 M per grid-pt x bin
     pk = peaks()
+    gp = gemm_peaks(dev)
     flops = (8.0 * M * M + 8.0 * M) * units
     map_avg = float(np.mean(map_ms))
     achieved_tf = flops / (map_avg / 1e3) / 1e12
     if form == 'f64':
-        roof = {'bound': 'fp64', 'achieved': achieved_tf, 'peak': None, 'unit': 'TFLOP/s', 'frac': None,
-                'traffic': None, 'kernel': 'map_plain_kernel', 'note': 'FP64 CUDA-core form; fp64 peak not measured'}
+        roof = {'bound': 'fp64', 'achieved': achieved_tf, 'peak': gp['fp64_tflops'], 'unit': 'TFLOP/s',
+                'frac': achieved_tf / gp['fp64_tflops'], 'traffic': None, 'kernel': 'map_plain_kernel',
+                'peak_kind': 'DGEMM measured in this run'}
+    elif prec == 'tf32':
+        # denominator: the measured sustained BF16 rate of the peak file (the conservative one: dense TF32
+        # runs at half the BF16 rate); the cuBLAS TF32 GEMM measured in this run is given beside it
+        roof = {'bound': 'tensor', 'achieved': achieved_tf, 'peak': pk['bf16_tflops_sustained'], 'unit': 'TFLOP/s',
+                'frac': achieved_tf / pk['bf16_tflops_sustained'], 'traffic': TC_TRAFFIC_PER_BIN * nbins,
+                'kernel': 'map_tc_kernel<3,true>', 'peak_kind': f"bf16 sustained ({pk['source']})",
+                'frac_of_tf32_gemm_here': achieved_tf / gp['tf32_tflops']}
     else:
         roof = {'bound': 'tensor', 'achieved': achieved_tf, 'peak': pk['bf16_tflops_sustained'], 'unit': 'TFLOP/s',
-                'frac': achieved_tf / pk['bf16_tflops_sustained'], 'traffic': None, 'kernel': 'map_tc_kernel',
-                'peak_kind': f"bf16 sustained ({pk['source']})"}
+                'frac': achieved_tf / pk['bf16_tflops_sustained'], 'traffic': TC_TRAFFIC_PER_BIN * nbins,
+                'kernel': 'map_tc_kernel<3,false>', 'peak_kind': f"bf16 sustained ({pk['source']})"}
+    if roof['traffic'] is not None:
+        roof['traffic_note'] = ('DRAM bytes per launch: ncu dram__bytes_read+write of a 4-bin capture, scaled by '
+                                'bins (R\' tiles per bin are the traffic; the grid and output add 8 B per point)')
 
     # end to end through the public API (pinned host samples -> host result)
     e2e = None
@@ -545,7 +616,7 @@ def main():
         for i in range(2 + max(1, min(args.steps, 3))):
             ps = ac.PowerSpectra(source=ts, block_size=N, window='Hanning', overlap='50%')
             st = ac.SteeringVector(grid=wl.grid, mics=wl.mics, steer_type=args.steer)
-            bb = ac.BeamformerBase(freq_data=ps, steer=st, r_diag=True, form=form)
+            bb = ac.BeamformerBase(freq_data=ps, steer=st, r_diag=True, form=form, tc_precision=prec)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             res = bb.result[0:nbins]
@@ -563,13 +634,19 @@ def main():
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': ws, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
-                'vs_baseline': None, 'dtype': 'f64' if form == 'f64' else 'bf16x3 (split) / f32 accum',
+                'vs_baseline': None,
+                'dtype': 'f64' if form == 'f64' else ('tf32 / f32 accum' if prec == 'tf32' else
+                                                       'bf16x3 (split) / f32 accum'),
                 'data': 'synthetic (seeded monopoles, GPU-generated)',
                 'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': nbins, 'block_size': N,
                            'windows': K, 'steer_type': args.steer, 'r_diag': True, 'form': form,
                            'l2': 'inputs larger than L2 (samples 524 MB, CSM 538 MB, map 660 MB)',
                            'parallelism': f'{ws} independent instances (one per GPU)'},
-                'map_ms_per_step': map_avg, 'roofline': roof, 'accuracy': accuracy, 'cpu_baseline': cpu, 'e2e': e2e,
+                'map_ms_per_step': map_avg, 'csm_ms_per_step': float(np.mean(csm_ms)),
+                'csm_rate': {'value': units / (float(np.mean(csm_ms)) / 1e3), 'unit': UNIT,
+                             'note': 'CSM stage alone (FFT + FP64 Welch Gram + finish), all bins'},
+                'forms': forms, 'gemm_peaks_here': gp,
+                'roofline': roof, 'accuracy': accuracy, 'cpu_baseline': cpu, 'e2e': e2e,
                 'gpu_launches': None, 'clocks': clk.summary()}
         line['gpu_launches'] = launches_per_step(F, nbins, K, M) * args.steps
         print(json.dumps(line), flush=True)
