@@ -17,13 +17,14 @@
 // passes of one (bin, tile) are shared among several items whose partial sums (B and the
 // normalisation sum S are both additive over chunks) are combined by the last item to finish, in
 // split order, before the steering-type normalisation.
-//   warp 0      : bulk copies of the R' tiles of chunk i (pre-laid in HBM in the shared-memory
+//   warp 5      : bulk copies of the R' tiles of chunk i (pre-laid in HBM in the shared-memory
 //                 core-matrix order by tc_prep_kernel) into a 32-tile ring, running ahead of the MMAs
 //   warp 1      : TMEM allocation; one thread issues tcgen05.mma (A = steering chunk, B = R'
 //                 tiles; products hi*hi + hi*lo + lo*hi) and commits to the stage's mbarrier
-//   warps 2..5  : epilogue: after the MMAs of chunk i, read its accumulator columns from TMEM and
-//                 dot them with the steering chunk read back from the A stage (hi + lo)
-//   warps 6..21 : steering synthesis of chunk i (four threads per grid point, 4 mics each):
+//   warps 0,9,2,3: epilogue (TMEM lane quarters 0..3): after the MMAs of chunk i, read its
+//                 accumulator columns from TMEM and dot them with the steering chunk read back
+//                 from the A stage (hi + lo)
+//   16 warps    : steering synthesis of chunk i (four threads per grid point, 4 mics each):
 //                 FP32 distance (Newton rsqrt), the phase k*r as an exact float-float product,
 //                 Cody-Waite reduction by a three-term 2*pi, hardware sincos, bf16 hi/lo split
 //                 into the A stage.  No FP64<->FP32 conversion and no TMEM access sits in the
@@ -48,15 +49,39 @@ constexpr int TC_MAX_MICS = 2048;          // mic positions live in shared memor
 constexpr int TC_TILE_ELEMS = TC_CHUNK * TC_CHUNK;
 constexpr int TC_TILE_BYTES = TC_TILE_ELEMS * 2;          // bf16
 constexpr int TC_A_BYTES = TC_ROWS * TC_CHUNK * 2;        // 8 KB per (stage, hi|lo)
-constexpr int TC_ASTAGES = 3;              // steering (A) ring: synthesis runs up to 2 chunks ahead
+// steering (A) ring: 3 to 5 stages, the most that fit in shared memory beside the batch's mic table
+// (synthesis runs up to stages - 1 chunks ahead of the MMAs)
+constexpr int TC_ASTAGES_MIN = 3;
+constexpr int TC_ASTAGES_MAX = 5;
 constexpr int TC_RING = 32;                // R' tile (B) ring: 32 tiles of hi + lo (128 KB)
 constexpr int TC_PARTS = 4;                 // synthesis threads per grid point (one per 4 mics of a chunk)
 constexpr int TC_SYNTH_WARPS = 4 * TC_PARTS;  // TC_PARTS warps per TMEM lane quarter
 constexpr int TC_SYNTH_THREADS = 32 * TC_SYNTH_WARPS;
 constexpr int TC_EPI_WARPS = 4;             // one per TMEM lane quarter
 constexpr int TC_EPI_THREADS = 32 * TC_EPI_WARPS;
-constexpr int TC_SYNTH_WARP0 = 2 + TC_EPI_WARPS;
-constexpr int TC_THREADS = 64 + TC_EPI_THREADS + TC_SYNTH_THREADS;
+// Warp layout.  A warp's scheduler (SM sub-partition) is warp % 4.  The single-thread MMA issuer must
+// not share its scheduler with many compute-bound synthesis warps: a scheduler that always has a
+// ready FMA warp leaves the issuer's scalar instructions waiting for issue slots, and the tensor pipe
+// idles (measured on B200: a tcgen05.mma stream 50x slower next to FMA-bound warps on the same
+// scheduler, unchanged when they sit on the other three).  Scheduler 1 holds the MMA issuer (warp 1),
+// the bulk-copy producer (warp 5), the epilogue warp of TMEM lane quarter 1 (warp 9; a warp reads the
+// TMEM lanes of quarter warp % 4) and one synthesis warp (13); warps 17 and 21 idle.  Schedulers 0, 2
+// and 3 hold one epilogue warp and five synthesis warps each.  Six warps per scheduler leave 80
+// registers per thread (registers are allocated per scheduler, 16,384 each).
+constexpr int TC_WARPS = 24;
+constexpr int TC_THREADS = 32 * TC_WARPS;
+constexpr int TC_WARP_MMA = 1;
+constexpr int TC_WARP_PRODUCER = 5;
+__host__ __device__ constexpr bool tc_is_epi(int w) { return w == 0 || w == 2 || w == 3 || w == 9; }
+// index 0..15 of a synthesis warp, -1 for other warps
+__host__ __device__ constexpr int tc_synth_index(int w)
+{
+    return (w < 4 || w >= TC_WARPS || w == 5 || w == 9 || w == 17 || w == 21)
+               ? -1
+               : (w - 4) - (w > 5) - (w > 9) - (w > 17) - (w > 21);
+}
+static_assert(tc_synth_index(4) == 0 && tc_synth_index(13) == 7 && tc_synth_index(23) == TC_SYNTH_WARPS - 1,
+              "synthesis warp indices");
 
 // 2*pi = P2A + P2B + P2C (Cody-Waite split; P2A has 8 significant bits so n*P2A is exact)
 __device__ constexpr float TC_P2A = 0x1.92p+2f;
@@ -112,6 +137,7 @@ constexpr int TC_MAX_INST = 64;
 struct TcBatch {
     int n_inst;
     int mp_max;                // largest padded mic count (shared-memory mic table size)
+    int nstages;               // A stages (TC_ASTAGES_MIN .. TC_ASTAGES_MAX)
     int64_t nitems;
     uint64_t wait_limit_ns;
     TcInst inst[TC_MAX_INST];
@@ -150,7 +176,17 @@ __device__ __forceinline__ int tile_off_tf32(int row, int col)
 }
 
 // Round an FP32 value to TF32 (nearest, ties away from zero), as the MMA reads only 19 bits.
-__device__ __forceinline__ uint32_t tf32_bits(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
+__device__ __forceinline__ uint32_t tf32_bits(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// Position of padding mics and of grid rows past the end of the grid: far away, so that 1/r and
+// its square vanish (1e-18, 1e-37) while r, r^2 and the phase stay finite.  Padding mics have zero
+// R' rows and columns, and the rows past the grid are never written, so neither needs masking.
+constexpr float TC_FAR = 1e18f;
 
 template <bool TF32>
 __global__ void __launch_bounds__(256) tc_prep_kernel(const double2 *__restrict__ csm, int M, int C, int r_diag,
@@ -196,20 +232,20 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const double2 *__restrict_
 }
 
 struct TcSmem {
-    // offsets in bytes from the 1024-aligned dynamic shared-memory base
+    // offsets in bytes from the 1024-aligned dynamic shared-memory base; ns = number of A stages
     __host__ __device__ static constexpr int a_off(int stage, int lo) { return (stage * 2 + lo) * TC_A_BYTES; }
-    __host__ __device__ static constexpr int b_base() { return TC_ASTAGES * 2 * TC_A_BYTES; }
+    __host__ __device__ static constexpr int b_base(int ns) { return ns * 2 * TC_A_BYTES; }
     // ring slot of R' tile pair: hi at b_off(slot, 0), lo at b_off(slot, 1)
-    __host__ __device__ static constexpr int b_off(int slot, int lo)
+    __host__ __device__ static constexpr int b_off(int ns, int slot, int lo)
     {
-        return b_base() + (lo * TC_RING + slot) * TC_TILE_BYTES;
+        return b_base(ns) + (lo * TC_RING + slot) * TC_TILE_BYTES;
     }
-    __host__ __device__ static constexpr int mic_off(int C) { return b_base() + 2 * TC_RING * TC_TILE_BYTES; }
-    __host__ __device__ static constexpr int red_off(int C, int Mp) { return mic_off(C) + Mp * 16; }
+    __host__ __device__ static constexpr int mic_off(int ns) { return b_base(ns) + 2 * TC_RING * TC_TILE_BYTES; }
+    __host__ __device__ static constexpr int red_off(int ns, int Mp) { return mic_off(ns) + Mp * 16; }
     // per-item normalisation partial sums, double-buffered by item parity: [2][parts][128]
-    __host__ __device__ static constexpr int bar_off(int C, int Mp) { return red_off(C, Mp) + 2 * TC_PARTS * TC_ROWS * 8; }
-    __host__ __device__ static constexpr int nbars() { return 2 * TC_ASTAGES + 3 * TC_NB + 2 + 2; }
-    __host__ __device__ static constexpr int total(int C, int Mp) { return bar_off(C, Mp) + nbars() * 8 + 16; }
+    __host__ __device__ static constexpr int bar_off(int ns, int Mp) { return red_off(ns, Mp) + 2 * TC_PARTS * TC_ROWS * 8; }
+    __host__ __device__ static constexpr int nbars() { return 2 * TC_ASTAGES_MAX + 3 * TC_NB + 2 + 2; }
+    __host__ __device__ static constexpr int total(int ns, int Mp) { return bar_off(ns, Mp) + nbars() * 8 + 16; }
 };
 
 // Normalisation of the steering type (acoular/fastFuncs.py:293-310) and clipping.
@@ -253,12 +289,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     // operand tiles start on a 1 KB boundary (the launch reserves 1 KB of slack for this)
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     const int MPX = b.mp_max;
-    float4 *mp4 = reinterpret_cast<float4 *>(smem + TcSmem::mic_off(0));          // [MPX] (x, y, z, 0)
-    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(0, MPX));     // [2][parts][128] sums S
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(0, MPX));
-    uint64_t *full_a = bars;                          // [3]  step T written to A stage T % 3
-    uint64_t *afree = bars + TC_ASTAGES;              // [3]  epilogue of step T has released A stage T % 3
-    uint64_t *full_b = bars + 2 * TC_ASTAGES;         // [8]  R' tiles of step T landed
+    const int NST = b.nstages;
+    float4 *mp4 = reinterpret_cast<float4 *>(smem + TcSmem::mic_off(NST));        // [MPX] (x, y, z, w)
+    double *red = reinterpret_cast<double *>(smem + TcSmem::red_off(NST, MPX));   // [2][parts][128] sums S
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TcSmem::bar_off(NST, MPX));
+    uint64_t *full_a = bars;                          // [NST] step T written to A stage T % NST
+    uint64_t *afree = bars + TC_ASTAGES_MAX;          // [NST] epilogue of step T has released A stage T % NST
+    uint64_t *full_b = bars + 2 * TC_ASTAGES_MAX;     // [8]  R' tiles of step T landed
     uint64_t *done = full_b + TC_NB;                  // [8]  MMAs of step T complete
     uint64_t *tfree = done + TC_NB;                   // [8]  epilogue has read all columns of window W
     uint64_t *s_ready = tfree + TC_NB;                // [2]  synthesis sums S of item parity written
@@ -270,7 +307,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     const uint32_t ncols = 512;   // the whole TMEM: accumulator windows rotate through it
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_ASTAGES; ++s) {
+        for (int s = 0; s < NST; ++s) {
             tc::mbar_init(&full_a[s], TC_SYNTH_THREADS);
             tc::mbar_init(&afree[s], TC_EPI_THREADS);
         }
@@ -294,7 +331,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     // [16p, je) with je = min(C, 16p + 16); in pass p the K chunks i = 0 .. je-1 run, chunk i feeding
     // the columns of chunks j in [max(i, 16p), je).  Chunk i's columns are final after step (p, i)
     // when i >= 16p; those steps also carry chunk i's dot product and normalisation sum.
-    if (warp == 0) {
+    if (warp == TC_WARP_PRODUCER) {
         // ---------------- producer: R' tiles of every step into the tile ring ----------------
         // Step T takes n consecutive ring tiles starting at the running tile counter U; tile U
         // reuses slot U % TC_RING, free once the step that held tile U - TC_RING is complete.
@@ -335,12 +372,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                             const int run = min(n - j, TC_RING - slot);
                             const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
                             if (TF32) {   // FP32 tiles of 4 KB, ring slot s at b_base + s * 4 KB
-                                tc::bulk_g2s(smem + TcSmem::b_base() + slot * 2 * TC_TILE_BYTES,
+                                tc::bulk_g2s(smem + TcSmem::b_base(NST) + slot * 2 * TC_TILE_BYTES,
                                              reinterpret_cast<const uint32_t *>(bh) + src + (int64_t)j * TC_TILE_ELEMS,
                                              2 * bytes, fb);
                             } else {
-                                tc::bulk_g2s(smem + TcSmem::b_off(slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
-                                tc::bulk_g2s(smem + TcSmem::b_off(slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                                tc::bulk_g2s(smem + TcSmem::b_off(NST, slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes,
+                                             fb);
+                                tc::bulk_g2s(smem + TcSmem::b_off(NST, slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes,
+                                             fb);
                             }
                             j += run;
                         }
@@ -354,7 +393,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 tc::mbar_wait(&full_b[lastT & (TC_NB - 1)], (uint32_t)((lastT / TC_NB) & 1), abort_flag,
                               4 * b.wait_limit_ns);
         }
-    } else if (warp == 1) {
+    } else if (warp == TC_WARP_MMA) {
         // ---------------- MMA issuer ----------------
         // Kept lean: it sits on every step's critical path.  Descriptors are built once and
         // advanced by adding byte offsets >> 4 to their 14-bit start-address field; ring and
@@ -364,7 +403,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             // TF32: 8-row x 4-element core matrices, 8 per row group (SBO 1024)
             constexpr uint32_t SBO = TF32 ? 1024 : 512;
             const uint64_t a_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::a_off(0, 0)), 128, SBO);
-            const uint64_t b_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::b_off(0, 0)), 128, SBO);
+            const uint64_t b_base = tc::sdesc_noswizzle(tc::smem_u32(smem + TcSmem::b_off(NST, 0, 0)), 128, SBO);
             constexpr uint32_t A_STEP = TC_A_BYTES >> 4;          // next (stage, hi|lo) block
             constexpr uint32_t T_STEP = (TF32 ? 2 : 1) * (TC_TILE_BYTES >> 4);   // next ring tile
             constexpr uint32_t LO_B = (TC_RING * TC_TILE_BYTES) >> 4;
@@ -445,15 +484,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         lastb = sb;
                         lastu = ub;
                         slot0 = (slot0 + (uint32_t)n) & (TC_RING - 1);
-                        if (++sa == TC_ASTAGES) { sa = 0; ua ^= 1; }
+                        if (++sa == NST) { sa = 0; ua ^= 1; }
                         if (++sb == TC_NB) { sb = 0; ub ^= 1; }
                     }
                 }
             }
             if (lastb >= 0) tc::mbar_wait(&done[lastb], (uint32_t)lastu, abort_flag, 4 * b.wait_limit_ns);
         }
-    } else if (warp < TC_SYNTH_WARP0) {
-        // ---------------- epilogue (warps 2..5): one thread per grid point ----------------
+    } else if (tc_is_epi(warp)) {
+        // ---------------- epilogue (warps 0, 9, 2, 3 for lane quarters 0..3): one thread per grid point
         // After step (p, i) with i >= 16p the accumulator columns of chunk i are final; dot them
         // with the steering chunk as the MMA saw it (hi + lo from the A stage).  Every step then
         // releases its A stage.
@@ -523,7 +562,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         tc::tc_fence_before();
                     }
                     tc::mbar_arrive(&afree[sa]);
-                    if (++sa == TC_ASTAGES) sa = 0;
+                    if (++sa == NST) sa = 0;
                 }
                 if (!ok) break;
                 tc::mbar_arrive(&tfree[W & (TC_NB - 1)]);
@@ -562,15 +601,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 finish_point<ST>(in, acc, S, in.gpos[g], in.gpos[in.G + g], in.gpos[2 * in.G + g], bin, g, in.out,
                                  in.out_norm);
         }
-    } else {
-        // ---------------- steering synthesis (warps 6..21) ----------------
-        // Warp w serves grid points 32q..32q+31 (q = w % 4) and part p of every chunk: mics
-        // 4p..4p+3 of the chunk's 16, i.e. one 16-byte core-matrix column of the A tile.
-        const int q = warp & 3;
-        const int p = (warp - TC_SYNTH_WARP0) >> 2;
+    } else if (tc_synth_index(warp) >= 0) {
+        // ---------------- steering synthesis (16 warps off scheduler 1) ----------------
+        // Synthesis warp s serves grid points 32q..32q+31 (q = s % 4) and part p = s / 4 of every
+        // chunk: mics 4p..4p+3 of the chunk's 16, i.e. one 16-byte core-matrix column of the A tile.
+        const int sidx = tc_synth_index(warp);
+        const int q = sidx & 3;
+        const int p = sidx >> 2;
         const int row = q * 32 + lane;
         const int a_off_row = (((row >> 3) * 4 + p) << 7) + ((row & 7) << 4);
-        const int sid = threadIdx.x - TC_SYNTH_WARP0 * 32;   // 0 .. TC_SYNTH_THREADS-1
+        const int sid = sidx * 32 + lane;   // 0 .. TC_SYNTH_THREADS-1
         int T = 0, sa = 0, ua = 0, cur_inst = -1;
         bool ok = true;
         for (int64_t li = 0; li < nmine && ok; ++li) {
@@ -580,9 +620,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             if (ii != cur_inst) {
                 // new instance: every synthesis thread is past the previous item, reload the mics
                 asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
-                // (x, y, z, weight): padding mics beyond M get weight 0 and a position off the grid
+                // (x, y, z, weight): padding mics beyond M sit far away with weight 0 (the weight is
+                // needed only by the inverse steering's sum of r^2)
                 for (int m = sid; m < in.Mp; m += TC_SYNTH_THREADS) {
-                    float4 v = make_float4(1.f, 1.f, 1.f, 0.f);
+                    float4 v = make_float4(TC_FAR, TC_FAR, TC_FAR, 0.f);
                     if (m < in.M)
                         v = make_float4((float)in.mpos[m], (float)in.mpos[in.M + m], (float)in.mpos[2 * in.M + m], 1.f);
                     mp4[m] = v;
@@ -595,7 +636,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             const int bin = it.bin;
             const int64_t g = it.tile * TC_ROWS + row;
             const bool gvalid = g < in.G;
-            float gxf = 0.f, gyf = 0.f, gzf = 0.f;
+            float gxf = -TC_FAR, gyf = -TC_FAR, gzf = -TC_FAR;
             if (gvalid) {
                 gxf = (float)in.gpos[g];
                 gyf = (float)in.gpos[in.G + g];
@@ -607,8 +648,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             for (int pp = it.pa; pp < it.pz && ok; ++pp) {
                 const int jb = pp * pw, je = min(C, jb + pw);
                 for (int t = 0; t < je; ++t, ++T) {
-                    if (T >= TC_ASTAGES) {
-                        // the A stage is free once the epilogue of step T - 3 has released it
+                    if (T >= NST) {
+                        // the A stage is free once the epilogue of step T - NST has released it
                         ok = __all_sync(0xffffffffu, tc::mbar_wait(&afree[sa], (uint32_t)(ua ^ 1), abort_flag,
                                                                    b.wait_limit_ns));
                         if (!ok) break;
@@ -634,11 +675,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         x += pl;
                         float sn, cs;
                         tc::sincos_approx(x, sn, cs);
-                        // steering weight: 1, r (inverse) or 1/r (true level / location), times the
-                        // mic's table weight (0 for padding mics)
-                        const float w = (ST == 2 ? r : (ST >= 3 ? y : 1.f)) * mv.w;
+                        // steering weight: 1, r (inverse, times the mic's table weight: 0 for padding)
+                        // or 1/r (true level / location)
+                        const float w = ST == 2 ? r * mv.w : (ST >= 3 ? y : 1.f);
                         if (ST == 2) s_part = fmaf(r2, mv.w, s_part);
-                        else if (ST >= 3) s_part = fmaf(y * y, mv.w, s_part);
+                        else if (ST >= 3) s_part = fmaf(y, y, s_part);
                         const float vr = cs * w, vi = -sn * w;
                         if (TF32) {   // FP32 operand rounded to TF32: (re, im) of mic e in hw[e], lw[e]
                             hw[e] = tf32_bits(vr);
@@ -652,10 +693,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         const float li_ = vi - __uint_as_float(hw[e] & 0xFFFF0000u);
                         const __nv_bfloat162 l2 = __floats2bfloat162_rn(lr, li_);
                         lw[e] = *reinterpret_cast<const uint32_t *>(&l2);
-                    }
-                    if (!gvalid) {   // grid points past the end of the grid contribute nothing
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) hw[e] = lw[e] = 0u;
                     }
                     if (TF32) {
                         // components 8p..8p+7 = core-matrix columns 2p, 2p+1 of the FP32 row
@@ -671,7 +708,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                     if (t >= jb) S += (double)s_part;   // each mic's term once, in its own pass
                     tc::fence_proxy_async_smem();
                     tc::mbar_arrive(&full_a[sa]);
-                    if (++sa == TC_ASTAGES) { sa = 0; ua ^= 1; }
+                    if (++sa == NST) { sa = 0; ua ^= 1; }
                 }
             }
             if (!ok) break;
@@ -818,12 +855,19 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
     }
     bt.mp_max = mp_max;
     bt.wait_limit_ns = 500ull * 1000 * 1000;
-    int smem = TcSmem::total(0, mp_max) + 1024;
+    int dev = 0, nsm = kNumSMs, smem_max = 232448;
+    if (cudaGetDevice(&dev) == cudaSuccess) {
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    }
+    // the deepest A ring that fits beside this batch's mic table (+1 KB of alignment slack)
+    int ns = TC_ASTAGES_MAX;
+    while (ns > TC_ASTAGES_MIN && TcSmem::total(ns, mp_max) + 1024 > smem_max) --ns;
+    bt.nstages = ns;
+    int smem = TcSmem::total(ns, mp_max) + 1024;
     // each CTA takes all 512 TMEM columns and must be alone on its SM: size the shared memory so
     // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)
     if (smem < 116 * 1024) smem = 116 * 1024;
-    int dev = 0, nsm = kNumSMs;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const dim3 grid((unsigned)(bt.nitems < nsm ? bt.nitems : nsm));
     const bool tf = precision == ACB_TC_TF32;
     auto kern = steer_type == 1 ? (tf ? map_tc_kernel<1, true> : map_tc_kernel<1, false>)
