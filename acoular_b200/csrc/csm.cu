@@ -27,7 +27,47 @@ void set_cuda_error(cudaError_t e) { g_last_cuda_error = cudaGetErrorString(e); 
 // ------------------------------------------------------------------------------------------------
 // Windowed real FFT.  One CTA = one window x `mpb` mics; FFT of the N/2-point complex sequence
 // z[j] = x[2j] + i x[2j+1], then the split into the N/2+1 real-input bins.
+//
+// The radix-2 DIT stages run in passes of up to three: a thread loads the 2^s points that s
+// consecutive stages combine among themselves, applies the s stages' butterflies in registers
+// (same operands, twiddles and operation order as one stage at a time, so the spectra are the
+// same bits) and stores them back: one shared-memory round trip and one barrier per pass instead
+// of per stage.
 // ------------------------------------------------------------------------------------------------
+// s (1..3) consecutive radix-2 DIT stages of lengths L1, 2 L1, .., on a bit-reversed sequence z of
+// H points (one mic).  Task `task` in [0, H / 2^s) owns points base + t * L1/2, t = 0 .. 2^s - 1.
+template <int S>
+__device__ __forceinline__ void fft_pass(double2 *__restrict__ z, int L1, int task, int N,
+                                         const double2 *__restrict__ tw)
+{
+    const int half1 = L1 >> 1;
+    const int Ls = L1 << (S - 1);            // length of the last stage of the pass
+    const int grp = task / half1, pos = task % half1;
+    const int base = grp * Ls + pos;
+    double2 v[1 << S];
+#pragma unroll
+    for (int t = 0; t < (1 << S); ++t) v[t] = z[base + t * half1];
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+        const int L = L1 << q, hf = L >> 1;
+        const int stride = N / L;
+#pragma unroll
+        for (int t = 0; t < (1 << S); ++t) {
+            if (t & (1 << q)) continue;
+            const int i0 = base + t * half1;
+            const double2 w = __ldg(tw + (i0 % hf) * stride);
+            const double2 b = v[t + (1 << q)];
+            const double br = b.x * w.x - b.y * w.y;
+            const double bi = b.x * w.y + b.y * w.x;
+            const double2 a = v[t];
+            v[t] = make_double2(a.x + br, a.y + bi);
+            v[t + (1 << q)] = make_double2(a.x - br, a.y - bi);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < (1 << S); ++t) z[base + t * half1] = v[t];
+}
+
 template <typename TS, bool C64>
 __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ samples, int M, int N, int hop,
                                                          int64_t w0, int64_t nw, int mpb,
@@ -55,25 +95,20 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
     }
     __syncthreads();
 
-    // radix-2 DIT butterflies
-    for (int len = 2; len <= H; len <<= 1) {
-        const int half = len >> 1;
-        const int stride = N / len;  // twiddle index step in the N-point table
-        for (int idx = threadIdx.x; idx < nm * (H >> 1); idx += blockDim.x) {
-            const int ml = idx / (H >> 1);
-            const int p = idx % (H >> 1);
-            const int grp = p / half, pos = p % half;
-            double2 *z = zs + ml * H;
-            const int i0 = grp * len + pos, i1 = i0 + half;
-            const double2 t = tw[pos * stride];
-            const double2 b = z[i1];
-            const double br = b.x * t.x - b.y * t.y;
-            const double bi = b.x * t.y + b.y * t.x;
-            const double2 a = z[i0];
-            z[i0] = make_double2(a.x + br, a.y + bi);
-            z[i1] = make_double2(a.x - br, a.y - bi);
+    // radix-2 DIT stages, up to three per pass
+    for (int st = 0; st < logH;) {
+        const int S = logH - st >= 3 ? 3 : logH - st;
+        const int L1 = 2 << st;
+        const int ntask = H >> S;
+        for (int idx = threadIdx.x; idx < nm * ntask; idx += blockDim.x) {
+            const int ml = idx / ntask;
+            const int task = idx - ml * ntask;
+            if (S == 3) fft_pass<3>(zs + ml * H, L1, task, N, tw);
+            else if (S == 2) fft_pass<2>(zs + ml * H, L1, task, N, tw);
+            else fft_pass<1>(zs + ml * H, L1, task, N, tw);
         }
         __syncthreads();
+        st += S;
     }
 
     // real-input split: X[k] = E + W^k O,  E = (Z[k] + conj(Z[H-k]))/2,  O = -i (Z[k] - conj(Z[H-k]))/2
@@ -241,9 +276,11 @@ __global__ void __launch_bounds__(256) finalize_kernel(const void *__restrict__ 
     }
 }
 
+// Mics per CTA: at most 32 KB of complex doubles (N/2 per mic), so that several CTAs share an SM
+// and hide each other's barrier and FP64 latency; one mic for N > 4096.
 static int fft_mics_per_block(int N)
 {
-    const int cap = 16384 / N;  // 128 KB of complex doubles per CTA
+    const int cap = 4096 / N;
     return cap >= 16 ? 16 : (cap < 1 ? 1 : cap);
 }
 
