@@ -16,7 +16,11 @@
 #include <string>
 #include <type_traits>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
+#include "csm_internal.h"
+#include "tc_layout.cuh"
 
 namespace acb {
 
@@ -68,12 +72,19 @@ __device__ __forceinline__ void fft_pass(double2 *__restrict__ z, int L1, int ta
     for (int t = 0; t < (1 << S); ++t) z[base + t * half1] = v[t];
 }
 
-template <typename TS, bool C64>
+// Output forms of the spectra (OUT): complex128 or complex64 [bin][window][mic] for the FP64 /
+// FP32 Gram; or the tensor-core Gram's operand tiles, TF32 (OUT_TF32) or split BF16 hi + lo
+// (OUT_BF16), 32 x 32 tiles [bin][window/32][component/32] with component 2m = Re, 2m + 1 = Im of
+// mic m (row) and the window within the chunk (column); `R` row tiles per bin and window block,
+// `KC` window blocks; BF16 lo tiles start `lo_elems` elements after the hi tiles.
+enum { OUT_C128 = 0, OUT_C64 = 1, OUT_TF32 = 2, OUT_BF16 = 3 };
+
+template <typename TS, int OUT>
 __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ samples, int M, int N, int hop,
                                                          int64_t w0, int64_t nw, int mpb,
                                                          const double *__restrict__ window,
                                                          const double2 *__restrict__ tw, int bin_lo, int nbins,
-                                                         void *__restrict__ out)
+                                                         void *__restrict__ out, int R, int KC, int64_t lo_elems)
 {
     extern __shared__ double2 zs[];  // [mpb][H]
     const int H = N >> 1;
@@ -125,9 +136,29 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
         else wk = make_double2(-1.0, 0.0);
         const double xr = er + (wk.x * orr - wk.y * oi);
         const double xi = ei + (wk.x * oi + wk.y * orr);
-        const int64_t o = ((int64_t)(k - bin_lo) * nw + blockIdx.y) * M + m0 + ml;
-        if (C64) reinterpret_cast<float2 *>(out)[o] = make_float2(__double2float_rn(xr), __double2float_rn(xi));
-        else reinterpret_cast<double2 *>(out)[o] = make_double2(xr, xi);
+        if (OUT <= OUT_C64) {
+            const int64_t o = ((int64_t)(k - bin_lo) * nw + blockIdx.y) * M + m0 + ml;
+            if (OUT == OUT_C64)
+                reinterpret_cast<float2 *>(out)[o] = make_float2(__double2float_rn(xr), __double2float_rn(xi));
+            else reinterpret_cast<double2 *>(out)[o] = make_double2(xr, xi);
+        } else {
+            const int rowc = 2 * (m0 + ml), col = blockIdx.y & 31;
+            const int64_t tile = ((int64_t)(k - bin_lo) * KC + (blockIdx.y >> 5)) * R + (rowc >> 5);
+            const float fr = __double2float_rn(xr), fi = __double2float_rn(xi);
+            if (OUT == OUT_TF32) {
+                uint32_t *t = reinterpret_cast<uint32_t *>(out) + tile * 1024;
+                t[tile_off_tf32(rowc & 31, col)] = tf32_bits(fr);
+                t[tile_off_tf32((rowc & 31) + 1, col)] = tf32_bits(fi);
+            } else {
+                __nv_bfloat16 *t = reinterpret_cast<__nv_bfloat16 *>(out) + tile * 1024;
+                const __nv_bfloat16 hr = __float2bfloat16_rn(fr), hi = __float2bfloat16_rn(fi);
+                const int o0 = tile_off(rowc & 31, col), o1 = tile_off((rowc & 31) + 1, col);
+                t[o0] = hr;
+                t[o1] = hi;
+                t[lo_elems + o0] = __float2bfloat16_rn(fr - __bfloat162float(hr));
+                t[lo_elems + o1] = __float2bfloat16_rn(fi - __bfloat162float(hi));
+            }
+        }
     }
 }
 
@@ -284,6 +315,35 @@ static int fft_mics_per_block(int N)
     return cap >= 16 ? 16 : (cap < 1 ? 1 : cap);
 }
 
+// Launch the windowed FFT of `num_windows` windows in output form `out_form`.
+int fft_launch(const void *samples, int sample_dtype, int out_form, int num_mics, int block_size, int hop,
+               int64_t first_window, int64_t num_windows, const double *window, const double2 *tw, int bin_lo,
+               int num_bins, void *out, int R, int KC, int64_t lo_elems, cudaStream_t s)
+{
+    const int mpb = fft_mics_per_block(block_size);
+    const dim3 g1((num_mics + mpb - 1) / mpb, (unsigned)num_windows);
+    const size_t smem = (size_t)mpb * (block_size / 2) * sizeof(double2);
+#define ACB_FFT_LAUNCH(TS, OF)                                                                                    \
+    do {                                                                                                          \
+        auto kern = fft_window_kernel<TS, OF>;                                                                    \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                       \
+        kern<<<g1, 256, smem, s>>>(reinterpret_cast<const TS *>(samples), num_mics, block_size, hop, first_window, \
+                                   num_windows, mpb, window, tw, bin_lo, num_bins, out, R, KC, lo_elems);        \
+    } while (0)
+#define ACB_FFT_FORMS(TS)                                                \
+    switch (out_form) {                                                  \
+    case OUT_C128: ACB_FFT_LAUNCH(TS, OUT_C128); break;                  \
+    case OUT_C64: ACB_FFT_LAUNCH(TS, OUT_C64); break;                    \
+    case OUT_TF32: ACB_FFT_LAUNCH(TS, OUT_TF32); break;                  \
+    default: ACB_FFT_LAUNCH(TS, OUT_BF16); break;                        \
+    }
+    if (sample_dtype == ACB_F32) { ACB_FFT_FORMS(float) }
+    else { ACB_FFT_FORMS(double) }
+#undef ACB_FFT_FORMS
+#undef ACB_FFT_LAUNCH
+    return check_launch();
+}
+
 }  // namespace acb
 
 using namespace acb;
@@ -329,6 +389,8 @@ int acb_calc_csm_c64(void *csm, const void *spec, int num_freqs, int num_mics, v
 size_t acb_csm_workspace_bytes(int num_mics, int num_bins, int64_t num_windows, int precision)
 {
     if (num_mics <= 0 || num_bins <= 0 || num_windows <= 0) return 0;
+    if (precision == ACB_CSM_TC_TF32 || precision == ACB_CSM_TC_BF16X3)
+        return csm_tc_workspace_bytes(num_mics, num_bins, num_windows);
     const size_t es = precision == ACB_C64 ? 8 : 16;
     return (size_t)num_mics * (size_t)num_bins * (size_t)num_windows * es;
 }
@@ -340,8 +402,10 @@ int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_sample
 {
     if (!samples || !window || !twiddle || !csm_upper) return ACB_ERR_ARG;
     if (sample_dtype != ACB_F32 && sample_dtype != ACB_F64) return ACB_ERR_ARG;
-    if (precision != ACB_C128 && precision != ACB_C64) return ACB_ERR_ARG;
+    const bool tc = precision == ACB_CSM_TC_TF32 || precision == ACB_CSM_TC_BF16X3;
+    if (precision != ACB_C128 && precision != ACB_C64 && !tc) return ACB_ERR_ARG;
     if (num_mics <= 0 || num_windows < 0 || first_window < 0 || hop <= 0) return ACB_ERR_SHAPE;
+    if (tc && csm_tc_row_tiles(num_mics) > 252) return ACB_ERR_UNSUPPORTED;
     if (block_size < 16 || (block_size & (block_size - 1))) return ACB_ERR_SHAPE;
     if (block_size > 16384) return ACB_ERR_UNSUPPORTED;
     if (bin_lo < 0 || num_bins <= 0 || bin_lo + num_bins > block_size / 2 + 1) return ACB_ERR_SHAPE;
@@ -351,26 +415,12 @@ int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_sample
     const size_t need = acb_csm_workspace_bytes(num_mics, num_bins, num_windows, precision);
     if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
     cudaStream_t s = as_stream(stream);
-    const int mpb = fft_mics_per_block(block_size);
-    const dim3 g1((num_mics + mpb - 1) / mpb, (unsigned)num_windows);
-    const size_t smem = (size_t)mpb * (block_size / 2) * sizeof(double2);
     const double2 *tw = reinterpret_cast<const double2 *>(twiddle);
-#define ACB_FFT_LAUNCH(TS, C64)                                                                              \
-    do {                                                                                                     \
-        auto kern = fft_window_kernel<TS, C64>;                                                              \
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                  \
-        kern<<<g1, 256, smem, s>>>(reinterpret_cast<const TS *>(samples), num_mics, block_size, hop,         \
-                                   first_window, num_windows, mpb, window, tw, bin_lo, num_bins, workspace); \
-    } while (0)
-    if (sample_dtype == ACB_F32) {
-        if (precision == ACB_C64) ACB_FFT_LAUNCH(float, true);
-        else ACB_FFT_LAUNCH(float, false);
-    } else {
-        if (precision == ACB_C64) ACB_FFT_LAUNCH(double, true);
-        else ACB_FFT_LAUNCH(double, false);
-    }
-#undef ACB_FFT_LAUNCH
-    int st = check_launch();
+    if (tc)
+        return csm_tc_accumulate(samples, sample_dtype, num_mics, block_size, hop, first_window, num_windows, window,
+                                 tw, bin_lo, num_bins, precision == ACB_CSM_TC_TF32, csm_upper, workspace, s);
+    int st = fft_launch(samples, sample_dtype, precision == ACB_C64 ? OUT_C64 : OUT_C128, num_mics, block_size, hop,
+                        first_window, num_windows, window, tw, bin_lo, num_bins, workspace, 0, 0, 0, s);
     if (st) return st;
     const int T = (num_mics + GT - 1) / GT;
     const dim3 g2(T * (T + 1) / 2, num_bins);

@@ -1,0 +1,24 @@
+// Internal interfaces between the CSM sources (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace acb {
+
+// Windowed FP64 rFFT of `num_windows` windows; out_form: 0 complex128 spectra, 1 complex64 spectra,
+// 2 TF32 operand tiles, 3 split-BF16 operand tiles (R row tiles, KC window blocks, lo tiles
+// `lo_elems` after the hi tiles).
+int fft_launch(const void *samples, int sample_dtype, int out_form, int num_mics, int block_size, int hop,
+               int64_t first_window, int64_t num_windows, const double *window, const double2 *tw, int bin_lo,
+               int num_bins, void *out, int R, int KC, int64_t lo_elems, cudaStream_t s);
+
+// Tensor-core Welch accumulation into the complex128 upper triangle (csm_tc.cu).
+int csm_tc_row_tiles(int num_mics);
+size_t csm_tc_workspace_bytes(int num_mics, int num_bins, int64_t num_windows);
+int csm_tc_accumulate(const void *samples, int sample_dtype, int num_mics, int block_size, int hop,
+                      int64_t first_window, int64_t num_windows, const double *window, const double2 *tw,
+                      int bin_lo, int num_bins, bool tf32, void *csm_upper, void *workspace, cudaStream_t s);
+
+}  // namespace acb

@@ -37,6 +37,7 @@
 
 #include "common.cuh"
 #include "tc_common.cuh"
+#include "tc_layout.cuh"
 
 namespace acb {
 
@@ -160,29 +161,9 @@ __host__ __device__ constexpr int tri_tiles(int C) { return C * (C + 1) / 2; }
 // index of tile (i, j >= i) in the row-major upper-triangular tile order
 __host__ __device__ constexpr int tile_index(int C, int i, int j) { return i * C - i * (i - 1) / 2 + (j - i); }
 
-// Element offset inside a 32x32 tile (row = n, col = k), K-major no-swizzle core-matrix order.
-__device__ __forceinline__ int tile_off(int row, int col)
-{
-    return (((row >> 3) * 4 + (col >> 3)) << 6) + ((row & 7) << 3) + (col & 7);
-}
-
 // ------------------------------------------------------------------------------------------------
 // R' in split-BF16, per bin: tiles (i, j >= i) of 32 x 32, stored row = n (column of D), col = k.
 // ------------------------------------------------------------------------------------------------
-// TF32 operand layout of a 32x32 tile: core matrices of 8 rows x 4 fp32 (16 bytes), 8 per row group.
-__device__ __forceinline__ int tile_off_tf32(int row, int col)
-{
-    return (((row >> 3) * 8 + (col >> 2)) << 5) + ((row & 7) << 2) + (col & 3);
-}
-
-// Round an FP32 value to TF32 (nearest, ties away from zero), as the MMA reads only 19 bits.
-__device__ __forceinline__ uint32_t tf32_bits(float x)
-{
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
-
 // Position of padding mics and of grid rows past the end of the grid: far away, so that 1/r and
 // its square vanish (1e-18, 1e-37) while r, r^2 and the phase stay finite.  Padding mics have zero
 // R' rows and columns, and the rows past the grid are never written, so neither needs masking.

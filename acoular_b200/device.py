@@ -76,6 +76,9 @@ def window_vector(window: str, block_size: int, device) -> tuple[torch.Tensor, f
     return v
 
 
+CSM_PRECISIONS = {'complex128': N.C128, 'complex64': N.C64, 'tc_tf32': N.CSM_TC_TF32, 'tc_bf16x3': N.CSM_TC_BF16X3}
+
+
 def csm_upper_accumulate(samples: torch.Tensor, block_size: int, window: str, overlap: str,
                          precision: str = 'complex128', bin_lo: int = 0, num_bins: int | None = None,
                          csm_upper: torch.Tensor | None = None, workspace: torch.Tensor | None = None,
@@ -83,6 +86,9 @@ def csm_upper_accumulate(samples: torch.Tensor, block_size: int, window: str, ov
                          windows: int | None = None):
     """Welch sum (upper triangle) of all windows of ``samples`` (device, (S, M) f32/f64).
 
+    ``precision``: ``'complex128'`` / ``'complex64'`` (the reference's CSM precisions, FP64 / FP32
+    Gram in the reference's accumulation order) or ``'tc_tf32'`` / ``'tc_bf16x3'`` (the tensor-core
+    Gram: TF32 or split-BF16 operands, FP32 accumulation per chunk of windows, complex128 sums).
     Returns ``(csm_upper, n_windows)``; ``csm_upper`` is (num_bins, M, M) complex128/complex64.
     """
     dev = samples.device
@@ -94,7 +100,7 @@ def csm_upper_accumulate(samples: torch.Tensor, block_size: int, window: str, ov
     hop = block_size // ov
     F = block_size // 2 + 1
     nb = F - bin_lo if num_bins is None else num_bins
-    prec = N.C64 if precision == 'complex64' else N.C128
+    prec = CSM_PRECISIONS[precision]
     cdt = torch.complex64 if prec == N.C64 else torch.complex128
     if csm_upper is None:
         csm_upper = torch.zeros((nb, M, M), dtype=cdt, device=dev)
@@ -105,10 +111,18 @@ def csm_upper_accumulate(samples: torch.Tensor, block_size: int, window: str, ov
         sd = N.F64
     wv, _ = window_vector(window, block_size, dev)
     tw = twiddles(block_size, dev)
-    per_win = N.lib().acb_csm_workspace_bytes(M, nb, 1, prec)
-    chunk = int(max(1, min(65535, max_workspace_bytes // max(per_win, 1), K if K > 0 else 1)))
-    if workspace is None or workspace.numel() < per_win * chunk:
-        workspace = torch.empty(per_win * chunk, dtype=torch.uint8, device=dev)
+    if prec in (N.CSM_TC_TF32, N.CSM_TC_BF16X3):
+        # the tensor-core operand pads every chunk to whole blocks of 32 windows
+        per32 = N.lib().acb_csm_workspace_bytes(M, nb, 32, prec)
+        chunk = int(max(32, min(65504, max_workspace_bytes // max(per32, 1) * 32)))
+        chunk = min(chunk, -(-max(K, 1) // 32) * 32)
+        need = N.lib().acb_csm_workspace_bytes(M, nb, chunk, prec)
+    else:
+        per_win = N.lib().acb_csm_workspace_bytes(M, nb, 1, prec)
+        chunk = int(max(1, min(65535, max_workspace_bytes // max(per_win, 1), K if K > 0 else 1)))
+        need = per_win * chunk
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=dev)
     st = N.stream_handle()
     L = N.lib()
     w = first_window

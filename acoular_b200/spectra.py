@@ -8,6 +8,10 @@ the source or a setting changes), ``indices`` / ``ind_low`` / ``ind_high`` / ``f
 reference returns; ``csm_device`` keeps the same matrix resident on the GPU for the beamformer.
 HDF5 result caching (``cached`` / ``config.global_caching``) is not implemented: every setting
 behaves like ``global_caching='none'``.
+
+Two settings have no counterpart in the reference: ``form`` ('f64', the default, the reference's
+arithmetic; or 'tc', the Welch Gram on the tensor cores) and ``tc_precision`` ('tf32' or 'bf16x3',
+the operand form of the tensor-core Gram).  Either way the CSM is complex128.
 """
 
 from __future__ import annotations
@@ -24,8 +28,10 @@ BLOCK_SIZES = (1024, 128, 256, 512, 2048, 4096, 8192, 16384, 32768, 65536)
 class PowerSpectra:
     def __init__(self, source=None, block_size: int = 1024, window: str = 'Rectangular', overlap: str = 'None',
                  precision: str = 'complex128', cached: bool = False, ind_low: int | None = None,
-                 ind_high: int | None = None, device=None):
+                 ind_high: int | None = None, device=None, form: str = 'f64', tc_precision: str = 'tf32'):
         self.source = source
+        self.form = form
+        self.tc_precision = tc_precision
         self.block_size = block_size
         self.window = window
         self.overlap = overlap
@@ -55,6 +61,12 @@ class PowerSpectra:
         if name == 'precision' and value not in ('complex128', 'complex64'):
             msg = f"precision must be 'complex128' or 'complex64', got {value!r}"
             raise ValueError(msg)
+        if name == 'form' and value not in ('f64', 'tc'):
+            msg = f"form must be 'f64' or 'tc', got {value!r}"
+            raise ValueError(msg)
+        if name == 'tc_precision' and value not in ('tf32', 'bf16x3'):
+            msg = f"tc_precision must be 'tf32' or 'bf16x3', got {value!r}"
+            raise ValueError(msg)
         object.__setattr__(self, name, value)
 
     @property
@@ -80,7 +92,8 @@ class PowerSpectra:
     @property
     def digest(self) -> str:
         src = getattr(self.source, 'digest', id(self.source))
-        return f'{src}|{self.block_size}|{self.window}|{self.overlap}|{self.precision}'
+        tc = f'|tc-{self.tc_precision}' if self.form == 'tc' else ''
+        return f'{src}|{self.block_size}|{self.window}|{self.overlap}|{self.precision}{tc}'
 
     def fftfreq(self):
         if self.source is not None:
@@ -175,7 +188,8 @@ class PowerSpectra:
             msg = 'PowerSpectra requires a finite source'
             raise ValueError(msg)
         x = self._samples_device()
-        return D.calc_csm(x, self.block_size, self.window, self.overlap, self.precision)
+        prec = f'tc_{self.tc_precision}' if self.form == 'tc' else self.precision
+        return D.calc_csm(x, self.block_size, self.window, self.overlap, prec)
 
     def calc_csm(self) -> np.ndarray:
         """CSM of the source for all ``block_size/2 + 1`` bins, (F, M, M) complex128."""

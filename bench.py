@@ -487,7 +487,10 @@ def main():
     norm = M / (M - 1.0)
     out = torch.empty((nbins, G), dtype=torch.float64, device=dev)
     K = D.num_windows(wl.num_samples, N, 2)
-    ws_bytes = NAT.lib().acb_csm_workspace_bytes(M, F, K, NAT.C128)
+    prec = args.tc_precision
+    # the CSM in the same form as the map: FP64 Gram for the FP64 form, tensor-core Gram otherwise
+    csm_prec = 'complex128' if form == 'f64' else f'tc_{prec}'
+    ws_bytes = NAT.lib().acb_csm_workspace_bytes(M, F, K, D.CSM_PRECISIONS[csm_prec])
     workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     csm_up = torch.zeros((F, M, M), dtype=torch.complex128, device=dev)
     csm_full = torch.empty((F, M, M), dtype=torch.complex128, device=dev)
@@ -496,13 +499,12 @@ def main():
     ev_map = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ev_csm = torch.cuda.Event(enable_timing=True)
     map_ms, csm_ms = [], []
-    prec = args.tc_precision
 
     def step(record=False):
         if record:
             ev_csm.record()
         csm_up.zero_()
-        D.csm_upper_accumulate(samples, N, 'Hanning', '50%', csm_upper=csm_up, workspace=workspace,
+        D.csm_upper_accumulate(samples, N, 'Hanning', '50%', precision=csm_prec, csm_upper=csm_up, workspace=workspace,
                                max_workspace_bytes=ws_bytes)
         D.csm_finalize(csm_up, scale, out=csm_full)
         c = csm_full if nbins == F else csm_full[:nbins]
@@ -555,7 +557,10 @@ def main():
         return ev[0].elapsed_time(ev[1]) / reps, r
 
     c_all = csm_full if nbins == F else csm_full[:nbins]
-    cs, ks = c_all[sel].contiguous(), kvec[sel].contiguous()
+    # reference: the FP64 CSM (the reference's arithmetic) and the plain FP64 map on it
+    del workspace
+    csm64 = c_all if csm_prec == 'complex128' else D.calc_csm(samples, N, 'Hanning', '50%', 'complex128')[:nbins]
+    cs, ks = csm64[sel].contiguous(), kvec[sel].contiguous()
     f64_ms, ref_t = timed(lambda: D.map_f64(cs, ks, mpos, gpos, args.steer, True, norm), reps=1)
     ref_map = ref_t.cpu().numpy()
     forms['f64'] = {'rate': len(acc_bins) * G / (f64_ms / 1e3), 'bins_timed': len(acc_bins)}
@@ -574,10 +579,14 @@ def main():
         for pr in ('bf16x3', 'tf32'):
             o = out if pr == prec else out2
             t_ms, _ = timed(lambda: D.map_tc(c_all, kvec, mpos, gpos, args.steer, True, norm, out=o, precision=pr))
-            forms[f'tc_{pr}'] = {'rate': units / (t_ms / 1e3), 'map_ms': t_ms, **acc_of(o),
-                                 'tc_over_f64': units / (t_ms / 1e3) / forms['f64']['rate']}
-        accuracy = {'vs': 'plain FP64 form (reference method on the GPU)', 'bins': acc_bins.tolist(),
-                    **acc_of(out),
+            forms[f'tc_{pr}'] = {'rate': units / (t_ms / 1e3), 'map_ms': t_ms, 'tc_over_f64':
+                                 units / (t_ms / 1e3) / forms['f64']['rate'],
+                                 'map_only_err': acc_of(D.map_tc(csm64, kvec, mpos, gpos, args.steer, True, norm,
+                                                                 precision=pr))}
+            if pr == prec:
+                forms[f'tc_{pr}']['end_to_end_err'] = acc_of(o)
+        accuracy = {'vs': 'FP64 CSM + plain FP64 map (the reference arithmetic on the GPU)',
+                    'timed_path': f'{csm_prec} CSM + tc {prec} map', 'bins': acc_bins.tolist(), **acc_of(out),
                     'definition': '|map - ref| / max|ref| per bin; L_p difference at the reference peak'}
 
     # map kernel roofline: algorithmic flops 8 M^2 + 8 M per grid-pt x bin
@@ -614,7 +623,8 @@ def main():
         ts = ac.TimeSamples(data=host, sample_freq=wl.fs)
         times = []
         for i in range(2 + max(1, min(args.steps, 3))):
-            ps = ac.PowerSpectra(source=ts, block_size=N, window='Hanning', overlap='50%')
+            ps = ac.PowerSpectra(source=ts, block_size=N, window='Hanning', overlap='50%',
+                                 form='f64' if form == 'f64' else 'tc', tc_precision=prec)
             st = ac.SteeringVector(grid=wl.grid, mics=wl.mics, steer_type=args.steer)
             bb = ac.BeamformerBase(freq_data=ps, steer=st, r_diag=True, form=form, tc_precision=prec)
             torch.cuda.synchronize()
@@ -639,12 +649,12 @@ def main():
                                                        'bf16x3 (split) / f32 accum'),
                 'data': 'synthetic (seeded monopoles, GPU-generated)',
                 'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': nbins, 'block_size': N,
-                           'windows': K, 'steer_type': args.steer, 'r_diag': True, 'form': form,
+                           'windows': K, 'steer_type': args.steer, 'r_diag': True, 'form': form, 'csm': csm_prec,
                            'l2': 'inputs larger than L2 (samples 524 MB, CSM 538 MB, map 660 MB)',
                            'parallelism': f'{ws} independent instances (one per GPU)'},
                 'map_ms_per_step': map_avg, 'csm_ms_per_step': float(np.mean(csm_ms)),
                 'csm_rate': {'value': units / (float(np.mean(csm_ms)) / 1e3), 'unit': UNIT,
-                             'note': 'CSM stage alone (FFT + FP64 Welch Gram + finish), all bins'},
+                             'note': f'CSM stage alone (FFT + {csm_prec} Welch Gram + finish), all bins'},
                 'forms': forms, 'gemm_peaks_here': gp,
                 'roofline': roof, 'accuracy': accuracy, 'cpu_baseline': cpu, 'e2e': e2e,
                 'gpu_launches': None, 'clocks': clk.summary()}

@@ -36,7 +36,10 @@ enum acb_status {
 };
 
 enum acb_steer { ACB_STEER_CLASSIC = 1, ACB_STEER_INVERSE = 2, ACB_STEER_TRUE_LEVEL = 3, ACB_STEER_TRUE_LOCATION = 4 };
-enum acb_precision { ACB_C128 = 0, ACB_C64 = 1 };
+/* CSM precision: complex128 / complex64 spectra and Welch sums (the reference's `precision`), or the
+ * tensor-core form (no counterpart in the reference): FP64 FFT, spectra rounded to TF32 or split
+ * into BF16 hi + lo, Gram on tcgen05 with FP32 accumulation, summed into a complex128 csm_upper. */
+enum acb_precision { ACB_C128 = 0, ACB_C64 = 1, ACB_CSM_TC_TF32 = 2, ACB_CSM_TC_BF16X3 = 3 };
 enum acb_sample_dtype { ACB_F32 = 0, ACB_F64 = 1 };
 
 /* Human-readable text of a status code (static storage). */
@@ -69,7 +72,8 @@ size_t acb_csm_workspace_bytes(int num_mics, int num_bins, int64_t num_windows, 
  *     csm_upper[f, r, c] += conj(X[f, c]) * X[f, r]     for r <= c       (in `precision`)
  * samples: [num_samples][num_mics], float32 or float64 (sample_dtype).
  * window: float64 [block_size].  twiddle: complex128 [block_size/2], exp(-2*pi*i*k/block_size).
- * csm_upper: [num_bins][num_mics][num_mics] in `precision`; only r <= c is written.
+ * csm_upper: [num_bins][num_mics][num_mics] in `precision` (complex128 for the tensor-core forms,
+ * num_mics <= 4032 there); only r <= c is written.
  * block_size: power of two, 16 <= block_size <= 16384.  workspace: >= acb_csm_workspace_bytes. */
 int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_samples, int num_mics,
                        int block_size, int hop, int64_t first_window, int64_t num_windows,
