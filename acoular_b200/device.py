@@ -136,6 +136,19 @@ def csm_upper_accumulate(samples: torch.Tensor, block_size: int, window: str, ov
     return csm_upper, K
 
 
+_copy_streams: dict = {}
+
+
+def copy_stream(device) -> torch.cuda.Stream:
+    """A side stream per device for host<->device copies that overlap the computation."""
+    key = str(device)
+    s = _copy_streams.get(key)
+    if s is None:
+        s = torch.cuda.Stream(device=device)
+        _copy_streams[key] = s
+    return s
+
+
 def csm_finalize(csm_upper: torch.Tensor, scale: float, out: torch.Tensor | None = None) -> torch.Tensor:
     nb, M, _ = csm_upper.shape
     prec = N.C64 if csm_upper.dtype == torch.complex64 else N.C128

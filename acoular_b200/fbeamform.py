@@ -24,23 +24,16 @@ from . import device as D
 from .environments import Environment
 
 
-def _zeros_pinned(shape, dtype):
-    """Zero-filled result array in page-locked host memory when a GPU is present (fast copies)."""
+def _result_array(shape, dtype):
+    """Result array in page-locked host memory when a GPU is present (fast, asynchronous copies).
+
+    Left uninitialised: ``LazyBfResult`` returns a bin only after ``_calc`` has written it, so no
+    unwritten row is ever read (zero-filling 0.5 GB of host memory would cost tens of ms per result).
+    """
     if torch.cuda.is_available():
-        t = torch.zeros(shape, dtype=getattr(torch, np.dtype(dtype).name), pin_memory=True)
+        t = torch.empty(shape, dtype=getattr(torch, np.dtype(dtype).name), pin_memory=True)
         return t.numpy()
     return np.zeros(shape, dtype=dtype)
-
-
-_copy_streams: dict = {}
-
-
-def _copy_stream(dev):
-    s = _copy_streams.get(str(dev))
-    if s is None:
-        s = torch.cuda.Stream(device=dev)
-        _copy_streams[str(dev)] = s
-    return s
 
 
 class SteeringVector:
@@ -173,7 +166,7 @@ class BeamformerBase:
             self._f = self.freq_data.fftfreq()
             self._numfreq = self._f.shape[0]
             self._assert_equal_channels()
-            self._ac = _zeros_pinned((self._numfreq, self.steer.grid.size), self.precision)
+            self._ac = _result_array((self._numfreq, self.steer.grid.size), self.precision)
             self._fr = np.zeros(self._numfreq, dtype='int8')
             self._key = key
         return LazyBfResult(self)
@@ -211,14 +204,14 @@ class BeamformerBase:
         G = gpos.shape[1]
         M = mpos.shape[1]
         cap = self.max_bins_per_launch or max(1, int((1 << 30) // max(1, G * 8 + M * M * 16)))
-        # a few launches so that the copy of one overlaps the next one's computation
-        cap = min(cap, max(1, -(-ind.size // 4)))
+        # several launches so that the copy of one overlaps the next one's computation
+        cap = min(cap, max(1, -(-ind.size // 8)))
         norm = self.sig_loss_norm()
         ref = self.steer.ref
         ac_t = torch.from_numpy(self._ac)
         pinned = ac_t.is_pinned()
         compute = torch.cuda.current_stream(dev)
-        copy = _copy_stream(dev)
+        copy = D.copy_stream(dev)
         pending = []
         for s0 in range(0, ind.size, cap):
             sub = ind[s0:s0 + cap]

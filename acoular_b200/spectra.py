@@ -162,9 +162,9 @@ class PowerSpectra:
     def _device(self):
         return D.require_cuda(self.device)
 
-    def _samples_device(self) -> torch.Tensor:
+    def _samples_host_or_device(self) -> torch.Tensor:
+        """The source samples as a (S, M) float32/float64 tensor, wherever they live."""
         t = self.source
-        dev = self._device()
         data = getattr(t, 'data', None)
         if data is None:
             data = t.as_array()
@@ -177,9 +177,51 @@ class PowerSpectra:
             x = torch.from_numpy(arr)
         if x.dtype not in (torch.float32, torch.float64):
             x = x.to(torch.float64)
+        return x
+
+    def _samples_device(self) -> torch.Tensor:
+        x = self._samples_host_or_device()
         if x.device.type == 'cpu':
-            x = x.to(dev, non_blocking=x.is_pinned())
+            x = x.to(self._device(), non_blocking=x.is_pinned())
         return x.contiguous()
+
+    def _csm_streamed(self, x: torch.Tensor, prec: str, nchunks: int = 8) -> torch.Tensor:
+        """CSM of pinned host samples: the samples go to the device in chunks of windows on a copy
+        stream, and each chunk's Welch sums are accumulated as soon as its rows have landed, so the
+        upload overlaps the FFT and Gram of the previous chunks.  Same sums as one pass."""
+        dev = self._device()
+        S, M = x.shape
+        N = self.block_size
+        ov = D.OVERLAPS[self.overlap]
+        hop = N // ov
+        K = D.num_windows(S, N, ov)
+        F = N // 2 + 1
+        xd = torch.empty((S, M), dtype=x.dtype, device=dev)
+        cdt = torch.complex64 if prec == 'complex64' else torch.complex128
+        up = torch.zeros((F, M, M), dtype=cdt, device=dev)
+        compute = torch.cuda.current_stream(dev)
+        copy = D.copy_stream(dev)
+        copy.wait_stream(compute)              # xd is ready for writing
+        per = -(-K // nchunks)                 # windows per chunk, in whole blocks of 32
+        wc = max(32, (per + 31) // 32 * 32)
+        rows = 0
+        for w0 in range(0, max(K, 1), wc):
+            w1 = min(K, w0 + wc)
+            need = S if w1 >= K else (w1 - 1) * hop + N
+            if need > rows:
+                with torch.cuda.stream(copy):
+                    xd[rows:need].copy_(x[rows:need], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy)
+                compute.wait_event(ev)
+                rows = need
+            if w1 > w0:
+                D.csm_upper_accumulate(xd, N, self.window, self.overlap, prec, csm_upper=up, first_window=w0,
+                                       windows=w1 - w0)
+        _, weight = D.window_vector(self.window, N, dev)
+        with np.errstate(divide='ignore', invalid='ignore'):
+            scale = np.float64(2.0 / N) / np.float64(weight) / np.float64(D.num_blocks(S, N, ov))
+        return D.csm_finalize(up, float(scale))
 
     def calc_csm_device(self) -> torch.Tensor:
         """The CSM (F, M, M) complex128 as a device tensor (see :meth:`calc_csm`)."""
@@ -187,8 +229,11 @@ class PowerSpectra:
         if t.num_samples == -1:
             msg = 'PowerSpectra requires a finite source'
             raise ValueError(msg)
-        x = self._samples_device()
         prec = f'tc_{self.tc_precision}' if self.form == 'tc' else self.precision
+        x = self._samples_host_or_device()
+        if x.device.type == 'cpu' and x.is_pinned() and x.is_contiguous() and x.numel() >= (1 << 22):
+            return self._csm_streamed(x, prec)
+        x = self._samples_device()
         return D.calc_csm(x, self.block_size, self.window, self.overlap, prec)
 
     def calc_csm(self) -> np.ndarray:

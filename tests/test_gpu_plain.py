@@ -209,3 +209,23 @@ def test_beamformer_base_end_to_end(golden, dev):
             assert (bb._fr[18:23] == 1).all() and bb._fr.sum() == 5
     lp = ac.L_p(pm)
     assert np.isfinite(lp).all()
+
+
+def test_powerspectra_streamed_upload_same_csm():
+    """Pinned host samples are uploaded in chunks that overlap the CSM accumulation; the result equals
+    the one-pass CSM of the same samples on the device (FP64: the same sums in the same order)."""
+    import acoular_b200 as ac
+    from acoular_b200 import device as D
+    rng = np.random.RandomState(11)
+    x = torch.from_numpy(rng.randn(300000, 24).astype(np.float32)).pin_memory()
+    ts = ac.TimeSamples(data=x, sample_freq=51200.0)
+    for form in ('f64', 'tc'):
+        ps = ac.PowerSpectra(source=ts, block_size=512, window='Hanning', overlap='50%', form=form)
+        got = ps.csm_device.cpu().numpy()
+        prec = 'complex128' if form == 'f64' else 'tc_tf32'
+        ref = D.calc_csm(x.cuda(), 512, 'Hanning', '50%', prec).cpu().numpy()
+        if form == 'f64':
+            assert np.array_equal(got, ref)
+        else:
+            # FP32 accumulation per chunk of windows instead of one chunk: a few ulp(FP32) apart
+            assert np.abs(got - ref).max() <= 2e-5 * np.abs(ref).max()
