@@ -364,7 +364,7 @@ const char *acb_status_string(int s)
     }
 }
 
-int acb_abi_version(void) { return 1; }
+int acb_abi_version(void) { return 2; }   // 2: tensor-core tuning fields, TC CSM forms, eigenvalue maps
 
 const char *acb_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
 

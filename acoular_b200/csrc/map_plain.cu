@@ -124,6 +124,34 @@ __device__ __forceinline__ void quad_block(const double2 *__restrict__ C, int M,
     }
 }
 
+// Normalisation of the steering type (acoular/fastFuncs.py:293-310) and clipping of negatives.
+__device__ __forceinline__ void finish_plain(const MapArgs &a, double scalar, double S, double r0, int bin, int64_t g,
+                                             double *out_map, double *out_norm)
+{
+    const double Md = (double)a.M;
+    double res, ns;
+    if (a.steer_type == 1) {
+        ns = 1.0 / Md;
+        res = scalar / (Md * Md) * a.norm;
+    } else if (a.steer_type == 2) {
+        const double nf = Md * r0;
+        const double nf2 = nf * nf;
+        ns = S / nf2;
+        res = scalar / nf2 * a.norm;
+    } else if (a.steer_type == 3) {
+        const double nf = r0 * S;
+        ns = 1.0 / (r0 * r0) / S;
+        res = scalar / (nf * nf) * a.norm;
+    } else {
+        const double nf = Md * S;
+        ns = 1.0 / Md;
+        res = scalar / nf * a.norm;
+    }
+    if (a.clip && res < 0.0) res = 0.0;
+    out_map[(int64_t)bin * a.G + g] = res;
+    if (out_norm) out_norm[(int64_t)bin * a.G + g] = ns;
+}
+
 template <bool USE_RM>
 __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2 *__restrict__ csm,
                                                         const double *__restrict__ wavenumber, double k_scalar,
@@ -201,28 +229,112 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
         if (a.ref_mode == 1) r0 = a.ref_dist;
         else if (USE_RM) r0 = r0_in[g];
         else r0 = dist3(g0, g1, g2, a.ref0, a.ref1, a.ref2);
-        const double Md = (double)M;
-        double res, ns;
-        if (a.steer_type == 1) {
-            ns = 1.0 / Md;
-            res = scalar / (Md * Md) * a.norm;
-        } else if (a.steer_type == 2) {
-            const double nf = Md * r0;
-            const double nf2 = nf * nf;
-            ns = S / nf2;
-            res = scalar / nf2 * a.norm;
-        } else if (a.steer_type == 3) {
-            const double nf = r0 * S;
-            ns = 1.0 / (r0 * r0) / S;
-            res = scalar / (nf * nf) * a.norm;
-        } else {
-            const double nf = Md * S;
-            ns = 1.0 / Md;
-            res = scalar / nf * a.norm;
+        finish_plain(a, scalar, S, r0, bin, g, out_map, out_norm);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Eigenvalue form of _freqBeamformer_EigValues (acoular/fastFuncs.py:313-411): with eigenvalues
+// lambda_e and eigenvectors V[:, e] of the CSM (E of them),
+//     scalar = sum_e lambda_e (|sum_m conj(V[m][e]) h[m]|^2 - [r_diag] sum_m |conj(V[m][e]) h[m]|^2),
+// then the steering-type normalisation of the full-CSM form.  Same steering synthesis (float32
+// phase, libm-faithful cos/sin) as map_plain_kernel; the warps take the eigenvectors in groups of
+// 32 (four per warp, partial sums in registers across mic chunks), each eigenvector's mic sum in
+// the reference's order.  Cost O(G M E) per bin.
+// ------------------------------------------------------------------------------------------------
+constexpr int kEigPerWarp = 4;
+
+template <bool USE_RM>
+__global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const double *__restrict__ eigval,
+                                                      const double2 *__restrict__ eigvec,
+                                                      const double *__restrict__ wavenumber, double k_scalar,
+                                                      const double *__restrict__ mpos, const double *__restrict__ gpos,
+                                                      const double *__restrict__ r0_in, const double *__restrict__ rm,
+                                                      int mc, double *__restrict__ out_map,
+                                                      double *__restrict__ out_norm)
+{
+    extern __shared__ double smem[];
+    const int M = a.M;
+    double *mp = smem;                                                     // [3][M]
+    double2 *hs = reinterpret_cast<double2 *>(smem + ((3 * M + 1) & ~1));  // [mc][32]
+    __shared__ double red_sc[kWarps][kLanes], red_s[kWarps][kLanes];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int bin = blockIdx.y;
+    const int64_t g = (int64_t)blockIdx.x * kLanes + lane;
+    const bool gvalid = g < a.G;
+    const double k = wavenumber ? wavenumber[bin] : k_scalar;
+    const double *lam = eigval + (int64_t)bin * E;
+    const double2 *V = eigvec + (int64_t)bin * M * E;
+
+    if (!USE_RM)
+        for (int i = threadIdx.x; i < 3 * M; i += blockDim.x) mp[i] = mpos[i];
+    double g0 = 0, g1 = 0, g2 = 0;
+    if (gvalid && !USE_RM) {
+        g0 = gpos[g];
+        g1 = gpos[a.G + g];
+        g2 = gpos[2 * a.G + g];
+    }
+    __syncthreads();
+
+    double s_part = 0.0;
+    if (gvalid && a.steer_type >= 2) {
+        for (int m = warp; m < M; m += kWarps) {
+            const double r = grid_mic_dist<USE_RM>(a, rm, g, m, g0, g1, g2, mp);
+            s_part += (a.steer_type == 2) ? r * r : 1.0 / (r * r);
         }
-        if (a.clip && res < 0.0) res = 0.0;
-        out_map[(int64_t)bin * a.G + g] = res;
-        if (out_norm) out_norm[(int64_t)bin * a.G + g] = ns;
+    }
+
+    double scal = 0.0;
+    const int nchunks = (M + mc - 1) / mc;
+    for (int eg = 0; eg < E; eg += kWarps * kEigPerWarp) {
+        double fr[kEigPerWarp], fi[kEigPerWarp], dg[kEigPerWarp];
+#pragma unroll
+        for (int j = 0; j < kEigPerWarp; ++j) fr[j] = fi[j] = dg[j] = 0.0;
+        const int e0 = eg + warp * kEigPerWarp;
+        for (int ca = 0; ca < nchunks; ++ca) {
+            const int m0 = ca * mc, n = min(mc, M - m0);
+            synth_chunk<USE_RM>(a, rm, k, g, gvalid, g0, g1, g2, mp, m0, n, hs);
+            __syncthreads();
+            for (int mm = 0; mm < n; ++mm) {
+                const double2 h = hs[mm * kLanes + lane];
+                const double2 *vrow = V + (int64_t)(m0 + mm) * E;
+#pragma unroll
+                for (int j = 0; j < kEigPerWarp; ++j) {
+                    if (e0 + j >= E) break;
+                    const double2 v = __ldg(vrow + e0 + j);
+                    // temp1 = conj(V[m][e]) * h[m]
+                    const double tr = v.x * h.x + v.y * h.y, ti = v.x * h.y - v.y * h.x;
+                    fr[j] += tr;
+                    fi[j] += ti;
+                    if (a.r_diag) dg[j] += tr * tr + ti * ti;
+                }
+            }
+            __syncthreads();   // hs is rewritten by the next chunk
+        }
+#pragma unroll
+        for (int j = 0; j < kEigPerWarp; ++j) {
+            if (e0 + j >= E) break;
+            const double full = fr[j] * fr[j] + fi[j] * fi[j];
+            scal += (a.r_diag ? full - dg[j] : full) * lam[e0 + j];
+        }
+    }
+
+    red_sc[warp][lane] = scal;
+    red_s[warp][lane] = s_part;
+    __syncthreads();
+    if (warp == 0 && gvalid) {
+        double sc = 0.0, S = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            sc += red_sc[w][lane];
+            S += red_s[w][lane];
+        }
+        double r0;
+        if (a.ref_mode == 1) r0 = a.ref_dist;
+        else if (USE_RM) r0 = r0_in[g];
+        else r0 = dist3(g0, g1, g2, a.ref0, a.ref1, a.ref2);
+        finish_plain(a, sc, S, r0, bin, g, out_map, out_norm);
     }
 }
 
@@ -270,6 +382,21 @@ static int launch_plain(const MapArgs &a, int nbins, const void *csm, const doub
     return check_launch();
 }
 
+template <bool USE_RM>
+static int launch_eig(const MapArgs &a, int nbins, int E, const double *eigval, const void *eigvec, const double *k,
+                      double k_scalar, const double *mpos, const double *gpos, const double *r0, const double *rm,
+                      double *out_map, double *out_norm, cudaStream_t s)
+{
+    const int mc = a.M <= 256 ? a.M : 128;
+    const size_t smem = (size_t)(((3 * a.M + 1) & ~1) * sizeof(double)) + (size_t)mc * kLanes * sizeof(double2);
+    auto kern = map_eig_kernel<USE_RM>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const dim3 grid((unsigned)((a.G + kLanes - 1) / kLanes), nbins);
+    kern<<<grid, kLanes * kWarps, smem, s>>>(a, E, eigval, reinterpret_cast<const double2 *>(eigvec), k, k_scalar, mpos,
+                                            gpos, r0, rm, mc, out_map, out_norm);
+    return check_launch();
+}
+
 }  // namespace acb
 
 using namespace acb;
@@ -287,6 +414,35 @@ int acb_map_f64(const acb_map_params *p, const void *csm, const double *wavenumb
     if ((a.G + kLanes - 1) / kLanes > 0x7fffffffLL) return ACB_ERR_SHAPE;
     return launch_plain<false>(a, p->num_bins, csm, wavenumber, 0.0, mpos, gpos, nullptr, nullptr, out_map,
                                out_steer_norm, as_stream(stream));
+}
+
+int acb_map_eig_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,
+                    const double *wavenumber, const double *mpos, const double *gpos, double *out_map,
+                    double *out_steer_norm, void *stream)
+{
+    MapArgs a;
+    int st = make_args(p, a);
+    if (st) return st;
+    if (!eigval || !eigvec || !wavenumber || !mpos || !gpos || !out_map) return ACB_ERR_ARG;
+    if (num_eigs < 1 || num_eigs > p->num_mics) return ACB_ERR_SHAPE;
+    if ((a.G + kLanes - 1) / kLanes > 0x7fffffffLL) return ACB_ERR_SHAPE;
+    return launch_eig<false>(a, p->num_bins, num_eigs, eigval, eigvec, wavenumber, 0.0, mpos, gpos, nullptr, nullptr,
+                             out_map, out_steer_norm, as_stream(stream));
+}
+
+int acb_beamformer_freq_eig_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,
+                                double wavenumber, const double *r0, const double *rm, double *out_map,
+                                double *out_steer_norm, void *stream)
+{
+    MapArgs a;
+    int st = make_args(p, a);
+    if (st) return st;
+    if (p->num_bins != 1) return ACB_ERR_SHAPE;
+    if (!eigval || !eigvec || !r0 || !rm || !out_map) return ACB_ERR_ARG;
+    if (num_eigs < 1 || num_eigs > p->num_mics) return ACB_ERR_SHAPE;
+    a.ref_mode = 0;
+    return launch_eig<true>(a, 1, num_eigs, eigval, eigvec, nullptr, wavenumber, nullptr, nullptr, r0, rm, out_map,
+                            out_steer_norm, as_stream(stream));
 }
 
 int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wavenumber, const double *r0,

@@ -277,6 +277,30 @@ def map_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, mpos: torch.Tensor, gp
     return out
 
 
+def map_eig_f64(eigval: torch.Tensor, eigvec: torch.Tensor, wavenumbers: torch.Tensor, mpos: torch.Tensor,
+                gpos: torch.Tensor, steer_type: str, r_diag: bool, norm: float, ref=None, clip_negative=None,
+                glibc_faithful=True, out: torch.Tensor | None = None,
+                steer_norm: torch.Tensor | None = None) -> torch.Tensor:
+    """Eigenvalue form of the plain FP64 map for B bins: eigval (B, E) float64, eigvec (B, M, E)
+    complex128 (columns = eigenvectors), wavenumbers (B,) -> (B, G) float64."""
+    B, M, E = eigvec.shape
+    if tuple(eigval.shape) != (B, E):
+        msg = 'eigval must be (num_bins, num_eigs) and eigvec (num_bins, num_mics, num_eigs)'
+        raise ValueError(msg)
+    if not (eigval.is_contiguous() and eigvec.is_contiguous()):
+        msg = 'eigval and eigvec must be contiguous'
+        raise ValueError(msg)
+    G = gpos.shape[1]
+    dev = eigvec.device
+    p = map_params(M, G, B, steer_type, r_diag, norm, clip_negative, ref, glibc_faithful, dev)
+    if out is None:
+        out = torch.empty((B, G), dtype=torch.float64, device=dev)
+    N.check(N.lib().acb_map_eig_f64(ctypes.byref(p), E, eigval.data_ptr(), eigvec.data_ptr(), wavenumbers.data_ptr(),
+                                    mpos.data_ptr(), gpos.data_ptr(), out.data_ptr(), N.ptr(steer_norm),
+                                    N.stream_handle()), 'acb_map_eig_f64')
+    return out
+
+
 _tc_ws: dict = {}
 
 

@@ -51,8 +51,8 @@ def calcCSM(csm: np.ndarray, SpecAllMics: np.ndarray) -> np.ndarray:  # noqa: N8
 
 def beamformerFreq(steerVecType, boolRemovedDiagOfCSM, normFactor, inputTupleSteer, inputTupleCsm,  # noqa: N802, N803
                    glibc_faithful: bool = True):
-    if steerVecType == 'custom' or isinstance(inputTupleCsm, tuple):
-        msg = "custom steering vectors and the eigenvalue form of beamformerFreq are not implemented"
+    if steerVecType == 'custom':
+        msg = "custom steering vectors of beamformerFreq are not implemented"
         raise NotImplementedError(msg)
     if steerVecType not in N.STEER_CODES:
         raise KeyError(steerVecType)
@@ -61,6 +61,9 @@ def beamformerFreq(steerVecType, boolRemovedDiagOfCSM, normFactor, inputTupleSte
         k = k.reshape(-1)[0]
     _check_contig(r0, np.float64, 'distGridToArrayCenter')
     _check_contig(rm, np.float64, 'distGridToAllMics')
+    if isinstance(inputTupleCsm, tuple):
+        return _beamformer_freq_eig(steerVecType, boolRemovedDiagOfCSM, normFactor, r0, rm, float(k), *inputTupleCsm,
+                                    glibc_faithful=glibc_faithful)
     _check_contig(inputTupleCsm, np.complex128, 'csm')
     G, M = rm.shape
     if r0.shape != (G,) or inputTupleCsm.shape != (M, M):
@@ -77,4 +80,33 @@ def beamformerFreq(steerVecType, boolRemovedDiagOfCSM, normFactor, inputTupleSte
     N.check(N.lib().acb_beamformer_freq_f64(ctypes.byref(p), csm_d.data_ptr(), float(k), r0_d.data_ptr(),
                                             rm_d.data_ptr(), out.data_ptr(), nrm.data_ptr(), N.stream_handle()),
             'beamformerFreq')
+    return out.cpu().numpy(), nrm.cpu().numpy()
+
+
+def _beamformer_freq_eig(steer_type, r_diag, norm, r0, rm, k, eigval, eigvec, glibc_faithful=True):
+    """beamformerFreq with an eigen tuple (eigVal[E] float64, eigVec[M, E] complex128):
+    _freqBeamformer_EigValues (acoular/fastFuncs.py:313-411) on the device."""
+    eigval = np.asarray(eigval)
+    eigvec = np.ascontiguousarray(eigvec)
+    _check_contig(eigval, np.float64, 'eigVal')
+    if eigvec.dtype != np.complex128:
+        msg = 'eigVec must be complex128'
+        raise TypeError(msg)
+    G, M = rm.shape
+    E = eigval.shape[0]
+    if r0.shape != (G,) or eigvec.shape != (M, E):
+        msg = 'shape mismatch between r0 (G,), rm (G, M), eigVal (E,) and eigVec (M, E)'
+        raise ValueError(msg)
+    dev = D.require_cuda()
+    ev_d = torch.from_numpy(eigval).to(dev)
+    evec_d = torch.from_numpy(eigvec).to(dev)
+    r0_d = torch.from_numpy(r0).to(dev)
+    rm_d = torch.from_numpy(rm).to(dev)
+    out = torch.empty(G, dtype=torch.float64, device=dev)
+    nrm = torch.empty(G, dtype=torch.float64, device=dev)
+    p = D.map_params(M, G, 1, steer_type, r_diag, norm, clip_negative=False, ref=None, glibc_faithful=glibc_faithful,
+                     device=dev)
+    N.check(N.lib().acb_beamformer_freq_eig_f64(ctypes.byref(p), E, ev_d.data_ptr(), evec_d.data_ptr(), float(k),
+                                                r0_d.data_ptr(), rm_d.data_ptr(), out.data_ptr(), nrm.data_ptr(),
+                                                N.stream_handle()), 'beamformerFreq')
     return out.cpu().numpy(), nrm.cpu().numpy()

@@ -319,6 +319,86 @@ class BeamformerBase:
         return h
 
 
+class BeamformerEig(BeamformerBase):
+    """Eigenvalue beamformer (acoular/fbeamform.py:821-888): the map of one eigen-component of the CSM.
+
+    ``n`` selects the component (0 = smallest eigenvalue ... num_mics - 1; negative counts from the
+    largest; default -1, the largest); ``na`` is the resolved index.  The eigen-decomposition runs on
+    the device (``PowerSpectra.evd_device``); the map runs in the plain FP64 form (``acb_map_eig_f64``,
+    cost O(G M) per bin and component), with the reference's steering arithmetic.
+    """
+
+    def __init__(self, *args, n: int = -1, **kw):
+        super().__init__(*args, **kw)
+        self.n = int(n)
+
+    @property
+    def digest(self) -> str:
+        return super().digest + f'|eig{self.n}'
+
+    @property
+    def na(self) -> int:
+        na = self.n
+        nm = self.steer.mics.num_mics
+        if na < 0:
+            na = max(nm + na, 0)
+        return min(nm - 1, na)
+
+    def _eig_select(self, ev, evec, ind):
+        na = self.na
+        return ev[ind, na:na + 1].contiguous(), evec[ind][:, :, na:na + 1].contiguous(), self.sig_loss_norm()
+
+    def _post(self, out):
+        if self.r_diag:
+            out.clamp_(min=0.0)
+        return out
+
+    def _calc(self, ind):
+        ind = np.asarray(ind, dtype=np.int64)
+        if ind.size == 0:
+            return
+        ev, evec = self.freq_data.evd_device
+        dev = ev.device
+        mpos, gpos = self._geometry(dev)
+        ind_d = torch.as_tensor(ind, device=dev)
+        lam, vec, norm = self._eig_select(ev, evec, ind_d)
+        k = torch.as_tensor(2 * np.pi * self._f[ind] / self.steer.env.c, dtype=torch.float64, device=dev)
+        out = D.map_eig_f64(lam, vec, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm, ref=self.steer.ref,
+                            clip_negative=False, glibc_faithful=self.glibc_faithful)
+        out = self._post(out)
+        if self.precision == 'float32':
+            out = out.float()
+        self._ac[ind] = out.cpu().numpy()
+        self._fr[ind] = 1
+
+
+class BeamformerMusic(BeamformerEig):
+    """MUSIC (acoular/fbeamform.py:891-944): the noise subspace, the ``num_mics - na`` smallest
+    eigen-components, full CSM; each bin's map is returned as 4e-10 * min / map.  ``n`` is the
+    assumed number of sources (default 1); ``r_diag`` is False and ``r_diag_norm`` 1.0."""
+
+    def __init__(self, *args, n: int = 1, **kw):
+        kw.setdefault('r_diag', False)
+        kw.setdefault('r_diag_norm', 1.0)
+        super().__init__(*args, n=n, **kw)
+        if self.r_diag:
+            msg = 'BeamformerMusic is defined for the full CSM only (r_diag=False)'
+            raise ValueError(msg)
+
+    @property
+    def digest(self) -> str:
+        return super().digest + '|music'
+
+    def _eig_select(self, ev, evec, ind):
+        M = self.steer.mics.num_mics
+        ne = int(M - self.na)
+        norm = self.sig_loss_norm() * float(self.freq_data.num_channels) ** 2
+        return ev[ind, :ne].contiguous(), evec[ind][:, :, :ne].contiguous(), norm
+
+    def _post(self, out):
+        return 4e-10 * out.min(dim=1, keepdim=True).values / out
+
+
 def L_p(x):
     """Sound pressure level 10 lg(x / 4e-10), floored at the dtype's eps (acoular/fbeamform.py:2412-2429)."""
     return 10 * np.log10(np.maximum(x / 4e-10, np.finfo(x.dtype).eps))

@@ -262,7 +262,25 @@ class PowerSpectra:
             self._csm_host = self.csm_device.cpu().numpy()
         return self._csm_host
 
-    # --- eigen-decomposition (acoular/spectra.py:351-364), host LAPACK ---------------------------
+    # --- eigen-decomposition (acoular/spectra.py:351-364) ---------------------------------------
+    @property
+    def evd_device(self):
+        """``(eigvals (F, M) float64, eigvecs (F, M, M) complex128)`` of the CSM on the device:
+        Hermitian eigh per bin (cuSOLVER through torch), eigenvalues ascending as numpy returns them.
+        The eigenvector phases may differ from LAPACK's; the eigenvalue beamformers depend on them only
+        through |v^H h|."""
+        self._refresh()
+        if getattr(self, '_evd_dev', None) is None or self._evd_dev[0] != self._cache_key:
+            csm = self.csm_device
+            ev = torch.empty(csm.shape[:2], dtype=torch.float64, device=csm.device)
+            evec = torch.empty_like(csm)
+            step = 64
+            for f0 in range(0, csm.shape[0], step):
+                ev[f0:f0 + step], evec[f0:f0 + step] = torch.linalg.eigh(csm[f0:f0 + step])
+            self._evd_dev = (self._cache_key, ev, evec)
+        return self._evd_dev[1], self._evd_dev[2]
+
+    # host LAPACK, as the reference
     def _get_evd(self):
         self._refresh()
         if self._evd is None:

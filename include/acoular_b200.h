@@ -123,6 +123,21 @@ typedef struct acb_map_params {
 int acb_map_f64(const acb_map_params *p, const void *csm, const double *wavenumber, const double *mpos,
                 const double *gpos, double *out_map, double *out_steer_norm, int *error_word, void *stream);
 
+/* Eigenvalue form, _freqBeamformer_EigValues (acoular/fastFuncs.py:313-411) batched over bins, as
+ * BeamformerEig._calc / BeamformerMusic._calc call it (acoular/fbeamform.py:852-944):
+ *   eigval: float64 [num_bins][num_eigs];  eigvec: complex128 [num_bins][M][num_eigs]
+ *   map = norm_steer(sum_e eigval[e] (|sum_m conj(eigvec[m][e]) h[m]|^2 - [r_diag] sum_m |..|^2))
+ * Plain FP64 form, the same steering synthesis as acb_map_f64.  1 <= num_eigs <= M. */
+int acb_map_eig_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,
+                    const double *wavenumber, const double *mpos, const double *gpos, double *out_map,
+                    double *out_steer_norm, void *stream);
+
+/* beamformerFreq with an eigen tuple (eigval[num_eigs], eigvec[M][num_eigs]) for one bin with
+ * precomputed distances r0 [G], rm [G][M] (acoular/fastFuncs.py:61-214). */
+int acb_beamformer_freq_eig_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,
+                                double wavenumber, const double *r0, const double *rm, double *out_map,
+                                double *out_steer_norm, void *stream);
+
 /* beamformerFreq drop-in (acoular/fastFuncs.py:61-214) for one bin with precomputed distances:
  *   r0: float64 [G] (distGridToArrayCenter), rm: float64 [G][M] (distGridToAllMics). */
 int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wavenumber, const double *r0,

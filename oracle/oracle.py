@@ -70,6 +70,8 @@ def lib():
         L.orc_dist_mat.argtypes = [dp, dp, i64, i64, dp]
         L.orc_beamformer_fullcsm.argtypes = [dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              ctypes.c_int, i64, i64, dp, dp]
+        L.orc_beamformer_eig.argtypes = [dp, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         i64, i64, i64, dp, dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -219,6 +221,65 @@ def beamformer_freq(steer_type: str, r_diag: bool, norm: float, r0: np.ndarray, 
     lib().orc_beamformer_fullcsm(_dp(csm), _dp(r0), _dp(rm), float(k), float(norm), int(bool(r_diag)),
                                  STEER_TYPES[steer_type], G, M, _dp(res), _dp(nrm))
     return res, nrm
+
+
+def beamformer_freq_eig(steer_type: str, r_diag: bool, norm: float, r0: np.ndarray, rm: np.ndarray, k: float,
+                        eigval: np.ndarray, eigvec: np.ndarray):
+    """``beamformerFreq`` with an eigen-decomposition tuple ``(eigval[E], eigvec[M, E])``
+    (fastFuncs.py:61-214 dispatching to _freqBeamformer_EigValues, fastFuncs.py:313-411)."""
+    eigval = np.ascontiguousarray(eigval, dtype=np.float64)
+    eigvec = np.ascontiguousarray(eigvec, dtype=np.complex128)
+    r0 = np.ascontiguousarray(r0, dtype=np.float64)
+    rm = np.ascontiguousarray(rm, dtype=np.float64)
+    G, M = rm.shape
+    E = eigval.shape[0]
+    res = np.zeros(G)
+    nrm = np.zeros(G)
+    lib().orc_beamformer_eig(_dp(eigval), _dp(eigvec), _dp(r0), _dp(rm), float(k), float(norm), int(bool(r_diag)),
+                             STEER_TYPES[steer_type], G, M, E, _dp(res), _dp(nrm))
+    return res, nrm
+
+
+def eig_na(n: int, num_mics: int) -> int:
+    """``BeamformerEig.na`` (acoular/fbeamform.py:844-850)."""
+    na = n
+    if na < 0:
+        na = max(num_mics + na, 0)
+    return min(num_mics - 1, na)
+
+
+def beamformer_eig_calc(eigvals, eigvecs, freqs, ind, r0, rm, c: float, steer_type: str, r_diag: bool, n: int = -1,
+                        r_diag_norm: float = 0.0, out=None):
+    """``BeamformerEig._calc`` (acoular/fbeamform.py:852-888): component ``na`` of each bin's eigh."""
+    G, M = rm.shape
+    if out is None:
+        out = np.zeros((eigvals.shape[0], G))
+    na = eig_na(n, M)
+    norm = sig_loss_norm(r_diag, M, r_diag_norm)
+    for i in ind:
+        b = beamformer_freq_eig(steer_type, r_diag, norm, r0, rm, 2 * np.pi * freqs[i] / c,
+                                np.array(eigvals[i], dtype='float64')[na:na + 1],
+                                np.array(eigvecs[i], dtype='complex128')[:, na:na + 1])[0]
+        if r_diag:
+            b[np.sign(b) < 0] = 0.0
+        out[i] = b
+    return out
+
+
+def beamformer_music_calc(eigvals, eigvecs, freqs, ind, r0, rm, c: float, steer_type: str, n: int = 1, out=None):
+    """``BeamformerMusic._calc`` (acoular/fbeamform.py:911-944): the M - na smallest components,
+    full CSM, normalised to 4e-10 * min / map."""
+    G, M = rm.shape
+    if out is None:
+        out = np.zeros((eigvals.shape[0], G))
+    ne = int(M - eig_na(n, M))
+    norm = sig_loss_norm(False, M, 1.0) * M ** 2
+    for i in ind:
+        b = beamformer_freq_eig(steer_type, False, norm, r0, rm, 2 * np.pi * freqs[i] / c,
+                                np.array(eigvals[i], dtype='float64')[:ne],
+                                np.array(eigvecs[i], dtype='complex128')[:, :ne])[0]
+        out[i] = 4e-10 * b.min() / b
+    return out
 
 
 def sig_loss_norm(r_diag: bool, num_mics: int, r_diag_norm: float = 0.0) -> float:

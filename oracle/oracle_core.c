@@ -178,6 +178,82 @@ void orc_beamformer_fullcsm(const double *csm, const double *r0, const double *r
     }
 }
 
+/* _freqBeamformer_EigValues (fastFuncs.py:313-411) for one frequency bin.
+ * eigval: [E]; eigvec: [M][E] interleaved complex128; r0: [G]; rm: [G][M]; k: wave number.
+ * Per grid point: steering as in the full-CSM kernel, then
+ *   scalar = sum_e eigval[e] * (|sum_m conj(V[m][e]) v[m]|^2 - [r_diag] sum_m |conj(V[m][e]) v[m]|^2).
+ * Writes result[G] and normsteer[G]. */
+void orc_beamformer_eig(const double *eigval, const double *eigvec, const double *r0, const double *rm, double k,
+                        double norm, int r_diag, int steer_type, int64_t G, int64_t M, int64_t E, double *result,
+                        double *normsteer)
+{
+    const int st2 = steer_type == 2;
+    const int st34 = steer_type == 3 || steer_type == 4;
+#pragma omp parallel
+    {
+        double *vr = (double *)__builtin_alloca(sizeof(double) * M);
+        double *vi = (double *)__builtin_alloca(sizeof(double) * M);
+#pragma omp for schedule(static)
+        for (int64_t gi = 0; gi < G; ++gi) {
+            const double *r = rm + gi * M;
+            double help = 0.0;
+            for (int64_t m = 0; m < M; ++m) {
+                const float arg = (float)(k * r[m]);
+                vr[m] = (double)cosf(arg);
+                vi[m] = -(double)sinf(arg);
+            }
+            if (st2) {
+                help = 0.0;
+                for (int64_t m = 0; m < M; ++m) {
+                    help += r[m] * r[m];
+                    vr[m] *= r[m];
+                    vi[m] *= r[m];
+                }
+            }
+            if (st34) {
+                help = 0.0;
+                for (int64_t m = 0; m < M; ++m) {
+                    help += 1.0 / (r[m] * r[m]);
+                    vr[m] /= r[m];
+                    vi[m] /= r[m];
+                }
+            }
+            double scalar = 0.0;
+            for (int64_t e = 0; e < E; ++e) {
+                double fr = 0.0, fi = 0.0, dg = 0.0;
+                for (int64_t m = 0; m < M; ++m) {
+                    /* temp1 = conj(V[m][e]) * v[m] */
+                    const double er = eigvec[2 * (m * E + e)], ei = -eigvec[2 * (m * E + e) + 1];
+                    const double tr = er * vr[m] - ei * vi[m], ti = er * vi[m] + ei * vr[m];
+                    fr += tr;
+                    fi += ti;
+                    if (r_diag) dg += tr * tr + ti * ti;
+                }
+                const double full = fr * fr + fi * fi;
+                scalar += (r_diag ? full - dg : full) * eigval[e];
+            }
+            if (steer_type == 1) {
+                const double nf = (double)M;
+                normsteer[gi] = 1.0 / (double)M;
+                result[gi] = scalar / (nf * nf) * norm;
+            } else if (steer_type == 2) {
+                const double nf = (double)M * r0[gi];
+                const double nf2 = nf * nf;
+                normsteer[gi] = help / nf2;
+                result[gi] = scalar / nf2 * norm;
+            } else if (steer_type == 3) {
+                const double nf = r0[gi] * help;
+                normsteer[gi] = 1.0 / (r0[gi] * r0[gi]) / help;
+                result[gi] = scalar / (nf * nf) * norm;
+            } else {
+                const double nf = (double)M * help;
+                normsteer[gi] = 1.0 / (double)M;
+                result[gi] = scalar / nf * norm;
+            }
+        }
+    }
+}
+
 /* Number of OpenMP threads the library will use (reported as the baseline's core count). */
 int orc_num_threads(void)
 {

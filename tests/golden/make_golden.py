@@ -16,6 +16,8 @@ their decorators removed, bound to plain stand-in objects:
 * ``Environment.apparent_r``                          acoular/environments.py:202-238
 * ``RectGrid`` / ``RectGrid3D`` ``_get_pos``          acoular/grids.py:350-358, 552-560
 * ``BeamformerBase.sig_loss_norm`` / ``_calc`` / ``synthetic``   acoular/fbeamform.py:438-593
+* ``PowerSpectra._get__evd`` (np.linalg.eigh per bin)  acoular/spectra.py:351-364
+* ``BeamformerEig._get_na`` / ``_calc``, ``BeamformerMusic._calc``   acoular/fbeamform.py:844-888, 911-944
 * ``WNoiseGenerator.signal``, ``SignalGenerator.usignal``, ``PointSource.result``,
   ``_fill_mic_signal_block``, ``Mixer.result``        (fixture time data)
 
@@ -97,6 +99,10 @@ calc_csm = _extract('acoular/spectra.py', 'PowerSpectra.calc_csm', NS)
 sig_loss_norm = _extract('acoular/fbeamform.py', 'BeamformerBase.sig_loss_norm', NS)
 bf_calc = _extract('acoular/fbeamform.py', 'BeamformerBase._calc', NS)
 synthetic = _extract('acoular/fbeamform.py', 'BeamformerBase.synthetic', NS)
+get_evd = _extract('acoular/spectra.py', 'PowerSpectra._get__evd', NS)
+eig_get_na = _extract('acoular/fbeamform.py', 'BeamformerEig._get_na', NS)
+eig_calc = _extract('acoular/fbeamform.py', 'BeamformerEig._calc', NS, rename='eig_calc')
+music_calc = _extract('acoular/fbeamform.py', 'BeamformerMusic._calc', NS, rename='music_calc')
 w_signal = _extract('acoular/signals.py', 'WNoiseGenerator.signal', NS)
 usignal = _extract('acoular/signals.py', 'SignalGenerator.usignal', NS)
 fill_py = _extract('acoular/sources.py', '_fill_mic_signal_block', NS)
@@ -324,8 +330,66 @@ def golden_config1():
     print('config1_band.npz written')
 
 
+def reference_eig_result(kind, csm, freqs, mpos, gpos, steer_type, r_diag, n, ind, c=343.0, r_diag_norm=0.0):
+    """``BeamformerEig._calc`` / ``BeamformerMusic._calc`` for bins ``ind`` with the reference's eigh."""
+    env = Env(c=c)
+    r0 = apparent_r(env, gpos)
+    rm = np.atleast_2d(apparent_r(env, gpos, mpos))
+    M = mpos.shape[1]
+    eva, eve = get_evd(SimpleNamespace(precision='complex128', csm=csm))
+    bf = SimpleNamespace(_f=freqs, r_diag=r_diag, r_diag_norm=r_diag_norm, n=n,
+                         steer=SimpleNamespace(mics=SimpleNamespace(num_mics=M)),
+                         freq_data=SimpleNamespace(num_channels=M, eigvals=eva, eigvecs=eve))
+    bf.na = eig_get_na(bf)
+    bf.sig_loss_norm = lambda: sig_loss_norm(bf)
+    bf._beamformer_params = lambda: (steer_type, lambda f: (r0, rm, 2 * np.pi * f / c))
+    bf._ac = np.zeros((csm.shape[0], gpos.shape[1]))
+    bf._fr = np.zeros(csm.shape[0], dtype='int8')
+    (eig_calc if kind == 'eig' else music_calc)(bf, np.asarray(ind))
+    return bf._ac[ind], eva[ind], eve[ind], bf.na
+
+
+def golden_eig():
+    """Eigenvalue beamformers (BeamformerEig for several components, BeamformerMusic) on the 8-mic
+    CSM of small_kat.npz and the 64-mic config-1 band, with the reference's own eigendecomposition."""
+    small = np.load(OUT / 'small_kat.npz')
+    out = {}
+    cases = [('s', small['csm0'], small['freqs0'], small['mpos'], small['gpos'], np.arange(10, 31))]
+    from acoular_b200 import workloads
+    wl = workloads.three_sources_64()
+    data_ref = reference_time_data(wl.mics.pos, wl.locs, wl.seeds, wl.rms, wl.fs, wl.num_samples)
+    csm64, freqs64 = reference_csm(data_ref, wl.fs, 128, 'Hanning', '50%', 'complex128')
+    cases.append(('c1', csm64, freqs64, wl.mics.pos, wl.grid.pos, np.arange(18, 23)))
+    for tag, csm, freqs, mpos, gpos, ind in cases:
+        M = mpos.shape[1]
+        out[f'{tag}_mpos'], out[f'{tag}_gpos'], out[f'{tag}_bins'] = mpos, gpos, ind
+        out[f'{tag}_freqs'] = freqs[ind]
+        first = True
+        for n in (-1, 0, M // 2):
+            for st in STEERS:
+                for rd in (False, True):
+                    res, eva, eve, na = reference_eig_result('eig', csm, freqs, mpos, gpos, st, rd, n, ind)
+                    out[f'{tag}_eig_n{n}_{st.replace(" ", "_")}_{int(rd)}'] = res
+                    out[f'{tag}_eig_n{n}_na'] = np.array(na)
+                    if first:
+                        out[f'{tag}_eigvals'], out[f'{tag}_eigvecs'] = eva, eve
+                        first = False
+        for n in (1, 3):
+            for st in STEERS:
+                res, _, _, na = reference_eig_result('music', csm, freqs, mpos, gpos, st, False, n, ind,
+                                                     r_diag_norm=1.0)
+                out[f'{tag}_music_n{n}_{st.replace(" ", "_")}'] = res
+                out[f'{tag}_music_n{n}_na'] = np.array(na)
+    np.savez_compressed(OUT / 'eig_kat.npz', **out)
+    print('eig_kat.npz written', len(out), 'arrays')
+
+
 if __name__ == '__main__':
+    if os.environ.get('ACB_GOLDEN_ONLY') == 'eig':
+        golden_eig()
+        sys.exit(0)
     golden_env()
     golden_small()
     golden_rank1()
     golden_config1()
+    golden_eig()

@@ -97,3 +97,28 @@ def test_config1_band_goldens(golden):
                                     range(18, 23), r0, rm, 343.0, steer, r_diag)
             key = f'map_{steer.replace(" ", "_")}_{int(r_diag)}'
             assert np.array_equal(res[18:23], d[key])
+
+
+# ---------------------------------------------------------------------------------------------
+# eigenvalue beamformers (BeamformerEig, BeamformerMusic) against the reference's own results
+# ---------------------------------------------------------------------------------------------
+@pytest.mark.parametrize('tag', ['s', 'c1'])
+def test_oracle_eig_beamformers_match_reference(golden, tag):
+    g = golden('eig_kat.npz')
+    mpos, gpos, bins, freqs = g[f'{tag}_mpos'], g[f'{tag}_gpos'], g[f'{tag}_bins'], g[f'{tag}_freqs']
+    eva, eve = g[f'{tag}_eigvals'], g[f'{tag}_eigvecs']
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    M = mpos.shape[1]
+    ind = np.arange(len(bins))
+    for n in (-1, 0, M // 2):
+        assert int(g[f'{tag}_eig_n{n}_na']) == O.eig_na(n, M)
+        for st in STEERS:
+            for rd in (False, True):
+                ref = g[f'{tag}_eig_n{n}_{st.replace(" ", "_")}_{int(rd)}']
+                got = O.beamformer_eig_calc(eva, eve, freqs, ind, r0, rm, 343.0, st, rd, n=n)
+                np.testing.assert_array_equal(got, ref)
+    for n in (1, 3):
+        for st in STEERS:
+            ref = g[f'{tag}_music_n{n}_{st.replace(" ", "_")}']
+            got = O.beamformer_music_calc(eva, eve, freqs, ind, r0, rm, 343.0, st, n=n)
+            np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0)
