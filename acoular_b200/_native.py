@@ -86,6 +86,9 @@ SIGNATURES = {
     'acb_map_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     'acb_beamformer_freq_f64': (_I, [ctypes.POINTER(MapParams), _VP, _D, _VP, _VP, _VP, _VP, _VP]),
     'acb_map_eig_f64': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    'acb_map_rm_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    'acb_map_custom_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP]),
+    'acb_map_eig_custom_f64': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP]),
     'acb_beamformer_freq_eig_f64': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _D, _VP, _VP, _VP, _VP, _VP]),
     'acb_sincos_table_build_host': (_I64, [_VP, _I64, ctypes.c_float, _I]),
     'acb_map_tc_workspace_bytes': (_SZ, [_I, _I, _I]),

@@ -45,16 +45,19 @@ __device__ __forceinline__ double grid_mic_dist(const MapArgs &a, const double *
     return dist3(g0, g1, g2, mp[m], mp[a.M + m], mp[2 * a.M + m]);
 }
 
-// Synthesise h for mics [m0, m0+n) of this CTA's 32 grid points into hs[m - m0][lane].
-template <bool USE_RM>
+// Synthesise h for mics [m0, m0+n) of this CTA's 32 grid points into hs[m - m0][lane]; with CUSTOM,
+// copy the caller's steering vectors hv[g][m] instead (custom steering, acoular/fastFuncs.py:414-559).
+template <bool USE_RM, bool CUSTOM = false>
 __device__ __forceinline__ void synth_chunk(const MapArgs &a, const double *__restrict__ rm, double k, int64_t g,
                                            bool gvalid, double g0, double g1, double g2, const double *mp, int m0,
-                                           int n, double2 *hs)
+                                           int n, double2 *hs, const double2 *__restrict__ hv = nullptr)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = warp; i < n; i += kWarps) {
         double2 h = make_double2(0.0, 0.0);
-        if (gvalid) {
+        if (CUSTOM) {
+            if (gvalid) h = __ldg(hv + g * a.M + m0 + i);
+        } else if (gvalid) {
             const double r = grid_mic_dist<USE_RM>(a, rm, g, m0 + i, g0, g1, g2, mp);
             const float arg = __double2float_rn(__dmul_rn(k, r));
             float c, s;
@@ -130,7 +133,10 @@ __device__ __forceinline__ void finish_plain(const MapArgs &a, double scalar, do
 {
     const double Md = (double)a.M;
     double res, ns;
-    if (a.steer_type == 1) {
+    if (a.steer_type == 0) {   // custom steering: no steering normalisation, S = sum |h|^2
+        ns = S;
+        res = scalar * a.norm;
+    } else if (a.steer_type == 1) {
         ns = 1.0 / Md;
         res = scalar / (Md * Md) * a.norm;
     } else if (a.steer_type == 2) {
@@ -152,7 +158,7 @@ __device__ __forceinline__ void finish_plain(const MapArgs &a, double scalar, do
     if (out_norm) out_norm[(int64_t)bin * a.G + g] = ns;
 }
 
-template <bool USE_RM>
+template <bool USE_RM, bool CUSTOM = false>
 __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2 *__restrict__ csm,
                                                         const double *__restrict__ wavenumber, double k_scalar,
                                                         const double *__restrict__ mpos,
@@ -160,7 +166,8 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
                                                         const double *__restrict__ r0_in,
                                                         const double *__restrict__ rm, int mc,
                                                         double *__restrict__ out_map,
-                                                        double *__restrict__ out_norm)
+                                                        double *__restrict__ out_norm,
+                                                        const double2 *__restrict__ steer = nullptr)
 {
     extern __shared__ double smem[];
     const int M = a.M;
@@ -175,20 +182,27 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
     const bool gvalid = g < a.G;
     const double k = wavenumber ? wavenumber[bin] : k_scalar;
     const double2 *C = csm + (int64_t)bin * M * M;
+    const double2 *hv = CUSTOM ? steer + (int64_t)bin * a.G * M : nullptr;
 
-    if (!USE_RM)
+    if (!USE_RM && !CUSTOM)
         for (int i = threadIdx.x; i < 3 * M; i += blockDim.x) mp[i] = mpos[i];
     double g0 = 0, g1 = 0, g2 = 0;
-    if (gvalid && !USE_RM) {
+    if (gvalid && !USE_RM && !CUSTOM) {
         g0 = gpos[g];
         g1 = gpos[a.G + g];
         g2 = gpos[2 * a.G + g];
     }
     __syncthreads();
 
-    // steering normalisation sum S (inverse: sum r^2; true level / location: sum 1/r^2)
+    // steering normalisation sum S (inverse: sum r^2; true level / location: sum 1/r^2; custom: sum |h|^2)
     double s_part = 0.0;
-    if (gvalid && a.steer_type >= 2) {
+    if (CUSTOM) {
+        if (gvalid)
+            for (int m = warp; m < M; m += kWarps) {
+                const double2 h = __ldg(hv + g * M + m);
+                s_part += h.x * h.x + h.y * h.y;
+            }
+    } else if (gvalid && a.steer_type >= 2) {
         for (int m = warp; m < M; m += kWarps) {
             const double r = grid_mic_dist<USE_RM>(a, rm, g, m, g0, g1, g2, mp);
             s_part += (a.steer_type == 2) ? r * r : 1.0 / (r * r);
@@ -199,13 +213,13 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
     const int nchunks = (M + mc - 1) / mc;
     for (int ca = 0; ca < nchunks; ++ca) {
         const int ma0 = ca * mc, na = min(mc, M - ma0);
-        synth_chunk<USE_RM>(a, rm, k, g, gvalid, g0, g1, g2, mp, ma0, na, ha);
+        synth_chunk<USE_RM, CUSTOM>(a, rm, k, g, gvalid, g0, g1, g2, mp, ma0, na, ha, hv);
         __syncthreads();
         quad_block(C, M, ha, ma0, na, ha, ma0, na, true, a.r_diag == 0, off, dsum);
         for (int cb = ca + 1; cb < nchunks; ++cb) {
             const int mb0 = cb * mc, nb = min(mc, M - mb0);
             __syncthreads();
-            synth_chunk<USE_RM>(a, rm, k, g, gvalid, g0, g1, g2, mp, mb0, nb, hb);
+            synth_chunk<USE_RM, CUSTOM>(a, rm, k, g, gvalid, g0, g1, g2, mp, mb0, nb, hb, hv);
             __syncthreads();
             quad_block(C, M, ha, ma0, na, hb, mb0, nb, false, false, off, dsum);
         }
@@ -225,8 +239,9 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
             S += red_s[w][lane];
         }
         const double scalar = 2.0 * o + d;
-        double r0;
-        if (a.ref_mode == 1) r0 = a.ref_dist;
+        double r0 = 0.0;
+        if (CUSTOM) r0 = 0.0;
+        else if (a.ref_mode == 1) r0 = a.ref_dist;
         else if (USE_RM) r0 = r0_in[g];
         else r0 = dist3(g0, g1, g2, a.ref0, a.ref1, a.ref2);
         finish_plain(a, scalar, S, r0, bin, g, out_map, out_norm);
@@ -244,14 +259,15 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
 // ------------------------------------------------------------------------------------------------
 constexpr int kEigPerWarp = 4;
 
-template <bool USE_RM>
+template <bool USE_RM, bool CUSTOM = false>
 __global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const double *__restrict__ eigval,
                                                       const double2 *__restrict__ eigvec,
                                                       const double *__restrict__ wavenumber, double k_scalar,
                                                       const double *__restrict__ mpos, const double *__restrict__ gpos,
                                                       const double *__restrict__ r0_in, const double *__restrict__ rm,
                                                       int mc, double *__restrict__ out_map,
-                                                      double *__restrict__ out_norm)
+                                                      double *__restrict__ out_norm,
+                                                      const double2 *__restrict__ steer = nullptr)
 {
     extern __shared__ double smem[];
     const int M = a.M;
@@ -266,11 +282,12 @@ __global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const do
     const double k = wavenumber ? wavenumber[bin] : k_scalar;
     const double *lam = eigval + (int64_t)bin * E;
     const double2 *V = eigvec + (int64_t)bin * M * E;
+    const double2 *hv = CUSTOM ? steer + (int64_t)bin * a.G * M : nullptr;
 
-    if (!USE_RM)
+    if (!USE_RM && !CUSTOM)
         for (int i = threadIdx.x; i < 3 * M; i += blockDim.x) mp[i] = mpos[i];
     double g0 = 0, g1 = 0, g2 = 0;
-    if (gvalid && !USE_RM) {
+    if (gvalid && !USE_RM && !CUSTOM) {
         g0 = gpos[g];
         g1 = gpos[a.G + g];
         g2 = gpos[2 * a.G + g];
@@ -278,7 +295,13 @@ __global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const do
     __syncthreads();
 
     double s_part = 0.0;
-    if (gvalid && a.steer_type >= 2) {
+    if (CUSTOM) {
+        if (gvalid)
+            for (int m = warp; m < M; m += kWarps) {
+                const double2 h = __ldg(hv + g * M + m);
+                s_part += h.x * h.x + h.y * h.y;
+            }
+    } else if (gvalid && a.steer_type >= 2) {
         for (int m = warp; m < M; m += kWarps) {
             const double r = grid_mic_dist<USE_RM>(a, rm, g, m, g0, g1, g2, mp);
             s_part += (a.steer_type == 2) ? r * r : 1.0 / (r * r);
@@ -294,7 +317,7 @@ __global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const do
         const int e0 = eg + warp * kEigPerWarp;
         for (int ca = 0; ca < nchunks; ++ca) {
             const int m0 = ca * mc, n = min(mc, M - m0);
-            synth_chunk<USE_RM>(a, rm, k, g, gvalid, g0, g1, g2, mp, m0, n, hs);
+            synth_chunk<USE_RM, CUSTOM>(a, rm, k, g, gvalid, g0, g1, g2, mp, m0, n, hs, hv);
             __syncthreads();
             for (int mm = 0; mm < n; ++mm) {
                 const double2 h = hs[mm * kLanes + lane];
@@ -330,8 +353,9 @@ __global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const do
             sc += red_sc[w][lane];
             S += red_s[w][lane];
         }
-        double r0;
-        if (a.ref_mode == 1) r0 = a.ref_dist;
+        double r0 = 0.0;
+        if (CUSTOM) r0 = 0.0;
+        else if (a.ref_mode == 1) r0 = a.ref_dist;
         else if (USE_RM) r0 = r0_in[g];
         else r0 = dist3(g0, g1, g2, a.ref0, a.ref1, a.ref2);
         finish_plain(a, sc, S, r0, bin, g, out_map, out_norm);
@@ -364,36 +388,36 @@ static int make_args(const acb_map_params *p, MapArgs &a)
     return ACB_OK;
 }
 
-template <bool USE_RM>
+template <bool USE_RM, bool CUSTOM = false>
 static int launch_plain(const MapArgs &a, int nbins, const void *csm, const double *k, double k_scalar,
                         const double *mpos,
                         const double *gpos, const double *r0, const double *rm, double *out_map, double *out_norm,
-                        cudaStream_t s)
+                        cudaStream_t s, const void *steer = nullptr)
 {
     const int mc = a.M <= 256 ? a.M : 128;
     const int nbuf = a.M <= mc ? 1 : 2;
     const size_t smem = (size_t)(((3 * a.M + 1) & ~1) * sizeof(double)) + (size_t)nbuf * mc * kLanes * sizeof(double2);
-    auto kern = map_plain_kernel<USE_RM>;
+    auto kern = map_plain_kernel<USE_RM, CUSTOM>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const dim3 grid((unsigned)((a.G + kLanes - 1) / kLanes), nbins);
     kern<<<grid, kLanes * kWarps, smem, s>>>(a, reinterpret_cast<const double2 *>(csm), k, k_scalar, mpos, gpos, r0,
-                                            rm, mc,
-                                            out_map, out_norm);
+                                            rm, mc, out_map, out_norm, reinterpret_cast<const double2 *>(steer));
     return check_launch();
 }
 
-template <bool USE_RM>
+template <bool USE_RM, bool CUSTOM = false>
 static int launch_eig(const MapArgs &a, int nbins, int E, const double *eigval, const void *eigvec, const double *k,
                       double k_scalar, const double *mpos, const double *gpos, const double *r0, const double *rm,
-                      double *out_map, double *out_norm, cudaStream_t s)
+                      double *out_map, double *out_norm, cudaStream_t s, const void *steer = nullptr)
 {
     const int mc = a.M <= 256 ? a.M : 128;
     const size_t smem = (size_t)(((3 * a.M + 1) & ~1) * sizeof(double)) + (size_t)mc * kLanes * sizeof(double2);
-    auto kern = map_eig_kernel<USE_RM>;
+    auto kern = map_eig_kernel<USE_RM, CUSTOM>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const dim3 grid((unsigned)((a.G + kLanes - 1) / kLanes), nbins);
     kern<<<grid, kLanes * kWarps, smem, s>>>(a, E, eigval, reinterpret_cast<const double2 *>(eigvec), k, k_scalar, mpos,
-                                            gpos, r0, rm, mc, out_map, out_norm);
+                                            gpos, r0, rm, mc, out_map, out_norm,
+                                            reinterpret_cast<const double2 *>(steer));
     return check_launch();
 }
 
@@ -443,6 +467,57 @@ int acb_beamformer_freq_eig_f64(const acb_map_params *p, int num_eigs, const dou
     a.ref_mode = 0;
     return launch_eig<true>(a, 1, num_eigs, eigval, eigvec, nullptr, wavenumber, nullptr, nullptr, r0, rm, out_map,
                             out_steer_norm, as_stream(stream));
+}
+
+int acb_map_rm_f64(const acb_map_params *p, const void *csm, const double *wavenumber, const double *r0,
+                   const double *rm, double *out_map, double *out_steer_norm, void *stream)
+{
+    MapArgs a;
+    int st = make_args(p, a);
+    if (st) return st;
+    if (!csm || !wavenumber || !r0 || !rm || !out_map) return ACB_ERR_ARG;
+    if ((a.G + kLanes - 1) / kLanes > 0x7fffffffLL) return ACB_ERR_SHAPE;
+    a.ref_mode = 0;
+    return launch_plain<true>(a, p->num_bins, csm, wavenumber, 0.0, nullptr, nullptr, r0, rm, out_map, out_steer_norm,
+                              as_stream(stream));
+}
+
+// Custom steering: p->steer_type is ignored; steer: complex128 [num_bins][G][M].
+static int custom_args(const acb_map_params *p, MapArgs &a)
+{
+    if (!p) return ACB_ERR_ARG;
+    acb_map_params q = *p;
+    q.steer_type = 1;            // any valid type for the shared checks; replaced below
+    q.glibc_faithful = 0;        // the steering is given: no phase synthesis
+    int st = make_args(&q, a);
+    if (st) return st;
+    a.steer_type = 0;
+    return ACB_OK;
+}
+
+int acb_map_custom_f64(const acb_map_params *p, const void *csm, const void *steer, double *out_map,
+                       double *out_steer_norm, void *stream)
+{
+    MapArgs a;
+    int st = custom_args(p, a);
+    if (st) return st;
+    if (!csm || !steer || !out_map) return ACB_ERR_ARG;
+    if ((a.G + kLanes - 1) / kLanes > 0x7fffffffLL) return ACB_ERR_SHAPE;
+    return launch_plain<false, true>(a, p->num_bins, csm, nullptr, 0.0, nullptr, nullptr, nullptr, nullptr, out_map,
+                                     out_steer_norm, as_stream(stream), steer);
+}
+
+int acb_map_eig_custom_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,
+                           const void *steer, double *out_map, double *out_steer_norm, void *stream)
+{
+    MapArgs a;
+    int st = custom_args(p, a);
+    if (st) return st;
+    if (!eigval || !eigvec || !steer || !out_map) return ACB_ERR_ARG;
+    if (num_eigs < 1 || num_eigs > p->num_mics) return ACB_ERR_SHAPE;
+    if ((a.G + kLanes - 1) / kLanes > 0x7fffffffLL) return ACB_ERR_SHAPE;
+    return launch_eig<false, true>(a, p->num_bins, num_eigs, eigval, eigvec, nullptr, 0.0, nullptr, nullptr, nullptr,
+                                   nullptr, out_map, out_steer_norm, as_stream(stream), steer);
 }
 
 int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wavenumber, const double *r0,

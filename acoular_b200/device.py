@@ -301,6 +301,62 @@ def map_eig_f64(eigval: torch.Tensor, eigvec: torch.Tensor, wavenumbers: torch.T
     return out
 
 
+def map_rm_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, r0: torch.Tensor, rm: torch.Tensor, steer_type: str,
+               r_diag: bool, norm: float, clip_negative=None, glibc_faithful=True, out: torch.Tensor | None = None,
+               steer_norm: torch.Tensor | None = None) -> torch.Tensor:
+    """Plain FP64 map with given distances r0 (G,), rm (G, M) (any environment) for B bins."""
+    B, M, _ = csm.shape
+    G = rm.shape[0]
+    dev = csm.device
+    p = map_params(M, G, B, steer_type, r_diag, norm, clip_negative, None, glibc_faithful, dev)
+    if out is None:
+        out = torch.empty((B, G), dtype=torch.float64, device=dev)
+    N.check(N.lib().acb_map_rm_f64(ctypes.byref(p), csm.data_ptr(), wavenumbers.data_ptr(), r0.data_ptr(),
+                                   rm.data_ptr(), out.data_ptr(), N.ptr(steer_norm), N.stream_handle()),
+            'acb_map_rm_f64')
+    return out
+
+
+def map_custom_f64(csm: torch.Tensor, steer: torch.Tensor, r_diag: bool, norm: float, clip_negative=False,
+                   out: torch.Tensor | None = None, steer_norm: torch.Tensor | None = None,
+                   eig: tuple | None = None) -> torch.Tensor:
+    """Map with custom steering vectors steer (B, G, M) complex128 for B bins; with ``eig`` =
+    (eigval (B, E), eigvec (B, M, E)) the eigenvalue form (``csm`` unused)."""
+    B, G, M = steer.shape
+    dev = steer.device
+    if not steer.is_contiguous():
+        msg = 'steer must be a contiguous (num_bins, num_grid, num_mics) complex128 tensor'
+        raise ValueError(msg)
+    p = map_params(M, G, B, 'classic', r_diag, norm, clip_negative, None, False, dev)
+    if out is None:
+        out = torch.empty((B, G), dtype=torch.float64, device=dev)
+    if eig is None:
+        N.check(N.lib().acb_map_custom_f64(ctypes.byref(p), csm.data_ptr(), steer.data_ptr(), out.data_ptr(),
+                                           N.ptr(steer_norm), N.stream_handle()), 'acb_map_custom_f64')
+    else:
+        ev, evec = eig
+        N.check(N.lib().acb_map_eig_custom_f64(ctypes.byref(p), ev.shape[1], ev.data_ptr(), evec.data_ptr(),
+                                               steer.data_ptr(), out.data_ptr(), N.ptr(steer_norm),
+                                               N.stream_handle()), 'acb_map_eig_custom_f64')
+    return out
+
+
+def map_eig_rm_f64(eigval: torch.Tensor, eigvec: torch.Tensor, k: float, r0: torch.Tensor, rm: torch.Tensor,
+                   steer_type: str, r_diag: bool, norm: float, glibc_faithful=True, out: torch.Tensor | None = None,
+                   steer_norm: torch.Tensor | None = None) -> torch.Tensor:
+    """Eigenvalue form for one bin with given distances r0 (G,), rm (G, M): eigval (1, E), eigvec (1, M, E)."""
+    _, M, E = eigvec.shape
+    G = rm.shape[0]
+    dev = eigvec.device
+    p = map_params(M, G, 1, steer_type, r_diag, norm, False, None, glibc_faithful, dev)
+    if out is None:
+        out = torch.empty(G, dtype=torch.float64, device=dev)
+    N.check(N.lib().acb_beamformer_freq_eig_f64(ctypes.byref(p), E, eigval.data_ptr(), eigvec.data_ptr(), float(k),
+                                                r0.data_ptr(), rm.data_ptr(), out.data_ptr(), N.ptr(steer_norm),
+                                                N.stream_handle()), 'acb_beamformer_freq_eig_f64')
+    return out
+
+
 _tc_ws: dict = {}
 
 

@@ -52,8 +52,7 @@ def calcCSM(csm: np.ndarray, SpecAllMics: np.ndarray) -> np.ndarray:  # noqa: N8
 def beamformerFreq(steerVecType, boolRemovedDiagOfCSM, normFactor, inputTupleSteer, inputTupleCsm,  # noqa: N802, N803
                    glibc_faithful: bool = True):
     if steerVecType == 'custom':
-        msg = "custom steering vectors of beamformerFreq are not implemented"
-        raise NotImplementedError(msg)
+        return _beamformer_freq_custom(boolRemovedDiagOfCSM, normFactor, inputTupleSteer, inputTupleCsm)
     if steerVecType not in N.STEER_CODES:
         raise KeyError(steerVecType)
     r0, rm, k = inputTupleSteer
@@ -110,3 +109,33 @@ def _beamformer_freq_eig(steer_type, r_diag, norm, r0, rm, k, eigval, eigvec, gl
                                                 r0_d.data_ptr(), rm_d.data_ptr(), out.data_ptr(), nrm.data_ptr(),
                                                 N.stream_handle()), 'beamformerFreq')
     return out.cpu().numpy(), nrm.cpu().numpy()
+
+
+def _beamformer_freq_custom(r_diag, norm, steer_vec, csm_or_eig):
+    """beamformerFreq('custom', ...) with a (G, M) complex128 steering matrix (acoular/fastFuncs.py:414-559)."""
+    h = np.asarray(steer_vec)
+    if h.dtype != np.complex128 or h.ndim != 2:
+        msg = 'custom steering vectors must be a (num_grid, num_mics) complex128 array'
+        raise TypeError(msg)
+    G, M = h.shape
+    dev = D.require_cuda()
+    h_d = torch.from_numpy(np.ascontiguousarray(h)).to(dev)[None]
+    out = torch.empty((1, G), dtype=torch.float64, device=dev)
+    nrm = torch.empty((1, G), dtype=torch.float64, device=dev)
+    if isinstance(csm_or_eig, tuple):
+        ev, evec = csm_or_eig
+        ev = np.ascontiguousarray(ev, dtype=np.float64)
+        evec = np.ascontiguousarray(evec, dtype=np.complex128)
+        if evec.shape != (M, ev.shape[0]):
+            msg = 'eigVec must be (num_mics, num_eigs)'
+            raise ValueError(msg)
+        eig = (torch.from_numpy(ev).to(dev)[None], torch.from_numpy(evec).to(dev)[None])
+        D.map_custom_f64(None, h_d, r_diag, float(norm), out=out, steer_norm=nrm, eig=eig)
+    else:
+        _check_contig(csm_or_eig, np.complex128, 'csm')
+        if csm_or_eig.shape != (M, M):
+            msg = 'csm must be (num_mics, num_mics)'
+            raise ValueError(msg)
+        c = torch.from_numpy(csm_or_eig).to(dev)[None]
+        D.map_custom_f64(c, h_d, r_diag, float(norm), out=out, steer_norm=nrm)
+    return out[0].cpu().numpy(), nrm[0].cpu().numpy()

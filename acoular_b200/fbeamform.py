@@ -198,6 +198,14 @@ class BeamformerBase:
         ind = np.asarray(ind, dtype=np.int64)
         if ind.size == 0:
             return
+        # the reference's _beamformer_params (acoular/fbeamform.py:464-472): the predefined steering
+        # vectors of a plain SteeringVector, else the object's own (custom) steering vectors
+        if type(self.steer) is not SteeringVector:
+            self._calc_custom(ind)
+            return
+        if type(self.steer.env) is not Environment:
+            self._calc_given_distances(ind)
+            return
         csm_all = self.freq_data.csm_device
         dev = csm_all.device
         mpos, gpos = self._geometry(dev)
@@ -246,6 +254,44 @@ class BeamformerBase:
             if sub is not None:
                 self._ac[sub] = host.numpy()
         self._fr[ind] = 1
+
+    def _store(self, ind, out):
+        if self.r_diag:   # set (unphysical) negative output values to 0 (acoular/fbeamform.py:506-508)
+            out.clamp_(min=0.0)
+        if self.precision == 'float32':
+            out = out.float()
+        self._ac[ind] = out.cpu().numpy()
+        self._fr[ind] = 1
+
+    def _calc_given_distances(self, ind):
+        """Environments whose apparent distances are not Euclidean (uniform flow): the map kernel
+        takes SteeringVector.r0 / .rm as given (FP64 form, also when ``form == 'tc'``)."""
+        csm_all = self.freq_data.csm_device
+        dev = csm_all.device
+        gk = ('rm', self.steer.digest, str(dev))
+        if getattr(self, '_rm_key', None) != gk:
+            self._r0_d = torch.as_tensor(np.ascontiguousarray(np.atleast_1d(self.steer.r0), dtype=np.float64),
+                                         device=dev)
+            self._rm_d = torch.as_tensor(np.ascontiguousarray(self.steer.rm, dtype=np.float64), device=dev)
+            self._rm_key = gk
+        ind_d = torch.as_tensor(ind, device=dev)
+        csm = csm_all.index_select(0, ind_d).contiguous()
+        k = torch.as_tensor(2 * np.pi * self._f[ind] / self.steer.env.c, dtype=torch.float64, device=dev)
+        out = D.map_rm_f64(csm, k, self._r0_d, self._rm_d, self.steer.steer_type, self.r_diag, self.sig_loss_norm(),
+                           clip_negative=False, glibc_faithful=self.glibc_faithful)
+        self._store(ind, out)
+
+    def _calc_custom(self, ind):
+        """Steering objects other than the plain SteeringVector: their steer_vector(f) (G, M) per bin,
+        materialised as the reference does, on the custom-steering kernel."""
+        csm_all = self.freq_data.csm_device
+        dev = csm_all.device
+        norm = self.sig_loss_norm()
+        for i in ind:
+            h = torch.as_tensor(np.ascontiguousarray(self.steer.steer_vector(self._f[i]), dtype=np.complex128),
+                                device=dev)
+            out = D.map_custom_f64(csm_all[int(i):int(i) + 1], h[None], self.r_diag, norm)
+            self._store(np.array([i]), out)
 
     # --- band synthesis and integration (acoular/fbeamform.py:512-685) -----------------------
     def synthetic(self, f, num=0):
@@ -359,12 +405,30 @@ class BeamformerEig(BeamformerBase):
             return
         ev, evec = self.freq_data.evd_device
         dev = ev.device
-        mpos, gpos = self._geometry(dev)
         ind_d = torch.as_tensor(ind, device=dev)
         lam, vec, norm = self._eig_select(ev, evec, ind_d)
-        k = torch.as_tensor(2 * np.pi * self._f[ind] / self.steer.env.c, dtype=torch.float64, device=dev)
-        out = D.map_eig_f64(lam, vec, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm, ref=self.steer.ref,
-                            clip_negative=False, glibc_faithful=self.glibc_faithful)
+        if type(self.steer) is not SteeringVector:
+            # custom steering vectors (acoular/fastFuncs.py:476-559), one bin at a time
+            out = torch.empty((ind.size, self.steer.grid.size), dtype=torch.float64, device=dev)
+            for j, i in enumerate(ind):
+                h = torch.as_tensor(np.ascontiguousarray(self.steer.steer_vector(self._f[i]), dtype=np.complex128),
+                                    device=dev)
+                D.map_custom_f64(None, h[None], self.r_diag, norm, out=out[j:j + 1],
+                                 eig=(lam[j:j + 1].contiguous(), vec[j:j + 1].contiguous()))
+        elif type(self.steer.env) is not Environment:
+            # distances of a non-Euclidean environment, given to the kernel as they are
+            r0 = torch.as_tensor(np.ascontiguousarray(np.atleast_1d(self.steer.r0), dtype=np.float64), device=dev)
+            rm = torch.as_tensor(np.ascontiguousarray(self.steer.rm, dtype=np.float64), device=dev)
+            out = torch.empty((ind.size, rm.shape[0]), dtype=torch.float64, device=dev)
+            for j, i in enumerate(ind):
+                D.map_eig_rm_f64(lam[j:j + 1].contiguous(), vec[j:j + 1].contiguous(),
+                                 2 * np.pi * self._f[i] / self.steer.env.c, r0, rm, self.steer.steer_type, self.r_diag,
+                                 norm, glibc_faithful=self.glibc_faithful, out=out[j])
+        else:
+            mpos, gpos = self._geometry(dev)
+            k = torch.as_tensor(2 * np.pi * self._f[ind] / self.steer.env.c, dtype=torch.float64, device=dev)
+            out = D.map_eig_f64(lam, vec, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm,
+                                ref=self.steer.ref, clip_negative=False, glibc_faithful=self.glibc_faithful)
         out = self._post(out)
         if self.precision == 'float32':
             out = out.float()

@@ -132,6 +132,25 @@ int acb_map_eig_f64(const acb_map_params *p, int num_eigs, const double *eigval,
                     const double *wavenumber, const double *mpos, const double *gpos, double *out_map,
                     double *out_steer_norm, void *stream);
 
+/* The plain FP64 map with the distances given instead of synthesised from positions, batched over
+ * bins: r0 float64 [G], rm float64 [G][M] (Environment.apparent_r of any environment, e.g. the
+ * uniform-flow one, acoular/environments.py:254-332, as SteeringVector.r0 / .rm pass them,
+ * acoular/fbeamform.py:187-197, 464-468).  ref_mode / ref_point are ignored (r0 is given). */
+int acb_map_rm_f64(const acb_map_params *p, const void *csm, const double *wavenumber, const double *r0,
+                   const double *rm, double *out_map, double *out_steer_norm, void *stream);
+
+/* Custom steering vectors (beamformerFreq('custom', ...), acoular/fastFuncs.py:414-473, as
+ * BeamformerBase._calc uses them for steering objects other than the plain SteeringVector,
+ * acoular/fbeamform.py:470-472): steer complex128 [num_bins][G][M];
+ *   map = norm * (2 Re sum_{a<b} conj(h_a) C_ab h_b + [!r_diag] sum_a C_aa |h_a|^2),
+ *   steer_norm = sum_a |h_a|^2.   p->steer_type, ref and glibc_faithful are ignored. */
+int acb_map_custom_f64(const acb_map_params *p, const void *csm, const void *steer, double *out_map,
+                       double *out_steer_norm, void *stream);
+
+/* Eigenvalue form with custom steering vectors (acoular/fastFuncs.py:476-559). */
+int acb_map_eig_custom_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,
+                           const void *steer, double *out_map, double *out_steer_norm, void *stream);
+
 /* beamformerFreq with an eigen tuple (eigval[num_eigs], eigvec[M][num_eigs]) for one bin with
  * precomputed distances r0 [G], rm [G][M] (acoular/fastFuncs.py:61-214). */
 int acb_beamformer_freq_eig_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,

@@ -72,6 +72,7 @@ def lib():
                                              ctypes.c_int, i64, i64, dp, dp]
         L.orc_beamformer_eig.argtypes = [dp, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                          i64, i64, i64, dp, dp]
+        L.orc_beamformer_custom.argtypes = [dp, dp, dp, i64, dp, ctypes.c_double, ctypes.c_int, i64, i64, dp, dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -238,6 +239,41 @@ def beamformer_freq_eig(steer_type: str, r_diag: bool, norm: float, r0: np.ndarr
     lib().orc_beamformer_eig(_dp(eigval), _dp(eigvec), _dp(r0), _dp(rm), float(k), float(norm), int(bool(r_diag)),
                              STEER_TYPES[steer_type], G, M, E, _dp(res), _dp(nrm))
     return res, nrm
+
+
+def beamformer_freq_custom(r_diag: bool, norm: float, steer: np.ndarray, csm=None, eig=None):
+    """``beamformerFreq('custom', ...)`` (fastFuncs.py:414-559): steer (G, M) complex128 with a full CSM
+    (M, M) or an eigen tuple (eigval[E], eigvec[M, E])."""
+    steer = np.ascontiguousarray(steer, dtype=np.complex128)
+    G, M = steer.shape
+    res = np.zeros(G)
+    nrm = np.zeros(G)
+    if eig is None:
+        c = np.ascontiguousarray(csm, dtype=np.complex128)
+        lib().orc_beamformer_custom(_dp(c), None, None, 0, _dp(steer), float(norm), int(bool(r_diag)), G, M,
+                                    _dp(res), _dp(nrm))
+    else:
+        ev = np.ascontiguousarray(eig[0], dtype=np.float64)
+        evec = np.ascontiguousarray(eig[1], dtype=np.complex128)
+        lib().orc_beamformer_custom(None, _dp(ev), _dp(evec), ev.shape[0], _dp(steer), float(norm),
+                                    int(bool(r_diag)), G, M, _dp(res), _dp(nrm))
+    return res, nrm
+
+
+def uniform_flow_apparent_r(gpos, mpos, ma: float, fdv):
+    """``UniformFlowEnvironment.apparent_r`` (acoular/environments.py:290-332): path length r and its
+    angle theta to the flow direction give r / (sqrt(ma^2 cos^2 theta - ma^2 + 1) - ma cos theta)."""
+    if np.isscalar(mpos):
+        mpos = np.array((0, 0, 0), dtype=np.float32)[:, np.newaxis]
+    fdv = np.asarray(fdv, dtype=np.float64)
+    u = fdv / np.sqrt((fdv * fdv).sum())
+    d = np.asarray(gpos)[:, :, np.newaxis] - np.asarray(mpos)[:, np.newaxis, :]
+    r = np.sqrt(np.sum(d * d, 0))
+    mc = (ma * np.sum(d.reshape((3, -1)) * u[:, np.newaxis], 0) / r.reshape(-1)).reshape(r.shape)
+    r = r * (1 / (-mc + np.sqrt(mc * mc - ma * ma + 1)))
+    if r.shape[1] == 1:
+        r = r[:, 0]
+    return r
 
 
 def eig_na(n: int, num_mics: int) -> int:

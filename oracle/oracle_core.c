@@ -254,6 +254,53 @@ void orc_beamformer_eig(const double *eigval, const double *eigvec, const double
     }
 }
 
+/* _freqBeamformer_SpecificSteerVec_FullCSM / _CsmRemovedDiag (fastFuncs.py:414-473) and the
+ * eigenvalue variants (fastFuncs.py:476-559): custom steering vectors h [G][M] (interleaved complex).
+ * eig != 0: eigval [E], eigvec [M][E] instead of csm.  result = scalar * norm, normsteer = sum |h|^2. */
+void orc_beamformer_custom(const double *csm, const double *eigval, const double *eigvec, int64_t E, const double *h,
+                           double norm, int r_diag, int64_t G, int64_t M, double *result, double *normsteer)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t gi = 0; gi < G; ++gi) {
+        const double *v = h + 2 * gi * M;
+        double help = 0.0, scalar = 0.0;
+        for (int64_t m = 0; m < M; ++m) help += v[2 * m] * v[2 * m] + v[2 * m + 1] * v[2 * m + 1];
+        if (!eigval) {
+            for (int64_t m = 0; m < M; ++m) {
+                double lr = 0.0, li = 0.0;
+                for (int64_t a = 0; a < m; ++a) {   /* csm[a, m] * conj(h[a]) */
+                    const double cr = csm[2 * (a * M + m)], ci = csm[2 * (a * M + m) + 1];
+                    const double hr = v[2 * a], hi = -v[2 * a + 1];
+                    lr += cr * hr - ci * hi;
+                    li += cr * hi + ci * hr;
+                }
+                scalar += 2.0 * (lr * v[2 * m] - li * v[2 * m + 1]);
+                if (!r_diag) {
+                    const double cr = csm[2 * (m * M + m)], ci = csm[2 * (m * M + m) + 1];
+                    const double hr = v[2 * m], hi = -v[2 * m + 1];
+                    const double pr = cr * hr - ci * hi, pi = cr * hi + ci * hr;
+                    scalar += pr * v[2 * m] - pi * v[2 * m + 1];
+                }
+            }
+        } else {
+            for (int64_t e = 0; e < E; ++e) {
+                double fr = 0.0, fi = 0.0, dg = 0.0;
+                for (int64_t m = 0; m < M; ++m) {
+                    const double er = eigvec[2 * (m * E + e)], ei = -eigvec[2 * (m * E + e) + 1];
+                    const double tr = er * v[2 * m] - ei * v[2 * m + 1], ti = er * v[2 * m + 1] + ei * v[2 * m];
+                    fr += tr;
+                    fi += ti;
+                    dg += tr * tr + ti * ti;
+                }
+                const double full = fr * fr + fi * fi;
+                scalar += (r_diag ? full - dg : full) * eigval[e];
+            }
+        }
+        normsteer[gi] = help;
+        result[gi] = scalar * norm;
+    }
+}
+
 /* Number of OpenMP threads the library will use (reported as the baseline's core count). */
 int orc_num_threads(void)
 {

@@ -18,6 +18,8 @@ their decorators removed, bound to plain stand-in objects:
 * ``BeamformerBase.sig_loss_norm`` / ``_calc`` / ``synthetic``   acoular/fbeamform.py:438-593
 * ``PowerSpectra._get__evd`` (np.linalg.eigh per bin)  acoular/spectra.py:351-364
 * ``BeamformerEig._get_na`` / ``_calc``, ``BeamformerMusic._calc``   acoular/fbeamform.py:844-888, 911-944
+* ``UniformFlowEnvironment.apparent_r``               acoular/environments.py:290-332
+* ``SteeringVector._steer_funcs_freq`` (as source text) acoular/fbeamform.py:145-153
 * ``WNoiseGenerator.signal``, ``SignalGenerator.usignal``, ``PointSource.result``,
   ``_fill_mic_signal_block``, ``Mixer.result``        (fixture time data)
 
@@ -103,6 +105,16 @@ get_evd = _extract('acoular/spectra.py', 'PowerSpectra._get__evd', NS)
 eig_get_na = _extract('acoular/fbeamform.py', 'BeamformerEig._get_na', NS)
 eig_calc = _extract('acoular/fbeamform.py', 'BeamformerEig._calc', NS, rename='eig_calc')
 music_calc = _extract('acoular/fbeamform.py', 'BeamformerMusic._calc', NS, rename='music_calc')
+uflow_apparent_r = _extract('acoular/environments.py', 'UniformFlowEnvironment.apparent_r', NS,
+                            rename='uflow_apparent_r')
+
+
+def _steer_funcs_freq():
+    """The reference's frequency-domain steering formulas, evaluated from its class body's source."""
+    src = (REF / 'acoular/fbeamform.py').read_text()
+    cls = next(n for n in ast.parse(src).body if isinstance(n, ast.ClassDef) and n.name == 'SteeringVector')
+    assign = next(n for n in cls.body if isinstance(n, ast.Assign) and n.targets[0].id == '_steer_funcs_freq')
+    return eval(compile(ast.Expression(assign.value.args[0]), 'fbeamform.py:_steer_funcs_freq', 'eval'), {'np': np})
 w_signal = _extract('acoular/signals.py', 'WNoiseGenerator.signal', NS)
 usignal = _extract('acoular/signals.py', 'SignalGenerator.usignal', NS)
 fill_py = _extract('acoular/sources.py', '_fill_mic_signal_block', NS)
@@ -384,12 +396,61 @@ def golden_eig():
     print('eig_kat.npz written', len(out), 'arrays')
 
 
+def golden_custom_flow():
+    """Custom steering vectors (beamformerFreq('custom', ...), full / removed diagonal / eigen) and
+    the uniform-flow environment on the 8-mic case of small_kat.npz."""
+    small = np.load(OUT / 'small_kat.npz')
+    csm, freqs, mpos, gpos = small['csm0'], small['freqs0'], small['mpos'], small['gpos']
+    M = mpos.shape[1]
+    env = Env(c=343.0)
+    r0, rm = apparent_r(env, gpos), np.atleast_2d(apparent_r(env, gpos, mpos))
+    funcs = _steer_funcs_freq()
+    eva, eve = get_evd(SimpleNamespace(precision='complex128', csm=csm))
+    out = {'bins': np.array([10, 20])}
+    for b in out['bins']:
+        k = 2 * np.pi * freqs[b] / 343.0
+        trans = fastFuncs.calcTransfer(r0, rm, np.array(k))
+        out[f'trans_{b}'] = trans
+        for st in STEERS:
+            h = np.ascontiguousarray(funcs[st](trans))
+            out[f'steer_{st.replace(" ", "_")}_{b}'] = h
+            for rd in (False, True):
+                res, nrm = fastFuncs.beamformerFreq('custom', rd, 1.25, h, np.ascontiguousarray(csm[b]))
+                out[f'cust_{st.replace(" ", "_")}_{int(rd)}_{b}'] = res
+                out[f'custn_{st.replace(" ", "_")}_{int(rd)}_{b}'] = nrm
+                res, nrm = fastFuncs.beamformerFreq('custom', rd, 1.25, h,
+                                                    (np.array(eva[b, M - 2:]), np.ascontiguousarray(eve[b][:, M - 2:])))
+                out[f'custe_{st.replace(" ", "_")}_{int(rd)}_{b}'] = res
+    out['eigvals'], out['eigvecs'] = eva[out['bins']], eve[out['bins']]
+    # uniform flow: Mach 0.3 along (1, 0.5, 0); the fast path of BeamformerBase._calc with its distances
+    fl = SimpleNamespace(ma=0.3, fdv=np.array((1.0, 0.5, 0.0)))
+    r0f, rmf = uflow_apparent_r(fl, gpos), np.atleast_2d(uflow_apparent_r(fl, gpos, mpos))
+    out['flow_r0'], out['flow_rm'] = r0f, rmf
+    ind = np.arange(10, 31)
+    for st in STEERS:
+        for rd in (False, True):
+            bf = SimpleNamespace(_f=freqs, r_diag=rd, r_diag_norm=0.0,
+                                 freq_data=SimpleNamespace(num_channels=M, csm=csm))
+            bf.sig_loss_norm = lambda bf=bf: sig_loss_norm(bf)
+            bf._beamformer_params = lambda st=st: (st, lambda f: (r0f, rmf, 2 * np.pi * f / 343.0))
+            bf._ac = np.zeros((csm.shape[0], gpos.shape[1]))
+            bf._fr = np.zeros(csm.shape[0], dtype='int8')
+            bf_calc(bf, ind)
+            out[f'flow_{st.replace(" ", "_")}_{int(rd)}'] = bf._ac[ind]
+    np.savez_compressed(OUT / 'custom_flow_kat.npz', **out)
+    print('custom_flow_kat.npz written', len(out), 'arrays')
+
+
 if __name__ == '__main__':
     if os.environ.get('ACB_GOLDEN_ONLY') == 'eig':
         golden_eig()
+        sys.exit(0)
+    if os.environ.get('ACB_GOLDEN_ONLY') == 'custom_flow':
+        golden_custom_flow()
         sys.exit(0)
     golden_env()
     golden_small()
     golden_rank1()
     golden_config1()
     golden_eig()
+    golden_custom_flow()

@@ -122,3 +122,59 @@ def test_oracle_eig_beamformers_match_reference(golden, tag):
             ref = g[f'{tag}_music_n{n}_{st.replace(" ", "_")}']
             got = O.beamformer_music_calc(eva, eve, freqs, ind, r0, rm, 343.0, st, n=n)
             np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0)
+
+
+# ---------------------------------------------------------------------------------------------
+# custom steering vectors and the uniform-flow environment against the reference's own results
+# ---------------------------------------------------------------------------------------------
+def test_oracle_custom_steering_and_flow_match_reference(golden):
+    g = golden('custom_flow_kat.npz')
+    s = golden('small_kat.npz')
+    csm, freqs, mpos, gpos = s['csm0'], s['freqs0'], s['mpos'], s['gpos']
+    M = mpos.shape[1]
+    for j, b in enumerate(g['bins']):
+        for st in STEERS:
+            h = g[f'steer_{st.replace(" ", "_")}_{b}']
+            for rd in (False, True):
+                ref = g[f'cust_{st.replace(" ", "_")}_{int(rd)}_{b}']
+                res, nrm = O.beamformer_freq_custom(rd, 1.25, h, csm=csm[b])
+                np.testing.assert_allclose(res, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+                np.testing.assert_allclose(nrm, g[f'custn_{st.replace(" ", "_")}_{int(rd)}_{b}'], rtol=1e-13)
+                ref = g[f'custe_{st.replace(" ", "_")}_{int(rd)}_{b}']
+                res, _ = O.beamformer_freq_custom(rd, 1.25, h, eig=(g['eigvals'][j, M - 2:],
+                                                                    g['eigvecs'][j][:, M - 2:]))
+                np.testing.assert_allclose(res, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    r0f = O.uniform_flow_apparent_r(gpos, 0.0, 0.3, (1.0, 0.5, 0.0))
+    rmf = O.uniform_flow_apparent_r(gpos, mpos, 0.3, (1.0, 0.5, 0.0))
+    np.testing.assert_array_equal(r0f, g['flow_r0'])
+    np.testing.assert_array_equal(rmf, g['flow_rm'])
+    ind = np.arange(10, 31)
+    for st in STEERS:
+        for rd in (False, True):
+            got = O.beamformer_calc(csm, freqs, ind, r0f, rmf, 343.0, st, rd)[ind]
+            ref = g[f'flow_{st.replace(" ", "_")}_{int(rd)}']
+            if st in ('classic', 'inverse'):
+                np.testing.assert_array_equal(got, ref)
+            else:
+                # the 1/r steering types differ from numba's complex-by-real division by 1 ulp on some
+                # non-Euclidean distances (bit-exact for the Euclidean ones of small_kat.npz)
+                np.testing.assert_allclose(got, ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
+
+
+def test_host_uniform_flow_and_steer_vector_match_reference(golden):
+    """The package's host-side UniformFlowEnvironment and SteeringVector.steer_vector restatements."""
+    import acoular_b200 as ac
+    from acoular_b200.environments import UniformFlowEnvironment
+    g = golden('custom_flow_kat.npz')
+    s = golden('small_kat.npz')
+    env = UniformFlowEnvironment(c=343.0, ma=0.3, fdv=(1.0, 0.5, 0.0))
+    np.testing.assert_array_equal(env.apparent_r(s['gpos'], s['mpos']), g['flow_rm'])
+    np.testing.assert_array_equal(env.apparent_r(s['gpos']), g['flow_r0'])
+    st = ac.SteeringVector(grid=ac.ImportGrid(pos=s['gpos']), mics=ac.MicGeom(pos_total=s['mpos']))
+    for b in g['bins']:
+        for t in STEERS:
+            st.steer_type = t
+            ref = g[f'steer_{t.replace(" ", "_")}_{b}']
+            got = st.steer_vector(s['freqs0'][b])
+            # float32 cos/sin of numpy vs the reference's numba (libm): a few float32 ulp
+            assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
