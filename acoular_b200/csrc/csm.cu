@@ -38,6 +38,12 @@ void set_cuda_error(cudaError_t e) { g_last_cuda_error = cudaGetErrorString(e); 
 // same bits) and stores them back: one shared-memory round trip and one barrier per pass instead
 // of per stage.
 // ------------------------------------------------------------------------------------------------
+// Shared-memory slot of point j of a mic's sequence: one padding slot after every 8 points, so that
+// 8 threads reading 16-byte points 8 apart (the first pass) or 64 apart hit different banks.
+__device__ __forceinline__ int zp(int j) { return j + (j >> 3); }
+// padded length of one mic's sequence of H points (an odd number of 16-byte slots past the padding)
+__host__ __device__ constexpr int fft_stride(int H) { return H + (H >> 3) + 1; }
+
 // s (1..3) consecutive radix-2 DIT stages of lengths L1, 2 L1, .., on a bit-reversed sequence z of
 // H points (one mic).  Task `task` in [0, H / 2^s) owns points base + t * L1/2, t = 0 .. 2^s - 1.
 template <int S>
@@ -50,7 +56,7 @@ __device__ __forceinline__ void fft_pass(double2 *__restrict__ z, int L1, int ta
     const int base = grp * Ls + pos;
     double2 v[1 << S];
 #pragma unroll
-    for (int t = 0; t < (1 << S); ++t) v[t] = z[base + t * half1];
+    for (int t = 0; t < (1 << S); ++t) v[t] = z[zp(base + t * half1)];
 #pragma unroll
     for (int q = 0; q < S; ++q) {
         const int L = L1 << q, hf = L >> 1;
@@ -69,7 +75,7 @@ __device__ __forceinline__ void fft_pass(double2 *__restrict__ z, int L1, int ta
         }
     }
 #pragma unroll
-    for (int t = 0; t < (1 << S); ++t) z[base + t * half1] = v[t];
+    for (int t = 0; t < (1 << S); ++t) z[zp(base + t * half1)] = v[t];
 }
 
 // Output forms of the spectra (OUT): complex128 or complex64 [bin][window][mic] for the FP64 /
@@ -86,7 +92,7 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
                                                          const double2 *__restrict__ tw, int bin_lo, int nbins,
                                                          void *__restrict__ out, int R, int KC, int64_t lo_elems)
 {
-    extern __shared__ double2 zs[];  // [mpb][H]
+    extern __shared__ double2 zs[];  // [mpb][fft_stride(H)], point j of mic ml at zs[ml * stride + zp(j)]
     const int H = N >> 1;
     int logH = 0;
     while ((1 << logH) < H) ++logH;
@@ -102,7 +108,7 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
         const double x0 = (double)src[(int64_t)(2 * j) * M + m0 + ml] * window[2 * j];
         const double x1 = (double)src[(int64_t)(2 * j + 1) * M + m0 + ml] * window[2 * j + 1];
         const int jr = (int)(__brev((unsigned)j) >> (32 - logH));
-        zs[ml * H + (logH ? jr : 0)] = make_double2(x0, x1);
+        zs[ml * fft_stride(H) + zp(logH ? jr : 0)] = make_double2(x0, x1);
     }
     __syncthreads();
 
@@ -114,9 +120,9 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
         for (int idx = threadIdx.x; idx < nm * ntask; idx += blockDim.x) {
             const int ml = idx / ntask;
             const int task = idx - ml * ntask;
-            if (S == 3) fft_pass<3>(zs + ml * H, L1, task, N, tw);
-            else if (S == 2) fft_pass<2>(zs + ml * H, L1, task, N, tw);
-            else fft_pass<1>(zs + ml * H, L1, task, N, tw);
+            if (S == 3) fft_pass<3>(zs + ml * fft_stride(H), L1, task, N, tw);
+            else if (S == 2) fft_pass<2>(zs + ml * fft_stride(H), L1, task, N, tw);
+            else fft_pass<1>(zs + ml * fft_stride(H), L1, task, N, tw);
         }
         __syncthreads();
         st += S;
@@ -126,9 +132,9 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
     for (int idx = threadIdx.x; idx < nbins * nm; idx += blockDim.x) {
         const int ml = idx % nm;
         const int k = bin_lo + idx / nm;
-        const double2 *z = zs + ml * H;
-        const double2 zk = z[k % H];
-        const double2 zc = z[(H - k % H) % H];
+        const double2 *z = zs + ml * fft_stride(H);
+        const double2 zk = z[zp(k % H)];
+        const double2 zc = z[zp((H - k % H) % H)];
         const double er = 0.5 * (zk.x + zc.x), ei = 0.5 * (zk.y - zc.y);
         const double orr = 0.5 * (zk.y + zc.y), oi = -0.5 * (zk.x - zc.x);
         double2 wk;
@@ -322,7 +328,7 @@ int fft_launch(const void *samples, int sample_dtype, int out_form, int num_mics
 {
     const int mpb = fft_mics_per_block(block_size);
     const dim3 g1((num_mics + mpb - 1) / mpb, (unsigned)num_windows);
-    const size_t smem = (size_t)mpb * (block_size / 2) * sizeof(double2);
+    const size_t smem = (size_t)mpb * fft_stride(block_size / 2) * sizeof(double2);
 #define ACB_FFT_LAUNCH(TS, OF)                                                                                    \
     do {                                                                                                          \
         auto kern = fft_window_kernel<TS, OF>;                                                                    \
