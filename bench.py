@@ -49,7 +49,7 @@ def parse():
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--bins', type=int, default=0, help='limit the number of map bins (profiling only)')
     ap.add_argument('--workload', default='precision256',
-                    choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed'])
+                    choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig'])
     ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     return ap.parse_args()
@@ -453,9 +453,87 @@ def run_serving(args, mixed: bool):
           clocks=clk.summary(), dtype=f'{args.tc_precision} / f32 accum')
 
 
+def run_eig(args):
+    """Eigenvalue beamformer (BeamformerEig, n = -1) on the 256-mic workload: per step the device
+    eigendecomposition of all 513 CSMs and the map of the largest component (plain FP64 form).
+    The CSM is computed once; the oracle checks 2 bins."""
+    import torch
+
+    from acoular_b200 import device as D
+    from acoular_b200 import workloads
+    from oracle import oracle as O
+    dev = torch.device('cuda', 0)
+    wl = workloads.precision_256()
+    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
+    F = N // 2 + 1
+    x = workloads.monopole_time_data_torch(wl, device=dev)
+    csm = D.calc_csm(x, N, 'Hanning', '50%', 'complex128')
+    del x
+    freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[:F])
+    k = torch.as_tensor(2 * np.pi * freqs / wl.c, device=dev)
+    mpos, gpos = torch.as_tensor(wl.mics.pos, device=dev), torch.as_tensor(wl.grid.pos, device=dev)
+    ev = torch.empty((F, M), dtype=torch.float64, device=dev)
+    evec = torch.empty_like(csm)
+    out = torch.empty((F, G), dtype=torch.float64, device=dev)
+    norm = M / (M - 1.0)
+    ev_ms, map_ms = [], []
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    def step(rec=False):
+        if rec:
+            e[0].record()
+        for f0 in range(0, F, 64):
+            ev[f0:f0 + 64], evec[f0:f0 + 64] = torch.linalg.eigh(csm[f0:f0 + 64])
+        if rec:
+            e[1].record()
+        D.map_eig_f64(ev[:, M - 1:].contiguous(), evec[:, :, M - 1:].contiguous(), k, mpos, gpos, 'true level', True,
+                      norm, clip_negative=True, out=out)
+        if rec:
+            e[2].record()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        t0.record()
+        for _ in range(args.steps):
+            step(rec=True)
+            e[2].synchronize()
+            ev_ms.append(e[0].elapsed_time(e[1]))
+            map_ms.append(e[1].elapsed_time(e[2]))
+        t1.record()
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / args.steps
+    # end to end against the oracle (numpy eigh + the reference's eigen kernel) on 2 bins
+    r0, rm = O.apparent_r(wl.grid.pos), O.apparent_r(wl.grid.pos, wl.mics.pos)
+    errs = []
+    for b in (100, 400):
+        c_h = csm[b].cpu().numpy()
+        w, v = np.linalg.eigh(c_h)
+        ref = O.beamformer_freq_eig('true level', True, norm, r0, rm, 2 * np.pi * freqs[b] / wl.c, w[M - 1:],
+                                    np.ascontiguousarray(v[:, M - 1:]))[0]
+        ref[ref < 0] = 0.0
+        errs.append(float(np.abs(out[b].cpu().numpy() - ref).max() / np.abs(ref).max()))
+    flops = 8.0 * M * G * F   # algorithmic: one complex M-vector product per grid-pt x bin
+    _line('eigenvalue beamformer grid-pts*bins/s (BeamformerEig n=-1, 256 mics, 401x401 grid, 513 bins)',
+          G * F / (ms / 1e3), UNIT, ms, args,
+          {'workload': 'eig_' + wl.name, 'mics': M, 'grid_points': G, 'bins': F, 'components': 1,
+           'steer_type': 'true level', 'r_diag': True, 'form': 'f64 (glibc-faithful steering)',
+           'csm': 'complex128, computed once'},
+          eigh_ms_per_step=float(np.mean(ev_ms)), map_ms_per_step=float(np.mean(map_ms)),
+          map_rate=G * F / (float(np.mean(map_ms)) / 1e3), map_tflops_algorithmic=flops / (np.mean(map_ms) / 1e3) / 1e12,
+          accuracy={'vs': 'oracle (numpy eigh + the reference eigen kernel restated)', 'bins': [100, 400],
+                    'max_rel_err': max(errs)},
+          gpu_launches_per_step='eigh (cuSOLVER, 9 batched calls) + 1 map_eig_kernel', clocks=clk.summary(),
+          dtype='f64')
+
+
 def main():
     args = parse()
     from acoular_b200 import workloads
+    if args.workload == 'eig':
+        return run_eig(args)
     if args.workload == 'batched64':
         return run_batched(args)
     if args.workload == 'large3d':
