@@ -58,7 +58,9 @@ __device__ __forceinline__ void sincos_exception(const uint64_t *__restrict__ ta
 }
 
 // Float32 cos/sin of a float32 argument: correctly rounded value through FP64 evaluation,
-// optionally corrected to the host C library's cosf/sinf by the exception table.
+// optionally corrected to the host C library's cosf/sinf by the exception table.  The table holds
+// non-negative arguments; a negative one is looked up by its magnitude (the C library's cosf is even
+// and its sinf odd, bit for bit, and a delta on the bits of a float changes its magnitude).
 __device__ __forceinline__ void sincos_f32_arg(float x, const uint64_t *table, uint64_t mask, bool faithful,
                                                float &c, float &s)
 {
@@ -68,7 +70,7 @@ __device__ __forceinline__ void sincos_f32_arg(float x, const uint64_t *table, u
     s = __double2float_rn(sd);
     if (faithful) {
         int dc, ds;
-        sincos_exception(table, mask, x, dc, ds);
+        sincos_exception(table, mask, fabsf(x), dc, ds);
         if (dc) c = __int_as_float(__float_as_int(c) + dc);
         if (ds) s = __int_as_float(__float_as_int(s) + ds);
     }

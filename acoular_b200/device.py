@@ -445,3 +445,51 @@ def map_tc_batch(instances, precision: str = 'bf16x3', error_word: torch.Tensor 
     N.check(N.lib().acb_map_tc_batch(params, io, n, prec, ws.data_ptr(), ws.numel(), N.ptr(error_word),
                                      N.stream_handle()), 'acb_map_tc_batch')
     return [it.out for it in instances]
+
+
+# ------------------------------------------------------------------------------------------------
+# point-spread functions and DAMAS
+# ------------------------------------------------------------------------------------------------
+def psf_f64(r0: torch.Tensor, rm: torch.Tensor, k: float, sources: torch.Tensor, steer_type: str,
+            round_f32: bool = False, glibc_faithful: bool = True, out: torch.Tensor | None = None) -> torch.Tensor:
+    """PSF (G, S) of unit sources at the grid points ``sources`` (int64, (S,)) for one wave number,
+    distances r0 (G,), rm (G, M) float64 on the device (calcPointSpreadFunction)."""
+    G, M = rm.shape
+    if not (r0.is_contiguous() and rm.is_contiguous()) or r0.dtype != torch.float64 or rm.dtype != torch.float64:
+        msg = 'r0 and rm must be contiguous float64 tensors'
+        raise ValueError(msg)
+    sources = sources.to(device=rm.device, dtype=torch.int64).contiguous()
+    S = sources.numel()
+    if S and (int(sources.min()) < 0 or int(sources.max()) >= G):
+        msg = f'source indices must lie in [0, {G})'
+        raise IndexError(msg)
+    p = map_params(M, G, 1, steer_type, False, 1.0, False, None, glibc_faithful, rm.device)
+    if out is None:
+        out = torch.empty((G, S), dtype=torch.float64, device=rm.device)
+    if S == 0:
+        return out
+    N.check(N.lib().acb_psf_f64(ctypes.byref(p), S, sources.data_ptr(), float(k), r0.data_ptr(), rm.data_ptr(),
+                                int(bool(round_f32)), out.data_ptr(), N.stream_handle()), 'acb_psf_f64')
+    return out
+
+
+def damas_gauss_seidel(psf: torch.Tensor, dirty_map: torch.Tensor, n_iter: int, relax: float,
+                       solution: torch.Tensor | None = None, cta_per_bin: int = 0) -> torch.Tensor:
+    """DAMAS Gauss-Seidel sweeps for B bins: psf (B, G, G), dirty_map (B, G) float64; ``solution``
+    (B, G) holds the start (default: the dirty map) and receives the result."""
+    B, G = dirty_map.shape
+    if tuple(psf.shape) != (B, G, G):
+        msg = f'psf must be (num_bins, num_grid, num_grid) = ({B}, {G}, {G}), got {tuple(psf.shape)}'
+        raise ValueError(msg)
+    for t in (psf, dirty_map):
+        if t.dtype != torch.float64 or not t.is_contiguous():
+            msg = 'psf and dirty_map must be contiguous float64 tensors'
+            raise ValueError(msg)
+    if solution is None:
+        solution = dirty_map.clone()
+    if B == 0 or G == 0:
+        return solution
+    N.check(N.lib().acb_damas_gauss_seidel_f64(psf.data_ptr(), G, B, dirty_map.data_ptr(), solution.data_ptr(),
+                                               int(n_iter), float(relax), int(cta_per_bin), N.stream_handle()),
+            'acb_damas_gauss_seidel_f64')
+    return solution

@@ -2,10 +2,14 @@
 
 * :func:`calcCSM`        -- fastFuncs.py:19-58; ``csm`` (F, M, M) c128/c64 C-contiguous is updated
   in place with ``conj(spec[f, c]) * spec[f, r]`` for r <= c; returns ``csm``.
-* :func:`beamformerFreq` -- fastFuncs.py:61-214 for the predefined steering types and a full CSM:
-  ``(steerVecType, boolRemovedDiagOfCSM, normFactor, (r0, rm, k), csm) -> (map, steerNorm)``.
-  The 'custom' steering and eigenvalue forms are not implemented by this build
-  (``NotImplementedError``).
+* :func:`beamformerFreq` -- fastFuncs.py:61-214:
+  ``(steerVecType, boolRemovedDiagOfCSM, normFactor, (r0, rm, k) | steer (G, M), csm | (eigval, eigvec))
+  -> (map, steerNorm)`` for the predefined steering types and 'custom' steering vectors, with a full
+  CSM or an eigen-decomposition tuple.
+* :func:`calcPointSpreadFunction` -- fastFuncs.py:563-801; ``(steerVecType, r0, rm, k, indSource,
+  dtype) -> (G, len(indSource))``.
+* :func:`damasSolverGaussSeidel` -- fastFuncs.py:804-855; ``(A (..., G, G), dirtyMap (..., G), nIterations,
+  relax, damasSolution (..., G))``, ``damasSolution`` overwritten with the result.
 
 Wrong dtypes or non-contiguous arrays raise ``TypeError`` where the reference's explicit numba
 signatures raise a typing error.  Every call uploads its inputs, runs the kernel and downloads the
@@ -139,3 +143,38 @@ def _beamformer_freq_custom(r_diag, norm, steer_vec, csm_or_eig):
         c = torch.from_numpy(csm_or_eig).to(dev)[None]
         D.map_custom_f64(c, h_d, r_diag, float(norm), out=out, steer_norm=nrm)
     return out[0].cpu().numpy(), nrm[0].cpu().numpy()
+
+
+def calcPointSpreadFunction(steerVecType, distGridToArrayCenter, distGridToAllMics, waveNumber, indSource,  # noqa: N802, N803
+                            dtype):
+    """PSF of unit sources at the grid points ``indSource``: (G, len(indSource)) of ``dtype``."""
+    if steerVecType not in N.STEER_CODES or steerVecType == 'custom':
+        raise KeyError(steerVecType)
+    dev = D.require_cuda()
+    rm = torch.as_tensor(np.ascontiguousarray(np.atleast_2d(distGridToAllMics), dtype=np.float64), device=dev)
+    r0 = torch.as_tensor(np.array(np.broadcast_to(distGridToArrayCenter, (rm.shape[0],)), dtype=np.float64),
+                         device=dev)
+    k = float(np.asarray(waveNumber).reshape(-1)[0])
+    src = torch.as_tensor(np.asarray(indSource, dtype=np.int64).reshape(-1), device=dev)
+    out = D.psf_f64(r0, rm, k, src, steerVecType, round_f32=np.dtype(dtype) == np.float32)
+    return out.cpu().numpy().astype(dtype)
+
+
+def damasSolverGaussSeidel(A, dirtyMap, nIterations, relax, damasSolution):  # noqa: N802, N803
+    """Gauss-Seidel DAMAS solver; ``damasSolution`` (float64, C-contiguous) holds the start and is
+    overwritten with the result after ``nIterations`` sweeps."""
+    _check_contig(damasSolution, np.float64, 'damasSolution')
+    dev = D.require_cuda()
+    y = np.asarray(dirtyMap, dtype=np.float64)
+    G = y.shape[-1]
+    B = int(np.prod(y.shape[:-1], dtype=np.int64))
+    if damasSolution.shape != y.shape or np.shape(A) != y.shape + (G,):
+        msg = 'A must be (..., G, G) and dirtyMap / damasSolution (..., G)'
+        raise ValueError(msg)
+    A_d = torch.as_tensor(np.ascontiguousarray(A, dtype=np.float64).reshape(B, G, G), device=dev)
+    y_d = torch.as_tensor(np.ascontiguousarray(y).reshape(B, G), device=dev)
+    x_d = torch.as_tensor(damasSolution.reshape(B, G), device=dev).clone()
+    D.damas_gauss_seidel(A_d, y_d, int(np.asarray(nIterations).reshape(-1)[0]),
+                         float(np.asarray(relax).reshape(-1)[0]), x_d)
+    damasSolution[...] = x_d.cpu().numpy().reshape(damasSolution.shape)
+    return damasSolution

@@ -463,6 +463,185 @@ class BeamformerMusic(BeamformerEig):
         return 4e-10 * out.min(dim=1, keepdim=True).values / out
 
 
+def _steer_distances_device(steer, dev, holder):
+    """SteeringVector.r0 / .rm (any environment) on the device, cached on ``holder`` by steer digest."""
+    key = ('r0rm', steer.digest, str(dev))
+    if getattr(holder, '_r0rm_key', None) != key:
+        holder._r0_dev = torch.as_tensor(np.array(np.broadcast_to(steer.r0, (steer.grid.size,)), dtype=np.float64),
+                                         device=dev)
+        holder._rm_dev = torch.as_tensor(np.ascontiguousarray(steer.rm, dtype=np.float64), device=dev)
+        holder._r0rm_key = key
+    return holder._r0_dev, holder._rm_dev
+
+
+class PointSpreadFunction:
+    """Point-spread function of a steering set-up (acoular/fbeamform.py:948-1124), on the GPU.
+
+    ``psf`` is the (G, len(grid_indices)) map of unit sources at ``grid_indices`` (all grid points,
+    (G, G), when empty) at frequency ``freq``, rounded to ``precision``.  For a plain
+    :class:`SteeringVector` (any environment) the predefined formulation runs on the PSF kernel
+    (``acb_psf_f64``, calcPointSpreadFunction); other steering objects take
+    |steer_vector^H transfer|^2 as a complex GEMM.  ``calcmode`` ('single', 'block', 'full',
+    'readonly') is kept for interface parity; nothing is cached between calls, so every mode
+    computes the requested columns (``'full'``: all of them).
+    """
+
+    CALCMODES = ('single', 'block', 'full', 'readonly')
+
+    def __init__(self, steer: SteeringVector | None = None, grid_indices=None, calcmode: str = 'single',
+                 precision: str = 'float64', freq: float = 1.0, cached: bool = False, glibc_faithful: bool = True):
+        if calcmode not in self.CALCMODES:
+            msg = f'calcmode must be one of {self.CALCMODES}, got {calcmode!r}'
+            raise ValueError(msg)
+        if precision not in ('float64', 'float32'):
+            msg = f"precision must be 'float64' or 'float32', got {precision!r}"
+            raise ValueError(msg)
+        self.steer = steer if steer is not None else SteeringVector()
+        self.grid_indices = np.array([], dtype=int) if grid_indices is None else np.asarray(grid_indices, dtype=int)
+        self.calcmode = calcmode
+        self.precision = precision
+        self.freq = float(freq)
+        self.cached = cached
+        self.glibc_faithful = glibc_faithful
+
+    @property
+    def digest(self) -> str:
+        return f'{self.steer.digest}|{self.precision}'
+
+    def _indices(self):
+        gs = self.steer.grid.size
+        return self.grid_indices if self.grid_indices.size else np.arange(gs)
+
+    def psf_device(self, ind=None, device=None, out: torch.Tensor | None = None) -> torch.Tensor:
+        """The PSF (G, len(ind)) as a float64 device tensor (values rounded to ``precision``);
+        written into ``out`` when given."""
+        dev = D.require_cuda(device)
+        gs = self.steer.grid.size
+        ind = self._indices() if ind is None else np.asarray(ind, dtype=int)
+        if self.calcmode == 'full':
+            cols = np.arange(gs)
+        else:
+            cols = ind
+        if cols.size and (cols.min() < -gs or cols.max() >= gs):
+            msg = f'grid indices must lie in [0, {gs})'
+            raise IndexError(msg)
+        cols = np.where(cols < 0, cols + gs, cols)
+        if type(self.steer) is SteeringVector:
+            r0, rm = _steer_distances_device(self.steer, dev, self)
+            k = 2 * np.pi * self.freq / self.steer.env.c
+            direct = out is not None and np.array_equal(ind, cols)
+            res = D.psf_f64(r0, rm, k, torch.as_tensor(cols, dtype=torch.int64, device=dev), self.steer.steer_type,
+                            round_f32=self.precision == 'float32', glibc_faithful=self.glibc_faithful,
+                            out=out if direct else None)
+            if direct:
+                return out
+        else:
+            # arbitrary steering objects (acoular/fbeamform.py:1119-1124)
+            h = torch.as_tensor(np.ascontiguousarray(self.steer.steer_vector(self.freq), dtype=np.complex128),
+                                device=dev)
+            t = torch.as_tensor(np.ascontiguousarray(np.atleast_2d(self.steer.transfer(self.freq, cols)),
+                                                     dtype=np.complex128), device=dev)
+            prod = h.conj() @ t.T
+            res = (prod * prod.conj()).real.contiguous()
+            if self.precision == 'float32':
+                res = res.float().double()
+        if self.calcmode == 'full' and not np.array_equal(ind, cols):
+            res = res[:, torch.as_tensor(ind, device=dev)]
+        if out is not None:
+            out.copy_(res)
+            return out
+        return res
+
+    @property
+    def psf(self) -> np.ndarray:
+        return self.psf_device().cpu().numpy().astype(self.precision)
+
+
+class BeamformerDamas(BeamformerBase):
+    """DAMAS deconvolution (acoular/fbeamform.py:1127-1208), on the GPU.
+
+    Per bin: the conventional map (negative values set to 0 with ``r_diag``), the full PSF of every
+    grid point at the bin's frequency (``acb_psf_f64``), and ``n_iter`` Gauss-Seidel sweeps with
+    relaxation ``damp`` starting from the map (``acb_damas_gauss_seidel_f64``).  Bins go to the device
+    in chunks whose PSFs fit ``psf_budget_bytes``.
+    """
+
+    def __init__(self, *args, n_iter: int = 100, damp: float = 1.0, psf_precision: str = 'float64',
+                 calcmode: str = 'full', psf_budget_bytes: int = 1 << 30, cta_per_bin: int = 0, **kw):
+        super().__init__(*args, **kw)
+        if psf_precision not in ('float64', 'float32'):
+            msg = f"psf_precision must be 'float64' or 'float32', got {psf_precision!r}"
+            raise ValueError(msg)
+        if calcmode not in PointSpreadFunction.CALCMODES:
+            msg = f'calcmode must be one of {PointSpreadFunction.CALCMODES}, got {calcmode!r}'
+            raise ValueError(msg)
+        self.n_iter = int(n_iter)
+        self.damp = float(damp)
+        self.psf_precision = psf_precision
+        self.calcmode = calcmode
+        self.psf_budget_bytes = int(psf_budget_bytes)
+        self.cta_per_bin = int(cta_per_bin)
+
+    @property
+    def digest(self) -> str:
+        return super().digest + f'|damas{self.n_iter}|{self.damp}|{self.psf_precision}'
+
+    def _dirty_map_device(self, ind, csm_all):
+        """Conventional maps (B, G) float64 of bins ``ind`` on the device, the reference's
+        beamformerFreq with negative values set to 0 when r_diag is set."""
+        dev = csm_all.device
+        norm = self.sig_loss_norm()
+        ind_d = torch.as_tensor(ind, device=dev)
+        if type(self.steer) is not SteeringVector:
+            out = torch.empty((ind.size, self.steer.grid.size), dtype=torch.float64, device=dev)
+            for j, i in enumerate(ind):
+                h = torch.as_tensor(np.ascontiguousarray(self.steer.steer_vector(self._f[i]), dtype=np.complex128),
+                                    device=dev)
+                D.map_custom_f64(csm_all[int(i):int(i) + 1], h[None], self.r_diag, norm, out=out[j:j + 1])
+        else:
+            csm = csm_all.index_select(0, ind_d).contiguous()
+            k = torch.as_tensor(2 * np.pi * self._f[ind] / self.steer.env.c, dtype=torch.float64, device=dev)
+            if type(self.steer.env) is not Environment:
+                r0, rm = _steer_distances_device(self.steer, dev, self)
+                out = D.map_rm_f64(csm, k, r0, rm, self.steer.steer_type, self.r_diag, norm, clip_negative=False,
+                                   glibc_faithful=self.glibc_faithful)
+            elif self.form == 'tc':
+                mpos, gpos = self._geometry(dev)
+                out = D.map_tc(csm, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm, ref=self.steer.ref,
+                               clip_negative=False, precision=self.tc_precision)
+            else:
+                mpos, gpos = self._geometry(dev)
+                out = D.map_f64(csm, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm, ref=self.steer.ref,
+                                clip_negative=False, glibc_faithful=self.glibc_faithful)
+        if self.r_diag:
+            out.clamp_(min=0.0)
+        return out
+
+    def _calc(self, ind):
+        ind = np.asarray(ind, dtype=np.int64)
+        if ind.size == 0:
+            return
+        csm_all = self.freq_data.csm_device
+        dev = csm_all.device
+        G = self.steer.grid.size
+        chunk = max(1, min(ind.size, self.psf_budget_bytes // max(1, G * G * 8)))
+        p = PointSpreadFunction(steer=self.steer, calcmode='full', precision=self.psf_precision,
+                                glibc_faithful=self.glibc_faithful)
+        for s0 in range(0, ind.size, chunk):
+            sub = ind[s0:s0 + chunk]
+            y = self._dirty_map_device(sub, csm_all)
+            psf = torch.empty((sub.size, G, G), dtype=torch.float64, device=dev)
+            for j, i in enumerate(sub):
+                p.freq = float(self._f[i])
+                p.psf_device(device=dev, out=psf[j])
+            x = D.damas_gauss_seidel(psf, y, self.n_iter, self.damp, cta_per_bin=self.cta_per_bin)
+            del psf
+            if self.precision == 'float32':
+                x = x.float()
+            self._ac[sub] = x.cpu().numpy()
+        self._fr[ind] = 1
+
+
 def L_p(x):
     """Sound pressure level 10 lg(x / 4e-10), floored at the dtype's eps (acoular/fbeamform.py:2412-2429)."""
     return 10 * np.log10(np.maximum(x / 4e-10, np.finfo(x.dtype).eps))

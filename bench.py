@@ -49,7 +49,7 @@ def parse():
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--bins', type=int, default=0, help='limit the number of map bins (profiling only)')
     ap.add_argument('--workload', default='precision256',
-                    choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig'])
+                    choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig', 'damas'])
     ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     return ap.parse_args()
@@ -529,11 +529,133 @@ def run_eig(args):
           dtype='f64')
 
 
+def run_damas(args):
+    """DAMAS (BeamformerDamas defaults: true level, r_diag, n_iter 100, damp 1.0) on the 64-mic, 41x41
+    workload's 8 kHz third-octave band (5 bins): per step the conventional maps, the 5 full PSFs
+    (1681 x 1681) and the Gauss-Seidel solution.  The CSM is computed once; the oracle checks 1 bin."""
+    import time
+
+    import torch
+
+    import acoular_b200 as ac
+    from acoular_b200 import device as D
+    from acoular_b200 import workloads
+    from oracle import oracle as O
+    dev = torch.device('cuda', 0)
+    wl = workloads.three_sources_64()
+    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
+    F = N // 2 + 1
+    x = workloads.monopole_time_data_torch(wl, device=dev)
+    csm = D.calc_csm(x, N, 'Hanning', '50%', 'complex128')
+    del x
+    freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[:F])
+    # the 8 kHz third-octave band as BeamformerBase.synthetic selects it
+    bins = np.arange(int(np.searchsorted(freqs, 8000.0 * 2.0 ** (-0.5 / 3))),
+                     int(np.searchsorted(freqs, 8000.0 * 2.0 ** (0.5 / 3))))
+    B = bins.size
+    n_iter, relax, st = 100, 1.0, 'true level'
+    norm = M / (M - 1.0)
+    mpos, gpos = torch.as_tensor(wl.mics.pos, device=dev), torch.as_tensor(wl.grid.pos, device=dev)
+    steer = ac.SteeringVector(grid=wl.grid, mics=wl.mics, steer_type=st)
+    r0_h, rm_h = np.ascontiguousarray(steer.r0), np.ascontiguousarray(steer.rm)
+    r0, rm = torch.as_tensor(r0_h, device=dev), torch.as_tensor(rm_h, device=dev)
+    csm_b = csm[torch.as_tensor(bins, device=dev)].contiguous()
+    psf = torch.empty((B, G, G), dtype=torch.float64, device=dev)
+    src = torch.arange(G, device=dev)
+    sol = torch.empty((B, G), dtype=torch.float64, device=dev)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    st_ms = {'map': [], 'psf': [], 'gauss_seidel': []}
+
+    kb_h = 2 * np.pi * freqs[bins] / wl.c
+    kb = [float(v) for v in kb_h]
+    kb_t = torch.as_tensor(kb_h, device=dev)
+
+    def step(rec=False):   # wave numbers as host floats: no synchronisation inside the step
+        if rec:
+            e[0].record()
+        y = D.map_f64(csm_b, kb_t, mpos, gpos, st, True, norm, clip_negative=True)
+        if rec:
+            e[1].record()
+        for j in range(B):
+            D.psf_f64(r0, rm, kb[j], src, st, out=psf[j])
+        if rec:
+            e[2].record()
+        sol.copy_(y)
+        D.damas_gauss_seidel(psf, y, n_iter, relax, solution=sol)
+        if rec:
+            e[3].record()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        t0.record()
+        for _ in range(args.steps):
+            step(rec=True)
+            e[3].synchronize()
+            st_ms['map'].append(e[0].elapsed_time(e[1]))
+            st_ms['psf'].append(e[1].elapsed_time(e[2]))
+            st_ms['gauss_seidel'].append(e[2].elapsed_time(e[3]))
+        t1.record()
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / args.steps
+    # accuracy: one bin against the oracle (the reference's PSF and Gauss-Seidel restated)
+    b0 = int(bins[B // 2])
+    c_h = csm[b0:b0 + 1].cpu().numpy()
+    tc = time.perf_counter()
+    ref = O.beamformer_damas_calc(c_h, freqs[b0:b0 + 1], [0], r0_h, rm_h, wl.c, st, True, n_iter, relax)[0]
+    cpu_s = time.perf_counter() - tc
+    got = sol[B // 2].cpu().numpy()
+    err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    # end to end through the public API: host CSM -> PowerSpectraImport -> BeamformerDamas -> band map
+    c_host = csm.cpu().numpy()
+    e2e_ms = []
+    for it in range(max(2, min(args.steps, 5)) + 1):
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        ps = ac.PowerSpectraImport(csm=c_host, frequencies=freqs)
+        bf = ac.BeamformerDamas(freq_data=ps, steer=steer, r_diag=True, n_iter=n_iter, damp=relax)
+        band = np.asarray(bf.result[int(bins[0]):int(bins[-1]) + 1])
+        if it:
+            e2e_ms.append((time.perf_counter() - ta) * 1e3)
+    e2e_err = float(np.abs(band[B // 2] - ref).max() / np.abs(ref).max())
+    gs_ms = float(np.mean(st_ms['gauss_seidel']))
+    pk = peaks()
+    gs_bytes = float(B) * n_iter * G * G * 8.0       # the PSF read once per sweep
+    achieved = gs_bytes / (gs_ms / 1e3) / 1e9
+    nblk = (G + 31) // 32
+    _line('DAMAS bins/s (BeamformerDamas, 64 mics, 41x41 grid, 8 kHz third-octave band, n_iter 100)',
+          B / (ms / 1e3), 'bins/s', ms, args,
+          {'workload': 'damas_' + wl.name, 'mics': M, 'grid_points': G, 'bins': B, 'n_iter': n_iter, 'damp': relax,
+           'steer_type': st, 'r_diag': True, 'psf': 'full (G x G per bin), float64',
+           'csm': 'complex128, computed once', 'l2': 'psf of the band (113 MB) read 100x per step'},
+          stage_ms={k: float(np.mean(v)) for k, v in st_ms.items()},
+          roofline={'kernel': 'damas_kernel', 'bound': 'hbm (latency: one 32-row block per step)',
+                    'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved / pk['hbm_gbs'],
+                    'traffic': None, 'bytes_per_launch': gs_bytes,
+                    'sequential_steps_per_launch': n_iter * nblk,
+                    'us_per_step': gs_ms * 1e3 / (n_iter * nblk)},
+          psf_rate_elems_per_s=B * G * G * M / (float(np.mean(st_ms['psf'])) / 1e3),
+          accuracy={'vs': 'oracle (the reference PSF and Gauss-Seidel restated)', 'bin': b0, 'max_rel_err': err,
+                    'e2e_max_rel_err': e2e_err},
+          e2e={'value': B / (float(np.median(e2e_ms)) / 1e3), 'unit': 'bins/s',
+               'ms': float(np.median(e2e_ms)),
+               'h2d_bytes_per_step': int(c_host.nbytes + r0_h.nbytes + rm_h.nbytes + 2 * 3 * 8 * (G + M)),
+               'd2h_bytes_per_step': int(B * G * 8)},
+          cpu_baseline={'value': 1.0 / cpu_s, 'unit': 'bins/s', 'cores': O.num_threads(), 'kind': 'port',
+                        'sample': f'1 bin (bin {b0}): map + full PSF + {n_iter} sweeps'},
+          gpu_launches=f'{1 + B + 1} per step (map_plain_kernel, {B} psf_kernel, damas_kernel) + 1 copy',
+          clocks=clk.summary(), dtype='f64')
+
+
 def main():
     args = parse()
     from acoular_b200 import workloads
     if args.workload == 'eig':
         return run_eig(args)
+    if args.workload == 'damas':
+        return run_damas(args)
     if args.workload == 'batched64':
         return run_batched(args)
     if args.workload == 'large3d':

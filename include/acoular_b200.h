@@ -208,6 +208,30 @@ size_t acb_map_tc_batch_workspace_bytes(const acb_map_params *params, int num_in
 int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num_instances, int precision,
                      void *workspace, size_t workspace_bytes, int *error_word, void *stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Point-spread functions and DAMAS deconvolution
+ * ------------------------------------------------------------------------------------------- */
+
+/* calcPointSpreadFunction (acoular/fastFuncs.py:563-801) for one wave number, as
+ * PointSpreadFunction._psf_call uses it (acoular/fbeamform.py:1093-1125):
+ *   out_psf[g][j] = PSF at grid point g of a unit source at grid point sources[j],
+ *   for p->steer_type (1..4), r0 float64 [G], rm float64 [G][M] (SteeringVector.r0 / .rm),
+ *   sources int64 [num_sources].  p->num_mics / num_grid / glibc_faithful / sincos_table are used.
+ *   round_f32 != 0 rounds each value to float32 (PointSpreadFunction.precision 'float32'). */
+int acb_psf_f64(const acb_map_params *p, int num_sources, const int64_t *sources, double wavenumber,
+                const double *r0, const double *rm, int round_f32, double *out_psf, void *stream);
+
+/* damasSolverGaussSeidel (acoular/fastFuncs.py:804-855) for num_bins independent bins, as
+ * BeamformerDamas._calc uses it (acoular/fbeamform.py:1167-1208):
+ *   psf float64 [num_bins][G][G] (row g = PSF values at g of every source), dirty_map float64
+ *   [num_bins][G]; solution float64 [num_bins][G] holds the starting solution and receives the
+ *   result after n_iter Gauss-Seidel sweeps with relaxation `relax` (negative values set to 0).
+ *   cta_per_bin: 1, 2, 4 or 8 CTAs (one cluster) per bin, 0 = choose from num_bins and the SM count.
+ *   ACB_ERR_UNSUPPORTED when a bin's solution (8 G bytes + 38 KB) exceeds a CTA's shared memory
+ *   (G above about 24,000). */
+int acb_damas_gauss_seidel_f64(const double *psf, int64_t num_grid, int num_bins, const double *dirty_map,
+                               double *solution, int n_iter, double relax, int cta_per_bin, void *stream);
+
 /* Size of the fixed device array behind acb_map_tc_noalloc (32 MiB per GPU, held until exit). */
 #define ACB_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 

@@ -73,6 +73,8 @@ def lib():
         L.orc_beamformer_eig.argtypes = [dp, dp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                          i64, i64, i64, dp, dp]
         L.orc_beamformer_custom.argtypes = [dp, dp, dp, i64, dp, ctypes.c_double, ctypes.c_int, i64, i64, dp, dp]
+        L.orc_psf.argtypes = [dp, dp, ctypes.c_double, ctypes.POINTER(i64), i64, ctypes.c_int, i64, i64, dp]
+        L.orc_damas_gauss_seidel_bins.argtypes = [dp, dp, i64, i64, i64, ctypes.c_double, dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -315,6 +317,51 @@ def beamformer_music_calc(eigvals, eigvecs, freqs, ind, r0, rm, c: float, steer_
                                 np.array(eigvals[i], dtype='float64')[:ne],
                                 np.array(eigvecs[i], dtype='complex128')[:, :ne])[0]
         out[i] = 4e-10 * b.min() / b
+    return out
+
+
+def psf(steer_type: str, r0: np.ndarray, rm: np.ndarray, k: float, ind, precision: str = 'float64'):
+    """``calcPointSpreadFunction`` (fastFuncs.py:563-801): (G, len(ind)) PSF of unit sources at the grid
+    points ``ind``, cast to ``precision`` as its output array is."""
+    r0 = np.ascontiguousarray(r0, dtype=np.float64)
+    rm = np.ascontiguousarray(rm, dtype=np.float64)
+    src = np.ascontiguousarray(ind, dtype=np.int64)
+    G, M = rm.shape
+    out = np.zeros((G, src.shape[0]))
+    lib().orc_psf(_dp(r0), _dp(rm), float(k), src.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), src.shape[0],
+                  STEER_TYPES[steer_type], G, M, _dp(out))
+    return out.astype(precision)
+
+
+def damas_gauss_seidel(A: np.ndarray, y: np.ndarray, n_iter: int, relax: float, x: np.ndarray) -> np.ndarray:
+    """``damasSolverGaussSeidel`` (fastFuncs.py:804-855) over leading bin axes: A (..., G, G),
+    y and x (..., G); x is the starting solution and is overwritten with the result (returned)."""
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    G = y.shape[-1]
+    F = int(np.prod(y.shape[:-1], dtype=np.int64))
+    xs = np.ascontiguousarray(x, dtype=np.float64).copy()
+    lib().orc_damas_gauss_seidel_bins(_dp(A), _dp(y), F, G, int(n_iter), float(relax), _dp(xs))
+    x[...] = xs
+    return x
+
+
+def beamformer_damas_calc(csm, freqs, ind, r0, rm, c: float, steer_type: str, r_diag: bool, n_iter: int = 100,
+                          damp: float = 1.0, psf_precision: str = 'float64', r_diag_norm: float = 0.0, out=None):
+    """``BeamformerDamas._calc`` (acoular/fbeamform.py:1167-1208) for a plain ``SteeringVector``: the
+    conventional map (negative values set to 0 with r_diag) deconvolved by Gauss-Seidel with the full PSF."""
+    G, M = rm.shape
+    if out is None:
+        out = np.zeros((csm.shape[0], G))
+    normfactor = sig_loss_norm(r_diag, M, r_diag_norm)
+    for i in ind:
+        k = 2 * np.pi * freqs[i] / c
+        y = beamformer_freq(steer_type, r_diag, normfactor, r0, rm, k, np.array(csm[i], dtype='complex128'))[0]
+        if r_diag:
+            y[np.sign(y) < 0] = 0.0
+        x = y.copy()
+        A = psf(steer_type, r0, rm, k, np.arange(G), psf_precision)
+        out[i] = damas_gauss_seidel(A, y, n_iter, damp, x)
     return out
 
 

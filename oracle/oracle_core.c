@@ -10,6 +10,10 @@
  *   orc_calc_csm_c128 / _c64   acoular/fastFuncs.py:19-58     (calcCSM)
  *   orc_dist_mat               acoular/environments.py:65-103 (dist_mat)
  *   orc_beamformer_fullcsm     acoular/fastFuncs.py:217-311   (_freqBeamformer_FullCSM)
+ *   orc_beamformer_eig         acoular/fastFuncs.py:313-411   (_freqBeamformer_EigValues)
+ *   orc_beamformer_custom      acoular/fastFuncs.py:414-559   (_freqBeamformer_SpecificSteerVec_*)
+ *   orc_psf                    acoular/fastFuncs.py:563-801   (calcPointSpreadFunction)
+ *   orc_damas_gauss_seidel     acoular/fastFuncs.py:804-855   (damasSolverGaussSeidel)
  * Parity of this restatement is pinned against golden vectors produced by running the reference's
  * own code (tests/golden/make_golden.py) and against the reference's committed regression arrays
  * for Environment.apparent_r.
@@ -318,4 +322,75 @@ void orc_set_num_threads(int n)
 #else
     (void)n;
 #endif
+}
+
+/* calcPointSpreadFunction (fastFuncs.py:563-801) for one wave number: the four
+ * _psf_Formulation* kernels.  r0: [G]; rm: [G][M]; src: [S] grid indices of the unit sources.
+ * out: [G][S], out[g][s] = |sum_m e^{-i fl32(k (rm[g][m] - rm[src][m]))} w_m|^2 * n^2 with the weights
+ * and normalisation of steering type steer_type (1..4), in the reference's order of operations. */
+void orc_psf(const double *r0, const double *rm, double k, const int64_t *src, int64_t S, int steer_type, int64_t G,
+             int64_t M, double *out)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < G; ++g) {
+        const double *rg = rm + g * M;
+        for (int64_t j = 0; j < S; ++j) {
+            const double *rs = rm + src[j] * M;
+            double pr = 0.0, pi = 0.0, help = 0.0;
+            for (int64_t m = 0; m < M; ++m) {
+                const float arg = (float)(k * (rg[m] - rs[m]));
+                double tr = (double)cosf(arg) / rs[m], ti = -(double)sinf(arg) / rs[m];
+                if (steer_type == 2) {
+                    tr *= rg[m];
+                    ti *= rg[m];
+                } else if (steer_type >= 3) {
+                    tr /= rg[m];
+                    ti /= rg[m];
+                    help += 1.0 / (rg[m] * rg[m]);
+                }
+                pr += tr;
+                pi += ti;
+            }
+            const double a2 = pr * pr + pi * pi;
+            double nf;
+            if (steer_type == 1) {
+                nf = r0[src[j]] / (double)M;
+                out[g * S + j] = a2 * (nf * nf);
+            } else if (steer_type == 2) {
+                nf = r0[src[j]] / r0[g] / (double)M;
+                out[g * S + j] = a2 * (nf * nf);
+            } else if (steer_type == 3) {
+                nf = r0[src[j]] / r0[g] / help;
+                out[g * S + j] = a2 * (nf * nf);
+            } else {
+                nf = r0[src[j]];
+                out[g * S + j] = a2 * (nf * nf) / (double)M / help;
+            }
+        }
+    }
+}
+
+/* damasSolverGaussSeidel (fastFuncs.py:804-855) for one bin: n_iter sweeps over g = 0..G-1, in order,
+ * x[g] = max(0, (1 - relax) x[g] + relax (y[g] - (sum_h A[g][h] x[h] - A[g][g] x[g]))) with the latest x.
+ * A: [G][G]; y: [G]; x: [G] starting solution, overwritten. */
+void orc_damas_gauss_seidel(const double *A, const double *y, int64_t G, int64_t n_iter, double relax, double *x)
+{
+    for (int64_t it = 0; it < n_iter; ++it) {
+        for (int64_t g = 0; g < G; ++g) {
+            const double *row = A + g * G;
+            double s = 0.0;
+            for (int64_t h = 0; h < G; ++h) s += row[h] * x[h];
+            s -= row[g] * x[g];
+            s = (1.0 - relax) * x[g] + relax * (y[g] - s);
+            x[g] = s > 0.0 ? s : 0.0;
+        }
+    }
+}
+
+/* damasSolverGaussSeidel over F independent bins (the guvectorize loop over the leading axis). */
+void orc_damas_gauss_seidel_bins(const double *A, const double *y, int64_t F, int64_t G, int64_t n_iter, double relax,
+                                 double *x)
+{
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t f = 0; f < F; ++f) orc_damas_gauss_seidel(A + f * G * G, y + f * G, G, n_iter, relax, x + f * G);
 }

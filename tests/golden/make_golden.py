@@ -20,6 +20,7 @@ their decorators removed, bound to plain stand-in objects:
 * ``BeamformerEig._get_na`` / ``_calc``, ``BeamformerMusic._calc``   acoular/fbeamform.py:844-888, 911-944
 * ``UniformFlowEnvironment.apparent_r``               acoular/environments.py:290-332
 * ``SteeringVector._steer_funcs_freq`` (as source text) acoular/fbeamform.py:145-153
+* ``PointSpreadFunction._psf_call``, ``BeamformerDamas._calc``   acoular/fbeamform.py:1096-1125, 1167-1208
 * ``WNoiseGenerator.signal``, ``SignalGenerator.usignal``, ``PointSource.result``,
   ``_fill_mic_signal_block``, ``Mixer.result``        (fixture time data)
 
@@ -107,6 +108,10 @@ eig_calc = _extract('acoular/fbeamform.py', 'BeamformerEig._calc', NS, rename='e
 music_calc = _extract('acoular/fbeamform.py', 'BeamformerMusic._calc', NS, rename='music_calc')
 uflow_apparent_r = _extract('acoular/environments.py', 'UniformFlowEnvironment.apparent_r', NS,
                             rename='uflow_apparent_r')
+NS['calcPointSpreadFunction'] = fastFuncs.calcPointSpreadFunction
+NS['damasSolverGaussSeidel'] = fastFuncs.damasSolverGaussSeidel
+psf_call = _extract('acoular/fbeamform.py', 'PointSpreadFunction._psf_call', NS, rename='psf_call')
+damas_calc = _extract('acoular/fbeamform.py', 'BeamformerDamas._calc', NS, rename='damas_calc')
 
 
 def _steer_funcs_freq():
@@ -210,6 +215,27 @@ def reference_csm(data, fs, block_size, window, overlap, precision):
 
 class Steer(SimpleNamespace):
     pass
+
+
+class PSFStandIn(SimpleNamespace):
+    """PointSpreadFunction without its cache: ``psf`` is the 'full' branch of ``calc_psf``
+    (acoular/fbeamform.py:1087-1089) cast to ``precision`` like its result array."""
+
+    freq = 1.0
+
+    def _psf_call(self, ind):
+        return psf_call(self, ind)
+
+    @property
+    def psf(self):
+        gs = self.steer.grid.size
+        ac = np.zeros((gs, gs), dtype=self.precision)
+        ac[:] = self._psf_call(np.arange(gs))
+        return ac
+
+
+NS['SteeringVector'] = Steer
+NS['PointSpreadFunction'] = PSFStandIn
 
 
 def reference_bf_result(csm, freqs, mpos, gpos, gshape, steer_type, r_diag, c=343.0, ref=None, r_diag_norm=0.0,
@@ -441,7 +467,72 @@ def golden_custom_flow():
     print('custom_flow_kat.npz written', len(out), 'arrays')
 
 
+def reference_damas_result(csm, freqs, r0, rm, steer_type, r_diag, n_iter, damp, psf_precision, ind, c=343.0):
+    """``BeamformerDamas._calc`` for bins ``ind`` with the reference's PSF and Gauss-Seidel kernels."""
+    G, M = rm.shape
+    steer = Steer(steer_type=steer_type, r0=r0, rm=rm, env=SimpleNamespace(c=c), grid=SimpleNamespace(size=G))
+    bf = SimpleNamespace(_f=freqs, r_diag=r_diag, r_diag_norm=0.0, n_iter=n_iter, damp=damp,
+                         psf_precision=psf_precision, calcmode='full', cached=False, steer=steer,
+                         freq_data=SimpleNamespace(num_channels=M, csm=csm))
+    bf.sig_loss_norm = lambda: sig_loss_norm(bf)
+    bf._beamformer_params = lambda: (steer_type, lambda f: (r0, rm, 2 * np.pi * f / c))
+    bf._ac = np.zeros((csm.shape[0], G))
+    bf._fr = np.zeros(csm.shape[0], dtype='int8')
+    damas_calc(bf, np.asarray(ind))
+    return bf._ac[ind]
+
+
+def golden_psf_damas():
+    """PointSpreadFunction._psf_call (full and selected sources, free field and uniform flow) and
+    BeamformerDamas._calc on the 8-mic case of small_kat.npz and two bins of the 64-mic band."""
+    small = np.load(OUT / 'small_kat.npz')
+    csm, freqs, mpos, gpos = small['csm0'], small['freqs0'], small['mpos'], small['gpos']
+    env = Env(c=343.0)
+    r0, rm = apparent_r(env, gpos), np.atleast_2d(apparent_r(env, gpos, mpos))
+    G = gpos.shape[1]
+    out = {'bins': np.array([12, 20, 28]), 'psf_bin': np.array(20), 'src': np.array([3, 40, 77])}
+    for st in STEERS:
+        key = st.replace(' ', '_')
+        p = PSFStandIn(steer=Steer(steer_type=st, r0=r0, rm=rm, env=env, grid=SimpleNamespace(size=G)),
+                       calcmode='full', precision='float64', cached=False)
+        p.freq = freqs[20]
+        out[f'psf_full_{key}'] = p.psf
+        p.precision = 'float32'
+        out[f'psf_full32_{key}'] = p.psf
+        out[f'psf_src_{key}'] = p._psf_call(out['src'])
+        for rd in (False, True):
+            out[f'damas_{key}_{int(rd)}'] = reference_damas_result(csm, freqs, r0, rm, st, rd, 10, 0.98, 'float64',
+                                                                   out['bins'])
+    out['damas_default_classic_0'] = reference_damas_result(csm, freqs, r0, rm, 'classic', False, 100, 1.0,
+                                                            'float64', out['bins'])
+    out['damas_f32_true_level_1'] = reference_damas_result(csm, freqs, r0, rm, 'true level', True, 10, 0.98,
+                                                           'float32', out['bins'])
+    fl = SimpleNamespace(ma=0.3, fdv=np.array((1.0, 0.5, 0.0)))
+    r0f, rmf = uflow_apparent_r(fl, gpos), np.atleast_2d(uflow_apparent_r(fl, gpos, mpos))
+    for st in STEERS:
+        p = PSFStandIn(steer=Steer(steer_type=st, r0=r0f, rm=rmf, env=env, grid=SimpleNamespace(size=G)),
+                       calcmode='block', precision='float64', cached=False)
+        p.freq = freqs[20]
+        out[f'psf_flow_{st.replace(" ", "_")}'] = p._psf_call(out['src'])
+    out['flow_r0'], out['flow_rm'] = r0f, rmf
+    from acoular_b200 import workloads
+    wl = workloads.three_sources_64()
+    data_ref = reference_time_data(wl.mics.pos, wl.locs, wl.seeds, wl.rms, wl.fs, wl.num_samples)
+    csm64, freqs64 = reference_csm(data_ref, wl.fs, 128, 'Hanning', '50%', 'complex128')
+    r064 = apparent_r(env, wl.grid.pos)
+    rm64 = np.atleast_2d(apparent_r(env, wl.grid.pos, wl.mics.pos))
+    out['c1_bins'] = np.array([18, 21])
+    for st, rd in (('classic', False), ('true level', True)):
+        out[f'c1_damas_{st.replace(" ", "_")}_{int(rd)}'] = reference_damas_result(
+            csm64, freqs64, r064, rm64, st, rd, 10, 0.98, 'float64', out['c1_bins'])
+    np.savez_compressed(OUT / 'psf_damas_kat.npz', **out)
+    print('psf_damas_kat.npz written', len(out), 'arrays')
+
+
 if __name__ == '__main__':
+    if os.environ.get('ACB_GOLDEN_ONLY') == 'psf_damas':
+        golden_psf_damas()
+        sys.exit(0)
     if os.environ.get('ACB_GOLDEN_ONLY') == 'eig':
         golden_eig()
         sys.exit(0)
@@ -454,3 +545,4 @@ if __name__ == '__main__':
     golden_config1()
     golden_eig()
     golden_custom_flow()
+    golden_psf_damas()

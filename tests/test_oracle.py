@@ -178,3 +178,48 @@ def test_host_uniform_flow_and_steer_vector_match_reference(golden):
             got = st.steer_vector(s['freqs0'][b])
             # float32 cos/sin of numpy vs the reference's numba (libm): a few float32 ulp
             assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_oracle_psf_and_damas_match_reference(golden):
+    """The oracle's calcPointSpreadFunction and Gauss-Seidel restatements against the reference's
+    PointSpreadFunction._psf_call and BeamformerDamas._calc (tests/golden/psf_damas_kat.npz)."""
+    g = golden('psf_damas_kat.npz')
+    s = golden('small_kat.npz')
+    csm, freqs, mpos, gpos = s['csm0'], s['freqs0'], s['mpos'], s['gpos']
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    G = gpos.shape[1]
+    k = 2 * np.pi * freqs[int(g['psf_bin'])] / 343.0
+    bins = g['bins']
+    for st in STEERS:
+        key = st.replace(' ', '_')
+        np.testing.assert_allclose(O.psf(st, r0, rm, k, np.arange(G)), g[f'psf_full_{key}'], rtol=1e-14,
+                                   atol=1e-14 * np.abs(g[f'psf_full_{key}']).max())
+        np.testing.assert_array_equal(O.psf(st, r0, rm, k, np.arange(G), 'float32'), g[f'psf_full32_{key}'])
+        np.testing.assert_array_equal(O.psf(st, r0, rm, k, g['src'], 'float32'), g[f'psf_src_{key}'])
+        ref = g[f'psf_flow_{key}']
+        np.testing.assert_allclose(O.psf(st, g['flow_r0'], g['flow_rm'], k, g['src']), ref, rtol=1e-14,
+                                   atol=1e-14 * np.abs(ref).max())
+        for rd in (False, True):
+            ref = g[f'damas_{key}_{int(rd)}']
+            got = O.beamformer_damas_calc(csm, freqs, bins, r0, rm, 343.0, st, rd, 10, 0.98)[bins]
+            np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-13 * np.abs(ref).max())
+    ref = g['damas_default_classic_0']
+    got = O.beamformer_damas_calc(csm, freqs, bins, r0, rm, 343.0, 'classic', False)[bins]
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-13 * np.abs(ref).max())
+    ref = g['damas_f32_true_level_1']
+    got = O.beamformer_damas_calc(csm, freqs, bins, r0, rm, 343.0, 'true level', True, 10, 0.98, 'float32')[bins]
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-13 * np.abs(ref).max())
+
+
+def test_oracle_gauss_seidel_known_answers():
+    """Hand-checkable Gauss-Seidel cases: identity PSF returns the (clipped) map after one sweep; a
+    2x2 system with relaxation follows the sweep formula row by row."""
+    y = np.array([1.0, -2.0, 3.0])
+    x = O.damas_gauss_seidel(np.eye(3), y, 1, 1.0, y.copy())
+    np.testing.assert_array_equal(x, [1.0, 0.0, 3.0])
+    A = np.array([[1.0, 0.5], [0.25, 1.0]])
+    y = np.array([2.0, 1.0])
+    x = O.damas_gauss_seidel(A, y, 1, 0.5, np.array([1.0, 1.0]))
+    x0 = 0.5 * 1.0 + 0.5 * (2.0 - 0.5 * 1.0)
+    x1 = 0.5 * 1.0 + 0.5 * (1.0 - 0.25 * x0)
+    np.testing.assert_allclose(x, [x0, x1], rtol=0, atol=1e-15)
