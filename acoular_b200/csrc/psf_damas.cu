@@ -110,15 +110,18 @@ __host__ __device__ inline int64_t damas_smem_doubles(int64_t G)
 // Blocked, pipelined Gauss-Seidel.  Rows are taken in blocks of 32; step t solves block k = t mod nblk.
 // Row i of block k needs sum_{h != i} A[i][h] x[h] with the latest x.  It is assembled from
 //   (a) the columns outside blocks k and k-1 (final values of this sweep left of k-1, values of the
-//       previous sweep right of k): computed one step AHEAD, while block k-1 is being solved, by every
-//       warp of the cluster except the solver, each CTA over its own column slice, and summed
+//       previous sweep right of k): computed one step AHEAD, while block k-1 is being solved, by the
+//       warps of the cluster (in the first CTA only those off the solver's SM sub-partition, which
+//       would otherwise take its issue slots), each CTA over its own column slice, and summed
 //       through distributed shared memory into the first CTA;
 //   (b) the columns of block k-1, whose new values are known at the start of step t (tile L);
-//   (c) the other columns of block k (tile D), old values, then updated as each row is solved.
+//   (c) the other columns of block k (tile D), old values for the rows after each row, new ones as
+//       they are solved.
 // The solving warp (warp 0 of the first CTA) takes (b), (c) and the rows of block k in order, lane i
-// owning row i: row j's new value is broadcast with a shuffle and every lane adds A[i][j] times its
-// change.  One cluster barrier per step publishes block k's values to every CTA and the partial sums
-// of block k+1 to the solver.  Sweeps continue across the wrap-around (block 0 follows block nblk-1).
+// owning row i: row j's new value is broadcast with a shuffle and every later lane subtracts its
+// contribution.  One cluster barrier per step publishes block k's values to every CTA and the
+// partial sums of block k+1 to the solver.  An L2 prefetch of block k+2's rows runs a step ahead
+// of their loads.  Sweeps continue across the wrap-around (block 0 follows block nblk-1).
 __global__ void __launch_bounds__(kDamasThreads) damas_kernel(const double *__restrict__ A, int64_t G,
                                                              const double *__restrict__ y, double *__restrict__ x,
                                                              int n_iter, double relax)
@@ -153,9 +156,10 @@ __global__ void __launch_bounds__(kDamasThreads) damas_kernel(const double *__re
     // CTA.  The same pass routes the columns of block k (tile D) and of block prev (tile L) to the
     // first CTA's tiles instead of summing them; a warp takes up to three rows at once so that all
     // of its loads of a step are in flight together.
-    auto prepare = [&](int k, int prev, int buf, int wfirst) {
-        const int w = warp - wfirst, nw = kDamasWarps - wfirst;
-        if (w < 0) return;
+    auto prepare = [&](int k, int prev, int buf, bool spare) {
+        if (spare && (warp & 3) == 0) return;
+        const int w = spare ? warp - (warp >> 2) - 1 : warp;
+        const int nw = spare ? kDamasWarps - kDamasWarps / 4 : kDamasWarps;
         const int64_t g0 = (int64_t)k * kDamasRows, p0 = (int64_t)prev * kDamasRows;
         const int nb = (int)min((int64_t)kDamasRows, G - g0);
         const int np = prev == k ? 0 : (int)min((int64_t)kDamasRows, G - p0);
@@ -164,31 +168,42 @@ __global__ void __launch_bounds__(kDamasThreads) damas_kernel(const double *__re
         double *lt0 = lT0 + buf * kDamasRows * kDamasPad;
         for (int rb = w; rb < nb; rb += 3 * nw) {
             const int r1 = rb + nw, r2 = rb + 2 * nw;
-            const bool v1 = r1 < nb, v2 = r2 < nb;
+            const bool v1ok = r1 < nb, v2ok = r2 < nb;
             const double *row0 = Ab + (g0 + rb) * G;
-            const double *row1 = Ab + (g0 + (v1 ? r1 : rb)) * G;
-            const double *row2 = Ab + (g0 + (v2 ? r2 : rb)) * G;
+            const double *row1 = Ab + (g0 + (v1ok ? r1 : rb)) * G;
+            const double *row2 = Ab + (g0 + (v2ok ? r2 : rb)) * G;
             double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-#pragma unroll 4
-            for (int64_t h = c0 + lane; h < c1; h += 32) {
-                const double a0 = __ldg(row0 + h);
-                const double a1 = v1 ? __ldg(row1 + h) : 0.0;
-                const double a2 = v2 ? __ldg(row2 + h) : 0.0;
-                if (h >= g0 && h < g0 + nb) {
-                    double *t = dt0 + (h - g0) * kDamasPad;
-                    t[rb] = a0;
-                    if (v1) t[r1] = a1;
-                    if (v2) t[r2] = a2;
-                } else if (h >= p0 && h < p0 + np) {
-                    double *t = lt0 + (h - p0) * kDamasPad;
-                    t[rb] = a0;
-                    if (v1) t[r1] = a1;
-                    if (v2) t[r2] = a2;
-                } else {
-                    const double xh = xs[h];
-                    acc0 = fma(a0, xh, acc0);
-                    acc1 = fma(a1, xh, acc1);
-                    acc2 = fma(a2, xh, acc2);
+            // chunks of 8 columns per lane: all loads of a chunk are issued before any use
+            for (int64_t base = c0 + lane; base < c1; base += 8 * 32) {
+                double v0[8], v1[8], v2[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int64_t h = base + u * 32;
+                    const bool in = h < c1;
+                    v0[u] = in ? __ldg(row0 + h) : 0.0;
+                    v1[u] = (in && v1ok) ? __ldg(row1 + h) : 0.0;
+                    v2[u] = (in && v2ok) ? __ldg(row2 + h) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int64_t h = base + u * 32;
+                    if (h >= c1) break;
+                    if (h >= g0 && h < g0 + nb) {
+                        double *t = dt0 + (h - g0) * kDamasPad;
+                        t[rb] = v0[u];
+                        if (v1ok) t[r1] = v1[u];
+                        if (v2ok) t[r2] = v2[u];
+                    } else if (h >= p0 && h < p0 + np) {
+                        double *t = lt0 + (h - p0) * kDamasPad;
+                        t[rb] = v0[u];
+                        if (v1ok) t[r1] = v1[u];
+                        if (v2ok) t[r2] = v2[u];
+                    } else {
+                        const double xh = xs[h];
+                        acc0 = fma(v0[u], xh, acc0);
+                        acc1 = fma(v1[u], xh, acc1);
+                        acc2 = fma(v2[u], xh, acc2);
+                    }
                 }
             }
 #pragma unroll
@@ -200,13 +215,17 @@ __global__ void __launch_bounds__(kDamasThreads) damas_kernel(const double *__re
             if (lane == 0) {
                 double *rp = red0 + buf * kDamasMaxCta * kDamasRows + crank * kDamasRows;
                 rp[rb] = acc0;
-                if (v1) rp[r1] = acc1;
-                if (v2) rp[r2] = acc2;
+                if (v1ok) rp[r1] = acc1;
+                if (v2ok) rp[r2] = acc2;
             }
         }
     };
 
     // Solve the rows of block k in order (warp 0 of the first CTA) and publish them to every CTA.
+    // Lane i keeps u_i = c_i - relax (s_i + sum_{l > i} A[i][l] x_l), c_i = (1 - relax) x_i + relax y_i
+    // and s_i the sum over the columns outside the block; row j's new value is max(0, u_j), and
+    // every lane then subtracts relax A[i][j] times it.  The chain per row is one FMA, one max and
+    // one shuffle; the sums feeding it use independent accumulators.
     auto solve = [&](int k, int prev, int buf) {
         const int64_t g0 = (int64_t)k * kDamasRows, p0 = (int64_t)prev * kDamasRows;
         const int nb = (int)min((int64_t)kDamasRows, G - g0);
@@ -214,44 +233,64 @@ __global__ void __launch_bounds__(kDamasThreads) damas_kernel(const double *__re
         const int i = lane;
         const double *dt = dT + buf * kDamasRows * kDamasPad;
         const double *lt = lT + buf * kDamasRows * kDamasPad;
-        double s = 0.0;
-        for (int c = 0; c < C; ++c) s += red[buf * kDamasMaxCta * kDamasRows + c * kDamasRows + i];
-        for (int j = 0; j < np; ++j) s = fma(lt[j * kDamasPad + i], xs[p0 + j], s);
-        double a[kDamasRows];
+        const double *rp = red + buf * kDamasMaxCta * kDamasRows + i;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-        for (int j = 0; j < kDamasRows; ++j) a[j] = dt[j * kDamasPad + i];
-        double xv = i < nb ? xs[g0 + i] : 0.0;
+        for (int c = 0; c < kDamasMaxCta; ++c)
+            if (c < C) acc[c & 3] += rp[c * kDamasRows];
+#pragma unroll
+        for (int j = 0; j < kDamasRows; ++j)
+            if (j < np) acc[j & 3] = fma(lt[j * kDamasPad + i], xs[p0 + j], acc[j & 3]);
+        double b[kDamasRows];
+#pragma unroll
+        for (int j = 0; j < kDamasRows; ++j) b[j] = dt[j * kDamasPad + i];
+        const double xold = i < nb ? xs[g0 + i] : 0.0;
 #pragma unroll
         for (int j = 0; j < kDamasRows; ++j) {
-            const double xj = __shfl_sync(0xffffffffu, xv, j);
-            if (j != i) s = fma(a[j], xj, s);
+            const double xj = __shfl_sync(0xffffffffu, xold, j);
+            if (j > i) acc[j & 3] = fma(b[j], xj, acc[j & 3]);
         }
-        const double yv = ys[buf * kDamasRows + i];
+        const double s = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        double u = (1.0 - relax) * xold + relax * (ys[buf * kDamasRows + i] - s);
+#pragma unroll
+        for (int j = 0; j < kDamasRows; ++j) b[j] = j < i ? relax * b[j] : 0.0;
+        double xv = 0.0;
 #pragma unroll
         for (int j = 0; j < kDamasRows; ++j) {
             if (j >= nb) break;
-            double d = 0.0;
-            if (i == j) {
-                double sol = (1.0 - relax) * xv + relax * (yv - s);
-                sol = sol > 0.0 ? sol : 0.0;
-                d = sol - xv;
-                xv = sol;
-            }
-            d = __shfl_sync(0xffffffffu, d, j);
-            if (i != j) s = fma(a[j], d, s);
+            const double xn = __shfl_sync(0xffffffffu, fmax(u, 0.0), j);
+            u = fma(-b[j], xn, u);
+            xv = i == j ? xn : xv;
         }
         if (i < nb)
             for (int r = 0; r < C; ++r) cluster.map_shared_rank(xs, r)[g0 + i] = xv;
     };
 
-    prepare(0, nblk - 1, 0, 0);
+    // L2 prefetch of this CTA's column slice of the rows of block k (read two steps later).
+    auto prefetch = [&](int k, bool spare) {
+        if (spare && (warp & 3) == 0) return;
+        const int w = spare ? warp - (warp >> 2) - 1 : warp;
+        const int64_t g0 = (int64_t)k * kDamasRows;
+        const int nb = (int)min((int64_t)kDamasRows, G - g0);
+        const int64_t nlines = (c1 - c0 + 15) / 16;     // 128-byte lines of 16 doubles
+        const int nthr = (spare ? kDamasWarps - kDamasWarps / 4 : kDamasWarps) * 32;
+        for (int64_t e = w * 32 + lane; e < nb * nlines; e += nthr) {
+            const double *ptr = Ab + (g0 + e / nlines) * G + c0 + (e % nlines) * 16;
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+        }
+    };
+
+    prepare(0, nblk - 1, 0, false);
+    if (nblk > 1) prefetch(1, false);
     cluster.sync();
     const int64_t steps = (int64_t)n_iter * nblk;
     for (int64_t t = 0; t < steps; ++t) {
         const int k = (int)(t % nblk);
         const int buf = (int)(t & 1);
+        const int kn = k + 1 == nblk ? 0 : k + 1;
         if (crank == 0 && warp == 0) solve(k, k == 0 ? nblk - 1 : k - 1, buf);
-        if (t + 1 < steps) prepare(k + 1 == nblk ? 0 : k + 1, k, buf ^ 1, crank == 0 ? 1 : 0);
+        if (t + 1 < steps) prepare(kn, k, buf ^ 1, crank == 0);
+        if (t + 2 < steps) prefetch(kn + 1 == nblk ? 0 : kn + 1, crank == 0);
         cluster.sync();
     }
     if (crank == 0)
