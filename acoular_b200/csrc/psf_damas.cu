@@ -39,8 +39,10 @@ __global__ void __launch_bounds__(256) psf_kernel(int M, int64_t G, int S, const
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t g = (int64_t)blockIdx.x * kPsfLanes + lane;
     const int sidx = blockIdx.y * kPsfWarps + warp;
+    int64_t s = sidx < S ? src[sidx] : 0;
+    const bool src_ok = s >= 0 && s < G;   // an index outside the grid yields NaN, never a stray read
+    s = src_ok ? s : 0;
     const bool valid = g < G && sidx < S;
-    const int64_t s = sidx < S ? src[sidx] : 0;
     const double *rs = rm + s * M;
     double re = 0.0, im = 0.0, help = 0.0;
     for (int m0 = 0; m0 < M; m0 += mc) {
@@ -91,6 +93,7 @@ __global__ void __launch_bounds__(256) psf_kernel(int M, int64_t G, int S, const
         const double nf = r0[s];
         res = a2 * (nf * nf) / Md / help;
     }
+    if (!src_ok) res = __longlong_as_double(0x7ff8000000000000ll);
     out[g * S + sidx] = round_f32 ? (double)__double2float_rn(res) : res;
 }
 

@@ -452,17 +452,21 @@ def map_tc_batch(instances, precision: str = 'bf16x3', error_word: torch.Tensor 
 # ------------------------------------------------------------------------------------------------
 def psf_f64(r0: torch.Tensor, rm: torch.Tensor, k: float, sources: torch.Tensor, steer_type: str,
             round_f32: bool = False, glibc_faithful: bool = True, out: torch.Tensor | None = None) -> torch.Tensor:
-    """PSF (G, S) of unit sources at the grid points ``sources`` (int64, (S,)) for one wave number,
+    """PSF (G, S) of unit sources at the grid points ``sources`` (int64, (S,), a numpy array, checked
+    here, or a device tensor, whose out-of-grid indices give NaN columns) for one wave number,
     distances r0 (G,), rm (G, M) float64 on the device (calcPointSpreadFunction)."""
     G, M = rm.shape
     if not (r0.is_contiguous() and rm.is_contiguous()) or r0.dtype != torch.float64 or rm.dtype != torch.float64:
         msg = 'r0 and rm must be contiguous float64 tensors'
         raise ValueError(msg)
+    if isinstance(sources, np.ndarray):
+        if sources.size and (sources.min() < 0 or sources.max() >= G):
+            msg = f'source indices must lie in [0, {G})'
+            raise IndexError(msg)
+        sources = torch.as_tensor(sources)
+    # indices of a device tensor are checked by the kernel: a column outside the grid is NaN
     sources = sources.to(device=rm.device, dtype=torch.int64).contiguous()
     S = sources.numel()
-    if S and (int(sources.min()) < 0 or int(sources.max()) >= G):
-        msg = f'source indices must lie in [0, {G})'
-        raise IndexError(msg)
     p = map_params(M, G, 1, steer_type, False, 1.0, False, None, glibc_faithful, rm.device)
     if out is None:
         out = torch.empty((G, S), dtype=torch.float64, device=rm.device)

@@ -155,7 +155,7 @@ def calcPointSpreadFunction(steerVecType, distGridToArrayCenter, distGridToAllMi
     r0 = torch.as_tensor(np.array(np.broadcast_to(distGridToArrayCenter, (rm.shape[0],)), dtype=np.float64),
                          device=dev)
     k = float(np.asarray(waveNumber).reshape(-1)[0])
-    src = torch.as_tensor(np.asarray(indSource, dtype=np.int64).reshape(-1), device=dev)
+    src = np.asarray(indSource, dtype=np.int64).reshape(-1)
     out = D.psf_f64(r0, rm, k, src, steerVecType, round_f32=np.dtype(dtype) == np.float32)
     return out.cpu().numpy().astype(dtype)
 

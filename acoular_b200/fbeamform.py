@@ -530,7 +530,7 @@ class PointSpreadFunction:
             r0, rm = _steer_distances_device(self.steer, dev, self)
             k = 2 * np.pi * self.freq / self.steer.env.c
             direct = out is not None and np.array_equal(ind, cols)
-            res = D.psf_f64(r0, rm, k, torch.as_tensor(cols, dtype=torch.int64, device=dev), self.steer.steer_type,
+            res = D.psf_f64(r0, rm, k, np.ascontiguousarray(cols, dtype=np.int64), self.steer.steer_type,
                             round_f32=self.precision == 'float32', glibc_faithful=self.glibc_faithful,
                             out=out if direct else None)
             if direct:

@@ -217,7 +217,8 @@ int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num
  *   out_psf[g][j] = PSF at grid point g of a unit source at grid point sources[j],
  *   for p->steer_type (1..4), r0 float64 [G], rm float64 [G][M] (SteeringVector.r0 / .rm),
  *   sources int64 [num_sources].  p->num_mics / num_grid / glibc_faithful / sincos_table are used.
- *   round_f32 != 0 rounds each value to float32 (PointSpreadFunction.precision 'float32'). */
+ *   round_f32 != 0 rounds each value to float32 (PointSpreadFunction.precision 'float32').
+ *   A source index outside [0, G) gives a column of NaN (the kernel reads nothing for it). */
 int acb_psf_f64(const acb_map_params *p, int num_sources, const int64_t *sources, double wavenumber,
                 const double *r0, const double *rm, int round_f32, double *out_psf, void *stream);
 

@@ -63,6 +63,19 @@ def test_psf_kernel_vs_reference(small, st):
         assert _rel(got, O.psf(st, r0, rm, kk, g['src'])) <= TOL
 
 
+def test_psf_source_index_checks(small):
+    """Host indices outside the grid raise; device indices outside it give NaN columns (no stray read)."""
+    from acoular_b200 import device as D
+    s, g, r0, rm = small
+    r0d, rmd = _dev(r0), _dev(rm)
+    with pytest.raises(IndexError):
+        D.psf_f64(r0d, rmd, 10.0, np.array([0, 81]), 'classic')
+    out = D.psf_f64(r0d, rmd, 10.0, torch.tensor([3, -1, 81, 40], device='cuda'), 'classic').cpu().numpy()
+    assert np.isnan(out[:, 1]).all() and np.isnan(out[:, 2]).all()
+    ref = O.psf('classic', r0, rm, 10.0, [3, 40])
+    assert _rel(out[:, [0, 3]], ref) <= TOL
+
+
 def test_psf_class_and_dropin(small):
     import acoular_b200 as ac
     from acoular_b200 import fastFuncs as F
