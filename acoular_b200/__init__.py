@@ -3,7 +3,8 @@
 Acoular-compatible classes (same names, attributes and semantics as the reference's):
 ``MicGeom``, ``RectGrid``, ``RectGrid3D``, ``ImportGrid``, ``Environment``, ``TimeSamples``,
 ``PowerSpectra``, ``PowerSpectraImport``, ``SteeringVector``, ``BeamformerBase``, ``BeamformerEig``,
-``BeamformerMusic``, ``PointSpreadFunction``, ``BeamformerDamas``, ``L_p``, ``integrate``; the kernel
+``BeamformerMusic``, ``BeamformerFunctional``, ``BeamformerOrth``, ``PointSpreadFunction``,
+``BeamformerDamas``, ``BeamformerCleansc``, ``L_p``, ``integrate``; the kernel
 entry points ``fastFuncs.calcCSM`` / ``beamformerFreq`` / ``calcPointSpreadFunction`` /
 ``damasSolverGaussSeidel``; and
 the device-level API in :mod:`acoular_b200.device`.  The compute runs in hand-written sm_100a
@@ -11,15 +12,17 @@ kernels (``lib/libacoular_b200.so``); there is no CPU fallback.
 """
 
 from .environments import Environment
-from .fbeamform import (BeamformerBase, BeamformerDamas, BeamformerEig, BeamformerMusic, L_p, LazyBfResult,
-                        PointSpreadFunction, SteeringVector, integrate)
+from .fbeamform import (BeamformerBase, BeamformerCleansc, BeamformerDamas, BeamformerEig, BeamformerFunctional,
+                        BeamformerMusic, BeamformerOrth, L_p, LazyBfResult, PointSpreadFunction, SteeringVector,
+                        integrate)
 from .grids import ImportGrid, RectGrid, RectGrid3D
 from .microphones import MicGeom
 from .sources import Mixer, PointSource, TimeSamples, WNoiseGenerator
 from .spectra import PowerSpectra, PowerSpectraImport
 
 __all__ = [
-    'BeamformerBase', 'BeamformerDamas', 'BeamformerEig', 'BeamformerMusic', 'Environment', 'ImportGrid', 'L_p', 'LazyBfResult', 'MicGeom', 'Mixer', 'PointSource', 'PointSpreadFunction',
+    'BeamformerBase', 'BeamformerCleansc', 'BeamformerDamas', 'BeamformerEig', 'BeamformerFunctional',
+    'BeamformerOrth', 'BeamformerMusic', 'Environment', 'ImportGrid', 'L_p', 'LazyBfResult', 'MicGeom', 'Mixer', 'PointSource', 'PointSpreadFunction',
     'PowerSpectra', 'PowerSpectraImport', 'RectGrid', 'RectGrid3D', 'SteeringVector', 'TimeSamples',
     'WNoiseGenerator', 'integrate',
 ]

@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "map_internal.h"
 
 namespace acb {
 
@@ -267,9 +268,11 @@ __global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const do
                                                       const double *__restrict__ r0_in, const double *__restrict__ rm,
                                                       int mc, double *__restrict__ out_map,
                                                       double *__restrict__ out_norm,
-                                                      const double2 *__restrict__ steer = nullptr)
+                                                      const double2 *__restrict__ steer = nullptr,
+                                                      const int *__restrict__ active = nullptr)
 {
     extern __shared__ double smem[];
+    if (active && !active[blockIdx.y]) return;   // a bin whose iteration has stopped (CLEAN-SC)
     const int M = a.M;
     double *mp = smem;                                                     // [3][M]
     double2 *hs = reinterpret_cast<double2 *>(smem + ((3 * M + 1) & ~1));  // [mc][32]
@@ -408,7 +411,8 @@ static int launch_plain(const MapArgs &a, int nbins, const void *csm, const doub
 template <bool USE_RM, bool CUSTOM = false>
 static int launch_eig(const MapArgs &a, int nbins, int E, const double *eigval, const void *eigvec, const double *k,
                       double k_scalar, const double *mpos, const double *gpos, const double *r0, const double *rm,
-                      double *out_map, double *out_norm, cudaStream_t s, const void *steer = nullptr)
+                      double *out_map, double *out_norm, cudaStream_t s, const void *steer = nullptr,
+                      const int *active = nullptr)
 {
     const int mc = a.M <= 256 ? a.M : 128;
     const size_t smem = (size_t)(((3 * a.M + 1) & ~1) * sizeof(double)) + (size_t)mc * kLanes * sizeof(double2);
@@ -417,8 +421,38 @@ static int launch_eig(const MapArgs &a, int nbins, int E, const double *eigval, 
     const dim3 grid((unsigned)((a.G + kLanes - 1) / kLanes), nbins);
     kern<<<grid, kLanes * kWarps, smem, s>>>(a, E, eigval, reinterpret_cast<const double2 *>(eigvec), k, k_scalar, mpos,
                                             gpos, r0, rm, mc, out_map, out_norm,
-                                            reinterpret_cast<const double2 *>(steer));
+                                            reinterpret_cast<const double2 *>(steer), active);
     return check_launch();
+}
+
+// Launchers for other translation units (map_internal.h).
+int map_plain_launch(const acb_map_params *p, int nbins, const void *csm, const double *k, const double *mpos,
+                     const double *gpos, const double *r0, const double *rm, double *out_map, cudaStream_t s)
+{
+    MapArgs a;
+    const int rc = make_args(p, a);
+    if (rc != ACB_OK) return rc;
+    if (rm) {
+        a.ref_mode = 0;   // r0 is given
+        return launch_plain<true>(a, nbins, csm, k, 0.0, nullptr, nullptr, r0, rm, out_map, nullptr, s);
+    }
+    return launch_plain<false>(a, nbins, csm, k, 0.0, mpos, gpos, nullptr, nullptr, out_map, nullptr, s);
+}
+
+int map_eig_launch(const acb_map_params *p, int nbins, int E, const double *eigval, const void *eigvec,
+                   const double *k, const double *mpos, const double *gpos, const double *r0, const double *rm,
+                   double *out_map, const int *active, cudaStream_t s)
+{
+    MapArgs a;
+    const int rc = make_args(p, a);
+    if (rc != ACB_OK) return rc;
+    if (rm) {
+        a.ref_mode = 0;
+        return launch_eig<true>(a, nbins, E, eigval, eigvec, k, 0.0, nullptr, nullptr, r0, rm, out_map, nullptr, s,
+                                nullptr, active);
+    }
+    return launch_eig<false>(a, nbins, E, eigval, eigvec, k, 0.0, mpos, gpos, nullptr, nullptr, out_map, nullptr, s,
+                             nullptr, active);
 }
 
 }  // namespace acb

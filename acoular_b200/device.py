@@ -497,3 +497,34 @@ def damas_gauss_seidel(psf: torch.Tensor, dirty_map: torch.Tensor, n_iter: int, 
                                                int(n_iter), float(relax), int(cta_per_bin), N.stream_handle()),
             'acb_damas_gauss_seidel_f64')
     return solution
+
+
+# ------------------------------------------------------------------------------------------------
+# CLEAN-SC
+# ------------------------------------------------------------------------------------------------
+def cleansc_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, steer_type: str, r_diag: bool, norm: float,
+                n_iter: int = 0, damp: float = 0.6, stopn: int = 3, mpos: torch.Tensor | None = None,
+                gpos: torch.Tensor | None = None, ref=None, r0: torch.Tensor | None = None,
+                rm: torch.Tensor | None = None, glibc_faithful: bool = True) -> torch.Tensor:
+    """CLEAN-SC for B bins: csm (B, M, M) complex128 (left unchanged: the iterations run on a copy),
+    wavenumbers (B,), geometry mpos (3, M) / gpos (3, G) or given distances r0 (G,), rm (G, M)
+    -> (B, G) float32, as BeamformerCleansc._calc's result rows."""
+    B, M, _ = csm.shape
+    if rm is None and (mpos is None or gpos is None):
+        msg = 'either mpos and gpos or r0 and rm are required'
+        raise ValueError(msg)
+    G = int(rm.shape[0]) if rm is not None else int(gpos.shape[1])
+    dev = csm.device
+    p = map_params(M, G, B, steer_type, r_diag, norm, False, None if rm is not None else ref, glibc_faithful, dev)
+    work = csm.to(torch.complex128).contiguous().clone()
+    nbytes = N.lib().acb_cleansc_workspace_bytes(M, G, B, int(n_iter))
+    if nbytes == 0:
+        msg = 'invalid CLEAN-SC sizes'
+        raise ValueError(msg)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = torch.empty((B, G), dtype=torch.float32, device=dev)
+    k = wavenumbers.to(device=dev, dtype=torch.float64).contiguous()
+    N.check(N.lib().acb_cleansc_f64(ctypes.byref(p), work.data_ptr(), k.data_ptr(), N.ptr(mpos), N.ptr(gpos),
+                                    N.ptr(r0), N.ptr(rm), int(n_iter), float(damp), int(stopn), out.data_ptr(),
+                                    ws.data_ptr(), nbytes, N.stream_handle()), 'acb_cleansc_f64')
+    return out

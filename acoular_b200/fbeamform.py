@@ -399,6 +399,38 @@ class BeamformerEig(BeamformerBase):
             out.clamp_(min=0.0)
         return out
 
+    def _eig_maps(self, f_rows, lam, vec, norm, r_diag, want_norm=False):
+        """Eigenvalue-form maps of B' rows (frequency f_rows[j], components lam (B', E), vec (B', M, E)),
+        routed as the reference's _beamformer_params: custom steering objects through their materialised
+        steer_vector, non-Euclidean environments through given distances, else the synthesising kernel.
+        Returns (maps (B', G), steering norms (B', G) or None)."""
+        dev = lam.device
+        G = self.steer.grid.size
+        out = torch.empty((len(f_rows), G), dtype=torch.float64, device=dev)
+        sn = torch.empty_like(out) if want_norm else None
+        if type(self.steer) is not SteeringVector:
+            # custom steering vectors (acoular/fastFuncs.py:476-559), one row at a time
+            for j, f in enumerate(f_rows):
+                h = torch.as_tensor(np.ascontiguousarray(self.steer.steer_vector(f), dtype=np.complex128), device=dev)
+                D.map_custom_f64(None, h[None], r_diag, norm, out=out[j:j + 1],
+                                 steer_norm=None if sn is None else sn[j:j + 1],
+                                 eig=(lam[j:j + 1].contiguous(), vec[j:j + 1].contiguous()))
+        elif type(self.steer.env) is not Environment:
+            # distances of a non-Euclidean environment, given to the kernel as they are
+            r0, rm = _steer_distances_device(self.steer, dev, self)
+            for j, f in enumerate(f_rows):
+                D.map_eig_rm_f64(lam[j:j + 1].contiguous(), vec[j:j + 1].contiguous(),
+                                 2 * np.pi * f / self.steer.env.c, r0, rm, self.steer.steer_type, r_diag,
+                                 norm, glibc_faithful=self.glibc_faithful, out=out[j],
+                                 steer_norm=None if sn is None else sn[j])
+        else:
+            mpos, gpos = self._geometry(dev)
+            k = torch.as_tensor(2 * np.pi * np.asarray(f_rows) / self.steer.env.c, dtype=torch.float64, device=dev)
+            D.map_eig_f64(lam.contiguous(), vec.contiguous(), k, mpos, gpos, self.steer.steer_type, r_diag, norm,
+                          ref=self.steer.ref, clip_negative=False, glibc_faithful=self.glibc_faithful, out=out,
+                          steer_norm=sn)
+        return out, sn
+
     def _calc(self, ind):
         ind = np.asarray(ind, dtype=np.int64)
         if ind.size == 0:
@@ -407,28 +439,7 @@ class BeamformerEig(BeamformerBase):
         dev = ev.device
         ind_d = torch.as_tensor(ind, device=dev)
         lam, vec, norm = self._eig_select(ev, evec, ind_d)
-        if type(self.steer) is not SteeringVector:
-            # custom steering vectors (acoular/fastFuncs.py:476-559), one bin at a time
-            out = torch.empty((ind.size, self.steer.grid.size), dtype=torch.float64, device=dev)
-            for j, i in enumerate(ind):
-                h = torch.as_tensor(np.ascontiguousarray(self.steer.steer_vector(self._f[i]), dtype=np.complex128),
-                                    device=dev)
-                D.map_custom_f64(None, h[None], self.r_diag, norm, out=out[j:j + 1],
-                                 eig=(lam[j:j + 1].contiguous(), vec[j:j + 1].contiguous()))
-        elif type(self.steer.env) is not Environment:
-            # distances of a non-Euclidean environment, given to the kernel as they are
-            r0 = torch.as_tensor(np.ascontiguousarray(np.atleast_1d(self.steer.r0), dtype=np.float64), device=dev)
-            rm = torch.as_tensor(np.ascontiguousarray(self.steer.rm, dtype=np.float64), device=dev)
-            out = torch.empty((ind.size, rm.shape[0]), dtype=torch.float64, device=dev)
-            for j, i in enumerate(ind):
-                D.map_eig_rm_f64(lam[j:j + 1].contiguous(), vec[j:j + 1].contiguous(),
-                                 2 * np.pi * self._f[i] / self.steer.env.c, r0, rm, self.steer.steer_type, self.r_diag,
-                                 norm, glibc_faithful=self.glibc_faithful, out=out[j])
-        else:
-            mpos, gpos = self._geometry(dev)
-            k = torch.as_tensor(2 * np.pi * self._f[ind] / self.steer.env.c, dtype=torch.float64, device=dev)
-            out = D.map_eig_f64(lam, vec, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm,
-                                ref=self.steer.ref, clip_negative=False, glibc_faithful=self.glibc_faithful)
+        out, _ = self._eig_maps(self._f[ind], lam, vec, norm, self.r_diag)
         out = self._post(out)
         if self.precision == 'float32':
             out = out.float()
@@ -639,6 +650,156 @@ class BeamformerDamas(BeamformerBase):
             if self.precision == 'float32':
                 x = x.float()
             self._ac[sub] = x.cpu().numpy()
+        self._fr[ind] = 1
+
+
+class BeamformerFunctional(BeamformerEig):
+    """Functional beamforming (acoular/fbeamform.py:688-786), full CSM only: the eigenvalues to the power
+    1/gamma, the eigenvalue-form map of all components divided by the steering norm, to the power gamma,
+    times the norm.  gamma = 1 is the conventional beamformer."""
+
+    def __init__(self, *args, gamma: float = 1.0, **kw):
+        kw.setdefault('r_diag', False)
+        kw.setdefault('r_diag_norm', 1.0)
+        super().__init__(*args, **kw)
+        if self.r_diag or self.r_diag_norm != 1.0:
+            msg = 'BeamformerFunctional is defined for the full CSM only (r_diag=False, r_diag_norm=1.0)'
+            raise ValueError(msg)
+        self.gamma = float(gamma)
+
+    @property
+    def digest(self) -> str:
+        return super().digest + f'|functional{self.gamma}'
+
+    def _calc(self, ind):
+        ind = np.asarray(ind, dtype=np.int64)
+        if ind.size == 0:
+            return
+        ev, evec = self.freq_data.evd_device
+        ind_d = torch.as_tensor(ind, device=ev.device)
+        lam = ev[ind_d].pow(1.0 / self.gamma).contiguous()   # negative round-off eigenvalues give NaN
+        out, sn = self._eig_maps(self._f[ind], lam, evec[ind_d].contiguous(), 1.0, False, want_norm=True)
+        out = out.div_(sn).pow_(self.gamma).mul_(sn).mul_(self.sig_loss_norm())
+        if self.precision == 'float32':
+            out = out.float()
+        self._ac[ind] = out.cpu().numpy()
+        self._fr[ind] = 1
+
+
+class BeamformerOrth(BeamformerEig):
+    """Orthogonal deconvolution (acoular/fbeamform.py:1333-1388): for each eigen-component in
+    ``eva_list`` (default the largest, ``[-1]``; ``n`` sets the n largest), its eigenvalue / num_mics
+    is placed at the argmax of that component's map.  All components of all bins are mapped in one
+    launch; the additions run in the list's order on the host."""
+
+    def __init__(self, *args, eva_list=None, n: int | None = None, **kw):
+        super().__init__(*args, **kw)
+        self._n = 1
+        self._eva_list = np.array([-1])
+        if n is not None:
+            self.n = n
+        if eva_list is not None:
+            self.eva_list = eva_list
+
+    @property
+    def n(self) -> int:
+        return getattr(self, '_n', 1)
+
+    @n.setter
+    def n(self, n):
+        self._n = int(n)
+        self._eva_list = np.arange(-1, -1 - self._n, -1)
+
+    @property
+    def eva_list(self) -> np.ndarray:
+        return self._eva_list
+
+    @eva_list.setter
+    def eva_list(self, v):
+        self._eva_list = np.atleast_1d(np.asarray(v, dtype=int))
+
+    @property
+    def digest(self) -> str:
+        return super().digest + f'|orth{self._eva_list.tobytes().hex()}'
+
+    def _calc(self, ind):
+        ind = np.asarray(ind, dtype=np.int64)
+        if ind.size == 0:
+            return
+        ev, evec = self.freq_data.evd_device
+        dev = ev.device
+        M = evec.shape[-1]
+        comps = np.asarray(self._eva_list, dtype=np.int64)
+        if comps.size and (comps.min() < -M or comps.max() >= M):
+            msg = f'eigenvalue indices must lie in [-{M}, {M})'
+            raise IndexError(msg)
+        comps = np.where(comps < 0, comps + M, comps)
+        L = comps.size
+        ind_d = torch.as_tensor(ind, device=dev)
+        comp_d = torch.as_tensor(comps, device=dev)
+        # rows (bin, component): unit eigenvalue, the component's eigenvector
+        vec = evec[ind_d][:, :, comp_d].permute(0, 2, 1).reshape(ind.size * L, M, 1).contiguous()
+        lam = torch.ones((ind.size * L, 1), dtype=torch.float64, device=dev)
+        f_rows = np.repeat(self._f[ind], L)
+        out, _ = self._eig_maps(f_rows, lam, vec, self.sig_loss_norm(), self.r_diag)
+        peaks = out.argmax(dim=1).view(ind.size, L).cpu().numpy()
+        ev_h = ev[ind_d].cpu().numpy()
+        nc = float(self.freq_data.num_channels)
+        res = np.zeros((ind.size, self.steer.grid.size))
+        for j in range(ind.size):
+            for li, c in enumerate(comps):
+                res[j, peaks[j, li]] += ev_h[j, c] / nc
+        self._ac[ind] = res
+        self._fr[ind] = 1
+
+
+class BeamformerCleansc(BeamformerBase):
+    """CLEAN-SC (acoular/fbeamform.py:1391-1490), on the GPU: ``n_iter`` iterations per bin (0 = up
+    to 2 num_mics, stopping when the peak exceeds the one ``stopn`` iterations before), damping
+    ``damp``.  All bins of a request iterate together on the device (``acb_cleansc_f64``); the
+    result rows are float32 values, as the reference's."""
+
+    def __init__(self, *args, n_iter: int = 0, damp: float = 0.6, stopn: int = 3, bin_budget_bytes: int = 1 << 30,
+                 **kw):
+        super().__init__(*args, **kw)
+        if not 0.01 <= float(damp) <= 1.0:
+            msg = f'damp must lie in [0.01, 1.0], got {damp!r}'
+            raise ValueError(msg)
+        self.n_iter = int(n_iter)
+        self.damp = float(damp)
+        self.stopn = int(stopn)
+        self.bin_budget_bytes = int(bin_budget_bytes)
+
+    @property
+    def digest(self) -> str:
+        return super().digest + f'|cleansc{self.n_iter}|{self.damp}|{self.stopn}'
+
+    def _calc(self, ind):
+        ind = np.asarray(ind, dtype=np.int64)
+        if ind.size == 0:
+            return
+        if type(self.steer) is not SteeringVector:
+            msg = 'BeamformerCleansc on the GPU needs a SteeringVector (custom steering objects are not built)'
+            raise NotImplementedError(msg)
+        csm_all = self.freq_data.csm_device
+        dev = csm_all.device
+        G = self.steer.grid.size
+        M = csm_all.shape[-1]
+        per_bin = 2 * G * 8 + 4 * G + 2 * M * M * 16
+        chunk = max(1, min(ind.size, self.bin_budget_bytes // per_bin))
+        kw = {}
+        if type(self.steer.env) is not Environment:
+            kw['r0'], kw['rm'] = _steer_distances_device(self.steer, dev, self)
+        else:
+            kw['mpos'], kw['gpos'] = self._geometry(dev)
+            kw['ref'] = self.steer.ref
+        for s0 in range(0, ind.size, chunk):
+            sub = ind[s0:s0 + chunk]
+            csm = csm_all.index_select(0, torch.as_tensor(sub, device=dev))
+            k = torch.as_tensor(2 * np.pi * self._f[sub] / self.steer.env.c, dtype=torch.float64, device=dev)
+            res = D.cleansc_f64(csm, k, self.steer.steer_type, self.r_diag, self.sig_loss_norm(), self.n_iter,
+                                self.damp, self.stopn, glibc_faithful=self.glibc_faithful, **kw)
+            self._ac[sub] = res.double().cpu().numpy()
         self._fr[ind] = 1
 
 

@@ -233,6 +233,24 @@ int acb_psf_f64(const acb_map_params *p, int num_sources, const int64_t *sources
 int acb_damas_gauss_seidel_f64(const double *psf, int64_t num_grid, int num_bins, const double *dirty_map,
                                double *solution, int n_iter, double relax, int cta_per_bin, void *stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * CLEAN-SC deconvolution
+ * ------------------------------------------------------------------------------------------- */
+
+/* Workspace (device bytes) of acb_cleansc_f64 for num_bins bins (n_iter 0 = 2 num_mics iterations). */
+size_t acb_cleansc_workspace_bytes(int num_mics, int64_t num_grid, int num_bins, int n_iter);
+
+/* BeamformerCleansc._calc (acoular/fbeamform.py:1424-1490) for p->num_bins bins at once:
+ *   csm complex128 [B][M][M], the working copy (updated in place: the cleaned CSM on return);
+ *   wavenumber [B]; geometry mpos [3][M] / gpos [3][G] with p->ref_*, or given distances r0 [G],
+ *   rm [G][M] (then mpos / gpos may be NULL); p->steer_type, r_diag, norm (sig_loss_norm) as for the
+ *   map, clip_negative ignored; n_iter 0 = 2 M; damp, stopn as the reference's traits;
+ *   result float32 [B][G] (damp * peak at each cleaned peak, as the reference's float32 result).
+ * Runs the iterations of all bins with no host synchronisation (2 launches per iteration). */
+int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber, const double *mpos,
+                    const double *gpos, const double *r0, const double *rm, int n_iter, double damp, int stopn,
+                    float *result, void *workspace, size_t workspace_bytes, void *stream);
+
 /* Size of the fixed device array behind acb_map_tc_noalloc (32 MiB per GPU, held until exit). */
 #define ACB_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 

@@ -75,6 +75,7 @@ def lib():
         L.orc_beamformer_custom.argtypes = [dp, dp, dp, i64, dp, ctypes.c_double, ctypes.c_int, i64, i64, dp, dp]
         L.orc_psf.argtypes = [dp, dp, ctypes.c_double, ctypes.POINTER(i64), i64, ctypes.c_int, i64, i64, dp]
         L.orc_damas_gauss_seidel_bins.argtypes = [dp, dp, i64, i64, i64, ctypes.c_double, dp]
+        L.orc_transfer.argtypes = [dp, dp, ctypes.c_double, i64, i64, dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -362,6 +363,107 @@ def beamformer_damas_calc(csm, freqs, ind, r0, rm, c: float, steer_type: str, r_
         x = y.copy()
         A = psf(steer_type, r0, rm, k, np.arange(G), psf_precision)
         out[i] = damas_gauss_seidel(A, y, n_iter, damp, x)
+    return out
+
+
+def transfer(r0, rm, k: float) -> np.ndarray:
+    """``calcTransfer`` (fastFuncs.py:857-897): (G, M) complex128 transfer functions."""
+    rm = np.ascontiguousarray(np.atleast_2d(rm), dtype=np.float64)
+    r0 = np.ascontiguousarray(np.broadcast_to(r0, (rm.shape[0],)), dtype=np.float64)
+    out = np.zeros(rm.shape, dtype=np.complex128)
+    lib().orc_transfer(_dp(r0), _dp(rm), float(k), rm.shape[0], rm.shape[1], _dp(out))
+    return out
+
+
+STEER_FUNCS = {   # SteeringVector._steer_funcs_freq (acoular/fbeamform.py:145-153)
+    'classic': lambda x: x / np.abs(x) / x.shape[-1],
+    'inverse': lambda x: 1.0 / x.conj() / x.shape[-1],
+    'true level': lambda x: x / np.einsum('ij,ij->i', x, x.conj())[:, np.newaxis],
+    'true location': lambda x: x / np.sqrt(np.einsum('ij,ij->i', x, x.conj()) * x.shape[-1])[:, np.newaxis],
+}
+
+
+def steer_vector(steer_type: str, r0, rm, k: float, ind=None) -> np.ndarray:
+    """``SteeringVector.steer_vector`` (fbeamform.py:233-258) through ``transfer`` (207-231)."""
+    if ind is not None:
+        r0, rm = np.atleast_1d(np.asarray(r0)[ind]), np.atleast_2d(np.asarray(rm)[ind])
+    return STEER_FUNCS[steer_type](transfer(r0, rm, k))
+
+
+def beamformer_functional_calc(eigvals, eigvecs, freqs, ind, r0, rm, c: float, steer_type: str, gamma: float,
+                               out=None):
+    """``BeamformerFunctional._calc`` (acoular/fbeamform.py:712-786), full CSM: eigenvalues to the power
+    1/gamma, the eigen map divided by the steering norm, to the power gamma, times the norm."""
+    G, M = rm.shape
+    if out is None:
+        out = np.zeros((eigvals.shape[0], G))
+    normfactor = sig_loss_norm(False, M, 1.0)
+    for i in ind:
+        with np.errstate(invalid='ignore'):
+            ev = np.array(eigvals[i], dtype='float64') ** (1.0 / gamma)
+        bo, sn = beamformer_freq_eig(steer_type, False, 1.0, r0, rm, 2 * np.pi * freqs[i] / c, ev,
+                                     np.array(eigvecs[i], dtype='complex128'))
+        bo /= sn
+        with np.errstate(invalid='ignore'):
+            out[i] = (bo ** gamma) * sn * normfactor
+    return out
+
+
+def beamformer_orth_calc(eigvals, eigvecs, freqs, ind, r0, rm, c: float, steer_type: str, r_diag: bool, eva_list,
+                         r_diag_norm: float = 0.0, out=None):
+    """``BeamformerOrth._calc`` (acoular/fbeamform.py:1366-1388): for each listed eigen-component, its
+    eigenvalue / num_mics is added at the argmax of that component's map."""
+    G, M = rm.shape
+    if out is None:
+        out = np.zeros((eigvals.shape[0], G))
+    normfactor = sig_loss_norm(r_diag, M, r_diag_norm)
+    for i in ind:
+        ev = np.array(eigvals[i], dtype='float64')
+        evec = np.array(eigvecs[i], dtype='complex128')
+        for n in eva_list:
+            bo = beamformer_freq_eig(steer_type, r_diag, normfactor, r0, rm, 2 * np.pi * freqs[i] / c, np.ones(1),
+                                     np.ascontiguousarray(evec[:, n].reshape((-1, 1))))[0]
+            out[i, bo.argmax()] += ev[n] / M
+    return out
+
+
+def beamformer_cleansc_calc(csm, freqs, ind, r0, rm, c: float, steer_type: str, r_diag: bool, n_iter: int = 0,
+                            damp: float = 0.6, stopn: int = 3, r_diag_norm: float = 0.0, out=None):
+    """``BeamformerCleansc._calc`` (acoular/fbeamform.py:1424-1490): per bin, CLEAN-SC iterations on the
+    conventional map; the result (float32, like the reference's) holds damp * peak at each peak."""
+    G, M = rm.shape
+    if out is None:
+        out = np.zeros((csm.shape[0], G))
+    normfactor = sig_loss_norm(r_diag, M, r_diag_norm)
+    result = np.zeros(G, 'f')
+    J = M * 2 if not n_iter else n_iter
+    powers = np.zeros(J, 'd')
+    for i in ind:
+        k = 2 * np.pi * freqs[i] / c
+        cs = np.array(csm[i], dtype='complex128', copy=True)
+        h = beamformer_freq(steer_type, r_diag, normfactor, r0, rm, k, cs)[0]
+        result *= 0.0
+        for j in range(J):
+            xi_max = h.argmax()
+            powers[j] = hmax = h[xi_max]
+            result[xi_max] += damp * hmax
+            if j > stopn and hmax > powers[j - stopn]:
+                break
+            wmax = steer_vector(steer_type, r0, rm, k, xi_max) * np.sqrt(normfactor)
+            wmax = wmax[0].conj()
+            hh = wmax.copy()
+            D1 = np.dot(cs.T - np.diag(np.diag(cs)), wmax) / hmax
+            ww = wmax.conj() * wmax
+            for _ in range(20):
+                H = hh.conj() * hh
+                hh = (D1 + H * wmax) / np.sqrt(1 + np.dot(ww, H))
+            hh = hh[:, np.newaxis]
+            csm1 = hmax * (hh * hh.conj().T)
+            h1 = beamformer_freq_eig(steer_type, r_diag, normfactor, r0, rm, k, np.array((hmax,)),
+                                     np.ascontiguousarray(hh.conj()))[0]
+            h -= damp * h1
+            cs -= damp * csm1.T
+        out[i] = result
     return out
 
 

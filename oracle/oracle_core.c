@@ -14,6 +14,7 @@
  *   orc_beamformer_custom      acoular/fastFuncs.py:414-559   (_freqBeamformer_SpecificSteerVec_*)
  *   orc_psf                    acoular/fastFuncs.py:563-801   (calcPointSpreadFunction)
  *   orc_damas_gauss_seidel     acoular/fastFuncs.py:804-855   (damasSolverGaussSeidel)
+ *   orc_transfer               acoular/fastFuncs.py:857-897   (calcTransfer)
  * Parity of this restatement is pinned against golden vectors produced by running the reference's
  * own code (tests/golden/make_golden.py) and against the reference's committed regression arrays
  * for Environment.apparent_r.
@@ -393,4 +394,19 @@ void orc_damas_gauss_seidel_bins(const double *A, const double *y, int64_t F, in
 {
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t f = 0; f < F; ++f) orc_damas_gauss_seidel(A + f * G * G, y + f * G, G, n_iter, relax, x + f * G);
+}
+
+/* calcTransfer / _transferCoreFunc (fastFuncs.py:857-897): out[g][m] = (cos a - i sin a) r0[g] / rm[g][m],
+ * a = fl32(k (rm[g][m] - r0[g])), cos/sin the C library's float32 ones.  out interleaved complex128. */
+void orc_transfer(const double *r0, const double *rm, double k, int64_t G, int64_t M, double *out)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < G; ++g) {
+        for (int64_t m = 0; m < M; ++m) {
+            const float arg = (float)(k * (rm[g * M + m] - r0[g]));
+            const double tr = (double)cosf(arg) * r0[g], ti = -(double)sinf(arg) * r0[g];
+            out[2 * (g * M + m)] = tr / rm[g * M + m];
+            out[2 * (g * M + m) + 1] = ti / rm[g * M + m];
+        }
+    }
 }

@@ -21,6 +21,8 @@ their decorators removed, bound to plain stand-in objects:
 * ``UniformFlowEnvironment.apparent_r``               acoular/environments.py:290-332
 * ``SteeringVector._steer_funcs_freq`` (as source text) acoular/fbeamform.py:145-153
 * ``PointSpreadFunction._psf_call``, ``BeamformerDamas._calc``   acoular/fbeamform.py:1096-1125, 1167-1208
+* ``BeamformerFunctional._calc``, ``BeamformerOrth._calc``, ``BeamformerCleansc._calc``,
+  ``SteeringVector.transfer`` / ``steer_vector``    acoular/fbeamform.py:712-786, 1366-1490, 207-258
 * ``WNoiseGenerator.signal``, ``SignalGenerator.usignal``, ``PointSource.result``,
   ``_fill_mic_signal_block``, ``Mixer.result``        (fixture time data)
 
@@ -112,6 +114,11 @@ NS['calcPointSpreadFunction'] = fastFuncs.calcPointSpreadFunction
 NS['damasSolverGaussSeidel'] = fastFuncs.damasSolverGaussSeidel
 psf_call = _extract('acoular/fbeamform.py', 'PointSpreadFunction._psf_call', NS, rename='psf_call')
 damas_calc = _extract('acoular/fbeamform.py', 'BeamformerDamas._calc', NS, rename='damas_calc')
+functional_calc = _extract('acoular/fbeamform.py', 'BeamformerFunctional._calc', NS, rename='functional_calc')
+orth_calc = _extract('acoular/fbeamform.py', 'BeamformerOrth._calc', NS, rename='orth_calc')
+cleansc_calc = _extract('acoular/fbeamform.py', 'BeamformerCleansc._calc', NS, rename='cleansc_calc')
+sv_transfer = _extract('acoular/fbeamform.py', 'SteeringVector.transfer', NS, rename='sv_transfer')
+sv_steer_vector = _extract('acoular/fbeamform.py', 'SteeringVector.steer_vector', NS, rename='sv_steer_vector')
 
 
 def _steer_funcs_freq():
@@ -529,7 +536,70 @@ def golden_psf_damas():
     print('psf_damas_kat.npz written', len(out), 'arrays')
 
 
+class SteerFull(SimpleNamespace):
+    """SteeringVector stand-in with the reference's transfer / steer_vector (fbeamform.py:207-258)."""
+
+    def transfer(self, f, ind=None):
+        return sv_transfer(self, f, ind)
+
+    def steer_vector(self, f, ind=None):
+        return sv_steer_vector(self, f, ind)
+
+
+def _eig_bf(csm, freqs, mpos, gpos, steer_type, r_diag, c=343.0, r_diag_norm=0.0, **kw):
+    env = Env(c=c)
+    r0, rm = apparent_r(env, gpos), np.atleast_2d(apparent_r(env, gpos, mpos))
+    M = mpos.shape[1]
+    eva, eve = get_evd(SimpleNamespace(precision='complex128', csm=csm))
+    steer = SteerFull(steer_type=steer_type, r0=r0, rm=rm, env=env, _steer_funcs_freq=_steer_funcs_freq(),
+                      grid=SimpleNamespace(size=gpos.shape[1]), mics=SimpleNamespace(num_mics=M))
+    bf = SimpleNamespace(_f=freqs, r_diag=r_diag, r_diag_norm=r_diag_norm, steer=steer,
+                         freq_data=SimpleNamespace(num_channels=M, csm=csm, eigvals=eva, eigvecs=eve), **kw)
+    bf.sig_loss_norm = lambda: sig_loss_norm(bf)
+    bf._beamformer_params = lambda: (steer_type, lambda f: (r0, rm, 2 * np.pi * f / c))
+    bf._ac = np.zeros((csm.shape[0], gpos.shape[1]))
+    bf._fr = np.zeros(csm.shape[0], dtype='int8')
+    return bf
+
+
+def golden_functional_orth_cleansc():
+    """BeamformerFunctional, BeamformerOrth and BeamformerCleansc (fbeamform.py:688-790, 1333-1492) on the
+    8-mic case of small_kat.npz and the 64-mic band, with the reference's own eigh, transfer and kernels."""
+    small = np.load(OUT / 'small_kat.npz')
+    cases = [('s', small['csm0'], small['freqs0'], small['mpos'], small['gpos'], np.array([12, 20, 28]))]
+    from acoular_b200 import workloads
+    wl = workloads.three_sources_64()
+    data_ref = reference_time_data(wl.mics.pos, wl.locs, wl.seeds, wl.rms, wl.fs, wl.num_samples)
+    csm64, freqs64 = reference_csm(data_ref, wl.fs, 128, 'Hanning', '50%', 'complex128')
+    cases.append(('c1', csm64, freqs64, wl.mics.pos, wl.grid.pos, np.array([18, 21])))
+    out = {}
+    for tag, csm, freqs, mpos, gpos, ind in cases:
+        out[f'{tag}_bins'] = ind
+        M = mpos.shape[1]
+        for st in STEERS:
+            key = st.replace(' ', '_')
+            for gamma in (1.0, 3.0):
+                bf = _eig_bf(csm, freqs, mpos, gpos, st, False, r_diag_norm=1.0, gamma=gamma)
+                functional_calc(bf, ind)
+                out[f'{tag}_functional_{key}_g{gamma:g}'] = bf._ac[ind]
+            for rd in (False, True):
+                for eva_list in ([-1], [-1, -2, -3], [M - 6, 2]):
+                    bf = _eig_bf(csm, freqs, mpos, gpos, st, rd, eva_list=np.array(eva_list))
+                    orth_calc(bf, ind)
+                    out[f'{tag}_orth_{key}_{int(rd)}_{"_".join(str(e) for e in eva_list)}'] = bf._ac[ind]
+            for rd in (False, True):
+                for n_iter, damp, stopn in ((0, 0.6, 3), (10, 0.9, 4)):
+                    bf = _eig_bf(csm, freqs, mpos, gpos, st, rd, n_iter=n_iter, damp=damp, stopn=stopn)
+                    cleansc_calc(bf, ind)
+                    out[f'{tag}_cleansc_{key}_{int(rd)}_{n_iter}_{damp:g}_{stopn}'] = bf._ac[ind]
+    np.savez_compressed(OUT / 'functional_orth_cleansc_kat.npz', **out)
+    print('functional_orth_cleansc_kat.npz written', len(out), 'arrays')
+
+
 if __name__ == '__main__':
+    if os.environ.get('ACB_GOLDEN_ONLY') == 'functional_orth_cleansc':
+        golden_functional_orth_cleansc()
+        sys.exit(0)
     if os.environ.get('ACB_GOLDEN_ONLY') == 'psf_damas':
         golden_psf_damas()
         sys.exit(0)
@@ -546,3 +616,4 @@ if __name__ == '__main__':
     golden_eig()
     golden_custom_flow()
     golden_psf_damas()
+    golden_functional_orth_cleansc()

@@ -223,3 +223,36 @@ def test_oracle_gauss_seidel_known_answers():
     x0 = 0.5 * 1.0 + 0.5 * (2.0 - 0.5 * 1.0)
     x1 = 0.5 * 1.0 + 0.5 * (1.0 - 0.25 * x0)
     np.testing.assert_allclose(x, [x0, x1], rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize('tag', ['s', 'c1'])
+def test_oracle_functional_orth_cleansc_match_reference(golden, tag):
+    """The oracle's BeamformerFunctional / BeamformerOrth / BeamformerCleansc restatements against the
+    reference's _calc methods (tests/golden/functional_orth_cleansc_kat.npz): bit for bit."""
+    from acoular_b200 import workloads
+    g = golden('functional_orth_cleansc_kat.npz')
+    if tag == 's':
+        s = golden('small_kat.npz')
+        csm, freqs, mpos, gpos = s['csm0'], s['freqs0'], s['mpos'], s['gpos']
+    else:
+        c1 = golden('config1_band.npz')
+        wl = workloads.three_sources_64()
+        freqs, mpos, gpos = c1['freqs'], wl.mics.pos, wl.grid.pos
+        csm = np.zeros((freqs.size, 64, 64), dtype=np.complex128)
+        csm[c1['band_bins']] = c1['csm_band']
+    ind = g[f'{tag}_bins']
+    M = mpos.shape[1]
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    eva, eve = np.linalg.eigh(csm)
+    for st in STEERS:
+        key = st.replace(' ', '_')
+        for gamma in (1.0, 3.0):
+            got = O.beamformer_functional_calc(eva, eve, freqs, ind, r0, rm, 343.0, st, gamma)[ind]
+            np.testing.assert_array_equal(got, g[f'{tag}_functional_{key}_g{gamma:g}'])
+        for rd in (False, True):
+            for el in ([-1], [-1, -2, -3], [M - 6, 2]):
+                got = O.beamformer_orth_calc(eva, eve, freqs, ind, r0, rm, 343.0, st, rd, el)[ind]
+                np.testing.assert_array_equal(got, g[f'{tag}_orth_{key}_{int(rd)}_{"_".join(str(e) for e in el)}'])
+            for n_iter, damp, stopn in ((0, 0.6, 3), (10, 0.9, 4)):
+                got = O.beamformer_cleansc_calc(csm, freqs, ind, r0, rm, 343.0, st, rd, n_iter, damp, stopn)[ind]
+                np.testing.assert_array_equal(got, g[f'{tag}_cleansc_{key}_{int(rd)}_{n_iter}_{damp:g}_{stopn}'])
