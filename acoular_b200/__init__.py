@@ -4,7 +4,8 @@ Acoular-compatible classes (same names, attributes and semantics as the referenc
 ``MicGeom``, ``RectGrid``, ``RectGrid3D``, ``ImportGrid``, ``Environment``, ``TimeSamples``,
 ``PowerSpectra``, ``PowerSpectraImport``, ``SteeringVector``, ``BeamformerBase``, ``BeamformerEig``,
 ``BeamformerMusic``, ``BeamformerFunctional``, ``BeamformerOrth``, ``PointSpreadFunction``,
-``BeamformerDamas``, ``BeamformerCleansc``, ``L_p``, ``integrate``; the kernel
+``BeamformerDamas``, ``BeamformerCleansc``, ``L_p``, ``integrate``; the block-wise generators ``RFFT``,
+``AutoPowerSpectra``, ``CrossPowerSpectra``; the kernel
 entry points ``fastFuncs.calcCSM`` / ``beamformerFreq`` / ``calcPointSpreadFunction`` /
 ``damasSolverGaussSeidel``; and
 the device-level API in :mod:`acoular_b200.device`.  The compute runs in hand-written sm_100a
@@ -15,12 +16,14 @@ from .environments import Environment
 from .fbeamform import (BeamformerBase, BeamformerCleansc, BeamformerDamas, BeamformerEig, BeamformerFunctional,
                         BeamformerMusic, BeamformerOrth, L_p, LazyBfResult, PointSpreadFunction, SteeringVector,
                         integrate)
+from .fprocess import RFFT, AutoPowerSpectra, CrossPowerSpectra
 from .grids import ImportGrid, RectGrid, RectGrid3D
 from .microphones import MicGeom
 from .sources import Mixer, PointSource, TimeSamples, WNoiseGenerator
 from .spectra import PowerSpectra, PowerSpectraImport
 
 __all__ = [
+    'RFFT', 'AutoPowerSpectra', 'CrossPowerSpectra',
     'BeamformerBase', 'BeamformerCleansc', 'BeamformerDamas', 'BeamformerEig', 'BeamformerFunctional',
     'BeamformerOrth', 'BeamformerMusic', 'Environment', 'ImportGrid', 'L_p', 'LazyBfResult', 'MicGeom', 'Mixer', 'PointSource', 'PointSpreadFunction',
     'PowerSpectra', 'PowerSpectraImport', 'RectGrid', 'RectGrid3D', 'SteeringVector', 'TimeSamples',

@@ -87,6 +87,11 @@ SIGNATURES = {
     'acb_beamformer_freq_f64': (_I, [ctypes.POINTER(MapParams), _VP, _D, _VP, _VP, _VP, _VP, _VP]),
     'acb_map_eig_f64': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     'acb_map_rm_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    'acb_spectra_workspace_bytes': (ctypes.c_size_t, [_I, _I, ctypes.c_int64]),
+    'acb_spectra': (_I, [_VP, _I, ctypes.c_int64, _I, _I, _I, ctypes.c_int64, ctypes.c_int64, _VP, _VP, _I, _D, _I,
+                         _VP, _VP, ctypes.c_size_t, _VP]),
+    'acb_auto_spectra': (_I, [_VP, ctypes.c_int64, _I, _I, _D, _VP, _VP]),
+    'acb_cross_spectra': (_I, [_VP, ctypes.c_int64, _I, _I, _I, _D, _VP, _VP]),
     'acb_cleansc_workspace_bytes': (ctypes.c_size_t, [_I, ctypes.c_int64, _I, _I]),
     'acb_cleansc_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _I, _D, _I, _VP, _VP,
                              ctypes.c_size_t, _VP]),

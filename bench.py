@@ -49,7 +49,8 @@ def parse():
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--bins', type=int, default=0, help='limit the number of map bins (profiling only)')
     ap.add_argument('--workload', default='precision256',
-                    choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig', 'damas'])
+                    choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig', 'damas',
+                             'cleansc'])
     ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     return ap.parse_args()
@@ -649,8 +650,91 @@ def run_damas(args):
           clocks=clk.summary(), dtype='f64')
 
 
+def run_cleansc(args):
+    """CLEAN-SC (BeamformerCleansc defaults: true level, r_diag, n_iter 0 = up to 2 M = 128 iterations,
+    damp 0.6, stopn 3) on the 64-mic, 41x41 workload's 8 kHz third-octave band (5 bins): per step the
+    conventional maps and every iteration of all 5 bins.  The CSM is computed once; the oracle checks 1 bin."""
+    import time
+
+    import torch
+
+    import acoular_b200 as ac
+    from acoular_b200 import device as D
+    from acoular_b200 import workloads
+    from oracle import oracle as O
+    dev = torch.device('cuda', 0)
+    wl = workloads.three_sources_64()
+    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
+    F = N // 2 + 1
+    x = workloads.monopole_time_data_torch(wl, device=dev)
+    csm = D.calc_csm(x, N, 'Hanning', '50%', 'complex128')
+    del x
+    freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[:F])
+    bins = np.arange(int(np.searchsorted(freqs, 8000.0 * 2.0 ** (-0.5 / 3))),
+                     int(np.searchsorted(freqs, 8000.0 * 2.0 ** (0.5 / 3))))
+    B = bins.size
+    st, n_iter, damp, stopn = 'true level', 0, 0.6, 3
+    norm = M / (M - 1.0)
+    mpos, gpos = torch.as_tensor(wl.mics.pos, device=dev), torch.as_tensor(wl.grid.pos, device=dev)
+    csm_b = csm[torch.as_tensor(bins, device=dev)].contiguous()
+    kb = torch.as_tensor(2 * np.pi * freqs[bins] / wl.c, device=dev)
+
+    def step():
+        return D.cleansc_f64(csm_b, kb, st, True, norm, n_iter, damp, stopn, mpos=mpos, gpos=gpos)
+
+    for _ in range(max(3, args.warmup)):
+        res = step()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        t0.record()
+        for _ in range(args.steps):
+            res = step()
+        t1.record()
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / args.steps
+    steer = ac.SteeringVector(grid=wl.grid, mics=wl.mics, steer_type=st)
+    r0_h, rm_h = np.ascontiguousarray(steer.r0), np.ascontiguousarray(steer.rm)
+    b0 = int(bins[B // 2])
+    c_h = csm[b0:b0 + 1].cpu().numpy()
+    tc = time.perf_counter()
+    ref = O.beamformer_cleansc_calc(c_h, freqs[b0:b0 + 1], [0], r0_h, rm_h, wl.c, st, True, n_iter, damp, stopn)[0]
+    cpu_s = time.perf_counter() - tc
+    got = res[B // 2].double().cpu().numpy()
+    err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    same_peaks = bool(np.array_equal(got != 0, ref != 0))
+    c_host = csm.cpu().numpy()
+    e2e_ms = []
+    for it in range(max(2, min(args.steps, 5)) + 1):
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        ps = ac.PowerSpectraImport(csm=c_host, frequencies=freqs)
+        bf = ac.BeamformerCleansc(freq_data=ps, steer=steer, r_diag=True, n_iter=n_iter, damp=damp, stopn=stopn)
+        band = np.asarray(bf.result[int(bins[0]):int(bins[-1]) + 1])
+        if it:
+            e2e_ms.append((time.perf_counter() - ta) * 1e3)
+    e2e_err = float(np.abs(band[B // 2] - ref).max() / np.abs(ref).max())
+    J = 2 * M
+    _line('CLEAN-SC bins/s (BeamformerCleansc, 64 mics, 41x41 grid, 8 kHz third-octave band)', B / (ms / 1e3),
+          'bins/s', ms, args,
+          {'workload': 'cleansc_' + wl.name, 'mics': M, 'grid_points': G, 'bins': B, 'n_iter': 'auto (<= 128)',
+           'damp': damp, 'stopn': stopn, 'steer_type': st, 'r_diag': True, 'csm': 'complex128, computed once'},
+          accuracy={'vs': 'oracle (the reference CLEAN-SC restated)', 'bin': b0, 'max_rel_err': err,
+                    'same_peaks': same_peaks, 'e2e_max_rel_err': e2e_err},
+          e2e={'value': B / (float(np.median(e2e_ms)) / 1e3), 'unit': 'bins/s', 'ms': float(np.median(e2e_ms)),
+               'h2d_bytes_per_step': int(c_host.nbytes + r0_h.nbytes + rm_h.nbytes),
+               'd2h_bytes_per_step': int(B * G * 4)},
+          cpu_baseline={'value': 1.0 / cpu_s, 'unit': 'bins/s', 'cores': O.num_threads(), 'kind': 'port',
+                        'sample': f'1 bin (bin {b0}): map + CLEAN-SC iterations'},
+          gpu_launches=f'{2 + 2 * J - 1} per step (init, map_plain_kernel, {J} cleansc_step_kernel, '
+                       f'{J - 1} map_eig_kernel; stopped bins return at once)',
+          clocks=clk.summary(), dtype='f64')
+
+
 def main():
     args = parse()
+    if args.workload == 'cleansc':
+        return run_cleansc(args)
     from acoular_b200 import workloads
     if args.workload == 'eig':
         return run_eig(args)

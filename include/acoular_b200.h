@@ -234,6 +234,34 @@ int acb_damas_gauss_seidel_f64(const double *psf, int64_t num_grid, int num_bins
                                double *solution, int n_iter, double relax, int cta_per_bin, void *stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Block-wise spectra generators (acoular/fprocess.py)
+ * ------------------------------------------------------------------------------------------- */
+
+/* Workspace (device bytes) of acb_spectra for num_windows windows. */
+size_t acb_spectra_workspace_bytes(int num_mics, int block_size, int64_t num_windows);
+
+/* RFFT.result (acoular/fprocess.py:35-181) for windows [first_window, first_window + num_windows) of the
+ * samples (the windows of BaseSpectra._get_source_data, acoular/spectra.py:171-184):
+ *   out[w][f][m] = rfft(samples[w*hop : w*hop + block_size, m] * window)[f], f = 0 .. block_size/2,
+ *   rounded to `precision` (ACB_C128 / ACB_C64); bins 1 .. block_size/2 - 1 doubled when double_inner
+ *   (scaling 'energy' / 'amplitude'), then times `scale`, both in the output precision.
+ * block_size: power of two, 16 .. 16384 (other even sizes: ACB_ERR_SHAPE / ACB_ERR_UNSUPPORTED). */
+int acb_spectra(const void *samples, int sample_dtype, int64_t num_samples, int num_mics, int block_size, int hop,
+                int64_t first_window, int64_t num_windows, const double *window, const void *twiddle, int precision,
+                double scale, int double_inner, void *out, void *workspace, size_t workspace_bytes, void *stream);
+
+/* AutoPowerSpectra.result (acoular/fprocess.py:286-366): out[i] = (X[i] conj(X[i])).real * scale for
+ * num_values spectra values X in `precision`, computed in that precision, stored as float64 or float32. */
+int acb_auto_spectra(const void *spectra, int64_t num_values, int precision, int out_float32, double scale, void *out,
+                     void *stream);
+
+/* CrossPowerSpectra.result (acoular/fprocess.py:369-467), calc_mode 'full': per window w and bin f,
+ *   out[w][f][r][c] = scale * (r <= c ? U[r][c] : conj(U[c][r])),  U[r][c] = conj(X[c]) X[r] (calcCSM),
+ * X = spectra[w][f][:] in `precision`; out in `precision`. */
+int acb_cross_spectra(const void *spectra, int64_t num_windows, int num_freqs, int num_mics, int precision,
+                      double scale, void *out, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
  * CLEAN-SC deconvolution
  * ------------------------------------------------------------------------------------------- */
 

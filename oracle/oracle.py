@@ -467,6 +467,77 @@ def beamformer_cleansc_calc(csm, freqs, ind, r0, rm, c: float, steer_type: str, 
     return out
 
 
+# ----------------------------------------------------------------------------------------------
+# Block-wise spectra generators (acoular/fprocess.py)
+# ----------------------------------------------------------------------------------------------
+def rfft_blocks(samples: np.ndarray, block_size: int, window: str, overlap: str, precision: str, scaling: str,
+                num: int):
+    """``RFFT.result`` (acoular/fprocess.py:128-181): blocks (n, num_freqs * M) of scaled spectra."""
+    wind = WINDOWS[window](block_size)
+    if scaling in ('none', 'energy'):
+        svalue = 1 / np.sqrt(np.dot(wind, wind) / block_size)
+    else:
+        svalue = 1 / wind.sum()
+    wind = wind[:, np.newaxis]
+    M = samples.shape[1]
+    nf = block_size // 2 + 1
+    fftdata = np.zeros((num, M * nf), dtype=precision)
+    j = 0
+    for i, data in enumerate(source_windows(samples, block_size, OVERLAPS[overlap])):
+        j = i % num
+        d = sfft.rfft(data * wind, n=block_size, axis=0).astype(precision)
+        if scaling in ('amplitude', 'energy'):
+            d[1:-1] *= 2.0
+        d *= svalue
+        fftdata[j] = d.reshape(-1)
+        if j == num - 1:
+            yield fftdata.copy()
+    if j < num - 1:
+        yield fftdata[: j + 1].copy()
+
+
+def power_scale(block_size: int, sample_freq: float, scaling: str, single_sided: bool) -> float:
+    """``AutoPowerSpectra._get_scaling_value`` (acoular/fprocess.py:323-329)."""
+    scale = 1 / block_size**2
+    if single_sided:
+        scale *= 2
+    if scaling == 'psd':
+        scale *= block_size * sample_freq
+    return scale
+
+
+def auto_power_blocks(blocks, scale: float, precision: str):
+    """``AutoPowerSpectra.result`` (acoular/fprocess.py:331-366)."""
+    for temp in blocks:
+        yield ((temp * temp.conjugate()).real * scale).astype(precision)
+
+
+def cross_power_blocks(blocks, num_freqs: int, num_mics: int, scale: float, precision: str):
+    """``CrossPowerSpectra.result`` (acoular/fprocess.py:425-467), calc_mode 'full': the per-snapshot
+    CSM from the calcCSM restatement, its conjugate lower triangle (diagonal once), times scale."""
+    csm_upper = np.zeros((num_freqs, num_mics, num_mics), dtype=precision)
+    for data in blocks:
+        flat = np.zeros((data.shape[0], num_freqs * num_mics * num_mics), dtype=precision)
+        for i in range(data.shape[0]):
+            spec = np.ascontiguousarray(data[i].astype(precision).reshape(num_freqs, num_mics))
+            calc_csm_upper(csm_upper, spec)
+            lower = csm_upper.conj().transpose(0, 2, 1)
+            for f in range(num_freqs):
+                np.fill_diagonal(lower[f], 0)
+            flat[i] = (lower + csm_upper).reshape(-1)
+            csm_upper[...] = 0
+        yield flat * scale
+
+
+def calc_csm_upper(csm: np.ndarray, spec: np.ndarray) -> None:
+    """``calcCSM`` (fastFuncs.py:19-58) for one snapshot, in the array's precision (C restatement)."""
+    F, M = spec.shape
+    if csm.dtype == np.complex64:
+        lib().orc_calc_csm_c64(_fp(csm), _fp(spec), F, M)
+    else:
+        lib().orc_calc_csm_c128(_dp(csm), _dp(spec), F, M)
+
+
 def sig_loss_norm(r_diag: bool, num_mics: int, r_diag_norm: float = 0.0) -> float:
     """acoular/fbeamform.py:438-451."""
     if not r_diag:

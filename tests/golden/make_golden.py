@@ -23,6 +23,8 @@ their decorators removed, bound to plain stand-in objects:
 * ``PointSpreadFunction._psf_call``, ``BeamformerDamas._calc``   acoular/fbeamform.py:1096-1125, 1167-1208
 * ``BeamformerFunctional._calc``, ``BeamformerOrth._calc``, ``BeamformerCleansc._calc``,
   ``SteeringVector.transfer`` / ``steer_vector``    acoular/fbeamform.py:712-786, 1366-1490, 207-258
+* ``RFFT.result`` / ``_scale``, ``AutoPowerSpectra._get_scaling_value`` / ``result``,
+  ``CrossPowerSpectra.result``                        acoular/fprocess.py:35-181, 286-467
 * ``WNoiseGenerator.signal``, ``SignalGenerator.usignal``, ``PointSource.result``,
   ``_fill_mic_signal_block``, ``Mixer.result``        (fixture time data)
 
@@ -119,6 +121,11 @@ orth_calc = _extract('acoular/fbeamform.py', 'BeamformerOrth._calc', NS, rename=
 cleansc_calc = _extract('acoular/fbeamform.py', 'BeamformerCleansc._calc', NS, rename='cleansc_calc')
 sv_transfer = _extract('acoular/fbeamform.py', 'SteeringVector.transfer', NS, rename='sv_transfer')
 sv_steer_vector = _extract('acoular/fbeamform.py', 'SteeringVector.steer_vector', NS, rename='sv_steer_vector')
+rfft_result = _extract('acoular/fprocess.py', 'RFFT.result', NS, rename='rfft_result')
+rfft_scale = _extract('acoular/fprocess.py', 'RFFT._scale', NS, rename='rfft_scale')
+aps_scaling = _extract('acoular/fprocess.py', 'AutoPowerSpectra._get_scaling_value', NS, rename='aps_scaling')
+aps_result = _extract('acoular/fprocess.py', 'AutoPowerSpectra.result', NS, rename='aps_result')
+cps_result = _extract('acoular/fprocess.py', 'CrossPowerSpectra.result', NS, rename='cps_result')
 
 
 def _steer_funcs_freq():
@@ -596,7 +603,65 @@ def golden_functional_orth_cleansc():
     print('functional_orth_cleansc_kat.npz written', len(out), 'arrays')
 
 
+class RfftStandIn(SimpleNamespace):
+    """RFFT (fprocess.py:35-181) over a Samples source, with the reference's generator and scaling."""
+
+    def _get_source_data(self):
+        return get_source_data(self)
+
+    def _scale(self, data, scaling_value):
+        return rfft_scale(self, data, scaling_value)
+
+    def result(self, num=1):
+        return rfft_result(self, num)
+
+
+class ApsStandIn(SimpleNamespace):
+    def _get_scaling_value(self):
+        return aps_scaling(self)
+
+    def result(self, num=1):
+        return (cps_result if hasattr(self, 'calc_mode') else aps_result)(self, num)
+
+
+def golden_fprocess():
+    """RFFT / AutoPowerSpectra / CrossPowerSpectra generators (fprocess.py:35-467) on the 8-mic time data
+    of small_kat.npz: every scaling, both precisions, overlaps and block counts that leave a short last
+    block."""
+    small = np.load(OUT / 'small_kat.npz')
+    data, fs = small['data'], float(small['fs'])
+    out = {}
+    cases = [(128, 'Hanning', '50%', 'complex128', 'none', 7), (256, 'Rectangular', 'None', 'complex128', 'energy', 3),
+             (64, 'Blackman', '75%', 'complex64', 'amplitude', 16), (128, 'Hamming', 'None', 'complex64', 'none', 4)]
+    for ci, (bs, win, ov, prec, scaling, num) in enumerate(cases):
+        src = Samples(data=data, num_samples=data.shape[0], num_channels=data.shape[1], sample_freq=fs)
+        rf = RfftStandIn(source=src, block_size=bs, window_=WINDOWS[win], overlap_=OVERLAPS[ov], precision=prec,
+                         scaling=scaling, workers=None, num_channels=data.shape[1], num_freqs=bs // 2 + 1,
+                         sample_freq=fs)
+        blocks = [b.copy() for b in rf.result(num)]
+        out[f'rfft{ci}_case'] = np.array([str(bs), win, ov, prec, scaling, str(num)])
+        out[f'rfft{ci}_sizes'] = np.array([b.shape[0] for b in blocks])
+        out[f'rfft{ci}'] = np.concatenate(blocks)
+        for ai, (sc, ss, ap) in enumerate([('power', True, 'float64'), ('psd', False, 'float32')]):
+            aps = ApsStandIn(source=rf, scaling=sc, single_sided=ss, precision=ap, block_size=bs, num_freqs=bs // 2 + 1,
+                             num_channels=data.shape[1])
+            out[f'aps{ci}_{ai}'] = np.concatenate([b.copy() for b in aps.result(num)])
+        cprec = 'complex64' if prec == 'complex64' else 'complex128'
+        cps = ApsStandIn(source=rf, scaling='psd' if ci % 2 else 'power', single_sided=True, precision=cprec,
+                         block_size=bs, num_freqs=bs // 2 + 1, num_channels=data.shape[1] ** 2, calc_mode='full')
+        blocks = [b.copy() for b in cps.result(num)]
+        allc = np.concatenate(blocks)
+        out[f'cps{ci}'] = allc[:2 * num]                      # the first two blocks in full
+        out[f'cps{ci}_sum'] = allc.astype(np.complex128).sum(axis=0)   # and a sum over every snapshot
+        out[f'cps{ci}_sizes'] = np.array([b.shape[0] for b in blocks])
+    np.savez_compressed(OUT / 'fprocess_kat.npz', **out)
+    print('fprocess_kat.npz written', len(out), 'arrays')
+
+
 if __name__ == '__main__':
+    if os.environ.get('ACB_GOLDEN_ONLY') == 'fprocess':
+        golden_fprocess()
+        sys.exit(0)
     if os.environ.get('ACB_GOLDEN_ONLY') == 'functional_orth_cleansc':
         golden_functional_orth_cleansc()
         sys.exit(0)
@@ -617,3 +682,4 @@ if __name__ == '__main__':
     golden_custom_flow()
     golden_psf_damas()
     golden_functional_orth_cleansc()
+    golden_fprocess()

@@ -256,3 +256,25 @@ def test_oracle_functional_orth_cleansc_match_reference(golden, tag):
             for n_iter, damp, stopn in ((0, 0.6, 3), (10, 0.9, 4)):
                 got = O.beamformer_cleansc_calc(csm, freqs, ind, r0, rm, 343.0, st, rd, n_iter, damp, stopn)[ind]
                 np.testing.assert_array_equal(got, g[f'{tag}_cleansc_{key}_{int(rd)}_{n_iter}_{damp:g}_{stopn}'])
+
+
+def test_oracle_fprocess_generators_match_reference(golden):
+    """The oracle's RFFT / AutoPowerSpectra / CrossPowerSpectra restatements against the reference's
+    generators (tests/golden/fprocess_kat.npz): block sizes and values bit for bit."""
+    g = golden('fprocess_kat.npz')
+    s = golden('small_kat.npz')
+    data, fs = s['data'], float(s['fs'])
+    for ci in range(4):
+        bs, win, ov, prec, scaling, num = g[f'rfft{ci}_case']
+        bs, num = int(bs), int(num)
+        blocks = list(O.rfft_blocks(data, bs, win, ov, prec, scaling, num))
+        assert [b.shape[0] for b in blocks] == list(g[f'rfft{ci}_sizes'])
+        np.testing.assert_array_equal(np.concatenate(blocks), g[f'rfft{ci}'])
+        for ai, (sc, ss, ap) in enumerate([('power', True, 'float64'), ('psd', False, 'float32')]):
+            a = np.concatenate(list(O.auto_power_blocks(blocks, O.power_scale(bs, fs, sc, ss), ap)))
+            np.testing.assert_array_equal(a, g[f'aps{ci}_{ai}'])
+        cprec = 'complex64' if prec == 'complex64' else 'complex128'
+        scale = O.power_scale(bs, fs, 'psd' if ci % 2 else 'power', True)
+        c = np.concatenate(list(O.cross_power_blocks(blocks, bs // 2 + 1, data.shape[1], scale, cprec)))
+        np.testing.assert_array_equal(c[:2 * num], g[f'cps{ci}'])
+        np.testing.assert_array_equal(c.astype(np.complex128).sum(axis=0), g[f'cps{ci}_sum'])
