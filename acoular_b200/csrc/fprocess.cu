@@ -67,34 +67,47 @@ __global__ void auto_spectra_kernel(const void *__restrict__ in, int64_t n, doub
 }
 
 // out[w][f][r][c] = scale * (r <= c ? U[r][c] : conj(U[c][r])), U[r][c] = conj(X[c]) X[r] in calcCSM's FMA form.
+// One CTA per (window, bin): the M spectra values sit in shared memory, the M x M outputs are written
+// in order (coalesced), indices in 32-bit arithmetic.
 template <bool C64>
-__global__ void cross_spectra_kernel(const void *__restrict__ in, int64_t nw, int F, int M, double scale,
-                                     void *__restrict__ out)
+__global__ void __launch_bounds__(256) cross_spectra_kernel(const void *__restrict__ in, int M, double scale,
+                                                            void *__restrict__ out)
 {
-    const int64_t mm = (int64_t)M * M;
-    const int64_t n = nw * F * mm;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % M);
-        const int r = (int)((i / M) % M);
-        const int64_t wf = i / mm;   // window * F + f
-        const int lo = r <= c ? r : c, hi = r <= c ? c : r;   // U[lo][hi]
-        if (C64) {
-            const float2 *X = reinterpret_cast<const float2 *>(in) + wf * M;
-            const float2 xr = X[lo], xc = X[hi];
+    extern __shared__ double2 xs_d[];
+    const int64_t wf = blockIdx.x;   // window * F + f
+    const int mm = M * M;
+    if (C64) {
+        float2 *xs = reinterpret_cast<float2 *>(xs_d);
+        const float2 *X = reinterpret_cast<const float2 *>(in) + wf * M;
+        for (int m = threadIdx.x; m < M; m += blockDim.x) xs[m] = X[m];
+        __syncthreads();
+        const float s = __double2float_rn(scale);
+        float2 *o = reinterpret_cast<float2 *>(out) + wf * mm;
+        for (int e = threadIdx.x; e < mm; e += blockDim.x) {
+            const int r = e / M, c = e - r * M;
+            const int lo = min(r, c), hi = max(r, c);
+            const float2 xr = xs[lo], xc = xs[hi];
             const float tr = xc.x, ti = -xc.y;
-            float ur = __fmaf_rn(-ti, xr.y, __fmaf_rn(tr, xr.x, 0.0f));
+            const float ur = __fmaf_rn(-ti, xr.y, __fmaf_rn(tr, xr.x, 0.0f));
             float ui = __fmaf_rn(tr, xr.y, __fmaf_rn(ti, xr.x, 0.0f));
             if (r > c) ui = -ui;
-            const float s = __double2float_rn(scale);
-            reinterpret_cast<float2 *>(out)[i] = make_float2(__fmul_rn(ur + 0.0f, s), __fmul_rn(ui + 0.0f, s));
-        } else {
-            const double2 *X = reinterpret_cast<const double2 *>(in) + wf * M;
-            const double2 xr = X[lo], xc = X[hi];
+            o[e] = make_float2(__fmul_rn(ur + 0.0f, s), __fmul_rn(ui + 0.0f, s));
+        }
+    } else {
+        double2 *xs = xs_d;
+        const double2 *X = reinterpret_cast<const double2 *>(in) + wf * M;
+        for (int m = threadIdx.x; m < M; m += blockDim.x) xs[m] = X[m];
+        __syncthreads();
+        double2 *o = reinterpret_cast<double2 *>(out) + wf * mm;
+        for (int e = threadIdx.x; e < mm; e += blockDim.x) {
+            const int r = e / M, c = e - r * M;
+            const int lo = min(r, c), hi = max(r, c);
+            const double2 xr = xs[lo], xc = xs[hi];
             const double tr = xc.x, ti = -xc.y;
-            double ur = __fma_rn(-ti, xr.y, __fma_rn(tr, xr.x, 0.0));
+            const double ur = __fma_rn(-ti, xr.y, __fma_rn(tr, xr.x, 0.0));
             double ui = __fma_rn(tr, xr.y, __fma_rn(ti, xr.x, 0.0));
             if (r > c) ui = -ui;
-            reinterpret_cast<double2 *>(out)[i] = make_double2(__dmul_rn(ur + 0.0, scale), __dmul_rn(ui + 0.0, scale));
+            o[e] = make_double2(__dmul_rn(ur + 0.0, scale), __dmul_rn(ui + 0.0, scale));
         }
     }
 }
@@ -173,13 +186,18 @@ int acb_cross_spectra(const void *spectra, int64_t num_windows, int num_freqs, i
     if (precision != ACB_C128 && precision != ACB_C64) return ACB_ERR_ARG;
     if (num_windows < 0 || num_freqs <= 0 || num_mics <= 0) return ACB_ERR_SHAPE;
     if (num_windows == 0) return ACB_OK;
+    if ((int64_t)num_mics * num_mics > 0x7fffffffLL) return ACB_ERR_SHAPE;
+    const int64_t nwf = num_windows * num_freqs;
+    if (nwf > 0x7fffffffLL) return ACB_ERR_SHAPE;
     cudaStream_t s = as_stream(stream);
-    const int64_t n = num_windows * num_freqs * (int64_t)num_mics * num_mics;
-    if (precision == ACB_C64)
-        cross_spectra_kernel<true><<<grid_for(n), 256, 0, s>>>(spectra, num_windows, num_freqs, num_mics, scale, out);
-    else
-        cross_spectra_kernel<false><<<grid_for(n), 256, 0, s>>>(spectra, num_windows, num_freqs, num_mics, scale,
-                                                                out);
+    const size_t smem = (size_t)num_mics * (precision == ACB_C64 ? sizeof(float2) : sizeof(double2));
+    if (precision == ACB_C64) {
+        cudaFuncSetAttribute(cross_spectra_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cross_spectra_kernel<true><<<(unsigned)nwf, 256, smem, s>>>(spectra, num_mics, scale, out);
+    } else {
+        cudaFuncSetAttribute(cross_spectra_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cross_spectra_kernel<false><<<(unsigned)nwf, 256, smem, s>>>(spectra, num_mics, scale, out);
+    }
     return check_launch();
 }
 

@@ -50,7 +50,7 @@ def parse():
     ap.add_argument('--bins', type=int, default=0, help='limit the number of map bins (profiling only)')
     ap.add_argument('--workload', default='precision256',
                     choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig', 'damas',
-                             'cleansc'])
+                             'cleansc', 'stream'])
     ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     return ap.parse_args()
@@ -731,8 +731,105 @@ def run_cleansc(args):
           clocks=clk.summary(), dtype='f64')
 
 
+def run_stream(args):
+    """Streaming spectra (RFFT -> CrossPowerSpectra, calc_mode 'full', complex128) of the 64-mic
+    workload's 1 s of samples (51,200 samples x 64 channels, block 128, Hanning, 50 %): per step every
+    snapshot's 65 bins x 64 x 64 matrix, in device blocks of 64 snapshots (samples resident)."""
+    import time
+
+    import torch
+
+    import acoular_b200 as ac
+    from acoular_b200 import workloads
+    from oracle import oracle as O
+    dev = torch.device('cuda', 0)
+    wl = workloads.three_sources_64()
+    data = wl.time_data()
+    ts_dev = ac.TimeSamples(data=torch.as_tensor(data, device=dev), sample_freq=wl.fs)
+    N, M = 128, wl.mics.num_mics
+    F = N // 2 + 1
+    num = 64
+    rf = ac.RFFT(source=ts_dev, block_size=N, window='Hanning', overlap='50%')
+    cps = ac.CrossPowerSpectra(source=rf)
+    K = (data.shape[0] - N) // (N // 2) + 1
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    sink = torch.zeros((F, M, M), dtype=torch.complex128, device=dev)
+
+    def step():
+        for b in cps.result_device(num):
+            sink.add_(b[-1])      # consume each block on the device (its last snapshot)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        ev[0].record()
+        for _ in range(args.steps):
+            step()
+        ev[1].record()
+        torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    # the cross-spectra kernel alone on one block, for the roofline (bytes written + spectra read)
+    spec = next(rf.result_device(num))
+    from acoular_b200 import _native as NAT
+    out = torch.empty((num, F, M, M), dtype=torch.complex128, device=dev)
+    for _ in range(3):
+        NAT.check(NAT.lib().acb_cross_spectra(spec.data_ptr(), num, F, M, NAT.C128, 1.0, out.data_ptr(),
+                                              NAT.stream_handle()), 'acb_cross_spectra')
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record()
+    for _ in range(reps):
+        NAT.check(NAT.lib().acb_cross_spectra(spec.data_ptr(), num, F, M, NAT.C128, 1.0, out.data_ptr(),
+                                              NAT.stream_handle()), 'acb_cross_spectra')
+    e1.record()
+    torch.cuda.synchronize()
+    k_ms = e0.elapsed_time(e1) / reps
+    k_bytes = num * F * M * M * 16.0 + num * F * M * 16.0
+    pk = peaks()
+    achieved = k_bytes / (k_ms / 1e3) / 1e9
+    # end to end from host samples: TimeSamples(numpy) -> RFFT -> CrossPowerSpectra.result (numpy blocks)
+    ts_host = ac.TimeSamples(data=data, sample_freq=wl.fs)
+    e2e = []
+    for it in range(3):
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        n_out = 0
+        for b in ac.CrossPowerSpectra(source=ac.RFFT(source=ts_host, block_size=N, window='Hanning',
+                                                     overlap='50%')).result(num):
+            n_out += b.shape[0]
+        if it:
+            e2e.append((time.perf_counter() - ta) * 1e3)
+    # oracle on a bounded sample: 64 snapshots
+    tc = time.perf_counter()
+    blocks = list(O.rfft_blocks(data[: (num + 1) * N // 2], N, 'Hanning', '50%', 'complex128', 'none', num))
+    ref = list(O.cross_power_blocks(blocks, F, M, O.power_scale(N, wl.fs, 'power', True), 'complex128'))
+    cpu_s = time.perf_counter() - tc
+    got = next(cps.result(num))
+    err = float(np.abs(got - ref[0]).max() / np.abs(ref[0]).max())
+    n_cpu = sum(b.shape[0] for b in ref)
+    _line('streaming cross-spectra snapshots/s (RFFT -> CrossPowerSpectra full, 64 mics, block 128, 65 bins)',
+          K / (ms / 1e3), 'snapshots/s', ms, args,
+          {'workload': 'stream_' + wl.name, 'mics': M, 'block_size': N, 'window': 'Hanning', 'overlap': '50%',
+           'snapshots': K, 'block_num': num, 'precision': 'complex128',
+           'out_bytes_per_step': K * F * M * M * 16},
+          roofline={'kernel': 'cross_spectra_kernel', 'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'],
+                    'unit': 'GB/s', 'frac': achieved / pk['hbm_gbs'], 'traffic': None, 'bytes_per_launch': k_bytes,
+                    'ms_per_launch': k_ms},
+          accuracy={'vs': 'oracle (the reference generators restated)', 'block': 0, 'max_rel_err': err},
+          e2e={'value': n_out / (float(np.median(e2e)) / 1e3), 'unit': 'snapshots/s', 'ms': float(np.median(e2e)),
+               'h2d_bytes_per_step': int(data.nbytes), 'd2h_bytes_per_step': int(n_out * F * M * M * 16)},
+          cpu_baseline={'value': n_cpu / cpu_s, 'unit': 'snapshots/s', 'cores': O.num_threads(), 'kind': 'port',
+                        'sample': f'{n_cpu} snapshots'},
+          gpu_launches=f'{3 * -(-K // num)} per step (fft_window_kernel, spectra_pack_kernel, cross_spectra_kernel '
+                       f'per block of {num}) + the consumer',
+          clocks=clk.summary(), dtype='f64')
+
+
 def main():
     args = parse()
+    if args.workload == 'stream':
+        return run_stream(args)
     if args.workload == 'cleansc':
         return run_cleansc(args)
     from acoular_b200 import workloads
