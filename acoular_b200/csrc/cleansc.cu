@@ -79,19 +79,6 @@ __device__ __forceinline__ double2 cdiv(double2 x, double2 y)
                         __dmul_rn(__dsub_rn(__dmul_rn(x.y, rat), x.x), scl));
 }
 
-__device__ __forceinline__ double block_sum(double v, double *scratch)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    __syncthreads();   // scratch may still be read by a previous call
-    if (lane == 0) scratch[warp] = v;
-    __syncthreads();
-    double t = 0.0;
-    for (int w = 0; w < kCscWarps; ++w) t += scratch[w];
-    return t;
-}
-
 __global__ void cleansc_init_kernel(int *active, float *result, int64_t n_result, int B)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -239,24 +226,29 @@ __global__ void __launch_bounds__(kCscThreads) cleansc_step_kernel(CscArgs a, in
     }
     __syncthreads();
 
-    // 4. 20 fixed-point steps: hh = (D1 + |hh|^2 w) / sqrt(1 + sum_m |w_m|^2 |hh_m|^2)
-    for (int it = 0; it < 20; ++it) {
-        double part = 0.0;
-        for (int m = threadIdx.x; m < M; m += kCscThreads) {
-            const double2 q = hh[m];
-            part = fma(ww[m], __dadd_rn(__dmul_rn(q.x, q.x), __dmul_rn(q.y, q.y)), part);
+    // 4. 20 fixed-point steps: hh = (D1 + |hh|^2 w) / sqrt(1 + sum_m |w_m|^2 |hh_m|^2), in warp 0 alone
+    //    (each lane owns mics lane, lane + 32, ...; the sum is a shuffle reduction, no block barrier)
+    if (warp == 0) {
+        for (int it = 0; it < 20; ++it) {
+            double part = 0.0;
+            for (int m = lane; m < M; m += 32) {
+                const double2 q = hh[m];
+                part = fma(ww[m], __dadd_rn(__dmul_rn(q.x, q.x), __dmul_rn(q.y, q.y)), part);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            const double den = __dsqrt_rn(__dadd_rn(1.0, part));
+            for (int m = lane; m < M; m += 32) {
+                const double2 q = hh[m];
+                const double H = __dadd_rn(__dmul_rn(q.x, q.x), __dmul_rn(q.y, q.y));
+                const double2 v = w[m], d = d1[m];
+                hh[m] = cdiv_real(make_double2(__dadd_rn(d.x, __dmul_rn(H, v.x)), __dadd_rn(d.y, __dmul_rn(H, v.y))),
+                                  den);
+            }
+            __syncwarp();
         }
-        const double dot = block_sum(part, scratch);
-        const double den = __dsqrt_rn(__dadd_rn(1.0, dot));
-        __syncthreads();   // every thread has read hh before it is rewritten
-        for (int m = threadIdx.x; m < M; m += kCscThreads) {
-            const double2 q = hh[m];
-            const double H = __dadd_rn(__dmul_rn(q.x, q.x), __dmul_rn(q.y, q.y));
-            const double2 v = w[m], d = d1[m];
-            hh[m] = cdiv_real(make_double2(__dadd_rn(d.x, __dmul_rn(H, v.x)), __dadd_rn(d.y, __dmul_rn(H, v.y))), den);
-        }
-        __syncthreads();
     }
+    __syncthreads();
 
     // 5. C[r][c] -= damp (hmax (hh_c conj(hh_r))); 6. the component for the map: (hmax, conj(hh))
     double2 *Cw = a.csm + (int64_t)b * M * M;
