@@ -9,10 +9,12 @@
 //   D1 = (C^T - diag C) w / hmax; 20 fixed-point steps hh = (D1 + |hh|^2 w) / sqrt(1 + sum |w|^2 |hh|^2);
 //   h -= damp * map of the single component (hmax, conj(hh)); C -= damp hmax (hh hh^H)^T.
 //
-// Device schedule per iteration: cleansc_step_kernel (one CTA per bin: the map update h -= damp h1 fused
-// with the argmax, then the peak's steering vector, D1, the fixed point and the CSM update) and the
-// eigenvalue-form map kernel for the new component (map_eig_launch, E = 1), both over all bins; a bin that
-// has stopped clears its active flag and both kernels skip it.  The scalar arithmetic of the steering
+// Device schedule: the steering vectors of every grid point are synthesised once per bin (normalised for
+// the steering type, cleansc_steer_kernel); then per iteration cleansc_step_kernel (one CTA per bin: the
+// map update h -= damp h1 fused with the argmax, then the peak's steering vector, D1, the fixed point and
+// the CSM update) and the eigenvalue-form map of the new component on the cached steering vectors
+// (map_eig_custom_launch, E = 1), both over all bins; a bin that has stopped clears its active flag and
+// both kernels skip it.  The scalar arithmetic of the steering
 // formulas and of the divisions follows numpy's complex arithmetic (x / y for a real y is x * (1 / y));
 // sums (einsum, BLAS dot products) are formed in mic order.
 #include <cuda_runtime.h>
@@ -77,6 +79,59 @@ __device__ __forceinline__ double2 cdiv(double2 x, double2 y)
     const double scl = __ddiv_rn(1.0, __dadd_rn(y.y, __dmul_rn(y.x, rat)));
     return make_double2(__dmul_rn(__dadd_rn(__dmul_rn(x.x, rat), x.y), scl),
                         __dmul_rn(__dsub_rn(__dmul_rn(x.y, rat), x.x), scl));
+}
+
+// Steering vectors of every grid point for the component maps, normalised so that the custom-steering
+// quadratic form equals the steering type's map: v_m = e^{-i fl32(k r_m)} (times r_m for 'inverse',
+// over r_m for 'true level' / 'true location'; the map kernel's synthesis), divided by M (classic),
+// M r0 (inverse), r0 S (true level) or sqrt(M S) (true location), S = sum r^2 or sum 1/r^2.
+// One warp per grid point, lanes over the mics; out (B, G, M).
+__global__ void __launch_bounds__(256) cleansc_steer_kernel(CscArgs a, double2 *__restrict__ out)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t g = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int b = blockIdx.y;
+    if (g >= a.G) return;
+    const int M = a.M;
+    const double k = a.k[b];
+    double gx = 0, gy = 0, gz = 0, r0;
+    if (a.rm) {
+        r0 = a.r0[g];
+    } else {
+        gx = a.gpos[g];
+        gy = a.gpos[a.G + g];
+        gz = a.gpos[2 * a.G + g];
+        r0 = a.ref_mode == 1 ? a.ref_dist : dist3(gx, gy, gz, a.ref0, a.ref1, a.ref2);
+    }
+    double2 *o = out + ((int64_t)b * a.G + g) * M;
+    double S = 0.0;
+    for (int m = lane; m < M; m += 32) {
+        const double r = a.rm ? a.rm[g * M + m] : dist3(gx, gy, gz, a.mpos[m], a.mpos[M + m], a.mpos[2 * M + m]);
+        const float arg = __double2float_rn(__dmul_rn(k, r));
+        float c, sn;
+        sincos_f32_arg(arg, a.table, a.mask, a.faithful != 0, c, sn);
+        double2 v = make_double2((double)c, -(double)sn);
+        if (a.steer_type == 2) {
+            v.x = __dmul_rn(v.x, r);
+            v.y = __dmul_rn(v.y, r);
+            S += r * r;
+        } else if (a.steer_type >= 3) {
+            v.x = __ddiv_rn(v.x, r);
+            v.y = __ddiv_rn(v.y, r);
+            S += 1.0 / (r * r);
+        }
+        o[m] = v;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) S += __shfl_xor_sync(0xffffffffu, S, off);
+    const double Md = (double)M;
+    const double nf = a.steer_type == 1 ? Md : a.steer_type == 2 ? Md * r0 : a.steer_type == 3 ? r0 * S : sqrt(Md * S);
+    const double inv = 1.0 / nf;
+    __syncwarp();
+    for (int m = lane; m < M; m += 32) {
+        const double2 v = o[m];
+        o[m] = make_double2(v.x * inv, v.y * inv);
+    }
 }
 
 __global__ void cleansc_init_kernel(int *active, float *result, int64_t n_result, int B)
@@ -267,7 +322,7 @@ __global__ void __launch_bounds__(kCscThreads) cleansc_step_kernel(CscArgs a, in
 }
 
 struct CscWorkspace {
-    size_t h, h1, powers, lam, vec, active, total;
+    size_t h, h1, powers, lam, vec, active, steer, total;
 };
 
 static CscWorkspace csc_layout(int M, int64_t G, int B, int J)
@@ -287,6 +342,8 @@ static CscWorkspace csc_layout(int M, int64_t G, int B, int J)
     off += up((size_t)B * M * sizeof(double2));
     w.active = off;
     off += up((size_t)B * sizeof(int));
+    w.steer = off;
+    off += up((size_t)B * G * M * sizeof(double2));
     w.total = off;
     return w;
 }
@@ -362,6 +419,10 @@ int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber
     if (st) return st;
     st = map_plain_launch(&q, B, csm, wavenumber, mpos, gpos, r0, rm, a.h, s);
     if (st) return st;
+    double2 *steer = reinterpret_cast<double2 *>(ws + lay.steer);
+    cleansc_steer_kernel<<<dim3((unsigned)((G + 7) / 8), B), 256, 0, s>>>(a, steer);
+    st = check_launch();
+    if (st) return st;
     const size_t smem = (size_t)M * (3 * sizeof(double2) + sizeof(double));
     if (cudaFuncSetAttribute(cleansc_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
@@ -371,8 +432,8 @@ int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber
         st = check_launch();
         if (st) return st;
         if (j + 1 < J) {
-            st = map_eig_launch(&q, B, 1, a.lam, a.vec, wavenumber, mpos, gpos, r0, rm,
-                                reinterpret_cast<double *>(ws + lay.h1), a.active, s);
+            st = map_eig_custom_launch(&q, B, 1, a.lam, a.vec, steer, reinterpret_cast<double *>(ws + lay.h1),
+                                       a.active, s);
             if (st) return st;
         }
     }

@@ -19,4 +19,10 @@ int map_eig_launch(const acb_map_params *p, int nbins, int E, const double *eigv
                    const double *k, const double *mpos, const double *gpos, const double *r0, const double *rm,
                    double *out_map, const int *active, cudaStream_t s);
 
+// Eigenvalue-form map with given steering vectors steer (nbins, G, M) complex128 (custom steering: the
+// result is the quadratic form times p->norm, no steering-type normalisation); bins with active[bin] == 0
+// are skipped.
+int map_eig_custom_launch(const acb_map_params *p, int nbins, int E, const double *eigval, const void *eigvec,
+                          const void *steer, double *out_map, const int *active, cudaStream_t s);
+
 }  // namespace acb

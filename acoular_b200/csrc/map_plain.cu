@@ -455,6 +455,9 @@ int map_eig_launch(const acb_map_params *p, int nbins, int E, const double *eigv
                              nullptr, active);
 }
 
+int map_eig_custom_launch(const acb_map_params *p, int nbins, int E, const double *eigval, const void *eigvec,
+                          const void *steer, double *out_map, const int *active, cudaStream_t s);
+
 }  // namespace acb
 
 using namespace acb;
@@ -569,3 +572,17 @@ int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wav
 }
 
 }  // extern "C"
+
+namespace acb {
+
+int map_eig_custom_launch(const acb_map_params *p, int nbins, int E, const double *eigval, const void *eigvec,
+                          const void *steer, double *out_map, const int *active, cudaStream_t s)
+{
+    MapArgs a;
+    const int rc = custom_args(p, a);
+    if (rc != ACB_OK) return rc;
+    return launch_eig<false, true>(a, nbins, E, eigval, eigvec, nullptr, 0.0, nullptr, nullptr, nullptr, nullptr,
+                                   out_map, nullptr, s, steer, active);
+}
+
+}  // namespace acb

@@ -785,7 +785,7 @@ class BeamformerCleansc(BeamformerBase):
         dev = csm_all.device
         G = self.steer.grid.size
         M = csm_all.shape[-1]
-        per_bin = 2 * G * 8 + 4 * G + 2 * M * M * 16
+        per_bin = 2 * G * 8 + 4 * G + 2 * M * M * 16 + G * M * 16
         chunk = max(1, min(ind.size, self.bin_budget_bytes // per_bin))
         kw = {}
         if type(self.steer.env) is not Environment:

@@ -274,7 +274,8 @@ size_t acb_cleansc_workspace_bytes(int num_mics, int64_t num_grid, int num_bins,
  *   rm [G][M] (then mpos / gpos may be NULL); p->steer_type, r_diag, norm (sig_loss_norm) as for the
  *   map, clip_negative ignored; n_iter 0 = 2 M; damp, stopn as the reference's traits;
  *   result float32 [B][G] (damp * peak at each cleaned peak, as the reference's float32 result).
- * Runs the iterations of all bins with no host synchronisation (2 launches per iteration). */
+ * Runs the iterations of all bins with no host synchronisation (2 launches per iteration); the workspace
+ * holds, among others, every bin's G x M steering vectors (16 G M bytes per bin). */
 int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber, const double *mpos,
                     const double *gpos, const double *r0, const double *rm, int n_iter, double damp, int stopn,
                     float *result, void *workspace, size_t workspace_bytes, void *stream);
