@@ -15,6 +15,7 @@ _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / 'lib' / 'libacoular_b200.so'
 
 ACB_OK = 0
+ACB_ERR_SHAPE, ACB_ERR_ARG, ACB_ERR_CUDA, ACB_ERR_UNSUPPORTED, ACB_ERR_WORKSPACE, ACB_ERR_TIMEOUT = 1, 2, 3, 4, 5, 6
 STATUS_NAMES = {0: 'ok', 1: 'ACB_ERR_SHAPE', 2: 'ACB_ERR_ARG', 3: 'ACB_ERR_CUDA', 4: 'ACB_ERR_UNSUPPORTED',
                 5: 'ACB_ERR_WORKSPACE', 6: 'ACB_ERR_TIMEOUT'}
 STEER_CODES = {'classic': 1, 'inverse': 2, 'true level': 3, 'true location': 4}
