@@ -12,7 +12,8 @@ the device-level API in :mod:`acoular_b200.device`.  The compute runs in hand-wr
 kernels (``lib/libacoular_b200.so``); there is no CPU fallback.
 """
 
-from .environments import Environment
+from .environments import (Environment, GeneralFlowEnvironment, OpenJet, RotatingFlow, SlotJet,
+                           UniformFlowEnvironment)
 from .fbeamform import (BeamformerBase, BeamformerCleansc, BeamformerDamas, BeamformerEig, BeamformerFunctional,
                         BeamformerMusic, BeamformerOrth, L_p, LazyBfResult, PointSpreadFunction, SteeringVector,
                         integrate)
@@ -25,7 +26,7 @@ from .spectra import PowerSpectra, PowerSpectraImport
 __all__ = [
     'RFFT', 'AutoPowerSpectra', 'CrossPowerSpectra',
     'BeamformerBase', 'BeamformerCleansc', 'BeamformerDamas', 'BeamformerEig', 'BeamformerFunctional',
-    'BeamformerOrth', 'BeamformerMusic', 'Environment', 'ImportGrid', 'L_p', 'LazyBfResult', 'MicGeom', 'Mixer', 'PointSource', 'PointSpreadFunction',
+    'BeamformerOrth', 'BeamformerMusic', 'Environment', 'GeneralFlowEnvironment', 'OpenJet', 'RotatingFlow', 'SlotJet', 'UniformFlowEnvironment', 'ImportGrid', 'L_p', 'LazyBfResult', 'MicGeom', 'Mixer', 'PointSource', 'PointSpreadFunction',
     'PowerSpectra', 'PowerSpectraImport', 'RectGrid', 'RectGrid3D', 'SteeringVector', 'TimeSamples',
     'WNoiseGenerator', 'integrate',
 ]

@@ -25,6 +25,8 @@ their decorators removed, bound to plain stand-in objects:
   ``SteeringVector.transfer`` / ``steer_vector``    acoular/fbeamform.py:712-786, 1366-1490, 207-258
 * ``RFFT.result`` / ``_scale``, ``AutoPowerSpectra._get_scaling_value`` / ``result``,
   ``CrossPowerSpectra.result``                        acoular/fprocess.py:35-181, 286-467
+* ``SlotJet.v``, ``OpenJet.v``, ``RotatingFlow.v``, ``spiral_sphere``, ``GeneralFlowEnvironment.apparent_r`` /
+  ``get_interpolator``                               acoular/environments.py:404-462, 518-573, 637-682, 685-980
 * ``WNoiseGenerator.signal``, ``SignalGenerator.usignal``, ``PointSource.result``,
   ``_fill_mic_signal_block``, ``Mixer.result``        (fixture time data)
 
@@ -126,6 +128,19 @@ rfft_scale = _extract('acoular/fprocess.py', 'RFFT._scale', NS, rename='rfft_sca
 aps_scaling = _extract('acoular/fprocess.py', 'AutoPowerSpectra._get_scaling_value', NS, rename='aps_scaling')
 aps_result = _extract('acoular/fprocess.py', 'AutoPowerSpectra.result', NS, rename='aps_result')
 cps_result = _extract('acoular/fprocess.py', 'CrossPowerSpectra.result', NS, rename='cps_result')
+from scipy.integrate import ode as _ode  # noqa: E402
+from scipy.interpolate import LinearNDInterpolator as _LNI  # noqa: E402
+from scipy.spatial import ConvexHull as _CH  # noqa: E402
+NS.update(ode=_ode, LinearNDInterpolator=_LNI, ConvexHull=_CH)
+spiral_sphere = _extract('acoular/environments.py', 'spiral_sphere', NS)
+NS['spiral_sphere'] = spiral_sphere
+openjet_v = _extract('acoular/environments.py', 'OpenJet.v', NS, rename='openjet_v')
+slotjet_v = _extract('acoular/environments.py', 'SlotJet.v', NS, rename='slotjet_v')
+rotflow_v = _extract('acoular/environments.py', 'RotatingFlow.v', NS, rename='rotflow_v')
+gflow_apparent_r = _extract('acoular/environments.py', 'GeneralFlowEnvironment.apparent_r', NS,
+                            rename='gflow_apparent_r')
+gflow_interp = _extract('acoular/environments.py', 'GeneralFlowEnvironment.get_interpolator', NS,
+                        rename='gflow_interp')
 
 
 def _steer_funcs_freq():
@@ -658,7 +673,40 @@ def golden_fprocess():
     print('fprocess_kat.npz written', len(out), 'arrays')
 
 
+def golden_general_flow():
+    """The flow fields' v() and GeneralFlowEnvironment.apparent_r (ray tracing, acoular/environments.py:335-980)
+    for an open jet, a slot jet and a rotating flow on a small grid and 3 microphones."""
+    rng = np.random.RandomState(5)
+    pts = rng.uniform(-0.5, 0.5, (12, 3)) + np.array((0.6, 0.0, 0.4))
+    fields = {
+        'openjet': (SimpleNamespace(v0=20.0, origin=np.zeros(3), D=0.4, l=6.2), openjet_v),
+        'slotjet': (SimpleNamespace(v0=15.0, origin=np.zeros(3), flow=np.array((1.0, 0.0, 0.0)),
+                                    plane=np.array((0.0, 1.0, 0.0)), B=0.3, l=5.2), slotjet_v),
+        'rotating': (SimpleNamespace(rps=2.0, v0=3.0, origin=np.zeros(3), omega=2 * np.pi * 2.0), rotflow_v),
+    }
+    out = {'pts': pts}
+    for name, (ff, vfun) in fields.items():
+        vs, js = zip(*[vfun(ff, p) for p in pts])
+        out[f'{name}_v'], out[f'{name}_jac'] = np.array(vs), np.array(js)
+    g = make_rect_grid(-0.2, 0.2, -0.2, 0.2, 0.6, 0.2)
+    mpos = np.array(((0.3, -0.2, 0.0), (-0.25, 0.1, 0.0), (0.0, 0.3, 0.05)))
+    out['gpos'], out['mpos'] = g.pos, mpos
+    for name, (ff, vfun) in fields.items():
+        ffo = SimpleNamespace(**vars(ff))
+        ffo.v = lambda x, ff=ff, vfun=vfun: vfun(ff, x)
+        env = SimpleNamespace(c=343.0, ff=ffo, N=64, Om=np.pi, roi=None, idict={})
+        env.get_interpolator = lambda roi, x0, env=env: gflow_interp(env, roi, x0)
+        out[f'{name}_rm'] = gflow_apparent_r(env, g.pos, mpos)
+        out[f'{name}_r0'] = gflow_apparent_r(env, g.pos)
+    out['sphere'] = spiral_sphere(40, np.pi, b=np.array((0.3, -0.5, 1.0)))
+    np.savez_compressed(OUT / 'general_flow_kat.npz', **out)
+    print('general_flow_kat.npz written', len(out), 'arrays')
+
+
 if __name__ == '__main__':
+    if os.environ.get('ACB_GOLDEN_ONLY') == 'general_flow':
+        golden_general_flow()
+        sys.exit(0)
     if os.environ.get('ACB_GOLDEN_ONLY') == 'fprocess':
         golden_fprocess()
         sys.exit(0)
@@ -683,3 +731,4 @@ if __name__ == '__main__':
     golden_psf_damas()
     golden_functional_orth_cleansc()
     golden_fprocess()
+    golden_general_flow()

@@ -79,3 +79,27 @@ def test_steering_subclass_takes_custom_path(golden):
     bf0 = ac.BeamformerBase(freq_data=ps, steer=ac.SteeringVector(grid=st.grid, mics=st.mics, steer_type='true level'),
                             r_diag=True)
     assert _rel(got, np.array(bf0.result[12])) <= 1e-5
+
+
+def test_general_flow_environment_map(golden):
+    """BeamformerBase with the ray-traced GeneralFlowEnvironment (a rotating flow): the map kernel takes
+    the environment's apparent distances as given; compared with the oracle on the same distances."""
+    import warnings
+
+    import acoular_b200 as ac
+    from oracle import oracle as O
+    s = golden('small_kat.npz')
+    env = ac.GeneralFlowEnvironment(c=343.0, ff=ac.RotatingFlow(rps=3.0, v0=2.0), N=200)   # rays cover the grid
+    ts = ac.TimeSamples(data=s['data'], sample_freq=float(s['fs']))
+    ps = ac.PowerSpectra(source=ts, block_size=128, window='Hanning', overlap='50%')
+    st = ac.SteeringVector(grid=ac.ImportGrid(pos=s['gpos']), mics=ac.MicGeom(pos_total=s['mpos']), env=env,
+                           steer_type='true level')
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore', RuntimeWarning)
+        r0, rm = np.atleast_1d(st.r0), st.rm
+    assert np.isfinite(rm).all() and np.isfinite(r0).all()
+    bf = ac.BeamformerBase(freq_data=ps, steer=st, r_diag=True)
+    ind = np.arange(10, 31)
+    got = np.array(bf.result[10:31])
+    ref = O.beamformer_calc(ps.csm, ps.fftfreq(), ind, r0, rm, 343.0, 'true level', True)[ind]
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()

@@ -148,3 +148,26 @@ def test_oracle_cleansc_known_answer():
     assert one[src] == np.float32(0.6 * h[src]) and np.count_nonzero(one) == 1
     more = O.beamformer_cleansc_calc(csm, np.array([f]), [0], r0, rm, 343.0, 'classic', False, 0, 0.6, 3)[0]
     assert more.argmax() == src
+
+
+def test_flow_fields_and_general_flow_environment_match_reference(golden):
+    """SlotJet / OpenJet / RotatingFlow velocities and Jacobians, spiral_sphere and the ray-traced
+    GeneralFlowEnvironment.apparent_r against the reference's (tests/golden/general_flow_kat.npz):
+    bit for bit (the host restatement takes the reference's steps and scipy calls)."""
+    import warnings
+
+    from acoular_b200.environments import spiral_sphere
+    g = golden('general_flow_kat.npz')
+    fields = {'openjet': ac.OpenJet(v0=20.0, D=0.4, l=6.2), 'slotjet': ac.SlotJet(v0=15.0, B=0.3, l=5.2),
+              'rotating': ac.RotatingFlow(rps=2.0, v0=3.0)}
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore', RuntimeWarning)   # the jets' formulas divide by x = 0 on the nozzle plane
+        for name, ff in fields.items():
+            vs, js = zip(*[ff.v(p) for p in g['pts']])
+            np.testing.assert_array_equal(np.array(vs), g[f'{name}_v'])
+            np.testing.assert_array_equal(np.array(js), g[f'{name}_jac'])
+            env = ac.GeneralFlowEnvironment(c=343.0, ff=ff, N=64, Om=np.pi)
+            np.testing.assert_array_equal(env.apparent_r(g['gpos'], g['mpos']), g[f'{name}_rm'])
+            np.testing.assert_array_equal(env.apparent_r(g['gpos']), g[f'{name}_r0'])
+            assert len(env.idict) == 4          # one interpolator per position (3 mics, the origin), reused
+    np.testing.assert_array_equal(spiral_sphere(40, np.pi, b=np.array((0.3, -0.5, 1.0))), g['sphere'])
