@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(256) psf_kernel(int M, int64_t G, int S, const
     const bool valid = g < G && sidx < S;
     const double *rs = rm + s * M;
     double re = 0.0, im = 0.0, help = 0.0;
+    double rs_l = 1.0, irs_l = 1.0;
     for (int m0 = 0; m0 < M; m0 += mc) {
         const int n = min(mc, M - m0);
         __syncthreads();
@@ -54,26 +55,32 @@ __global__ void __launch_bounds__(256) psf_kernel(int M, int64_t G, int S, const
             rg_s[i] = gg < G ? rm[gg * M + m0 + mm] : 1.0;
         }
         __syncthreads();
-        if (valid) {
-            for (int mm = 0; mm < n; ++mm) {
-                const double rg = rg_s[mm * kPsfLanes + lane];
-                const double rsm = __ldg(rs + m0 + mm);
-                const float arg = __double2float_rn(__dmul_rn(k, __dsub_rn(rg, rsm)));
-                float c, sn;
-                sincos_f32_arg(arg, table, mask, faithful != 0, c, sn);
-                // (cos - i sin) / rs  [* rg (inverse) | / rg (true level, true location)]
-                double tr = __ddiv_rn((double)c, rsm), ti = __ddiv_rn(-(double)sn, rsm);
-                if (ST == 2) {
-                    tr = __dmul_rn(tr, rg);
-                    ti = __dmul_rn(ti, rg);
-                } else if (ST >= 3) {
-                    tr = __ddiv_rn(tr, rg);
-                    ti = __ddiv_rn(ti, rg);
-                    help += 1.0 / (rg * rg);
-                }
-                re += tr;
-                im += ti;
+        // every lane runs the loop (the shuffles need the whole warp); invalid lanes write nothing
+        for (int mm = 0; mm < n; ++mm) {
+            if ((mm & 31) == 0) {   // lane l holds the source distance of mic mm + l and its reciprocal
+                rs_l = mm + lane < n ? __ldg(rs + m0 + mm + lane) : 1.0;
+                irs_l = 1.0 / rs_l;
             }
+            const double rsm = __shfl_sync(0xffffffffu, rs_l, mm & 31);
+            const double irs = __shfl_sync(0xffffffffu, irs_l, mm & 31);
+            const double rg = rg_s[mm * kPsfLanes + lane];
+            const float arg = __double2float_rn(__dmul_rn(k, __dsub_rn(rg, rsm)));
+            float c, sn;
+            sincos_f32_arg(arg, table, mask, faithful != 0, c, sn);
+            // (cos - i sin) / rs  [* rg (inverse) | / rg (true level, true location)]; the divisions as
+            // products with reciprocals (within an ulp of the quotients)
+            double tr = __dmul_rn((double)c, irs), ti = __dmul_rn(-(double)sn, irs);
+            if (ST == 2) {
+                tr = __dmul_rn(tr, rg);
+                ti = __dmul_rn(ti, rg);
+            } else if (ST >= 3) {
+                const double ig = 1.0 / rg;
+                tr = __dmul_rn(tr, ig);
+                ti = __dmul_rn(ti, ig);
+                help += ig * ig;
+            }
+            re += tr;
+            im += ti;
         }
     }
     if (!valid) return;
