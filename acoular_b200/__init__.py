@@ -1,7 +1,8 @@
 """B200-native frequency-domain beamforming for Acoular: CSM estimation + steered-response map.
 
 Acoular-compatible classes (same names, attributes and semantics as the reference's):
-``MicGeom``, ``RectGrid``, ``RectGrid3D``, ``ImportGrid``, ``Environment``, ``TimeSamples``,
+``MicGeom``, ``RectGrid``, ``RectGrid3D``, ``ImportGrid``, ``LineGrid``, ``MergeGrid``, the sectors
+(``RectSector``, ``RectSector3D``, ``CircSector``, ``PolySector``, ``ConvexSector``, ``MultiSector``), ``Environment``, ``TimeSamples``,
 ``PowerSpectra``, ``PowerSpectraImport``, ``SteeringVector``, ``BeamformerBase``, ``BeamformerEig``,
 ``BeamformerMusic``, ``BeamformerFunctional``, ``BeamformerOrth``, ``PointSpreadFunction``,
 ``BeamformerDamas``, ``BeamformerCleansc``, ``L_p``, ``integrate``; the block-wise generators ``RFFT``,
@@ -18,7 +19,8 @@ from .fbeamform import (BeamformerBase, BeamformerCleansc, BeamformerDamas, Beam
                         BeamformerMusic, BeamformerOrth, L_p, LazyBfResult, PointSpreadFunction, SteeringVector,
                         integrate)
 from .fprocess import RFFT, AutoPowerSpectra, CrossPowerSpectra
-from .grids import ImportGrid, RectGrid, RectGrid3D
+from .grids import (CircSector, ConvexSector, ImportGrid, LineGrid, MergeGrid, MultiSector, PolySector, RectGrid,
+                    RectGrid3D, RectSector, RectSector3D, Sector, SingleSector)
 from .microphones import MicGeom
 from .sources import Mixer, PointSource, TimeSamples, WNoiseGenerator
 from .spectra import PowerSpectra, PowerSpectraImport
@@ -28,5 +30,6 @@ __all__ = [
     'BeamformerBase', 'BeamformerCleansc', 'BeamformerDamas', 'BeamformerEig', 'BeamformerFunctional',
     'BeamformerOrth', 'BeamformerMusic', 'Environment', 'GeneralFlowEnvironment', 'OpenJet', 'RotatingFlow', 'SlotJet', 'UniformFlowEnvironment', 'ImportGrid', 'L_p', 'LazyBfResult', 'MicGeom', 'Mixer', 'PointSource', 'PointSpreadFunction',
     'PowerSpectra', 'PowerSpectraImport', 'RectGrid', 'RectGrid3D', 'SteeringVector', 'TimeSamples',
-    'WNoiseGenerator', 'integrate',
+    'WNoiseGenerator', 'integrate', 'LineGrid', 'MergeGrid', 'Sector', 'SingleSector', 'RectSector', 'RectSector3D',
+    'CircSector', 'PolySector', 'ConvexSector', 'MultiSector',
 ]

@@ -82,6 +82,7 @@ SIGNATURES = {
     'acb_calc_csm_c128': (_I, [_VP, _VP, _I, _I, _VP]),
     'acb_calc_csm_c64': (_I, [_VP, _VP, _I, _I, _VP]),
     'acb_csm_workspace_bytes': (_SZ, [_I, _I, _I64, _I]),
+    'acb_csm_workspace_bytes_block': (_SZ, [_I, _I, _I64, _I, _I]),
     'acb_csm_accumulate': (_I, [_VP, _I, _I64, _I, _I, _I, _I64, _I64, _VP, _VP, _I, _I, _I, _VP, _VP, _SZ, _VP]),
     'acb_csm_finalize': (_I, [_VP, _I, _I, _I, _D, _VP, _VP]),
     'acb_map_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
@@ -96,6 +97,8 @@ SIGNATURES = {
     'acb_cleansc_workspace_bytes': (ctypes.c_size_t, [_I, ctypes.c_int64, _I, _I]),
     'acb_cleansc_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _I, _D, _I, _VP, _VP,
                              ctypes.c_size_t, _VP]),
+    'acb_cleansc_custom_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _I, _D, _I, _VP, _VP, ctypes.c_size_t,
+                                    _VP]),
     'acb_psf_f64': (_I, [ctypes.POINTER(MapParams), _I, _VP, _D, _VP, _VP, _I, _VP, _VP]),
     'acb_damas_gauss_seidel_f64': (_I, [_VP, ctypes.c_int64, _I, _VP, _VP, _I, _D, _I, _VP]),
     'acb_map_custom_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP]),
@@ -103,6 +106,7 @@ SIGNATURES = {
     'acb_beamformer_freq_eig_f64': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _D, _VP, _VP, _VP, _VP, _VP]),
     'acb_sincos_table_build_host': (_I64, [_VP, _I64, ctypes.c_float, _I]),
     'acb_map_tc_workspace_bytes': (_SZ, [_I, _I, _I]),
+    'acb_tc_set_wait_limit_ns': (ctypes.c_uint64, [ctypes.c_uint64]),
     'acb_map_tc': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _SZ, _VP, _VP]),
     'acb_map_tc_noalloc': (_I, [ctypes.POINTER(MapParams), _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     'acb_map_tc_batch_workspace_bytes': (_SZ, [ctypes.POINTER(MapParams), _I, _I]),

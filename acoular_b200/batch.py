@@ -84,7 +84,8 @@ class BatchPlan:
                 self.scale.append(float(np.float64(2.0 / it.block_size) / np.float64(weight) /
                                         np.float64(D.num_blocks(S, it.block_size, ov))))
             prec = N.C64 if it.precision == 'complex64' else N.C128
-            ws_bytes = max(ws_bytes, N.lib().acb_csm_workspace_bytes(M, it.num_bins, max(K, 1), prec))
+            ws_bytes = max(ws_bytes, N.lib().acb_csm_workspace_bytes_block(M, it.num_bins, max(K, 1), prec,
+                                                                             it.block_size))
             if it.r_diag:
                 self.norm.append(it.r_diag_norm if it.r_diag_norm != 0.0 else M / (M - 1.0))
             else:

@@ -55,6 +55,7 @@ struct CscArgs {
     int *active;       // (B)
     double *lam;       // (B) component eigenvalue (hmax)
     double2 *vec;      // (B, M) component vector conj(hh)
+    const double2 *given;   // (B, G, M) a steering object's own vectors (custom steering), else nullptr
 };
 
 // numpy's complex division (Smith's method with a reciprocal scale), for a real divisor y = (yr, 0).
@@ -210,6 +211,18 @@ __global__ void __launch_bounds__(kCscThreads) cleansc_step_kernel(CscArgs a, in
     }
     if (stop) return;
 
+    if (a.given) {
+        // 2'. custom steering: the object's own steering vector of the peak, w = conj(v sqrt(norm))
+        const double2 *v = a.given + ((int64_t)b * G + xi) * M;
+        for (int m = threadIdx.x; m < M; m += kCscThreads) {
+            const double2 x = v[m];
+            const double2 c = make_double2(__dmul_rn(x.x, a.sqrt_norm), -__dmul_rn(x.y, a.sqrt_norm));
+            w[m] = c;
+            ww[m] = __dadd_rn(__dmul_rn(c.x, c.x), __dmul_rn(c.y, c.y));
+            hh[m] = c;
+        }
+        __syncthreads();
+    } else {
     // 2. steering vector of the peak: transfer x_m = (cos p - i sin p) r0 / rm, p = fl32(k (rm - r0))
     const double k = a.k[b];
     double gx = 0, gy = 0, gz = 0, r0x;
@@ -260,6 +273,7 @@ __global__ void __launch_bounds__(kCscThreads) cleansc_step_kernel(CscArgs a, in
         hh[m] = v;
     }
     __syncthreads();
+    }
 
     // 3. D1 = (C^T - diag C) w / hmax: D1_a = sum_{m != a} C[m][a] w_m, a warp per row a
     const double2 *C = a.csm + (int64_t)b * M * M;
@@ -412,6 +426,7 @@ int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber
     a.active = reinterpret_cast<int *>(ws + lay.active);
     a.lam = reinterpret_cast<double *>(ws + lay.lam);
     a.vec = reinterpret_cast<double2 *>(ws + lay.vec);
+    a.given = nullptr;
 
     const int64_t n_init = (int64_t)B * G > B ? (int64_t)B * G : B;
     cleansc_init_kernel<<<(unsigned)((n_init + 255) / 256), 256, 0, s>>>(a.active, result, (int64_t)B * G, B);
@@ -422,6 +437,63 @@ int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber
     double2 *steer = reinterpret_cast<double2 *>(ws + lay.steer);
     cleansc_steer_kernel<<<dim3((unsigned)((G + 7) / 8), B), 256, 0, s>>>(a, steer);
     st = check_launch();
+    if (st) return st;
+    const size_t smem = (size_t)M * (3 * sizeof(double2) + sizeof(double));
+    if (cudaFuncSetAttribute(cleansc_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return ACB_ERR_CUDA;
+    for (int j = 0; j < J; ++j) {
+        cleansc_step_kernel<<<B, kCscThreads, smem, s>>>(a, j);
+        st = check_launch();
+        if (st) return st;
+        if (j + 1 < J) {
+            st = map_eig_custom_launch(&q, B, 1, a.lam, a.vec, steer, reinterpret_cast<double *>(ws + lay.h1),
+                                       a.active, s);
+            if (st) return st;
+        }
+    }
+    return ACB_OK;
+}
+
+int acb_cleansc_custom_f64(const acb_map_params *p, void *csm, const void *steer, int n_iter, double damp, int stopn,
+                           float *result, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!p || !csm || !steer || !result || !workspace) return ACB_ERR_ARG;
+    const int M = p->num_mics, B = p->num_bins;
+    const int64_t G = p->num_grid;
+    if (M < 2 || M > 2048 || G <= 0 || B <= 0 || B > 65535 || n_iter < 0) return ACB_ERR_SHAPE;
+    const int J = n_iter > 0 ? n_iter : 2 * M;
+    const CscWorkspace lay = csc_layout(M, G, B, J);
+    if (workspace_bytes < lay.steer) return ACB_ERR_WORKSPACE;   // the steering region is not needed
+    cudaStream_t s = as_stream(stream);
+    char *ws = static_cast<char *>(workspace);
+
+    acb_map_params q = *p;
+    q.clip_negative = 0;   // CLEAN-SC works on the unclipped map
+    q.glibc_faithful = 0;  // no phase synthesis: the vectors are given
+    CscArgs a = {};
+    a.M = M;
+    a.G = G;
+    a.J = J;
+    a.stopn = stopn;
+    a.damp = damp;
+    a.sqrt_norm = sqrt(p->norm);
+    a.steer_type = 0;
+    a.csm = static_cast<double2 *>(csm);
+    a.h = reinterpret_cast<double *>(ws + lay.h);
+    a.h1 = reinterpret_cast<const double *>(ws + lay.h1);
+    a.powers = reinterpret_cast<double *>(ws + lay.powers);
+    a.result = result;
+    a.active = reinterpret_cast<int *>(ws + lay.active);
+    a.lam = reinterpret_cast<double *>(ws + lay.lam);
+    a.vec = reinterpret_cast<double2 *>(ws + lay.vec);
+    a.given = static_cast<const double2 *>(steer);
+
+    const int64_t n_init = (int64_t)B * G > B ? (int64_t)B * G : B;
+    cleansc_init_kernel<<<(unsigned)((n_init + 255) / 256), 256, 0, s>>>(a.active, result, (int64_t)B * G, B);
+    int st = check_launch();
+    if (st) return st;
+    st = acb_map_custom_f64(&q, csm, steer, a.h, nullptr, stream);
     if (st) return st;
     const size_t smem = (size_t)M * (3 * sizeof(double2) + sizeof(double));
     if (cudaFuncSetAttribute(cleansc_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=

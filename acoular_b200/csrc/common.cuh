@@ -11,6 +11,9 @@ namespace acb {
 // Record the last CUDA error text for acb_last_cuda_error().
 void set_cuda_error(cudaError_t e);
 
+// Limit of one bounded device-side wait of the tensor-core kernels (acb_tc_set_wait_limit_ns).
+uint64_t tc_wait_limit_ns();
+
 inline int check_launch()
 {
     cudaError_t e = cudaGetLastError();

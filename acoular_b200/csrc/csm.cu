@@ -85,6 +85,36 @@ __device__ __forceinline__ void fft_pass(double2 *__restrict__ z, int L1, int ta
 // `KC` window blocks; BF16 lo tiles start `lo_elems` elements after the hi tiles.
 enum { OUT_C128 = 0, OUT_C64 = 1, OUT_TF32 = 2, OUT_BF16 = 3 };
 
+// Store bin `b` (relative to bin_lo) of window `wi` (within the chunk of nw windows), mic m, in form OUT.
+template <int OUT>
+__device__ __forceinline__ void put_bin(void *__restrict__ out, int64_t nw, int wi, int M, int m, int b, double xr,
+                                        double xi, int R, int KC, int64_t lo_elems)
+{
+    if (OUT <= OUT_C64) {
+        const int64_t o = ((int64_t)b * nw + wi) * M + m;
+        if (OUT == OUT_C64)
+            reinterpret_cast<float2 *>(out)[o] = make_float2(__double2float_rn(xr), __double2float_rn(xi));
+        else reinterpret_cast<double2 *>(out)[o] = make_double2(xr, xi);
+    } else {
+        const int rowc = 2 * m, col = wi & 31;
+        const int64_t tile = ((int64_t)b * KC + (wi >> 5)) * R + (rowc >> 5);
+        const float fr = __double2float_rn(xr), fi = __double2float_rn(xi);
+        if (OUT == OUT_TF32) {
+            uint32_t *t = reinterpret_cast<uint32_t *>(out) + tile * 1024;
+            t[tile_off_tf32(rowc & 31, col)] = tf32_bits(fr);
+            t[tile_off_tf32((rowc & 31) + 1, col)] = tf32_bits(fi);
+        } else {
+            __nv_bfloat16 *t = reinterpret_cast<__nv_bfloat16 *>(out) + tile * 1024;
+            const __nv_bfloat16 hr = __float2bfloat16_rn(fr), hi = __float2bfloat16_rn(fi);
+            const int o0 = tile_off(rowc & 31, col), o1 = tile_off((rowc & 31) + 1, col);
+            t[o0] = hr;
+            t[o1] = hi;
+            t[lo_elems + o0] = __float2bfloat16_rn(fr - __bfloat162float(hr));
+            t[lo_elems + o1] = __float2bfloat16_rn(fi - __bfloat162float(hi));
+        }
+    }
+}
+
 template <typename TS, int OUT>
 __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ samples, int M, int N, int hop,
                                                          int64_t w0, int64_t nw, int mpb,
@@ -142,29 +172,105 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
         else wk = make_double2(-1.0, 0.0);
         const double xr = er + (wk.x * orr - wk.y * oi);
         const double xi = ei + (wk.x * oi + wk.y * orr);
-        if (OUT <= OUT_C64) {
-            const int64_t o = ((int64_t)(k - bin_lo) * nw + blockIdx.y) * M + m0 + ml;
-            if (OUT == OUT_C64)
-                reinterpret_cast<float2 *>(out)[o] = make_float2(__double2float_rn(xr), __double2float_rn(xi));
-            else reinterpret_cast<double2 *>(out)[o] = make_double2(xr, xi);
-        } else {
-            const int rowc = 2 * (m0 + ml), col = blockIdx.y & 31;
-            const int64_t tile = ((int64_t)(k - bin_lo) * KC + (blockIdx.y >> 5)) * R + (rowc >> 5);
-            const float fr = __double2float_rn(xr), fi = __double2float_rn(xi);
-            if (OUT == OUT_TF32) {
-                uint32_t *t = reinterpret_cast<uint32_t *>(out) + tile * 1024;
-                t[tile_off_tf32(rowc & 31, col)] = tf32_bits(fr);
-                t[tile_off_tf32((rowc & 31) + 1, col)] = tf32_bits(fi);
-            } else {
-                __nv_bfloat16 *t = reinterpret_cast<__nv_bfloat16 *>(out) + tile * 1024;
-                const __nv_bfloat16 hr = __float2bfloat16_rn(fr), hi = __float2bfloat16_rn(fi);
-                const int o0 = tile_off(rowc & 31, col), o1 = tile_off((rowc & 31) + 1, col);
-                t[o0] = hr;
-                t[o1] = hi;
-                t[lo_elems + o0] = __float2bfloat16_rn(fr - __bfloat162float(hr));
-                t[lo_elems + o1] = __float2bfloat16_rn(fi - __bfloat162float(hi));
-            }
+        put_bin<OUT>(out, nw, (int)blockIdx.y, M, m0 + ml, k - bin_lo, xr, xi, R, KC, lo_elems);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Large blocks (N > 16384): one mic's N/2-point sequence no longer fits a CTA's shared memory.  It is
+// split by decimation in time into D = N / 16384 interleaved sub-sequences z[d + D i] of 8192 points:
+// fft_sub_kernel transforms each one in shared memory with the passes above (sub-spectra Y_d to a
+// scratch region [window][mic][d][8192]), and fft_combine_kernel forms, for the requested bins only,
+// Z[k] = sum_d W_H^{d k} Y_d[k mod 8192] and Z[H - k] before the same real split.
+// ------------------------------------------------------------------------------------------------
+constexpr int FFT_MAX_N = 16384;                 // largest block transformed by one CTA
+constexpr int FFT_SUB_H = FFT_MAX_N / 2;         // points of each sub-sequence of a larger block
+
+size_t fft_scratch_bytes(int num_mics, int block_size, int64_t num_windows)
+{
+    if (block_size <= FFT_MAX_N) return 0;
+    return (size_t)num_windows * (size_t)num_mics * (size_t)(block_size / 2) * sizeof(double2);
+}
+
+template <typename TS>
+__global__ void __launch_bounds__(256) fft_sub_kernel(const TS *__restrict__ samples, int M, int N, int hop,
+                                                      int64_t w0, const double *__restrict__ window,
+                                                      const double2 *__restrict__ tw, double2 *__restrict__ scratch)
+{
+    extern __shared__ double2 zs[];   // [zp(j)], j < FFT_SUB_H
+    const int D = (N >> 1) / FFT_SUB_H;
+    int logHs = 0;
+    while ((1 << logHs) < FFT_SUB_H) ++logHs;
+    const int64_t wi = blockIdx.y;
+    const int m = blockIdx.x, d = blockIdx.z;
+    const TS *src = samples + ((w0 + wi) * (int64_t)hop) * M + m;
+    for (int i = threadIdx.x; i < FFT_SUB_H; i += blockDim.x) {
+        const int64_t j = d + (int64_t)D * i;    // complex point j = (x[2j], x[2j+1])
+        const double x0 = (double)src[(2 * j) * M] * window[2 * j];
+        const double x1 = (double)src[(2 * j + 1) * M] * window[2 * j + 1];
+        zs[zp((int)(__brev((unsigned)i) >> (32 - logHs)))] = make_double2(x0, x1);
+    }
+    __syncthreads();
+    for (int st = 0; st < logHs;) {
+        const int S = logHs - st >= 3 ? 3 : logHs - st;
+        const int L1 = 2 << st;
+        const int ntask = FFT_SUB_H >> S;
+        for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+            if (S == 3) fft_pass<3>(zs, L1, task, N, tw);
+            else if (S == 2) fft_pass<2>(zs, L1, task, N, tw);
+            else fft_pass<1>(zs, L1, task, N, tw);
         }
+        __syncthreads();
+        st += S;
+    }
+    double2 *dst = scratch + ((wi * M + m) * D + d) * (int64_t)FFT_SUB_H;
+    for (int k = threadIdx.x; k < FFT_SUB_H; k += blockDim.x) dst[k] = zs[zp(k)];
+}
+
+// W_N^e for any integer exponent e (the table holds e < N/2; W_N^{e + N/2} = -W_N^e)
+__device__ __forceinline__ double2 twiddle_any(const double2 *__restrict__ tw, int N, int64_t e)
+{
+    e %= N;
+    const int h = N >> 1;
+    if (e < h) return tw[e];
+    const double2 t = tw[e - h];
+    return make_double2(-t.x, -t.y);
+}
+
+// Z[k] of one (window, mic) from its D sub-spectra
+__device__ __forceinline__ double2 combine_point(const double2 *__restrict__ y, int N, int D, int k,
+                                                 const double2 *__restrict__ tw)
+{
+    const int kk = k % FFT_SUB_H;
+    double zr = 0.0, zi = 0.0;
+    for (int d = 0; d < D; ++d) {
+        const double2 v = y[(int64_t)d * FFT_SUB_H + kk];
+        const double2 w = twiddle_any(tw, N, 2 * (int64_t)d * k);   // W_H^{d k} = W_N^{2 d k}
+        zr += v.x * w.x - v.y * w.y;
+        zi += v.x * w.y + v.y * w.x;
+    }
+    return make_double2(zr, zi);
+}
+
+template <int OUT>
+__global__ void __launch_bounds__(256) fft_combine_kernel(const double2 *__restrict__ scratch, int M, int N,
+                                                          int64_t nw, int bin_lo, int nbins,
+                                                          const double2 *__restrict__ tw, void *__restrict__ out,
+                                                          int R, int KC, int64_t lo_elems)
+{
+    const int H = N >> 1, D = H / FFT_SUB_H;
+    const int wi = blockIdx.y;
+    const int k = bin_lo + blockIdx.x;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        const double2 *y = scratch + ((int64_t)wi * M + m) * D * FFT_SUB_H;
+        const double2 zk = combine_point(y, N, D, k % H, tw);
+        const double2 zc = combine_point(y, N, D, (H - k % H) % H, tw);
+        const double er = 0.5 * (zk.x + zc.x), ei = 0.5 * (zk.y - zc.y);
+        const double orr = 0.5 * (zk.y + zc.y), oi = -0.5 * (zk.x - zc.x);
+        const double2 wk = k < H ? tw[k] : make_double2(-1.0, 0.0);
+        const double xr = er + (wk.x * orr - wk.y * oi);
+        const double xi = ei + (wk.x * oi + wk.y * orr);
+        put_bin<OUT>(out, nw, wi, M, m, k - bin_lo, xr, xi, R, KC, lo_elems);
     }
 }
 
@@ -324,8 +430,38 @@ static int fft_mics_per_block(int N)
 // Launch the windowed FFT of `num_windows` windows in output form `out_form`.
 int fft_launch(const void *samples, int sample_dtype, int out_form, int num_mics, int block_size, int hop,
                int64_t first_window, int64_t num_windows, const double *window, const double2 *tw, int bin_lo,
-               int num_bins, void *out, int R, int KC, int64_t lo_elems, cudaStream_t s)
+               int num_bins, void *out, int R, int KC, int64_t lo_elems, void *scratch, cudaStream_t s)
 {
+    if (block_size > FFT_MAX_N) {
+        if (!scratch) return ACB_ERR_WORKSPACE;
+        double2 *sc = reinterpret_cast<double2 *>(scratch);
+        const dim3 gs((unsigned)num_mics, (unsigned)num_windows, (unsigned)(block_size / 2 / FFT_SUB_H));
+        const size_t smem = (size_t)fft_stride(FFT_SUB_H) * sizeof(double2);
+        if (sample_dtype == ACB_F32) {
+            cudaFuncSetAttribute(fft_sub_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            fft_sub_kernel<float><<<gs, 256, smem, s>>>(reinterpret_cast<const float *>(samples), num_mics, block_size,
+                                                        hop, first_window, window, tw, sc);
+        } else {
+            cudaFuncSetAttribute(fft_sub_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            fft_sub_kernel<double><<<gs, 256, smem, s>>>(reinterpret_cast<const double *>(samples), num_mics,
+                                                         block_size, hop, first_window, window, tw, sc);
+        }
+        int st = check_launch();
+        if (st) return st;
+        const dim3 gc((unsigned)num_bins, (unsigned)num_windows);
+        const int nt = num_mics < 256 ? (num_mics + 31) / 32 * 32 : 256;
+        switch (out_form) {
+        case OUT_C128: fft_combine_kernel<OUT_C128><<<gc, nt, 0, s>>>(sc, num_mics, block_size, num_windows, bin_lo,
+                                                                      num_bins, tw, out, R, KC, lo_elems); break;
+        case OUT_C64: fft_combine_kernel<OUT_C64><<<gc, nt, 0, s>>>(sc, num_mics, block_size, num_windows, bin_lo,
+                                                                    num_bins, tw, out, R, KC, lo_elems); break;
+        case OUT_TF32: fft_combine_kernel<OUT_TF32><<<gc, nt, 0, s>>>(sc, num_mics, block_size, num_windows, bin_lo,
+                                                                      num_bins, tw, out, R, KC, lo_elems); break;
+        default: fft_combine_kernel<OUT_BF16><<<gc, nt, 0, s>>>(sc, num_mics, block_size, num_windows, bin_lo,
+                                                                num_bins, tw, out, R, KC, lo_elems); break;
+        }
+        return check_launch();
+    }
     const int mpb = fft_mics_per_block(block_size);
     const dim3 g1((num_mics + mpb - 1) / mpb, (unsigned)num_windows);
     const size_t smem = (size_t)mpb * fft_stride(block_size / 2) * sizeof(double2);
@@ -401,6 +537,14 @@ size_t acb_csm_workspace_bytes(int num_mics, int num_bins, int64_t num_windows, 
     return (size_t)num_mics * (size_t)num_bins * (size_t)num_windows * es;
 }
 
+size_t acb_csm_workspace_bytes_block(int num_mics, int num_bins, int64_t num_windows, int precision, int block_size)
+{
+    const size_t base = acb_csm_workspace_bytes(num_mics, num_bins, num_windows, precision);
+    if (base == 0) return 0;
+    const size_t sc = fft_scratch_bytes(num_mics, block_size, num_windows);
+    return sc ? (base + 255) / 256 * 256 + sc : base;
+}
+
 int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_samples, int num_mics, int block_size,
                        int hop, int64_t first_window, int64_t num_windows, const double *window,
                        const void *twiddle, int bin_lo, int num_bins, int precision, void *csm_upper,
@@ -413,20 +557,25 @@ int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_sample
     if (num_mics <= 0 || num_windows < 0 || first_window < 0 || hop <= 0) return ACB_ERR_SHAPE;
     if (tc && csm_tc_row_tiles(num_mics) > 252) return ACB_ERR_UNSUPPORTED;
     if (block_size < 16 || (block_size & (block_size - 1))) return ACB_ERR_SHAPE;
-    if (block_size > 16384) return ACB_ERR_UNSUPPORTED;
+    if (block_size > 4 * FFT_MAX_N) return ACB_ERR_UNSUPPORTED;
     if (bin_lo < 0 || num_bins <= 0 || bin_lo + num_bins > block_size / 2 + 1) return ACB_ERR_SHAPE;
     if (num_windows == 0) return ACB_OK;
     if ((first_window + num_windows - 1) * (int64_t)hop + block_size > num_samples) return ACB_ERR_SHAPE;
     if (num_windows > 65535) return ACB_ERR_SHAPE;  // one grid row per window
-    const size_t need = acb_csm_workspace_bytes(num_mics, num_bins, num_windows, precision);
+    const size_t need = acb_csm_workspace_bytes_block(num_mics, num_bins, num_windows, precision, block_size);
     if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
+    // blocks above 16384 samples: the FFT's sub-spectra go to a scratch region after the spectra
+    void *scratch = nullptr;
+    if (block_size > FFT_MAX_N)
+        scratch = reinterpret_cast<uint8_t *>(workspace) +
+                  (acb_csm_workspace_bytes(num_mics, num_bins, num_windows, precision) + 255) / 256 * 256;
     cudaStream_t s = as_stream(stream);
     const double2 *tw = reinterpret_cast<const double2 *>(twiddle);
     if (tc)
         return csm_tc_accumulate(samples, sample_dtype, num_mics, block_size, hop, first_window, num_windows, window,
-                                 tw, bin_lo, num_bins, precision == ACB_CSM_TC_TF32, csm_upper, workspace, s);
+                                 tw, bin_lo, num_bins, precision == ACB_CSM_TC_TF32, csm_upper, workspace, scratch, s);
     int st = fft_launch(samples, sample_dtype, precision == ACB_C64 ? OUT_C64 : OUT_C128, num_mics, block_size, hop,
-                        first_window, num_windows, window, tw, bin_lo, num_bins, workspace, 0, 0, 0, s);
+                        first_window, num_windows, window, tw, bin_lo, num_bins, workspace, 0, 0, 0, scratch, s);
     if (st) return st;
     const int T = (num_mics + GT - 1) / GT;
     const dim3 g2(T * (T + 1) / 2, num_bins);

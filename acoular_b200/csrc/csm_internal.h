@@ -9,16 +9,19 @@ namespace acb {
 
 // Windowed FP64 rFFT of `num_windows` windows; out_form: 0 complex128 spectra, 1 complex64 spectra,
 // 2 TF32 operand tiles, 3 split-BF16 operand tiles (R row tiles, KC window blocks, lo tiles
-// `lo_elems` after the hi tiles).
+// `lo_elems` after the hi tiles).  Blocks above 16384 samples need `scratch` of
+// fft_scratch_bytes(num_mics, block_size, num_windows) bytes (null otherwise).
 int fft_launch(const void *samples, int sample_dtype, int out_form, int num_mics, int block_size, int hop,
                int64_t first_window, int64_t num_windows, const double *window, const double2 *tw, int bin_lo,
-               int num_bins, void *out, int R, int KC, int64_t lo_elems, cudaStream_t s);
+               int num_bins, void *out, int R, int KC, int64_t lo_elems, void *scratch, cudaStream_t s);
+size_t fft_scratch_bytes(int num_mics, int block_size, int64_t num_windows);
 
 // Tensor-core Welch accumulation into the complex128 upper triangle (csm_tc.cu).
 int csm_tc_row_tiles(int num_mics);
 size_t csm_tc_workspace_bytes(int num_mics, int num_bins, int64_t num_windows);
 int csm_tc_accumulate(const void *samples, int sample_dtype, int num_mics, int block_size, int hop,
                       int64_t first_window, int64_t num_windows, const double *window, const double2 *tw,
-                      int bin_lo, int num_bins, bool tf32, void *csm_upper, void *workspace, cudaStream_t s);
+                      int bin_lo, int num_bins, bool tf32, void *csm_upper, void *workspace, void *fft_scratch,
+                      cudaStream_t s);
 
 }  // namespace acb

@@ -125,9 +125,14 @@ __global__ void __launch_bounds__(GTC_THREADS, 1) gram_tc_kernel(const __grid_co
                     if (++s == GTC_STAGES) { s = 0; u ^= 1; }
                 }
             }
-            // on an abort, let the last copies land before the CTA releases its shared memory
-            if (*abort_flag && lastS >= 0)
-                tc::mbar_wait(&full[lastS], (uint32_t)lastU, abort_flag, 4 * a.wait_limit_ns);
+            // on an abort, let every copy still in flight land before the CTA releases its shared
+            // memory: the last GTC_STAGES issued stages (n of them at most)
+            if (*abort_flag)
+                for (int j = 0; j < GTC_STAGES && j < n; ++j) {
+                    const int st = (lastS - j + GTC_STAGES) % GTC_STAGES;
+                    tc::mbar_drain(&full[st], (uint32_t)(lastS - j >= 0 ? lastU : lastU ^ 1),
+                                   tc::drain_limit_ns(a.wait_limit_ns));
+                }
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer
@@ -135,7 +140,9 @@ __global__ void __launch_bounds__(GTC_THREADS, 1) gram_tc_kernel(const __grid_co
             constexpr uint32_t SBO = TF32 ? 1024 : 512;
             const uint64_t sbase = tc::sdesc_noswizzle(tc::smem_u32(smem), 128, SBO);
             const uint32_t idesc0 = tc::idesc_m128(TF32 ? 2 : 1, 0);
-            int s = 0, u = 0, lastB = -1, lastU = 0;
+            int s = 0, u = 0;
+            uint64_t *lastBar = nullptr;   // barrier of the last commit (commits complete in order)
+            uint32_t lastPar = 0;
             bool ok = true;
             for (int64_t li = 0; li < nmine && ok; ++li) {
                 const int64_t item = blockIdx.x + li * gridDim.x;
@@ -170,14 +177,17 @@ __global__ void __launch_bounds__(GTC_THREADS, 1) gram_tc_kernel(const __grid_co
                         }
                     }
                     tc::mma_commit(&empty[s]);
+                    lastBar = &empty[s];
+                    lastPar = (uint32_t)u;
                     if (++s == GTC_STAGES) { s = 0; u ^= 1; }
                 }
                 if (!ok) break;
                 tc::mma_commit(&accf[buf]);
-                lastB = buf;
-                lastU = (int)((li >> 1) & 1);
+                lastBar = &accf[buf];
+                lastPar = (uint32_t)((li >> 1) & 1);
             }
-            if (lastB >= 0) tc::mbar_wait(&accf[lastB], (uint32_t)lastU, abort_flag, 4 * a.wait_limit_ns);
+            // before TMEM is released: every MMA issued has completed
+            if (lastBar) tc::mbar_drain(lastBar, lastPar, tc::drain_limit_ns(a.wait_limit_ns));
         }
     } else {
         // ---------------- epilogue (warps 2..5: TMEM lane quarters 2, 3, 0, 1)
@@ -244,7 +254,8 @@ size_t csm_tc_workspace_bytes(int num_mics, int num_bins, int64_t num_windows)
 
 int csm_tc_accumulate(const void *samples, int sample_dtype, int num_mics, int block_size, int hop,
                       int64_t first_window, int64_t num_windows, const double *window, const double2 *tw,
-                      int bin_lo, int num_bins, bool tf32, void *csm_upper, void *workspace, cudaStream_t s)
+                      int bin_lo, int num_bins, bool tf32, void *csm_upper, void *workspace, void *fft_scratch,
+                      cudaStream_t s)
 {
     const int R = csm_tc_row_tiles(num_mics);
     const int KC = (int)((num_windows + 31) / 32);
@@ -257,7 +268,7 @@ int csm_tc_accumulate(const void *samples, int sample_dtype, int num_mics, int b
     }
     const int64_t lo_elems = (int64_t)num_bins * KC * R * 1024;   // BF16: lo tiles after the hi tiles
     int st = fft_launch(samples, sample_dtype, tf32 ? 2 : 3, num_mics, block_size, hop, first_window, num_windows,
-                        window, tw, bin_lo, num_bins, workspace, R, KC, lo_elems, s);
+                        window, tw, bin_lo, num_bins, workspace, R, KC, lo_elems, fft_scratch, s);
     if (st) return st;
 
     GtcArgs a;
@@ -280,7 +291,7 @@ int csm_tc_accumulate(const void *samples, int sample_dtype, int num_mics, int b
     a.nper = n;
     a.nitems = (int64_t)n * num_bins;
     a.csm = reinterpret_cast<double2 *>(csm_upper);
-    a.wait_limit_ns = 500ull * 1000 * 1000;
+    a.wait_limit_ns = tc_wait_limit_ns();
     int dev = 0, nsm = kNumSMs;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const unsigned grid = (unsigned)(a.nitems < nsm ? a.nitems : nsm);

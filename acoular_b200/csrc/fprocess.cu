@@ -127,7 +127,9 @@ extern "C" {
 size_t acb_spectra_workspace_bytes(int num_mics, int block_size, int64_t num_windows)
 {
     if (num_mics <= 0 || block_size < 2 || num_windows < 0) return 0;
-    return (size_t)(block_size / 2 + 1) * (size_t)num_windows * (size_t)num_mics * sizeof(double2);
+    const size_t spec = (size_t)(block_size / 2 + 1) * (size_t)num_windows * (size_t)num_mics * sizeof(double2);
+    const size_t sc = fft_scratch_bytes(num_mics, block_size, num_windows);   // blocks above 16384 samples
+    return sc ? (spec + 255) / 256 * 256 + sc : spec;
 }
 
 int acb_spectra(const void *samples, int sample_dtype, int64_t num_samples, int num_mics, int block_size, int hop,
@@ -139,7 +141,7 @@ int acb_spectra(const void *samples, int sample_dtype, int64_t num_samples, int 
     if (precision != ACB_C128 && precision != ACB_C64) return ACB_ERR_ARG;
     if (num_mics <= 0 || hop <= 0 || first_window < 0 || num_windows < 0) return ACB_ERR_SHAPE;
     if (block_size < 16 || (block_size & (block_size - 1))) return ACB_ERR_SHAPE;
-    if (block_size > 16384) return ACB_ERR_UNSUPPORTED;
+    if (block_size > 65536) return ACB_ERR_UNSUPPORTED;
     if (num_windows == 0) return ACB_OK;
     if ((first_window + num_windows - 1) * (int64_t)hop + block_size > num_samples) return ACB_ERR_SHAPE;
     if (num_windows > 65535) return ACB_ERR_SHAPE;
@@ -147,8 +149,12 @@ int acb_spectra(const void *samples, int sample_dtype, int64_t num_samples, int 
     if (!workspace || workspace_bytes < acb_spectra_workspace_bytes(num_mics, block_size, num_windows))
         return ACB_ERR_WORKSPACE;
     cudaStream_t s = as_stream(stream);
+    void *scratch = nullptr;
+    if (fft_scratch_bytes(num_mics, block_size, num_windows))
+        scratch = static_cast<uint8_t *>(workspace) +
+                  ((size_t)F * (size_t)num_windows * (size_t)num_mics * sizeof(double2) + 255) / 256 * 256;
     int st = fft_launch(samples, sample_dtype, 0, num_mics, block_size, hop, first_window, num_windows, window,
-                        reinterpret_cast<const double2 *>(twiddle), 0, F, workspace, 0, 0, 0, s);
+                        reinterpret_cast<const double2 *>(twiddle), 0, F, workspace, 0, 0, 0, scratch, s);
     if (st) return st;
     const int64_t n = num_windows * F * num_mics;
     if (precision == ACB_C64)

@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "map_internal.h"
+#include "tc_common.cuh"
 
 namespace acb {
 
@@ -250,6 +251,251 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
 }
 
 // ------------------------------------------------------------------------------------------------
+// Staged variant for M <= 256 (one mic chunk): the same steering synthesis and quadratic form, but the
+// CSM rows come through shared memory.  Each warp streams the rows of its 8-row blocks in column
+// chunks of kCB through a two-stage ring that lane 0 fills with bulk copies (cp.async.bulk, no
+// multicast; one copy per row, completion on the stage's mbarrier); the next chunk is in flight while
+// the warp works on the current one.  Every loaded C value then feeds the 32 grid points of the warp
+// from shared memory instead of a broadcast load through L1/L2 per complex FMA, and the masking of the
+// triangle is confined to the diagonal 8 x 8 block.  Waits are bounded; a CTA that gives up raises the
+// error word, writes NaN and returns after its own copies have landed.
+// ------------------------------------------------------------------------------------------------
+constexpr int kCB = 32;                                  // C columns per staged chunk
+constexpr int kCStageElems = kRowBlock * kCB;            // double2 per (warp, stage)
+constexpr uint64_t kPlainWaitNs = 500ull * 1000 * 1000;  // limit of one wait
+
+struct StagedSmem {
+    // byte offsets; M mics
+    __host__ __device__ static constexpr size_t mp(int) { return 0; }
+    __host__ __device__ static constexpr size_t ha(int M) { return (size_t)((3 * M + 1) & ~1) * 8; }
+    __host__ __device__ static constexpr size_t cst(int M) { return ha(M) + (size_t)M * kLanes * 16; }
+    __host__ __device__ static constexpr size_t bars(int M) { return cst(M) + (size_t)kWarps * 2 * kCStageElems * 16; }
+    __host__ __device__ static constexpr size_t total(int M) { return bars(M) + kWarps * 2 * 8 + 16; }
+};
+
+// the chunk sequence of one warp: its row blocks in snake order, each block's columns [a0, M) in kCB chunks
+struct ChunkCursor {
+    int j;    // row block (local index into the warp's list: j-th block of this warp)
+    int c0;   // first column of the chunk
+};
+
+__device__ __forceinline__ int warp_block(int warp, int t)
+{
+    // t-th row block of `warp` in the snake assignment 0..7, 7..0, 0..7, ...
+    return t * kWarps + ((t & 1) ? (kWarps - 1 - warp) : warp);
+}
+
+template <bool USE_RM, bool CUSTOM>
+__global__ void __launch_bounds__(256, 1) map_plain_staged_kernel(MapArgs a, const double2 *__restrict__ csm,
+                                                                  const double *__restrict__ wavenumber, double k_scalar,
+                                                                  const double *__restrict__ mpos,
+                                                                  const double *__restrict__ gpos,
+                                                                  const double *__restrict__ r0_in,
+                                                                  const double *__restrict__ rm,
+                                                                  double *__restrict__ out_map,
+                                                                  double *__restrict__ out_norm,
+                                                                  const double2 *__restrict__ steer, int *err)
+{
+    extern __shared__ __align__(16) uint8_t smem_b[];
+    const int M = a.M;
+    double *mp = reinterpret_cast<double *>(smem_b);
+    double2 *ha = reinterpret_cast<double2 *>(smem_b + StagedSmem::ha(M));     // [M][32]
+    double2 *cst = reinterpret_cast<double2 *>(smem_b + StagedSmem::cst(M));   // [warp][stage][8][kCB]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_b + StagedSmem::bars(M));   // [warp][stage]
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + kWarps * 2);
+    __shared__ double red_off[kWarps][kLanes], red_diag[kWarps][kLanes], red_s[kWarps][kLanes];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int bin = blockIdx.y;
+    const int64_t g = (int64_t)blockIdx.x * kLanes + lane;
+    const bool gvalid = g < a.G;
+    const double k = wavenumber ? wavenumber[bin] : k_scalar;
+    const double2 *C = csm + (int64_t)bin * M * M;
+    const double2 *hv = CUSTOM ? steer + (int64_t)bin * a.G * M : nullptr;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kWarps * 2; ++i) tc::mbar_init(&bars[i], 1);
+        *abort_flag = 0;
+        tc::fence_mbar_init();
+    }
+    if (!USE_RM && !CUSTOM)
+        for (int i = threadIdx.x; i < 3 * M; i += blockDim.x) mp[i] = mpos[i];
+    double g0 = 0, g1 = 0, g2 = 0;
+    if (gvalid && !USE_RM && !CUSTOM) {
+        g0 = gpos[g];
+        g1 = gpos[a.G + g];
+        g2 = gpos[2 * a.G + g];
+    }
+    __syncthreads();
+
+    // this warp's chunk sequence
+    const int nblk = (M + kRowBlock - 1) / kRowBlock;
+    int nmine = 0;
+    while (warp_block(warp, nmine) < nblk) ++nmine;
+    double2 *wst = cst + (size_t)warp * 2 * kCStageElems;
+    uint64_t *wbar = bars + warp * 2;
+    // lane 0: issue the copies of chunk (t, c0) into stage st
+    auto issue = [&](int t, int c0, int st) {
+        const int a0 = warp_block(warp, t) * kRowBlock;
+        const int na = min(kRowBlock, M - a0), nc = min(kCB, M - c0);
+        tc::mbar_arrive_expect_tx(&wbar[st], (uint32_t)(na * nc * 16));
+        for (int r = 0; r < na; ++r)
+            tc::bulk_g2s(wst + (size_t)st * kCStageElems + r * kCB, C + (int64_t)(a0 + r) * M + c0, (uint32_t)(nc * 16),
+                         &wbar[st]);
+    };
+    auto next = [&](int &t, int &c0) {
+        c0 += kCB;
+        if (c0 >= M) {
+            ++t;
+            if (t < nmine) c0 = warp_block(warp, t) * kRowBlock;
+        }
+    };
+    // the first two chunks go out before the steering synthesis, so their latency hides under it
+    int it_t = 0, it_c = nmine > 0 ? warp_block(warp, 0) * kRowBlock : 0;   // issue cursor
+    int issued = 0;
+    if (lane == 0)
+        for (int q = 0; q < 2 && it_t < nmine; ++q, ++issued) {
+            issue(it_t, it_c, q);
+            next(it_t, it_c);
+        }
+    issued = __shfl_sync(0xffffffffu, issued, 0);
+    it_t = __shfl_sync(0xffffffffu, it_t, 0);
+    it_c = __shfl_sync(0xffffffffu, it_c, 0);
+
+    // steering normalisation sum S (inverse: sum r^2; true level / location: sum 1/r^2; custom: sum |h|^2)
+    double s_part = 0.0;
+    if (CUSTOM) {
+        if (gvalid)
+            for (int m = warp; m < M; m += kWarps) {
+                const double2 h = __ldg(hv + g * M + m);
+                s_part += h.x * h.x + h.y * h.y;
+            }
+    } else if (gvalid && a.steer_type >= 2) {
+        for (int m = warp; m < M; m += kWarps) {
+            const double r = grid_mic_dist<USE_RM>(a, rm, g, m, g0, g1, g2, mp);
+            s_part += (a.steer_type == 2) ? r * r : 1.0 / (r * r);
+        }
+    }
+    synth_chunk<USE_RM, CUSTOM>(a, rm, k, g, gvalid, g0, g1, g2, mp, 0, M, ha, hv);
+    __syncthreads();
+
+    double off = 0.0, dsum = 0.0;
+    const bool with_diag = a.r_diag == 0;
+    int q = 0;   // chunk counter: stage q & 1, phase (q >> 1) & 1
+    bool ok = true;
+    for (int t = 0; t < nmine && ok; ++t) {
+        const int a0 = warp_block(warp, t) * kRowBlock;
+        const int na = min(kRowBlock, M - a0);
+        double yr[kRowBlock], yi[kRowBlock];
+#pragma unroll
+        for (int r = 0; r < kRowBlock; ++r) yr[r] = yi[r] = 0.0;
+        for (int c0 = a0; c0 < M; c0 += kCB, ++q) {
+            const int st = q & 1;
+            ok = __all_sync(0xffffffffu, tc::mbar_wait(&wbar[st], (uint32_t)((q >> 1) & 1), abort_flag, kPlainWaitNs));
+            if (!ok) break;
+            const double2 *cs = wst + (size_t)st * kCStageElems;
+            const int nc = min(kCB, M - c0);
+            int bb = 0;
+            if (c0 == a0) {
+                // the diagonal 8 x 8 block: row r takes columns b > a0 + r (and its diagonal term)
+#pragma unroll
+                for (int d = 0; d < kRowBlock; ++d) {
+                    if (d >= nc) break;
+                    const double2 h = ha[(c0 + d) * kLanes + lane];
+#pragma unroll
+                    for (int r = 0; r < kRowBlock; ++r) {
+                        if (r >= na) continue;
+                        const double2 c = cs[r * kCB + d];
+                        if (d > r) {
+                            yr[r] = fma(c.x, h.x, fma(-c.y, h.y, yr[r]));
+                            yi[r] = fma(c.x, h.y, fma(c.y, h.x, yi[r]));
+                        } else if (d == r && with_diag) {
+                            // (C_aa * conj(h)) * h, real part
+                            const double pr = c.x * h.x + c.y * h.y;
+                            const double pi = -c.x * h.y + c.y * h.x;
+                            dsum += pr * h.x - pi * h.y;
+                        }
+                    }
+                }
+                bb = kRowBlock;
+            }
+            if (na == kRowBlock) {
+#pragma unroll 4
+                for (; bb < nc; ++bb) {
+                    const double2 h = ha[(c0 + bb) * kLanes + lane];
+#pragma unroll
+                    for (int r = 0; r < kRowBlock; ++r) {
+                        const double2 c = cs[r * kCB + bb];
+                        yr[r] = fma(c.x, h.x, fma(-c.y, h.y, yr[r]));
+                        yi[r] = fma(c.x, h.y, fma(c.y, h.x, yi[r]));
+                    }
+                }
+            } else {
+                for (; bb < nc; ++bb) {
+                    const double2 h = ha[(c0 + bb) * kLanes + lane];
+#pragma unroll
+                    for (int r = 0; r < kRowBlock; ++r) {
+                        if (r >= na) continue;
+                        const double2 c = cs[r * kCB + bb];
+                        yr[r] = fma(c.x, h.x, fma(-c.y, h.y, yr[r]));
+                        yi[r] = fma(c.x, h.y, fma(c.y, h.x, yi[r]));
+                    }
+                }
+            }
+            // the stage is consumed: lane 0 refills it with the chunk two ahead
+            __syncwarp();
+            if (it_t < nmine) {
+                if (lane == 0) {
+                    tc::fence_proxy_async_smem();
+                    issue(it_t, it_c, st);
+                }
+                next(it_t, it_c);
+                ++issued;
+            }
+        }
+        if (!ok) break;
+#pragma unroll
+        for (int r = 0; r < kRowBlock; ++r) {
+            if (r < na) {
+                const double2 h = ha[(a0 + r) * kLanes + lane];
+                off = fma(h.x, yr[r], fma(h.y, yi[r], off));   // Re(conj(h) y)
+            }
+        }
+    }
+    if (!ok && lane == 0) {
+        // let this warp's copies still in flight (chunks q .. issued - 1) land before the CTA exits
+        for (int qq = q; qq < issued; ++qq)
+            tc::mbar_drain(&wbar[qq & 1], (uint32_t)((qq >> 1) & 1), tc::drain_limit_ns(kPlainWaitNs));
+    }
+
+    red_off[warp][lane] = off;
+    red_diag[warp][lane] = dsum;
+    red_s[warp][lane] = s_part;
+    __syncthreads();
+    if (warp == 0 && gvalid) {
+        double o = 0.0, d = 0.0, S = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            o += red_off[w][lane];
+            d += red_diag[w][lane];
+            S += red_s[w][lane];
+        }
+        double r0 = 0.0;
+        if (CUSTOM) r0 = 0.0;
+        else if (a.ref_mode == 1) r0 = a.ref_dist;
+        else if (USE_RM) r0 = r0_in[g];
+        else r0 = dist3(g0, g1, g2, a.ref0, a.ref1, a.ref2);
+        if (*abort_flag) {
+            out_map[(int64_t)bin * a.G + g] = __longlong_as_double(0x7ff8000000000000ll);
+            if (out_norm) out_norm[(int64_t)bin * a.G + g] = __longlong_as_double(0x7ff8000000000000ll);
+        } else {
+            finish_plain(a, 2.0 * o + d, S, r0, bin, g, out_map, out_norm);
+        }
+    }
+    if (threadIdx.x == 0 && *abort_flag && err) atomicOr(err, 1);
+}
+
+// ------------------------------------------------------------------------------------------------
 // Eigenvalue form of _freqBeamformer_EigValues (acoular/fastFuncs.py:313-411): with eigenvalues
 // lambda_e and eigenvectors V[:, e] of the CSM (E of them),
 //     scalar = sum_e lambda_e (|sum_m conj(V[m][e]) h[m]|^2 - [r_diag] sum_m |conj(V[m][e]) h[m]|^2),
@@ -395,8 +641,18 @@ template <bool USE_RM, bool CUSTOM = false>
 static int launch_plain(const MapArgs &a, int nbins, const void *csm, const double *k, double k_scalar,
                         const double *mpos,
                         const double *gpos, const double *r0, const double *rm, double *out_map, double *out_norm,
-                        cudaStream_t s, const void *steer = nullptr)
+                        cudaStream_t s, const void *steer = nullptr, int *err = nullptr)
 {
+    if (a.M <= 256) {   // one mic chunk: the staged kernel
+        const size_t smem = StagedSmem::total(a.M);
+        auto kern = map_plain_staged_kernel<USE_RM, CUSTOM>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const dim3 grid((unsigned)((a.G + kLanes - 1) / kLanes), nbins);
+        kern<<<grid, kLanes * kWarps, smem, s>>>(a, reinterpret_cast<const double2 *>(csm), k, k_scalar, mpos, gpos,
+                                                r0, rm, out_map, out_norm, reinterpret_cast<const double2 *>(steer),
+                                                err);
+        return check_launch();
+    }
     const int mc = a.M <= 256 ? a.M : 128;
     const int nbuf = a.M <= mc ? 1 : 2;
     const size_t smem = (size_t)(((3 * a.M + 1) & ~1) * sizeof(double)) + (size_t)nbuf * mc * kLanes * sizeof(double2);
@@ -467,14 +723,13 @@ extern "C" {
 int acb_map_f64(const acb_map_params *p, const void *csm, const double *wavenumber, const double *mpos,
                 const double *gpos, double *out_map, double *out_steer_norm, int *error_word, void *stream)
 {
-    (void)error_word;
     MapArgs a;
     int st = make_args(p, a);
     if (st) return st;
     if (!csm || !wavenumber || !mpos || !gpos || !out_map) return ACB_ERR_ARG;
     if ((a.G + kLanes - 1) / kLanes > 0x7fffffffLL) return ACB_ERR_SHAPE;
     return launch_plain<false>(a, p->num_bins, csm, wavenumber, 0.0, mpos, gpos, nullptr, nullptr, out_map,
-                               out_steer_norm, as_stream(stream));
+                               out_steer_norm, as_stream(stream), nullptr, error_word);
 }
 
 int acb_map_eig_f64(const acb_map_params *p, int num_eigs, const double *eigval, const void *eigvec,

@@ -35,11 +35,18 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "common.cuh"
 #include "tc_common.cuh"
 #include "tc_layout.cuh"
 
 namespace acb {
+
+constexpr uint64_t TC_DEFAULT_WAIT_LIMIT_NS = 500ull * 1000 * 1000;
+static std::atomic<uint64_t> g_tc_wait_limit_ns{TC_DEFAULT_WAIT_LIMIT_NS};
+
+uint64_t tc_wait_limit_ns() { return g_tc_wait_limit_ns.load(std::memory_order_relaxed); }
 
 constexpr int TC_ROWS = 128;
 constexpr int TC_CHUNK = 32;               // real components per chunk
@@ -369,10 +376,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                     }
                 }
             }
-            // on an abort, let the last copies land before the CTA releases its shared memory
-            if (*abort_flag && lastT >= 0)
-                tc::mbar_wait(&full_b[lastT & (TC_NB - 1)], (uint32_t)((lastT / TC_NB) & 1), abort_flag,
-                              4 * b.wait_limit_ns);
+            // on an abort, let every copy still in flight land before the CTA releases its shared
+            // memory: the last TC_NB steps (the producer runs at most TC_NB - 1 steps ahead) each own
+            // one barrier slot
+            if (*abort_flag)
+                for (int t = max(0, lastT - (TC_NB - 1)); t <= lastT; ++t)
+                    tc::mbar_drain(&full_b[t & (TC_NB - 1)], (uint32_t)((t / TC_NB) & 1),
+                                   tc::drain_limit_ns(b.wait_limit_ns));
         }
     } else if (warp == TC_WARP_MMA) {
         // ---------------- MMA issuer ----------------
@@ -470,7 +480,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                     }
                 }
             }
-            if (lastb >= 0) tc::mbar_wait(&done[lastb], (uint32_t)lastu, abort_flag, 4 * b.wait_limit_ns);
+            // MMAs complete in issue order: the last commit covers all of them
+            if (lastb >= 0) tc::mbar_drain(&done[lastb], (uint32_t)lastu, tc::drain_limit_ns(b.wait_limit_ns));
         }
     } else if (tc_is_epi(warp)) {
         // ---------------- epilogue (warps 0, 9, 2, 3 for lane quarters 0..3): one thread per grid point
@@ -586,12 +597,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
         // ---------------- steering synthesis (16 warps off scheduler 1) ----------------
         // Synthesis warp s serves grid points 32q..32q+31 (q = s % 4) and part p = s / 4 of every
         // chunk: mics 4p..4p+3 of the chunk's 16, i.e. one 16-byte core-matrix column of the A tile.
+        // The arithmetic runs on mic pairs in packed FP32 (.f32x2): one instruction per pair.
         const int sidx = tc_synth_index(warp);
         const int q = sidx & 3;
         const int p = sidx >> 2;
         const int row = q * 32 + lane;
         const int a_off_row = (((row >> 3) * 4 + p) << 7) + ((row & 7) << 4);
         const int sid = sidx * 32 + lane;   // 0 .. TC_SYNTH_THREADS-1
+        const uint64_t NHALF = tc::f2_splat(-0.5f), THALF = tc::f2_splat(1.5f);
         int T = 0, sa = 0, ua = 0, cur_inst = -1;
         bool ok = true;
         for (int64_t li = 0; li < nmine && ok; ++li) {
@@ -601,13 +614,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             if (ii != cur_inst) {
                 // new instance: every synthesis thread is past the previous item, reload the mics
                 asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
-                // (x, y, z, weight): padding mics beyond M sit far away with weight 0 (the weight is
-                // needed only by the inverse steering's sum of r^2)
+                // pair layout: mics 2j, 2j+1 as (x, x', y, y') (z, z', w, w') in float4s 2j, 2j+1;
+                // padding mics beyond M sit far away with weight 0 (the weight is needed only by the
+                // inverse steering's sum of r^2)
+                float *mpf = reinterpret_cast<float *>(mp4);
                 for (int m = sid; m < in.Mp; m += TC_SYNTH_THREADS) {
                     float4 v = make_float4(TC_FAR, TC_FAR, TC_FAR, 0.f);
                     if (m < in.M)
                         v = make_float4((float)in.mpos[m], (float)in.mpos[in.M + m], (float)in.mpos[2 * in.M + m], 1.f);
-                    mp4[m] = v;
+                    float *d = mpf + (m >> 1) * 8 + (m & 1);
+                    d[0] = v.x;
+                    d[2] = v.y;
+                    d[4] = v.z;
+                    d[6] = v.w;
                 }
                 asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
                 cur_inst = ii;
@@ -623,8 +642,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 gyf = (float)in.gpos[in.G + g];
                 gzf = (float)in.gpos[2 * in.G + g];
             }
+            const uint64_t GX = tc::f2_splat(gxf), GY = tc::f2_splat(gyf), GZ = tc::f2_splat(gzf);
             const double k = in.k[bin];
             const float khi = (float)k, klo = (float)(k - (double)khi);
+            const uint64_t KH = tc::f2_splat(khi), KL = tc::f2_splat(klo);
+            const uint64_t NKH = tc::f2_splat(-khi), NKL = tc::f2_splat(-klo);
             double S = 0.0;
             for (int pp = it.pa; pp < it.pz && ok; ++pp) {
                 const int jb = pp * pw, je = min(C, jb + pw);
@@ -635,45 +657,77 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                                                                    b.wait_limit_ns));
                         if (!ok) break;
                     }
-                    float s_part = 0.f;
+                    uint64_t s2 = 0;   // packed normalisation partial sums (0.0f, 0.0f)
                     uint32_t hw[4], lw[4];
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int m = t * TC_MPC + p * 4 + e;
-                        const float4 mv = mp4[m];
-                        const float dx = gxf - mv.x, dy = gyf - mv.y, dz = gzf - mv.z;
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        const float y = tc::rsqrt_approx(r2);           // 1/r, ~2^-22 relative
-                        float r = r2 * y;
-                        r = fmaf(fmaf(-r, r, r2), 0.5f * y, r);         // r to ~0.5 ulp
-                        // phase k*r as an exact float-float product, reduced by the 3-term 2*pi
-                        const float ph = khi * r;
-                        const float pl = fmaf(klo, r, fmaf(khi, r, -ph));
-                        const float nq = __fsub_rn(__fmaf_rn(ph, TC_INV2PI, 12582912.f), 12582912.f);
-                        float x = fmaf(-nq, TC_P2A, ph);
-                        x = fmaf(-nq, TC_P2B, x);
-                        x = fmaf(-nq, TC_P2C, x);
-                        x += pl;
-                        float sn, cs;
-                        tc::sincos_approx(x, sn, cs);
-                        // steering weight: 1, r (inverse, times the mic's table weight: 0 for padding)
-                        // or 1/r (true level / location)
-                        const float w = ST == 2 ? r * mv.w : (ST >= 3 ? y : 1.f);
-                        if (ST == 2) s_part = fmaf(r2, mv.w, s_part);
-                        else if (ST >= 3) s_part = fmaf(y, y, s_part);
-                        const float vr = cs * w, vi = -sn * w;
-                        if (TF32) {   // FP32 operand rounded to TF32: (re, im) of mic e in hw[e], lw[e]
-                            hw[e] = tf32_bits(vr);
-                            lw[e] = tf32_bits(vi);
-                            continue;
+                    for (int e2 = 0; e2 < 2; ++e2) {
+                        const int j = t * (TC_MPC / 2) + p * 2 + e2;   // mics 2j, 2j+1
+                        const float4 pa = mp4[2 * j], pb = mp4[2 * j + 1];
+                        const uint64_t dx = tc::f2_sub(GX, tc::f2(pa.x, pa.y));
+                        const uint64_t dy = tc::f2_sub(GY, tc::f2(pa.z, pa.w));
+                        const uint64_t dz = tc::f2_sub(GZ, tc::f2(pb.x, pb.y));
+                        const uint64_t r2 = tc::f2_fma(dz, dz, tc::f2_fma(dy, dy, tc::f2_mul(dx, dx)));
+                        float r2a, r2b;
+                        tc::f2_split(r2, r2a, r2b);
+                        // 1/r: hardware rsqrt (~2^-22 relative) and one Newton step y *= 1.5 - 0.5 r^2 y^2
+                        uint64_t y = tc::f2(tc::rsqrt_approx(r2a), tc::rsqrt_approx(r2b));
+                        y = tc::f2_mul(y, tc::f2_fma(tc::f2_mul(tc::f2_mul(r2, y), y), NHALF, THALF));
+                        const uint64_t r = tc::f2_mul(r2, y);
+                        // xn = -(k r) reduced: cos(xn) = Re h / w and sin(xn) = Im h / w
+                        float xa, xb;
+                        if (TF32) {
+                            // TF32 keeps 11 significant bits: -k r in FP32 (k as a float-float) feeds the
+                            // hardware sincos directly, which reduces the argument by whole turns
+                            tc::f2_split(tc::f2_fma(NKL, r, tc::f2_mul(NKH, r)), xa, xb);
+                        } else {
+                            // k r as an exact float-float product, reduced by the 3-term 2*pi
+                            const uint64_t ph = tc::f2_mul(KH, r);
+                            const uint64_t pl = tc::f2_fma(KL, r, tc::f2_fma(KH, r, tc::f2_mul(NKH, r)));
+                            const uint64_t MAG = tc::f2_splat(12582912.f);
+                            const uint64_t nnq = tc::f2_sub(MAG, tc::f2_fma(ph, tc::f2_splat(TC_INV2PI), MAG));
+                            uint64_t x = tc::f2_fma(nnq, tc::f2_splat(TC_P2A), ph);
+                            x = tc::f2_fma(nnq, tc::f2_splat(TC_P2B), x);
+                            x = tc::f2_fma(nnq, tc::f2_splat(TC_P2C), x);
+                            tc::f2_split(tc::f2_add(x, pl), xa, xb);
+                            xa = -xa;
+                            xb = -xb;
                         }
-                        // split-BF16: hi = bf16(x) (packed pair conversion), lo = bf16(x - hi)
-                        const __nv_bfloat162 h2 = __floats2bfloat162_rn(vr, vi);
-                        hw[e] = *reinterpret_cast<const uint32_t *>(&h2);
-                        const float lr = vr - __uint_as_float(hw[e] << 16);
-                        const float li_ = vi - __uint_as_float(hw[e] & 0xFFFF0000u);
-                        const __nv_bfloat162 l2 = __floats2bfloat162_rn(lr, li_);
-                        lw[e] = *reinterpret_cast<const uint32_t *>(&l2);
+                        float sa_, ca_, sb_, cb_;
+                        tc::sincos_approx(xa, sa_, ca_);
+                        tc::sincos_approx(xb, sb_, cb_);
+                        uint64_t vre = tc::f2(ca_, cb_), vim = tc::f2(sa_, sb_);
+                        // steering weight: 1, r (inverse, times the mics' table weights: 0 for padding)
+                        // or 1/r (true level / location)
+                        if (ST == 2) {
+                            const uint64_t wt = tc::f2(pb.z, pb.w);
+                            const uint64_t w = tc::f2_mul(r, wt);
+                            s2 = tc::f2_fma(r2, wt, s2);
+                            vre = tc::f2_mul(vre, w);
+                            vim = tc::f2_mul(vim, w);
+                        } else if (ST >= 3) {
+                            s2 = tc::f2_fma(y, y, s2);
+                            vre = tc::f2_mul(vre, y);
+                            vim = tc::f2_mul(vim, y);
+                        }
+                        float vr[2], vi[2];
+                        tc::f2_split(vre, vr[0], vr[1]);
+                        tc::f2_split(vim, vi[0], vi[1]);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int e = 2 * e2 + h;
+                            if (TF32) {   // FP32 operand rounded to TF32: (re, im) of mic e in hw[e], lw[e]
+                                hw[e] = tf32_bits(vr[h]);
+                                lw[e] = tf32_bits(vi[h]);
+                                continue;
+                            }
+                            // split-BF16: hi = bf16(x) (packed pair conversion), lo = bf16(x - hi)
+                            const __nv_bfloat162 h2 = __floats2bfloat162_rn(vr[h], vi[h]);
+                            hw[e] = *reinterpret_cast<const uint32_t *>(&h2);
+                            const float lr = vr[h] - __uint_as_float(hw[e] << 16);
+                            const float li_ = vi[h] - __uint_as_float(hw[e] & 0xFFFF0000u);
+                            const __nv_bfloat162 l2 = __floats2bfloat162_rn(lr, li_);
+                            lw[e] = *reinterpret_cast<const uint32_t *>(&l2);
+                        }
                     }
                     if (TF32) {
                         // components 8p..8p+7 = core-matrix columns 2p, 2p+1 of the FP32 row
@@ -686,7 +740,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
                             make_uint4(lw[0], lw[1], lw[2], lw[3]);
                     }
-                    if (t >= jb) S += (double)s_part;   // each mic's term once, in its own pass
+                    if (ST >= 2 && t >= jb) {   // each mic's term once, in its own pass
+                        float sa2, sb2;
+                        tc::f2_split(s2, sa2, sb2);
+                        S += (double)(sa2 + sb2);
+                    }
                     tc::fence_proxy_async_smem();
                     tc::mbar_arrive(&full_a[sa]);
                     if (++sa == NST) { sa = 0; ua ^= 1; }
@@ -835,7 +893,7 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
         mp_max = max(mp_max, in.Mp);
     }
     bt.mp_max = mp_max;
-    bt.wait_limit_ns = 500ull * 1000 * 1000;
+    bt.wait_limit_ns = tc_wait_limit_ns();
     int dev = 0, nsm = kNumSMs, smem_max = 232448;
     if (cudaGetDevice(&dev) == cudaSuccess) {
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -865,6 +923,11 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
 using namespace acb;
 
 extern "C" {
+
+uint64_t acb_tc_set_wait_limit_ns(uint64_t limit_ns)
+{
+    return g_tc_wait_limit_ns.exchange(limit_ns ? limit_ns : TC_DEFAULT_WAIT_LIMIT_NS);
+}
 
 size_t acb_map_tc_workspace_bytes(int num_mics, int num_bins, int precision)
 {

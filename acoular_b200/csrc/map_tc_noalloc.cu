@@ -26,7 +26,8 @@ static __device__ __align__(256) unsigned char g_map_tc_scratch[kScratchBytes];
 std::mutex g_mutex;
 void *g_scratch_ptr[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device (looked up on first use).
+// Device address of the scratch array on the current device (looked up on first use and kept for
+// the life of the process; a cudaDeviceReset of that device invalidates it).
 int scratch_for_current_device(void **out)
 {
     int dev = 0;
@@ -58,12 +59,15 @@ int acb_map_tc_noalloc(const acb_map_params *p, int precision, const void *csm, 
                        const double *mpos, const double *gpos, double *out_map, double *out_steer_norm,
                        int *error_word, void *stream)
 {
-    if (!p) return ACB_ERR_ARG;
+    // the argument checks of acb_map_tc, with its status codes: given no workspace it validates
+    // everything and returns ACB_ERR_WORKSPACE, before any CUDA call, only when the arguments are good
+    const int chk = acb_map_tc(p, precision, csm, wavenumber, mpos, gpos, out_map, out_steer_norm, nullptr, 0,
+                               error_word, stream);
+    if (chk != ACB_ERR_WORKSPACE) return chk;
     // the whole R' copy for this call must fit the fixed array; larger requests are rejected
     // before anything is enqueued (split the bins over several calls instead)
     const size_t need = acb_map_tc_workspace_bytes(p->num_mics, p->num_bins, precision);
-    if (need == 0) return ACB_ERR_SHAPE;
-    if (need > kScratchBytes) return ACB_ERR_SHAPE;
+    if (need == 0 || need > kScratchBytes) return ACB_ERR_SHAPE;
     void *scratch = nullptr;
     const int st = scratch_for_current_device(&scratch);
     if (st) return st;

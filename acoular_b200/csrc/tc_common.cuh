@@ -39,7 +39,7 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
 
 // try_wait with a suspend-time hint: the thread sleeps in hardware until the phase completes or
 // the hint (ns) expires, instead of spinning on the issue slots the other warps need.
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity, uint32_t hint_ns = 1000000u)
 {
     uint32_t ok;
     asm volatile(
@@ -47,25 +47,45 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(1000000u)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
 
 // Wait for the phase with `parity` to complete.  Gives up after `limit_ns` or when another thread
-// of the CTA has raised `*abort`; returns false then (the caller records the timeout).
+// of the CTA has raised `*abort`; returns false then (the caller records the timeout).  The hardware
+// suspend of one try_wait is capped at the limit (and at 1 ms), so a short limit is honoured.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort, uint64_t limit_ns)
 {
-    if (mbar_try_wait(bar, parity)) return true;
+    const uint32_t hint = limit_ns < 1000000u ? (uint32_t)limit_ns : 1000000u;
+    if (mbar_try_wait(bar, parity, hint)) return true;
     const uint64_t t0 = globaltimer_ns();
     while (true) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait(bar, parity, hint)) return true;
         if (*abort) return false;
         if (globaltimer_ns() - t0 > limit_ns) {
             *abort = 1;
             return false;
         }
     }
+}
+
+// Wait for asynchronous work this thread issued itself (bulk copies, MMAs) to finish before the CTA
+// releases shared memory or tensor memory after an abort.  Such work completes on its own, so the
+// abort flag is ignored and the limit is generous; returns false only if even that runs out.
+__device__ __forceinline__ bool mbar_drain(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
+{
+    const uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    }
+    return true;
+}
+
+// Drain limit for a wait limit: four times the limit, at least 200 ms.
+__host__ __device__ constexpr uint64_t drain_limit_ns(uint64_t limit_ns)
+{
+    return 4 * limit_ns > 200000000ull ? 4 * limit_ns : 200000000ull;
 }
 
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -168,6 +188,44 @@ __device__ __forceinline__ void sincos_approx(float x, float &s, float &c)
 {
     asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
+}
+
+// Packed FP32 pairs (sm_100a .f32x2 arithmetic): one instruction does the same operation on the
+// two halves of a 64-bit register pair, so two mics' steering terms issue as one instruction.
+__device__ __forceinline__ uint64_t f2(float lo, float hi)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_split(uint64_t v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_splat(float x) { return f2(x, x); }
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c)
+{
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
 }
 
 __device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, float (&v)[8])

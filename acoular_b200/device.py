@@ -113,14 +113,14 @@ def csm_upper_accumulate(samples: torch.Tensor, block_size: int, window: str, ov
     tw = twiddles(block_size, dev)
     if prec in (N.CSM_TC_TF32, N.CSM_TC_BF16X3):
         # the tensor-core operand pads every chunk to whole blocks of 32 windows
-        per32 = N.lib().acb_csm_workspace_bytes(M, nb, 32, prec)
+        per32 = N.lib().acb_csm_workspace_bytes_block(M, nb, 32, prec, block_size)
         chunk = int(max(32, min(65504, max_workspace_bytes // max(per32, 1) * 32)))
         chunk = min(chunk, -(-max(K, 1) // 32) * 32)
-        need = N.lib().acb_csm_workspace_bytes(M, nb, chunk, prec)
+        need = N.lib().acb_csm_workspace_bytes_block(M, nb, chunk, prec, block_size)
     else:
-        per_win = N.lib().acb_csm_workspace_bytes(M, nb, 1, prec)
+        per_win = N.lib().acb_csm_workspace_bytes_block(M, nb, 1, prec, block_size)
         chunk = int(max(1, min(65535, max_workspace_bytes // max(per_win, 1), K if K > 0 else 1)))
-        need = per_win * chunk
+        need = N.lib().acb_csm_workspace_bytes_block(M, nb, chunk, prec, block_size)
     if workspace is None or workspace.numel() < need:
         workspace = torch.empty(need, dtype=torch.uint8, device=dev)
     st = N.stream_handle()
@@ -527,4 +527,29 @@ def cleansc_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, steer_type: str, r
     N.check(N.lib().acb_cleansc_f64(ctypes.byref(p), work.data_ptr(), k.data_ptr(), N.ptr(mpos), N.ptr(gpos),
                                     N.ptr(r0), N.ptr(rm), int(n_iter), float(damp), int(stopn), out.data_ptr(),
                                     ws.data_ptr(), nbytes, N.stream_handle()), 'acb_cleansc_f64')
+    return out
+
+
+def cleansc_custom_f64(csm: torch.Tensor, steer: torch.Tensor, r_diag: bool, norm: float, n_iter: int = 0,
+                       damp: float = 0.6, stopn: int = 3) -> torch.Tensor:
+    """CLEAN-SC for B bins with a steering object's own vectors: csm (B, M, M) complex128 (left unchanged),
+    steer (B, G, M) complex128 (its steer_vector(f) per bin) -> (B, G) float32."""
+    B, M, _ = csm.shape
+    G = int(steer.shape[1])
+    if steer.shape != (B, G, M) or steer.dtype != torch.complex128 or not steer.is_contiguous():
+        msg = 'steer must be a contiguous complex128 (num_bins, num_grid, num_mics) tensor'
+        raise ValueError(msg)
+    dev = csm.device
+    p = map_params(M, G, B, 'classic', r_diag, norm, False, None, False, dev)
+    work = csm.to(torch.complex128).contiguous().clone()
+    nbytes = N.lib().acb_cleansc_workspace_bytes(M, G, B, int(n_iter))
+    if nbytes == 0:
+        msg = 'invalid CLEAN-SC sizes'
+        raise ValueError(msg)
+    nbytes -= 16 * G * M * B          # the steering region: the vectors are given
+    ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+    out = torch.empty((B, G), dtype=torch.float32, device=dev)
+    N.check(N.lib().acb_cleansc_custom_f64(ctypes.byref(p), work.data_ptr(), steer.data_ptr(), int(n_iter),
+                                           float(damp), int(stopn), out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                           N.stream_handle()), 'acb_cleansc_custom_f64')
     return out

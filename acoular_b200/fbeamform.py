@@ -328,11 +328,7 @@ class BeamformerBase:
 
     def integrate(self, sector, frange=None, num=0):
         grid = self.steer.grid
-        if hasattr(grid, 'indices'):
-            ind = grid.indices(*sector)
-        else:
-            msg = f'Grid of type {grid.__class__.__name__} does not have an indices method!'
-            raise NotImplementedError(msg)
+        ind = _sector_indices(grid, sector)
         gshape = grid.shape
         num_freqs = self.freq_data.fftfreq().shape[0]
         if num == 0 or frange is None:
@@ -778,15 +774,25 @@ class BeamformerCleansc(BeamformerBase):
         ind = np.asarray(ind, dtype=np.int64)
         if ind.size == 0:
             return
-        if type(self.steer) is not SteeringVector:
-            msg = 'BeamformerCleansc on the GPU needs a SteeringVector (custom steering objects are not built)'
-            raise NotImplementedError(msg)
         csm_all = self.freq_data.csm_device
         dev = csm_all.device
         G = self.steer.grid.size
         M = csm_all.shape[-1]
         per_bin = 2 * G * 8 + 4 * G + 2 * M * M * 16 + G * M * 16
         chunk = max(1, min(ind.size, self.bin_budget_bytes // per_bin))
+        if type(self.steer) is not SteeringVector:
+            # a steering object of its own: its steer_vector(f) per bin, materialised as the reference's
+            # _beamformer_params does (acoular/fbeamform.py:470-472), on the custom-steering iterations
+            for s0 in range(0, ind.size, chunk):
+                sub = ind[s0:s0 + chunk]
+                csm = csm_all.index_select(0, torch.as_tensor(sub, device=dev))
+                steer = torch.as_tensor(np.ascontiguousarray(
+                    np.stack([self.steer.steer_vector(self._f[i]) for i in sub]), dtype=np.complex128), device=dev)
+                res = D.cleansc_custom_f64(csm, steer, self.r_diag, self.sig_loss_norm(), self.n_iter, self.damp,
+                                           self.stopn)
+                self._ac[sub] = res.double().cpu().numpy()
+            self._fr[ind] = 1
+            return
         kw = {}
         if type(self.steer.env) is not Environment:
             kw['r0'], kw['rm'] = _steer_distances_device(self.steer, dev, self)
@@ -808,13 +814,22 @@ def L_p(x):
     return 10 * np.log10(np.maximum(x / 4e-10, np.finfo(x.dtype).eps))
 
 
+def _sector_indices(grid, sector):
+    """Grid indices of ``sector``: a :class:`~acoular_b200.grids.Sector` through ``grid.subdomain``, or the
+    array forms (x1, y1, x2, y2) / (x, y, r) / 3-D box through ``grid.indices`` (acoular/fbeamform.py:2475-2487)."""
+    from .grids import Sector
+    if isinstance(sector, Sector):
+        return grid.subdomain(sector)
+    if hasattr(grid, 'indices'):
+        return grid.indices(*sector)
+    msg = (f'Grid of type {grid.__class__.__name__} does not have an indices method! Please use a sector '
+           'derived instance of type Sector instead of type numpy.array.')
+    raise NotImplementedError(msg)
+
+
 def integrate(data, grid, sector):
     """Sum of a map (or of each row of a (F, G) result) over a grid sector (acoular/fbeamform.py:2435-2497)."""
-    if hasattr(grid, 'indices'):
-        ind = grid.indices(*sector)
-    else:
-        msg = f'Grid of type {grid.__class__.__name__} does not have an indices method!'
-        raise NotImplementedError(msg)
+    ind = _sector_indices(grid, sector)
     gshape = grid.shape
     gsize = grid.size
     if np.size(data) == gsize:

@@ -6,7 +6,7 @@ Same attributes, generator contract and block layout as the reference: ``result(
 channels interlaced.  Each class also has ``result_device(num)``, which yields the same blocks as
 ``(n, num_freqs, channels...)`` device tensors; chained objects consume their source's device blocks,
 so samples -> spectra -> auto/cross spectra never leave the GPU.  The FFT is the CSM path's FP64 kernel
-(block sizes: powers of two, 16 ... 16384); the windows are those of ``BaseSpectra._get_source_data``.
+(block sizes: powers of two, 16 ... 65536); the windows are those of ``BaseSpectra._get_source_data``.
 ``workers`` is accepted and ignored (there are no host FFT threads).
 """
 
@@ -112,8 +112,8 @@ class RFFT:
     def result_device(self, num: int = 1):
         """Blocks of at most ``num`` spectra as device tensors (n, num_freqs, num_channels)."""
         N_ = self.block_size
-        if N_ < 16 or N_ > 16384 or N_ & (N_ - 1):
-            msg = f'block_size {N_}: the FFT kernel takes powers of two from 16 to 16384'
+        if N_ < 16 or N_ > 65536 or N_ & (N_ - 1):
+            msg = f'block_size {N_}: the FFT kernel takes powers of two from 16 to 65536'
             raise ValueError(msg)
         x = self._samples()
         dev = x.device

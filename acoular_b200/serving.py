@@ -253,6 +253,7 @@ class BeamformingServer:
         for r in batch:
             r.t_done = now
             r.future.latency = now - r.t_submit     # submit -> result ready, seconds
+            r.future.units = r.stream.out.numel()   # grid points x bins mapped for this request
             r.future.set_result(r.stream.h_band.numpy().reshape(r.stream.gshape).copy())
         self.batches.append(len(batch))
 

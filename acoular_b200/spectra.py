@@ -1,7 +1,7 @@
 """``PowerSpectra`` with the CSM computed on the B200 (acoular/spectra.py:52-588).
 
-Same attributes and semantics as the reference: ``block_size`` (128 ... 65536; this build's FFT
-kernel covers up to 16384), ``window``, ``overlap``, ``precision`` ('complex128' | 'complex64'),
+Same attributes and semantics as the reference: ``block_size`` (128 ... 65536; blocks above 16384
+samples take the FFT as interleaved 8192-point sub-transforms and a combining pass), ``window``, ``overlap``, ``precision`` ('complex128' | 'complex64'),
 ``fftfreq()``, ``num_blocks`` (the reference's float formula), ``csm`` (lazy, recomputed when
 the source or a setting changes), ``indices`` / ``ind_low`` / ``ind_high`` / ``freq_range``,
 ``eigvals`` / ``eigvecs``.  ``calc_csm()`` returns the complex128 (F, M, M) numpy array the

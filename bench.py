@@ -53,6 +53,8 @@ def parse():
                              'cleansc', 'stream'])
     ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
+    ap.add_argument('--no-extra', action='store_true',
+                    help='skip the other configurations\' blocks of the default line (profiling runs)')
     return ap.parse_args()
 
 
@@ -168,92 +170,102 @@ def gemm_peaks(dev, n: int = 8192) -> dict:
     return out
 
 
+def host_info() -> dict:
+    """Host cores, CPU model and C library of the machine the CPU baselines run on."""
+    import platform
+    model = None
+    try:
+        for ln in Path('/proc/cpuinfo').read_text().splitlines():
+            if ln.startswith('model name'):
+                model = ln.split(':', 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {'nproc': os.cpu_count(), 'threads_available': len(os.sched_getaffinity(0)), 'cpu_model': model,
+            'libc': ' '.join(platform.libc_ver())}
+
+
+# Map bins of the CPU sample: a spread over the band, so that the C library's cosf/sinf cost (which
+# grows with the phase argument) is averaged the same way in both arms.
+CPU_SAMPLE_BINS = (100, 256, 400)
+
+
+class CpuSample:
+    """The CPU oracle (C/OpenMP port of the reference's numba calcCSM and _freqBeamformer_FullCSM) on a
+    bounded sample of the 256-mic workload, on all host threads: one map bin over the full grid (bins
+    rotating through ``CPU_SAMPLE_BINS``) plus one bin's share of the CSM (the Welch accumulation of 65
+    windows over all bins, scaled by K / 65 / F).  ``value`` = grid points / (map time + CSM share) per
+    bin.  The bench line's ``cpu_baseline`` and the ``--impl reference`` arm both use this class."""
+
+    def __init__(self, wl, steer):
+        from acoular_b200 import device as D
+        from oracle import oracle as O
+        self.O = O
+        self.ncores = len(os.sched_getaffinity(0))
+        O.set_num_threads(self.ncores)
+        self.wl, self.steer = wl, steer
+        self.M, self.G, self.N = wl.mics.num_mics, wl.grid.size, wl.block_size
+        self.F = self.N // 2 + 1
+        self.K = D.num_windows(wl.num_samples, self.N, 2)
+        self.r0 = O.apparent_r(wl.grid.pos)
+        self.rm = O.apparent_r(wl.grid.pos, wl.mics.pos)
+        rng = np.random.RandomState(1)
+        X = rng.randn(2 * self.M, self.M) + 1j * rng.randn(2 * self.M, self.M)
+        self.csm_bin = (X.conj().T @ X) / (2 * self.M)
+        self.freqs = O.fftfreq(self.N, wl.fs)
+        self.data = rng.randn(64 * (self.N // 2) + self.N, self.M)   # 65 windows; values do not change the cost
+        self.norm = O.sig_loss_norm(True, self.M)
+        self.i = 0
+        O.beamformer_freq(steer, True, 1.0, self.r0[:64], self.rm[:64], 1.0, self.csm_bin)   # warm the pool
+
+    def step(self) -> float:
+        """One bin's map plus one bin's CSM share; returns seconds (the bin's equivalent time)."""
+        O, wl = self.O, self.wl
+        b = CPU_SAMPLE_BINS[self.i % len(CPU_SAMPLE_BINS)]
+        self.i += 1
+        t0 = time.perf_counter()
+        O.beamformer_freq(self.steer, True, self.norm, self.r0, self.rm, 2 * np.pi * self.freqs[b] / wl.c, self.csm_bin)
+        t1 = time.perf_counter()
+        O.calc_csm(self.data, self.N, 'Hanning', '50%', 'complex128')
+        t2 = time.perf_counter()
+        return (t1 - t0) + (t2 - t1) * (self.K / 65.0) / self.F
+
+    def describe(self, nsteps: int) -> str:
+        return (f'{nsteps} x (map of 1 bin over {self.G} grid points, bins cycling {list(CPU_SAMPLE_BINS)}, + the CSM '
+                f'of 65 windows x all {self.F} bins scaled to one bin\'s share K/65/F, K = {self.K}); C/OpenMP port of '
+                f'the reference numba calcCSM and _freqBeamformer_FullCSM, {self.ncores} threads')
+
+
 def run_reference(args, wl):
-    """CPU oracle (C/OpenMP port of the reference's numba kernels), bounded sample per step."""
-    from acoular_b200 import device as D
-    from oracle import oracle as O
+    """CPU arm: the oracle port of the reference's CPU path, bounded sample per step (:class:`CpuSample`)."""
     ws = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
-    ncores = len(os.sched_getaffinity(0))
-    O.set_num_threads(ncores)
-    G = wl.grid.size
-    M = wl.mics.num_mics
-    N = wl.block_size
-    F = N // 2 + 1
-    K = D.num_windows(wl.num_samples, N, 2)
-    kw = max(1, round(K / F))  # one bin's share of the CSM work: K/F windows for all bins
-    hop = N // 2
-    gpos = wl.grid.pos
-    r0 = O.apparent_r(gpos)
-    rm = O.apparent_r(gpos, wl.mics.pos)
-    rng = np.random.RandomState(0)
-    data = rng.randn((kw - 1) * hop + N, M)  # sample values do not change the CPU cost
-    X = rng.randn(2 * M, M) + 1j * rng.randn(2 * M, M)
-    csm_bin = (X.conj().T @ X) / (2 * M)
-    freqs = O.fftfreq(N, wl.fs)
-    b = F // 2
-    norm = O.sig_loss_norm(True, M)
-
-    def step():
-        seg = data[: (kw - 1) * hop + N]
-        O.calc_csm(seg, N, 'Hanning', '50%', 'complex128')
-        res, _ = O.beamformer_freq(args.steer, True, norm, r0, rm, 2 * np.pi * freqs[b] / wl.c, csm_bin)
-        return res
-
+    cs = CpuSample(wl, args.steer)
     for _ in range(args.warmup):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-    dt = (time.perf_counter() - t0) / args.steps
-    value = G / dt
+        cs.step()
+    dt = sum(cs.step() for _ in range(args.steps)) / args.steps
+    value = cs.G / dt
     line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': ws, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': dt * 1e3, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded monopoles)',
-            'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': F, 'block_size': N,
+            'config': {'workload': wl.name, 'mics': cs.M, 'grid_points': cs.G, 'bins': cs.F, 'block_size': cs.N,
                        'steer_type': args.steer, 'r_diag': True},
-            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': ncores, 'kind': 'port',
-                             'sample': f'per step: CSM of {kw} windows x all {F} bins (1/{F} of the CSM) + map of '
-                                       f'1 bin over {G} grid points (C/OpenMP port of calcCSM and '
-                                       f'_freqBeamformer_FullCSM, {ncores} threads)'},
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cs.ncores, 'kind': 'port',
+                             'sample': cs.describe(args.steps)},
+            'host': host_info(),
             'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_sample(wl, steer):
-    """Oracle timing on the host cores for the bench line's cpu_baseline (rank 0, N=1)."""
-    from acoular_b200 import device as D
-    from oracle import oracle as O
-    ncores = len(os.sched_getaffinity(0))
-    O.set_num_threads(ncores)
-    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
-    F = N // 2 + 1
-    K = D.num_windows(wl.num_samples, N, 2)
-    gpos = wl.grid.pos
-    r0 = O.apparent_r(gpos)
-    rm = O.apparent_r(gpos, wl.mics.pos)
-    rng = np.random.RandomState(1)
-    X = rng.randn(2 * M, M) + 1j * rng.randn(2 * M, M)
-    csm_bin = (X.conj().T @ X) / (2 * M)
-    freqs = O.fftfreq(N, wl.fs)
-    data = rng.randn(64 * (N // 2) + N, M)
-    O.beamformer_freq(steer, True, 1.0, r0[:64], rm[:64], 1.0, csm_bin)  # warm
-    t0 = time.perf_counter()
-    nb = 0
-    while nb < 3 and (nb == 0 or time.perf_counter() - t0 < 20):
-        O.beamformer_freq(steer, True, 1.0, r0, rm, 2 * np.pi * freqs[100 + 50 * nb] / wl.c, csm_bin)
-        nb += 1
-    t_map = (time.perf_counter() - t0) / nb
-    t1 = time.perf_counter()
-    O.calc_csm(data, N, 'Hanning', '50%', 'complex128')
-    t_csm_64 = time.perf_counter() - t1
-    t_csm_bin = t_csm_64 * (K / 65.0) / F  # per-bin share of the full CSM
-    value = G / (t_map + t_csm_bin)
-    return {'value': value, 'unit': UNIT, 'cores': ncores, 'kind': 'port',
-            'sample': f'map of {nb} bins x {G} grid points + CSM of 65 windows x {F} bins, scaled to one bin '
-                      f'(C/OpenMP port of the reference numba kernels, {ncores} threads)'}
+def cpu_baseline_sample(wl, steer, nsteps: int = 6):
+    """Oracle timing on the host cores for the bench line's cpu_baseline (rank 0, N=1): the same sample
+    as the reference arm, two passes over the sample bins."""
+    cs = CpuSample(wl, steer)
+    dt = sum(cs.step() for _ in range(nsteps)) / nsteps
+    return {'value': cs.G / dt, 'unit': UNIT, 'cores': cs.ncores, 'kind': 'port', 'sample': cs.describe(nsteps),
+            'host': host_info()}
 
 
 def _line(metric, value, unit, ms, args, config, **extra):
@@ -264,10 +276,23 @@ def _line(metric, value, unit, ms, args, config, **extra):
     print(json.dumps(d), flush=True)
 
 
-def run_batched(args):
-    """64 uneven instances: per-instance CSM of 30 bins (complex64) + one batched tensor-core map."""
+def _err_vs(got: np.ndarray, ref: np.ndarray) -> dict:
+    """max / rms of |got - ref| / max|ref| per row (bin) and the L_p difference at each row's peak."""
+    got, ref = np.atleast_2d(got), np.atleast_2d(ref)
+    err = np.abs(got - ref) / np.abs(ref).max(axis=1, keepdims=True)
+    lp = lambda x: 10 * np.log10(np.maximum(x / 4e-10, np.finfo(np.float64).eps))  # noqa: E731
+    pk = ref.argmax(axis=1)
+    rows = np.arange(ref.shape[0])
+    return {'max_rel_err': float(err.max()), 'rms_rel_err': float(np.sqrt((err ** 2).mean())),
+            'peak_level_err_db': float(np.abs(lp(got[rows, pk]) - lp(ref[rows, pk])).max())}
+
+
+def batched_block(steps, warmup, precision):
+    """64 uneven instances: per-instance CSM of 30 bins (complex64) + one batched tensor-core map, as one
+    CUDA graph.  Accuracy: three instances' maps against the plain FP64 form on the same CSMs."""
     import torch
 
+    from acoular_b200 import device as D
     from acoular_b200 import workloads
     from acoular_b200.batch import BatchPlan, Instance
     dev = torch.device('cuda', 0)
@@ -278,34 +303,51 @@ def run_batched(args):
         insts.append(Instance(samples=x, mpos=wl.mics.pos, gpos=wl.grid.pos, sample_freq=wl.fs,
                               block_size=wl.block_size, bin_lo=int(wl.bins[0]), num_bins=len(wl.bins),
                               precision='complex64'))
-    plan = BatchPlan(insts, tc_precision=args.tc_precision).capture()
-    for _ in range(args.warmup):
+    plan = BatchPlan(insts, tc_precision=precision).capture()
+    for _ in range(max(3, warmup)):
         plan.run()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
         e0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             plan.run()
         e1.record()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = e0.elapsed_time(e1) / steps
     units = plan.units()
+    errs = {}
+    for i in (0, len(wls) // 2, len(wls) - 1):
+        mi = plan.map_instances[i]
+        ref = D.map_f64(mi.csm, mi.wavenumbers, mi.mpos, mi.gpos, mi.steer_type, mi.r_diag, mi.norm,
+                        clip_negative=mi.clip_negative)
+        errs[f'inst{i}'] = dict(_err_vs(plan.out[i].cpu().numpy(), ref.cpu().numpy()), mics=int(wls[i].mics.num_mics),
+                                grid_points=int(wls[i].grid.size))
+    worst = {k: max(e[k] for e in errs.values()) for k in ('max_rel_err', 'rms_rel_err', 'peak_level_err_db')}
     mics = sorted({int(w.mics.num_mics) for w in wls})
-    _line('batched maps grid-pts*bins/s (64 uneven instances, CSM + map, one CUDA graph)', units / (ms / 1e3),
-          UNIT, ms, args, {'workload': 'batched64', 'instances': len(wls), 'mics': mics,
-                           'grid_points': [int(w.grid.size) for w in wls][:8] + ['...'],
-                           'block_sizes': sorted({int(w.block_size) for w in wls}), 'bins_per_instance': 30,
-                           'csm': 'complex64', 'form': f'tc {args.tc_precision}'},
-          units_per_step=units, gpu_launches_per_step='1 graph', clocks=clk.summary(),
-          dtype=f'{args.tc_precision} / f32 accum')
+    return {'value': units / (ms / 1e3), 'unit': UNIT, 'ms_per_step': ms, 'steps': steps, 'units_per_step': units,
+            'config': {'workload': 'batched64', 'instances': len(wls), 'mics': mics,
+                       'grid_points_range': [int(min(w.grid.size for w in wls)), int(max(w.grid.size for w in wls))],
+                       'block_sizes': sorted({int(w.block_size) for w in wls}), 'bins_per_instance': 30,
+                       'csm': 'complex64', 'form': f'tc {precision}', 'steer_type': 'true level', 'r_diag': True},
+            'accuracy': {'vs': 'plain FP64 form on the same CSMs', **worst, 'instances': errs},
+            'gpu_launches_per_step': '1 graph (per instance: FFT, Welch Gram, finalize; 1 batched map)',
+            'clocks': clk.summary(), 'dtype': f'{precision} / f32 accum'}
 
 
-def run_large3d(args):
+def run_batched(args):
+    d = batched_block(args.steps, args.warmup, args.tc_precision)
+    _line('batched maps grid-pts*bins/s (64 uneven instances, CSM + map, one CUDA graph)', d['value'], UNIT,
+          d['ms_per_step'], args, d['config'], units_per_step=d['units_per_step'], accuracy=d['accuracy'],
+          gpu_launches_per_step=d['gpu_launches_per_step'], clocks=d['clocks'], dtype=d['dtype'])
+
+
+def large3d_block(steps, warmup, precision):
     """1024-mic log spiral, 101x101x41 grid, 200 bins in 1-16 kHz, true location, r_diag.
 
     The CSM of the 200 bins is computed once (in contiguous bin chunks, then gathered); the timed step
-    is the tensor-core map over all 200 bins and 418,241 grid points.
+    is the tensor-core map over all 200 bins and 418,241 grid points.  Accuracy and the FP64 form's rate
+    on 3 bins.
     """
     import torch
 
@@ -335,20 +377,19 @@ def run_large3d(args):
     norm = M / (M - 1.0)
 
     def step():
-        D.map_tc(c, k, mpos, gpos, 'true location', True, norm, out=out, precision=args.tc_precision)
+        D.map_tc(c, k, mpos, gpos, 'true location', True, norm, out=out, precision=precision)
 
-    for _ in range(args.warmup):
+    for _ in range(max(3, warmup)):
         step()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
         e0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
         e1.record()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    # accuracy against the plain FP64 form on 3 bins (timed too: the TC/FP64 rate ratio on this shape)
+    ms = e0.elapsed_time(e1) / steps
     sel = torch.as_tensor([0, nb // 2, nb - 1], device=dev)
     cs, ks = c[sel].contiguous(), k[sel].contiguous()
     D.map_f64(cs, ks, mpos, gpos, 'true location', True, norm)
@@ -358,20 +399,26 @@ def run_large3d(args):
     e1.record()
     torch.cuda.synchronize()
     f64_rate = 3 * G / (e0.elapsed_time(e1) / 1e3)
-    ref = ref.cpu().numpy()
-    got = out[sel].cpu().numpy()
-    err = float((np.abs(got - ref) / np.abs(ref).max(axis=1, keepdims=True)).max())
     rate = G * nb / (ms / 1e3)
-    _line('map grid-pts*bins/s (1024 mics, 101x101x41 grid, 200 bins)', rate, UNIT, ms, args,
-          {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': nb, 'block_size': N,
-           'steer_type': 'true location', 'r_diag': True, 'form': f'tc {args.tc_precision}',
-           'csm': 'complex128, computed once outside the timed map steps'},
-          accuracy={'max_rel_err_vs_f64': err, 'bins_checked': 3}, f64_form_rate=f64_rate,
-          tc_over_f64=rate / f64_rate, csm_seconds_once=csm_s, clocks=clk.summary(),
-          dtype=f'{args.tc_precision} / f32 accum')
+    del c
+    return {'value': rate, 'unit': UNIT, 'ms_per_step': ms, 'steps': steps,
+            'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': nb, 'block_size': N,
+                       'steer_type': 'true location', 'r_diag': True, 'form': f'tc {precision}',
+                       'csm': 'complex128, computed once outside the timed map steps'},
+            'accuracy': {'vs': 'plain FP64 form', 'bins': [int(bins[0]), int(bins[nb // 2]), int(bins[-1])],
+                         **_err_vs(out[sel].cpu().numpy(), ref.cpu().numpy())},
+            'f64_form_rate': f64_rate, 'tc_over_f64': rate / f64_rate, 'csm_seconds_once': csm_s,
+            'clocks': clk.summary(), 'dtype': f'{precision} / f32 accum'}
 
 
-def run_serving(args, mixed: bool):
+def run_large3d(args):
+    d = large3d_block(args.steps, args.warmup, args.tc_precision)
+    _line('map grid-pts*bins/s (1024 mics, 101x101x41 grid, 200 bins)', d['value'], UNIT, d['ms_per_step'], args,
+          d['config'], accuracy=d['accuracy'], f64_form_rate=d['f64_form_rate'], tc_over_f64=d['tc_over_f64'],
+          csm_seconds_once=d['csm_seconds_once'], clocks=d['clocks'], dtype=d['dtype'])
+
+
+def serving_block(mixed: bool, duration: float, precision: str, verbose: bool = False):
     """Poisson arrivals from 32 streams, 0.1 s of 51.2 kHz samples per request, one third-octave band."""
     import torch
 
@@ -379,7 +426,7 @@ def run_serving(args, mixed: bool):
     from acoular_b200.serving import BeamformingServer
     rng = np.random.RandomState(7)
     n_streams = 32
-    srv = BeamformingServer(hbm_budget_bytes=120 << 30, tc_precision=args.tc_precision)
+    srv = BeamformingServer(hbm_budget_bytes=120 << 30, tc_precision=precision)
     specs = []
     for i in range(n_streams):
         M = int(rng.choice([64, 128, 256, 512])) if mixed else 64
@@ -402,19 +449,9 @@ def run_serving(args, mixed: bool):
     for f in [srv.submit(i, blocks[i]) for i in range(n_streams)]:
         f.result(timeout=120)
     torch.cuda.synchronize()
-    import gc
-    gc_pauses = []
-
-    def _gc_cb(phase, info, _t=[0.0]):
-        if phase == 'start':
-            _t[0] = time.perf_counter()
-        else:
-            gc_pauses.append((info['generation'], (time.perf_counter() - _t[0]) * 1e3))
-    gc.callbacks.append(_gc_cb)
-    if os.environ.get('ACB_BENCH_GC_FREEZE') == '1':
-        gc.freeze()
     rate = 10.0 * n_streams            # real time: each stream sends 0.1 s of data every 0.1 s
-    t_end = time.perf_counter() + args.duration
+    t_start = time.perf_counter()
+    t_end = t_start + duration
     futs = []
     t_next = time.perf_counter()
     with ClockSampler(0) as clk:
@@ -424,34 +461,166 @@ def run_serving(args, mixed: bool):
             if delay > 0:
                 time.sleep(delay)
             sid = int(rng.randint(n_streams))
-            t0 = time.perf_counter()
-            futs.append((t0, srv.submit(sid, blocks[sid])))
-        for _, f in futs:
+            futs.append(srv.submit(sid, blocks[sid]))
+        for f in futs:
             f.result(timeout=120)
+        t_done = time.perf_counter()
     srv.close()
-    lat = np.array([f.latency for _, f in futs]) * 1e3
-    bt = np.array([b for b in srv.batch_times if b[1] >= futs[0][0]]) if futs else np.zeros((0, 5))
-    if len(bt):
+    lat = np.array([f.latency for f in futs]) * 1e3
+    units = sum(f.units for f in futs) if all(hasattr(f, 'units') for f in futs) else None
+    if verbose and srv.batch_times:
+        bt = np.array(srv.batch_times)
         dur = (bt[:, 4] - bt[:, 1]) * 1e3
         top = np.argsort(dur)[-5:][::-1]
         print('slowest batches (n, inputs+csm issue ms, map issue ms, gpu wait ms):',
               [(int(bt[i, 0]), round((bt[i, 2] - bt[i, 1]) * 1e3, 2), round((bt[i, 3] - bt[i, 2]) * 1e3, 2),
                 round((bt[i, 4] - bt[i, 3]) * 1e3, 2)) for i in top], file=sys.stderr)
-        gaps = np.diff(bt[:, 1]) * 1e3
-        g2 = [ms for g, ms in gc_pauses if g == 2]
-        print(f'gc: {len(gc_pauses)} collections, gen2 {len(g2)} totalling {sum(g2):.1f} ms (max '
-              f'{max(g2) if g2 else 0:.1f} ms); max any {max((m for _, m in gc_pauses), default=0):.1f} ms',
-              file=sys.stderr)
-        print('largest gaps between batch starts (ms):', np.sort(gaps)[-5:].round(2).tolist(), file=sys.stderr)
-    n = len(futs)
+    return {'p50_ms': float(np.percentile(lat, 50)), 'p99_ms': float(np.percentile(lat, 99)),
+            'max_ms': float(lat.max()), 'requests': len(futs),
+            'throughput_req_s': len(futs) / (t_done - t_start),
+            'throughput_grid_pts_bins_s': (units / (t_done - t_start)) if units else None,
+            'mean_batch': float(np.mean(srv.batches)) if srv.batches else None,
+            'config': {'workload': 'serving-mixed' if mixed else 'serving-64mic', 'streams': n_streams,
+                       'mics': sorted({s_[0] for s_ in specs}),
+                       'grid_sides': [min(s_[1] for s_ in specs), max(s_[1] for s_ in specs)],
+                       'block_sizes': sorted({s_[2] for s_ in specs}), 'offered_rate_req_s': rate,
+                       'duration_s': duration, 'arrivals': 'Poisson', 'hbm_budget_gb': 120},
+            'latency': 'wall clock from submit() to the host result, per request',
+            'clocks': clk.summary(), 'dtype': f'{precision} / f32 accum'}
+
+
+def run_serving(args, mixed: bool):
+    d = serving_block(mixed, args.duration, args.tc_precision, verbose=True)
     _line('serving latency p50/p99 ms (Poisson arrivals, 32 streams, 0.1 s requests, one third-octave band)',
-          float(np.percentile(lat, 99)), 'ms (p99)', float(np.percentile(lat, 50)), args,
-          {'workload': 'serving-mixed' if mixed else 'serving-64mic', 'streams': n_streams,
-           'mics': sorted({s[0] for s in specs}), 'grid_sides': [min(s[1] for s in specs), max(s[1] for s in specs)],
-           'block_sizes': sorted({s[2] for s in specs}), 'offered_rate_req_s': rate, 'duration_s': args.duration},
-          higher_is_better=False, p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
-          max_ms=float(lat.max()), requests=n, mean_batch=float(np.mean(srv.batches)) if srv.batches else None,
-          clocks=clk.summary(), dtype=f'{args.tc_precision} / f32 accum')
+          d['p99_ms'], 'ms (p99)', d['p50_ms'], args, d['config'], higher_is_better=False, p50_ms=d['p50_ms'],
+          p99_ms=d['p99_ms'], max_ms=d['max_ms'], requests=d['requests'], throughput_req_s=d['throughput_req_s'],
+          throughput_grid_pts_bins_s=d['throughput_grid_pts_bins_s'], mean_batch=d['mean_batch'],
+          clocks=d['clocks'], dtype=d['dtype'])
+
+
+STEER_TYPES = ('classic', 'inverse', 'true level', 'true location')
+
+
+def precision_matrix_block(csm64, kvec, mpos, gpos, acc_bins):
+    """Every steering type x r_diag x tensor-core precision on the 256-mic workload's FP64 CSM (all bins,
+    timed), each against the plain FP64 form on the bins ``acc_bins`` (errors) -- the map-only error of
+    each tensor-core form -- and the rate ratio of the two forms (``tc_over_f64``)."""
+    import torch
+
+    from acoular_b200 import device as D
+    dev = csm64.device
+    nb, M, _ = csm64.shape
+    G = gpos.shape[1]
+    sel = torch.as_tensor(acc_bins, device=dev)
+    cs, ks = csm64[sel].contiguous(), kvec[sel].contiguous()
+    o = torch.empty((nb, G), dtype=torch.float64, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        r = fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]), r
+
+    entries = {}
+    for st in STEER_TYPES:
+        for rd in (True, False):
+            norm = M / (M - 1.0) if rd else 1.0
+            f64_ms, ref = timed(lambda: D.map_f64(cs, ks, mpos, gpos, st, rd, norm))
+            ref = ref.cpu().numpy()
+            f64_rate = len(acc_bins) * G / (f64_ms / 1e3)
+            for pr in ('tf32', 'bf16x3'):
+                tc_ms, _ = timed(lambda: D.map_tc(csm64, kvec, mpos, gpos, st, rd, norm, out=o, precision=pr))
+                rate = nb * G / (tc_ms / 1e3)
+                entries[f'{st}|r_diag={rd}|{pr}'] = dict(_err_vs(o[sel].cpu().numpy(), ref), tc_rate=rate,
+                                                         f64_rate=f64_rate, tc_over_f64=rate / f64_rate)
+    worst = {k: max(e[k] for e in entries.values()) for k in ('max_rel_err', 'rms_rel_err', 'peak_level_err_db')}
+    return {'vs': 'plain FP64 form (FP64 phase, libm-faithful float32 cos/sin) on the same FP64 CSM',
+            'bins': [int(b) for b in acc_bins], 'worst': worst,
+            'min_tc_over_f64': min(e['tc_over_f64'] for e in entries.values()),
+            'definition': 'max/rms of |tc - f64| / max|f64| per bin over the listed bins; L_p difference at the '
+                          'FP64 peak; tc_rate over all bins, f64_rate over the listed bins',
+            'entries': entries}
+
+
+def config1_block(steps, warmup):
+    """The 64-mic, 41x41 workload (three monopoles, 51,200 samples, block 128, Hanning, 50 %): the full
+    complex128 CSM (65 bins, 799 windows) and the plain FP64 map of the 8 kHz third-octave band (5 bins,
+    'true level', r_diag) summed as BeamformerBase.synthetic sums it.  Device-timed with the samples
+    resident, end to end through PowerSpectra + BeamformerBase.synthetic from host samples, and the CPU
+    oracle on all host threads; the device band map against the oracle's."""
+    import torch
+
+    import acoular_b200 as ac
+    from acoular_b200 import device as D
+    from acoular_b200 import workloads
+    from oracle import oracle as O
+    dev = torch.device('cuda', 0)
+    wl = workloads.three_sources_64()
+    data = wl.time_data()
+    M, G, N = wl.mics.num_mics, wl.grid.size, wl.block_size
+    F = N // 2 + 1
+    freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[:F])
+    bins = np.arange(int(np.searchsorted(freqs, 8000.0 * 2.0 ** (-0.5 / 3))),
+                     int(np.searchsorted(freqs, 8000.0 * 2.0 ** (0.5 / 3))))
+    x = torch.as_tensor(data, device=dev)
+    mpos, gpos = torch.as_tensor(wl.mics.pos, device=dev), torch.as_tensor(wl.grid.pos, device=dev)
+    bsel = torch.as_tensor(bins, device=dev)
+    kb = torch.as_tensor(2 * np.pi * freqs[bins] / wl.c, device=dev)
+    norm = M / (M - 1.0)
+
+    def step():
+        csm = D.calc_csm(x, N, 'Hanning', '50%', 'complex128')
+        return D.map_f64(csm[bsel].contiguous(), kb, mpos, gpos, 'true level', True, norm, clip_negative=True).sum(0)
+
+    for _ in range(max(3, warmup)):
+        band = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        band = step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    got = band.cpu().numpy()
+    e2e = []
+    for it in range(4):
+        t0 = time.perf_counter()
+        ps = ac.PowerSpectra(source=ac.TimeSamples(data=data, sample_freq=wl.fs), block_size=N, window='Hanning',
+                             overlap='50%')
+        bf = ac.BeamformerBase(freq_data=ps, steer=ac.SteeringVector(grid=wl.grid, mics=wl.mics,
+                                                                     steer_type='true level'), r_diag=True)
+        syn = bf.synthetic(8000.0, 3)
+        if it:
+            e2e.append(time.perf_counter() - t0)
+    O.set_num_threads(len(os.sched_getaffinity(0)))
+    r0, rm = O.apparent_r(wl.grid.pos), O.apparent_r(wl.grid.pos, wl.mics.pos)
+    cpu = []
+    for it in range(3):
+        t0 = time.perf_counter()
+        c_ref = O.calc_csm(data, N, 'Hanning', '50%', 'complex128')
+        ref = O.beamformer_calc(c_ref, freqs, bins, r0, rm, wl.c, 'true level', True)[bins].sum(0)
+        if it:
+            cpu.append(time.perf_counter() - t0)
+    units = G * len(bins)
+    err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    err_e2e = float(np.abs(np.asarray(syn).ravel() - ref).max() / np.abs(ref).max())
+    return {'value': units / (ms / 1e3), 'unit': UNIT, 'ms_per_step': ms, 'steps': steps,
+            'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'csm_bins': F, 'map_bins': [int(b) for b in bins],
+                       'block_size': N, 'windows': D.num_windows(wl.num_samples, N, 2), 'steer_type': 'true level',
+                       'r_diag': True, 'form': 'f64', 'csm': 'complex128'},
+            'e2e': {'value': units / float(np.median(e2e)), 'unit': UNIT, 'ms': float(np.median(e2e)) * 1e3,
+                    'h2d_bytes_per_step': int(data.nbytes), 'd2h_bytes_per_step': int(G * 8),
+                    'api': 'TimeSamples -> PowerSpectra -> BeamformerBase.synthetic(8000, 3)'},
+            'cpu_baseline': {'value': units / float(np.median(cpu)), 'unit': UNIT, 'ms': float(np.median(cpu)) * 1e3,
+                             'cores': O.num_threads(), 'kind': 'port',
+                             'sample': 'the whole step: CSM of 799 windows x 65 bins + the 5-bin band map'},
+            'accuracy': {'vs': 'oracle', 'max_rel_err': err, 'e2e_max_rel_err': err_e2e},
+            'gpu_launches_per_step': 4, 'dtype': 'f64'}
 
 
 def run_eig(args):
@@ -969,6 +1138,9 @@ def main():
         accuracy = {'vs': 'FP64 CSM + plain FP64 map (the reference arithmetic on the GPU)',
                     'timed_path': f'{csm_prec} CSM + tc {prec} map', 'bins': acc_bins.tolist(), **acc_of(out),
                     'definition': '|map - ref| / max|ref| per bin; L_p difference at the reference peak'}
+    pmatrix = None
+    if form != 'f64' and not args.no_extra and rank == 0:
+        pmatrix = precision_matrix_block(csm64, kvec, mpos, gpos, acc_bins)
 
     # map kernel roofline: algorithmic flops 8 M^2 + 8 M per grid-pt x bin
     pk = peaks()
@@ -1022,6 +1194,19 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(wl, args.steer)
 
+    # the other configurations, each timed on its own (rank 0 at N = 1): their rates, errors and latencies
+    extra = {}
+    if rank == 0 and ws == 1 and not args.no_extra:
+        del samples, csm_up, csm_full, out, csm64, cs, ks
+        torch.cuda.empty_cache()
+        extra['config1'] = config1_block(20, 3)
+        extra['batched64'] = batched_block(10, 3, prec)
+        torch.cuda.empty_cache()
+        extra['large3d'] = large3d_block(2, 3, prec)
+        torch.cuda.empty_cache()
+        extra['serving'] = serving_block(False, 5.0, prec)
+        extra['serving_mixed'] = serving_block(True, 5.0, prec)
+
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': ws, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
@@ -1039,6 +1224,9 @@ def main():
                 'forms': forms, 'gemm_peaks_here': gp,
                 'roofline': roof, 'accuracy': accuracy, 'cpu_baseline': cpu, 'e2e': e2e,
                 'gpu_launches': None, 'clocks': clk.summary()}
+        if pmatrix is not None:
+            line['precision_matrix'] = pmatrix
+        line.update(extra)
         line['gpu_launches'] = launches_per_step(F, nbins, K, M) * args.steps
         print(json.dumps(line), flush=True)
     if ws > 1:

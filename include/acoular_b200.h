@@ -60,8 +60,13 @@ int acb_calc_csm_c128(void *csm, const void *spec, int num_freqs, int num_mics, 
 /* Same for complex64 CSM and spectra. */
 int acb_calc_csm_c64(void *csm, const void *spec, int num_freqs, int num_mics, void *stream);
 
-/* Bytes of workspace acb_csm_accumulate needs for `num_windows` windows of `num_bins` bins. */
+/* Bytes of workspace acb_csm_accumulate needs for `num_windows` windows of `num_bins` bins, for
+ * block sizes up to 16384 (the spectra of the chunk). */
 size_t acb_csm_workspace_bytes(int num_mics, int num_bins, int64_t num_windows, int precision);
+/* The same for any block size: blocks of 32768 and 65536 samples (the largest of the reference's
+ * block_size choices, acoular/spectra.py:105-116) add a scratch region for the FFT's sub-spectra,
+ * num_windows * num_mics * block_size / 2 complex doubles. */
+size_t acb_csm_workspace_bytes_block(int num_mics, int num_bins, int64_t num_windows, int precision, int block_size);
 
 /* Welch accumulation of PowerSpectra.calc_csm (acoular/spectra.py:366-416, windows as yielded by
  * BaseSpectra._get_source_data, acoular/spectra.py:171-184):
@@ -74,7 +79,7 @@ size_t acb_csm_workspace_bytes(int num_mics, int num_bins, int64_t num_windows, 
  * window: float64 [block_size].  twiddle: complex128 [block_size/2], exp(-2*pi*i*k/block_size).
  * csm_upper: [num_bins][num_mics][num_mics] in `precision` (complex128 for the tensor-core forms,
  * num_mics <= 4032 there); only r <= c is written.
- * block_size: power of two, 16 <= block_size <= 16384.  workspace: >= acb_csm_workspace_bytes. */
+ * block_size: power of two, 16 <= block_size <= 65536.  workspace: >= acb_csm_workspace_bytes_block. */
 int acb_csm_accumulate(const void *samples, int sample_dtype, int64_t num_samples, int num_mics,
                        int block_size, int hop, int64_t first_window, int64_t num_windows,
                        const double *window, const void *twiddle, int bin_lo, int num_bins,
@@ -171,6 +176,14 @@ enum acb_tc_precision {
 /* Bytes of workspace acb_map_tc needs (the per-bin split-BF16 copy of the real-embedded CSM). */
 size_t acb_map_tc_workspace_bytes(int num_mics, int num_bins, int precision);
 
+/* Limit of each bounded device-side wait in the tensor-core kernels (acb_map_tc, acb_map_tc_batch,
+ * acb_map_tc_noalloc and the tensor-core CSM forms of acb_csm_accumulate); no counterpart in the
+ * reference.  A wait that runs out sets the launch's error word to 1 (where one is given), the CTA
+ * lets its own copies and MMAs finish, frees its tensor memory and exits, so the device context stays
+ * usable.  Applies to launches enqueued after the call; 0 restores the default of 0.5 s.  Returns
+ * the previous limit.  Process-wide (all devices and host threads). */
+uint64_t acb_tc_set_wait_limit_ns(uint64_t limit_ns);
+
 /* Tensor-core form of the same map (acoular/fastFuncs.py:217-311 semantics, same arguments and
  * outputs as acb_map_f64): the quadratic form h^H C h is evaluated as the real quadratic form
  * v^T R v of the 2M-dimensional real embedding, R = [[Re C, -Im C], [Im C, Re C]], on tcgen05
@@ -245,7 +258,7 @@ size_t acb_spectra_workspace_bytes(int num_mics, int block_size, int64_t num_win
  *   out[w][f][m] = rfft(samples[w*hop : w*hop + block_size, m] * window)[f], f = 0 .. block_size/2,
  *   rounded to `precision` (ACB_C128 / ACB_C64); bins 1 .. block_size/2 - 1 doubled when double_inner
  *   (scaling 'energy' / 'amplitude'), then times `scale`, both in the output precision.
- * block_size: power of two, 16 .. 16384 (other even sizes: ACB_ERR_SHAPE / ACB_ERR_UNSUPPORTED). */
+ * block_size: power of two, 16 .. 65536 (other even sizes: ACB_ERR_SHAPE / ACB_ERR_UNSUPPORTED). */
 int acb_spectra(const void *samples, int sample_dtype, int64_t num_samples, int num_mics, int block_size, int hop,
                 int64_t first_window, int64_t num_windows, const double *window, const void *twiddle, int precision,
                 double scale, int double_inner, void *out, void *workspace, size_t workspace_bytes, void *stream);
@@ -280,6 +293,15 @@ int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber
                     const double *gpos, const double *r0, const double *rm, int n_iter, double damp, int stopn,
                     float *result, void *workspace, size_t workspace_bytes, void *stream);
 
+/* BeamformerCleansc._calc (acoular/fbeamform.py:1424-1490) with a steering object other than the plain
+ * SteeringVector (custom steering, as _beamformer_params routes it, acoular/fbeamform.py:470-472):
+ * steer complex128 [B][G][M] = the object's steer_vector(f) of each bin; the maps are the custom-steering
+ * forms of beamformerFreq (acoular/fastFuncs.py:414-559) and the peak's vector is row xi of steer.
+ * csm, n_iter, damp, stopn, result as acb_cleansc_f64 (p->steer_type, ref, glibc_faithful ignored); the
+ * workspace may omit the steering region: acb_cleansc_workspace_bytes - 16 G M B bytes suffice. */
+int acb_cleansc_custom_f64(const acb_map_params *p, void *csm, const void *steer, int n_iter, double damp, int stopn,
+                           float *result, void *workspace, size_t workspace_bytes, void *stream);
+
 /* Size of the fixed device array behind acb_map_tc_noalloc (32 MiB per GPU, held until exit). */
 #define ACB_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 
@@ -291,8 +313,11 @@ int acb_cleansc_f64(const acb_map_params *p, void *csm, const double *wavenumber
  * Limit: acb_map_tc_workspace_bytes(num_mics, num_bins, precision) must not exceed
  * ACB_NOALLOC_SCRATCH_BYTES (e.g. 60 bins at 256 mics); larger requests return ACB_ERR_SHAPE before
  * any work is enqueued -- split the bins over several calls.
+ * Argument errors return the same status codes as acb_map_tc.
  * The first call on a device looks up the array's device address (once per device, with that
- * device current); make that first call before capturing a stream.
+ * device current) and keeps it for the life of the process; make that first call before capturing a
+ * stream, and do not call this entry point again on a device after a cudaDeviceReset of it (the
+ * reset unloads the array and the kept address goes stale).
  * All calls share the one array: calls whose GPU work overlaps (different streams, or different
  * host threads on one device) race on it; order them on one stream. */
 int acb_map_tc_noalloc(const acb_map_params *p, int precision, const void *csm, const double *wavenumber,

@@ -467,6 +467,50 @@ def beamformer_cleansc_calc(csm, freqs, ind, r0, rm, c: float, steer_type: str, 
     return out
 
 
+def beamformer_cleansc_custom_calc(csm, freqs, ind, steer_vectors, r_diag: bool, n_iter: int = 0, damp: float = 0.6,
+                                   stopn: int = 3, r_diag_norm: float = 0.0, out=None):
+    """``BeamformerCleansc._calc`` (acoular/fbeamform.py:1424-1490) with a steering object of its own
+    (``_beamformer_params`` routes it as 'custom', acoular/fbeamform.py:470-472): ``steer_vectors(f)`` gives
+    its (G, M) steering vectors; the maps are beamformerFreq('custom', ...) and the peak's vector is row
+    xi_max of the same matrix (the object's steer_vector(f, xi_max))."""
+    M = csm.shape[-1]
+    normfactor = sig_loss_norm(r_diag, M, r_diag_norm)
+    J = M * 2 if not n_iter else n_iter
+    powers = np.zeros(J, 'd')
+    res = None
+    for i in ind:
+        sv = np.ascontiguousarray(steer_vectors(freqs[i]), dtype=np.complex128)
+        G = sv.shape[0]
+        if out is None:
+            out = np.zeros((csm.shape[0], G))
+        if res is None:
+            res = np.zeros(G, 'f')
+        cs = np.array(csm[i], dtype='complex128', copy=True)
+        h = beamformer_freq_custom(r_diag, normfactor, sv, csm=cs)[0]
+        res *= 0.0
+        for j in range(J):
+            xi_max = h.argmax()
+            powers[j] = hmax = h[xi_max]
+            res[xi_max] += damp * hmax
+            if j > stopn and hmax > powers[j - stopn]:
+                break
+            wmax = (sv[xi_max:xi_max + 1] * np.sqrt(normfactor))[0].conj()
+            hh = wmax.copy()
+            D1 = np.dot(cs.T - np.diag(np.diag(cs)), wmax) / hmax
+            ww = wmax.conj() * wmax
+            for _ in range(20):
+                H = hh.conj() * hh
+                hh = (D1 + H * wmax) / np.sqrt(1 + np.dot(ww, H))
+            hh = hh[:, np.newaxis]
+            csm1 = hmax * (hh * hh.conj().T)
+            h1 = beamformer_freq_custom(r_diag, normfactor, sv, eig=(np.array((hmax,)),
+                                                                    np.ascontiguousarray(hh.conj())))[0]
+            h -= damp * h1
+            cs -= damp * csm1.T
+        out[i] = res
+    return out
+
+
 # ----------------------------------------------------------------------------------------------
 # Block-wise spectra generators (acoular/fprocess.py)
 # ----------------------------------------------------------------------------------------------

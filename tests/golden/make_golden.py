@@ -1,9 +1,9 @@
 """Generate the golden fixtures in this folder by running the reference's own code.
 
-Run once, in a container that holds the reference sources (default location below, or
-``ACOULAR_REFERENCE``)::
+Run once, in a container that holds the reference sources, with ``ACOULAR_REFERENCE`` naming the
+reference checkout (the folder that contains the ``acoular`` package)::
 
-    python tests/golden/make_golden.py
+    ACOULAR_REFERENCE=<path to the acoular checkout> python tests/golden/make_golden.py
 
 The reference (Acoular 26.08) cannot be imported whole here (``traits``/``tables`` are absent), so
 this script loads its numba kernel module ``acoular/fastFuncs.py`` (+ ``internal.py``) under a stub
@@ -21,8 +21,9 @@ their decorators removed, bound to plain stand-in objects:
 * ``UniformFlowEnvironment.apparent_r``               acoular/environments.py:290-332
 * ``SteeringVector._steer_funcs_freq`` (as source text) acoular/fbeamform.py:145-153
 * ``PointSpreadFunction._psf_call``, ``BeamformerDamas._calc``   acoular/fbeamform.py:1096-1125, 1167-1208
-* ``BeamformerFunctional._calc``, ``BeamformerOrth._calc``, ``BeamformerCleansc._calc``,
-  ``SteeringVector.transfer`` / ``steer_vector``    acoular/fbeamform.py:712-786, 1366-1490, 207-258
+* ``BeamformerFunctional._calc``, ``BeamformerOrth._calc``, ``BeamformerCleansc._calc`` (also with a
+  custom steering object), ``SteeringVector.transfer`` / ``steer_vector``   acoular/fbeamform.py:712-786,
+  1366-1490, 207-258
 * ``RFFT.result`` / ``_scale``, ``AutoPowerSpectra._get_scaling_value`` / ``result``,
   ``CrossPowerSpectra.result``                        acoular/fprocess.py:35-181, 286-467
 * ``SlotJet.v``, ``OpenJet.v``, ``RotatingFlow.v``, ``spiral_sphere``, ``GeneralFlowEnvironment.apparent_r`` /
@@ -50,7 +51,9 @@ import scipy.linalg as spla
 from scipy import fft
 from scipy.signal import resample
 
-REF = Path(os.environ.get('ACOULAR_REFERENCE', '/root/reference'))
+if 'ACOULAR_REFERENCE' not in os.environ:
+    raise SystemExit('set ACOULAR_REFERENCE to the reference checkout (the folder holding the acoular package)')
+REF = Path(os.environ['ACOULAR_REFERENCE'])
 OUT = Path(__file__).resolve().parent
 sys.path.insert(0, str(OUT.parent.parent))
 
@@ -618,6 +621,48 @@ def golden_functional_orth_cleansc():
     print('functional_orth_cleansc_kat.npz written', len(out), 'arrays')
 
 
+class SteerShaded(SteerFull):
+    """A steering object of its own (a SteeringVector subclass): the reference's steer_vector shaded by a
+    per-mic weight; BeamformerCleansc routes it through the custom-steering kernels."""
+
+    def steer_vector(self, f, ind=None):
+        return sv_steer_vector(self, f, ind) * self.shade[np.newaxis, :]
+
+
+def cleansc_shade(M):
+    """Per-mic shading of the custom steering object in cleansc_custom_kat.npz (a Hann taper over the mics)."""
+    return 0.5 + 0.5 * np.cos(np.pi * (np.arange(M) - (M - 1) / 2) / M)
+
+
+def golden_cleansc_custom():
+    """BeamformerCleansc._calc (fbeamform.py:1424-1490) with a steering object other than the plain
+    SteeringVector: _beamformer_params gives ('custom', steer.steer_vector) (fbeamform.py:470-472), so the
+    maps use beamformerFreq('custom', ...) and the peak's vector is the object's steer_vector(f, xi)."""
+    small = np.load(OUT / 'small_kat.npz')
+    csm, freqs, mpos, gpos = small['csm0'], small['freqs0'], small['mpos'], small['gpos']
+    ind = np.array([12, 20, 28])
+    out = {'bins': ind}
+    env = Env(c=343.0)
+    r0, rm = apparent_r(env, gpos), np.atleast_2d(apparent_r(env, gpos, mpos))
+    M = mpos.shape[1]
+    for st in ('true level', 'classic'):
+        steer = SteerShaded(steer_type=st, r0=r0, rm=rm, env=env, _steer_funcs_freq=_steer_funcs_freq(),
+                            grid=SimpleNamespace(size=gpos.shape[1]), mics=SimpleNamespace(num_mics=M),
+                            shade=cleansc_shade(M))
+        for rd in (False, True):
+            for n_iter, damp, stopn in ((0, 0.6, 3), (10, 0.9, 4)):
+                bf = SimpleNamespace(_f=freqs, r_diag=rd, r_diag_norm=0.0, steer=steer, n_iter=n_iter, damp=damp,
+                                     stopn=stopn, freq_data=SimpleNamespace(num_channels=M, csm=csm))
+                bf.sig_loss_norm = lambda bf=bf: sig_loss_norm(bf)
+                bf._beamformer_params = lambda steer=steer: ('custom', steer.steer_vector)
+                bf._ac = np.zeros((csm.shape[0], gpos.shape[1]))
+                bf._fr = np.zeros(csm.shape[0], dtype='int8')
+                cleansc_calc(bf, ind)
+                out[f'{st.replace(" ", "_")}_{int(rd)}_{n_iter}_{damp:g}_{stopn}'] = bf._ac[ind]
+    np.savez_compressed(OUT / 'cleansc_custom_kat.npz', **out)
+    print('cleansc_custom_kat.npz written', len(out), 'arrays')
+
+
 class RfftStandIn(SimpleNamespace):
     """RFFT (fprocess.py:35-181) over a Samples source, with the reference's generator and scaling."""
 
@@ -710,6 +755,9 @@ if __name__ == '__main__':
     if os.environ.get('ACB_GOLDEN_ONLY') == 'fprocess':
         golden_fprocess()
         sys.exit(0)
+    if os.environ.get('ACB_GOLDEN_ONLY') == 'cleansc_custom':
+        golden_cleansc_custom()
+        sys.exit(0)
     if os.environ.get('ACB_GOLDEN_ONLY') == 'functional_orth_cleansc':
         golden_functional_orth_cleansc()
         sys.exit(0)
@@ -730,5 +778,6 @@ if __name__ == '__main__':
     golden_custom_flow()
     golden_psf_damas()
     golden_functional_orth_cleansc()
+    golden_cleansc_custom()
     golden_fprocess()
     golden_general_flow()

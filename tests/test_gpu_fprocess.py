@@ -110,3 +110,18 @@ def test_edge_cases(src):
     ref = np.concatenate(list(O.cross_power_blocks([spec], 33, 1, O.power_scale(64, float(s['fs']), 'power', True),
                                                    'complex128')))
     assert np.abs(full - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_rfft_large_block():
+    """RFFT with a 32768-sample block (sub-transforms of 8192 points and a combining pass) against the
+    oracle's generator, complex128 at 1e-12 of each block's max."""
+    import acoular_b200 as ac
+    rng = np.random.RandomState(11)
+    data = rng.randn(3 * 32768, 3)
+    ts = ac.TimeSamples(data=data, sample_freq=48000.0)
+    rf = ac.RFFT(source=ts, block_size=32768, window='Hanning', overlap='50%', scaling='amplitude')
+    got = list(rf.result(2))
+    ref = list(O.rfft_blocks(data, 32768, 'Hanning', '50%', 'complex128', 'amplitude', 2))
+    assert [b.shape for b in got] == [b.shape for b in ref]
+    for a, b in zip(got, ref):
+        _close(a, b, 1e-12)

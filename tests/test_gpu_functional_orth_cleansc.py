@@ -135,3 +135,30 @@ def test_cleansc_errors(cases):
     bf = ac.BeamformerCleansc(freq_data=ps, steer=MySteer(grid=grid, mics=mics))
     with pytest.raises(NotImplementedError):
         bf.result[20]
+
+
+def test_cleansc_custom_steering_object(golden):
+    """BeamformerCleansc with a steering object of its own (a SteeringVector subclass whose steer_vector is
+    the plain one shaded per mic) runs the custom-steering iterations (acb_cleansc_custom_f64) and gives the
+    reference's result on that object (tests/golden/cleansc_custom_kat.npz): the same peaks, <= 1e-5 of max."""
+    import acoular_b200 as ac
+    s = golden('small_kat.npz')
+    g = golden('cleansc_custom_kat.npz')
+    M = s['mpos'].shape[1]
+    shade = 0.5 + 0.5 * np.cos(np.pi * (np.arange(M) - (M - 1) / 2) / M)
+
+    class ShadedSteering(ac.SteeringVector):
+        def steer_vector(self, f, ind=None):
+            return super().steer_vector(f, ind) * shade[np.newaxis, :]
+
+    ps = ac.PowerSpectraImport(csm=s['csm0'], frequencies=s['freqs0'])
+    ind = g['bins']
+    for st in ('true level', 'classic'):
+        steer = ShadedSteering(grid=ac.ImportGrid(pos=s['gpos']), mics=ac.MicGeom(pos_total=s['mpos']), steer_type=st)
+        for rd in (False, True):
+            for n_iter, damp, stopn in ((0, 0.6, 3), (10, 0.9, 4)):
+                bf = ac.BeamformerCleansc(freq_data=ps, steer=steer, r_diag=rd, n_iter=n_iter, damp=damp, stopn=stopn)
+                got = np.array([bf.result[int(i)] for i in ind])
+                ref = g[f'{st.replace(" ", "_")}_{int(rd)}_{n_iter}_{damp:g}_{stopn}']
+                assert np.array_equal(got != 0, ref != 0), (st, rd, n_iter)
+                assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max(), (st, rd, n_iter)

@@ -64,7 +64,7 @@ def test_csm_float32_samples_and_bin_subset(dev):
 
 
 @pytest.mark.parametrize('M,N,ov', [(1, 128, 'None'), (2, 16, '50%'), (65, 512, '87.5%'), (130, 2048, '50%'),
-                                    (7, 16384, 'None')])
+                                    (7, 16384, 'None'), (3, 32768, '50%'), (33, 65536, '75%')])
 def test_csm_shapes(dev, M, N, ov):
     from acoular_b200 import device as D
     rng = np.random.RandomState(M + N)
@@ -73,6 +73,28 @@ def test_csm_shapes(dev, M, N, ov):
     ref = O.calc_csm(data, N, 'Blackman', ov, 'complex128')
     got = D.calc_csm(torch.as_tensor(data, device=dev), N, 'Blackman', ov).cpu().numpy()
     assert rel(got, ref) <= 1e-12
+
+
+def test_csm_large_blocks_all_forms(dev):
+    """Blocks of 32768 and 65536 samples (sub-transforms of 8192 points and a combining pass) in every CSM
+    form and a bin subset: complex128 against the oracle at 1e-12, complex64 at 1e-5, the tensor-core
+    Grams within their bars of the complex128 CSM."""
+    from acoular_b200 import device as D
+    for N, M in ((32768, 5), (65536, 40)):
+        rng = np.random.RandomState(N + M)
+        data = rng.randn(3 * N, M).astype(np.float32)
+        ref = O.calc_csm(data.astype(np.float64), N, 'Hanning', '50%', 'complex128')
+        x = torch.as_tensor(data, device=dev)
+        lo, nb = N // 8, 300
+        got = D.calc_csm(x, N, 'Hanning', '50%', 'complex128', bin_lo=lo, num_bins=nb).cpu().numpy()
+        assert rel(got, ref[lo:lo + nb]) <= 1e-12
+        got64 = D.calc_csm(x, N, 'Hanning', '50%', 'complex64', bin_lo=lo, num_bins=nb).cpu().numpy()
+        assert rel(got64, ref[lo:lo + nb]) <= 1e-5
+        for prec, tol in (('tc_tf32', 2e-3), ('tc_bf16x3', 1e-4)):
+            up, K = D.csm_upper_accumulate(x, N, 'Hanning', '50%', precision=prec, bin_lo=lo, num_bins=nb)
+            _, w = D.window_vector('Hanning', N, dev)
+            full = D.csm_finalize(up, 2.0 / N / w / D.num_blocks(3 * N, N, 2)).cpu().numpy()
+            assert rel(full, ref[lo:lo + nb]) <= tol, prec
 
 
 def test_csm_config1_band(golden, dev):

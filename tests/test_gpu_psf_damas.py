@@ -63,6 +63,24 @@ def test_psf_kernel_vs_reference(small, st):
         assert _rel(got, O.psf(st, r0, rm, kk, g['src'])) <= TOL
 
 
+@pytest.mark.parametrize('M', [45, 300])
+@pytest.mark.parametrize('st', STEERS)
+def test_psf_kernel_mic_counts(st, M):
+    """Mic counts past one 32-mic group and not a multiple of 32 (45: a partial last group), and past one
+    256-mic shared-memory chunk (300: a second chunk, itself partial), against the oracle at 1e-10."""
+    from acoular_b200 import device as D
+    rng = np.random.RandomState(M)
+    mpos = np.vstack([rng.uniform(-0.6, 0.6, (2, M)), rng.uniform(-0.02, 0.02, (1, M))])
+    g = np.linspace(-0.3, 0.3, 17)
+    gx, gy = np.meshgrid(g, g, indexing='ij')
+    gpos = np.vstack([gx.ravel(), gy.ravel(), np.full(gx.size, 0.8)])
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    src = np.array([0, 50, 144, 288])
+    for k in (3.0, 90.0):
+        got = D.psf_f64(_dev(r0), _dev(rm), k, _dev(src), st).cpu().numpy()
+        assert _rel(got, O.psf(st, r0, rm, k, src)) <= TOL
+
+
 def test_psf_source_index_checks(small):
     """Host indices outside the grid raise; device indices outside it give NaN columns (no stray read)."""
     from acoular_b200 import device as D

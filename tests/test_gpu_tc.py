@@ -228,3 +228,42 @@ def test_tc_split_graph_replay_and_mix():
     torch.cuda.synchronize()
     for it, a in zip(its, alone):
         assert torch.equal(it.out, a)
+
+
+@pytest.fixture(scope='module')
+def precision256_reduced():
+    """The 256-mic workload's geometry and sources (256 mics in a 1 m disk, 8 monopoles at z = -1 m, 10 s
+    at 51.2 kHz, block 1024, Hanning, 50 %) with its grid reduced to 101 x 101 points over [-1, 1]^2 and
+    8 bins spread over the band; the complex128 CSM comes from the device path (itself pinned to the
+    oracle to 1e-12 elsewhere) and is handed to the oracle as is."""
+    from acoular_b200 import device as D
+    from acoular_b200 import workloads
+    from acoular_b200.grids import RectGrid
+    wl = workloads.precision_256()
+    dev = torch.device('cuda')
+    x = workloads.monopole_time_data_torch(wl, device=dev)
+    N = wl.block_size
+    bins = np.array([20, 80, 150, 220, 290, 360, 430, 500])
+    csm = D.calc_csm(x, N, 'Hanning', '50%', 'complex128')[torch.as_tensor(bins, device=dev)].contiguous()
+    del x
+    grid = RectGrid(x_min=-1.0, x_max=1.0, y_min=-1.0, y_max=1.0, z=-1.0, increment=0.02)
+    freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[bins])
+    return wl.mics.pos, grid.pos, freqs, csm.cpu().numpy()
+
+
+@pytest.mark.parametrize('precision', ['tf32', 'bf16x3'])
+@pytest.mark.parametrize('steer', STEERS)
+def test_precision_matrix_256mic_reduced_grid(precision256_reduced, steer, precision):
+    """The precision matrix of the 256-mic workload at a reduced size: each steering type x r_diag x
+    tensor-core precision against the FP64 oracle, <= 1e-3 of max and <= 0.05 dB at each bin's peak."""
+    mpos, gpos, freqs, csm = precision256_reduced
+    assert gpos.shape[1] == 101 * 101
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    nb = len(freqs)
+    for r_diag in (True, False):
+        ref = O.beamformer_calc(csm, freqs, range(nb), r0, rm, 343.0, steer, r_diag)
+        got = _tc(csm, freqs, mpos, gpos, steer, r_diag, precision=precision)
+        for b in range(nb):
+            assert rel(got[b], ref[b]) <= TOL, (b, r_diag, rel(got[b], ref[b]))
+            pk = ref[b].argmax()
+            assert abs(O.L_p(got[b][pk:pk + 1]) - O.L_p(ref[b][pk:pk + 1]))[0] <= 0.05

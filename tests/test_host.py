@@ -40,7 +40,7 @@ def test_argument_errors_are_reported_without_a_gpu(native):
     p.steer_type = 9
     assert native.acb_map_f64(ctypes.byref(p), 1, 1, 1, 1, 1, None, None, None) == 2
     # block size beyond the FFT kernel, non power of two, window range past the samples
-    assert native.acb_csm_accumulate(1, 0, 100000, 4, 32768, 16384, 0, 2, 1, 1, 0, 3, 0, 1, 1, 1 << 30, None) == 4
+    assert native.acb_csm_accumulate(1, 0, 300000, 4, 131072, 65536, 0, 2, 1, 1, 0, 3, 0, 1, 1, 1 << 30, None) == 4
     assert native.acb_csm_accumulate(1, 0, 100000, 4, 1000, 500, 0, 2, 1, 1, 0, 3, 0, 1, 1, 1 << 30, None) == 1
     assert native.acb_csm_accumulate(1, 0, 1000, 4, 512, 256, 0, 4, 1, 1, 0, 3, 0, 1, 1, 1 << 30, None) == 1
     assert native.acb_csm_accumulate(1, 0, 10000, 4, 512, 256, 0, 4, 1, 1, 0, 3, 0, 1, 1, 10, None) == 5
@@ -198,3 +198,33 @@ def test_committed_tuning_table_is_valid():
         assert prec in ('bf16x3', 'tf32') and ib in ('tiny', 'few', 'mid', 'many')
         assert (ent['pass_chunks'], ent['splits']) in A.candidates(M)
         assert ent['ms'] == min(ent['candidates_ms'].values())
+
+
+def test_noalloc_entry_point_argument_codes_match_workspace_entry_point():
+    """acb_map_tc_noalloc reports argument errors with acb_map_tc's status codes (the checks return before
+    any CUDA call, so this runs without a GPU); a valid request beyond its fixed array is ACB_ERR_SHAPE."""
+    import ctypes
+
+    from acoular_b200 import _native as N
+    from acoular_b200 import build
+    from acoular_b200 import device as D
+    build.build()
+    L = N.lib()
+
+    def both(p, prec, csm=1):
+        a = L.acb_map_tc(ctypes.byref(p), prec, csm, 1, 1, 1, 1, None, None, 0, None, None)
+        b = L.acb_map_tc_noalloc(ctypes.byref(p), prec, csm, 1, 1, 1, 1, None, None, None)
+        return a, b
+
+    ok = D.map_params(64, 1000, 4, 'true level', True, 1.0)
+    assert both(ok, 7) == (N.ACB_ERR_UNSUPPORTED, N.ACB_ERR_UNSUPPORTED)     # unknown precision
+    assert both(ok, 0, csm=None) == (N.ACB_ERR_ARG, N.ACB_ERR_ARG)           # null CSM
+    for bad, code in (({'steer_type': 9}, N.ACB_ERR_ARG), ({'num_mics': 4096}, N.ACB_ERR_UNSUPPORTED),
+                      ({'num_bins': 0}, N.ACB_ERR_SHAPE), ({'num_grid': 0}, N.ACB_ERR_SHAPE),
+                      ({'tc_pass_chunks': 5}, N.ACB_ERR_ARG)):
+        p = D.map_params(64, 1000, 4, 'true level', True, 1.0)
+        for k, v in bad.items():
+            setattr(p, k, v)
+        assert both(p, 0) == (code, code), bad
+    big = D.map_params(256, 1000, 100, 'classic', True, 1.0)                 # 100 bins x 544 KB > 32 MiB
+    assert L.acb_map_tc_noalloc(ctypes.byref(big), 0, 1, 1, 1, 1, 1, None, None, None) == N.ACB_ERR_SHAPE

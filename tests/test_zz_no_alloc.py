@@ -16,7 +16,6 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-3  # the tensor-core tolerance of the other map tests
 
 
 def _inputs(M, G, nb, seed):
@@ -51,7 +50,8 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls():
             torch.cuda.synchronize()
             a, b = out.cpu().numpy(), ref.cpu().numpy()
             assert np.isfinite(a).all()
-            assert np.abs(a - b).max() <= TOL * np.abs(b).max()
+            # the same kernel on the same inputs, only the scratch memory differs: bit for bit
+            assert np.array_equal(a, b)
 
 
 def test_noalloc_rejects_requests_beyond_its_array():
