@@ -502,6 +502,27 @@ def damas_gauss_seidel(psf: torch.Tensor, dirty_map: torch.Tensor, n_iter: int, 
 # ------------------------------------------------------------------------------------------------
 # CLEAN-SC
 # ------------------------------------------------------------------------------------------------
+def heevd_f64(csm: torch.Tensor, chunk_bytes: int = 1 << 30):
+    """Hermitian eigendecomposition of every bin: csm (B, M, M) complex128 on the device ->
+    (eigvals (B, M) float64 ascending, eigvecs (B, M, M) complex128, eigenvectors in the columns, info (B,)
+    int32), the layout numpy.linalg.eigh returns; bins in chunks whose workspace fits ``chunk_bytes``."""
+    B, M, _ = csm.shape
+    dev = csm.device
+    c = csm.to(torch.complex128).contiguous()
+    ev = torch.empty((B, M), dtype=torch.float64, device=dev)
+    vec = torch.empty((B, M, M), dtype=torch.complex128, device=dev)
+    info = torch.zeros(B, dtype=torch.int32, device=dev)
+    per = max(1, N.lib().acb_heevd_workspace_bytes(M, 1))
+    step = int(max(1, min(B, chunk_bytes // per)))
+    ws = torch.empty(N.lib().acb_heevd_workspace_bytes(M, step), dtype=torch.uint8, device=dev)
+    for b0 in range(0, B, step):
+        nb = min(step, B - b0)
+        N.check(N.lib().acb_heevd_f64(c[b0].data_ptr(), nb, M, ev[b0].data_ptr(), vec[b0].data_ptr(),
+                                      info[b0].data_ptr(), ws.data_ptr(), ws.numel(), N.stream_handle()),
+                'acb_heevd_f64')
+    return ev, vec, info
+
+
 def cleansc_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, steer_type: str, r_diag: bool, norm: float,
                 n_iter: int = 0, damp: float = 0.6, stopn: int = 3, mpos: torch.Tensor | None = None,
                 gpos: torch.Tensor | None = None, ref=None, r0: torch.Tensor | None = None,

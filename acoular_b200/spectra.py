@@ -265,18 +265,16 @@ class PowerSpectra:
     # --- eigen-decomposition (acoular/spectra.py:351-364) ---------------------------------------
     @property
     def evd_device(self):
-        """``(eigvals (F, M) float64, eigvecs (F, M, M) complex128)`` of the CSM on the device:
-        Hermitian eigh per bin (cuSOLVER through torch), eigenvalues ascending as numpy returns them.
-        The eigenvector phases may differ from LAPACK's; the eigenvalue beamformers depend on them only
-        through |v^H h|."""
+        """``(eigvals (F, M) float64, eigvecs (F, M, M) complex128)`` of the CSM on the device: the
+        library's batched Hermitian eigendecomposition (``acb_heevd_f64``), eigenvalues ascending as numpy
+        returns them.  The eigenvector phases may differ from LAPACK's; the eigenvalue beamformers depend on
+        them only through |v^H h|."""
         self._refresh()
         if getattr(self, '_evd_dev', None) is None or self._evd_dev[0] != self._cache_key:
-            csm = self.csm_device
-            ev = torch.empty(csm.shape[:2], dtype=torch.float64, device=csm.device)
-            evec = torch.empty_like(csm)
-            step = 64
-            for f0 in range(0, csm.shape[0], step):
-                ev[f0:f0 + step], evec[f0:f0 + step] = torch.linalg.eigh(csm[f0:f0 + step])
+            ev, evec, info = D.heevd_f64(self.csm_device)
+            if int(info.max()):
+                msg = 'acb_heevd_f64: the QL iteration did not converge for some bins'
+                raise RuntimeError(msg)
             self._evd_dev = (self._cache_key, ev, evec)
         return self._evd_dev[1], self._evd_dev[2]
 

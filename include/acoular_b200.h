@@ -278,6 +278,18 @@ int acb_cross_spectra(const void *spectra, int64_t num_windows, int num_freqs, i
  * CLEAN-SC deconvolution
  * ------------------------------------------------------------------------------------------- */
 
+/* Workspace (device bytes) of acb_heevd_f64. */
+size_t acb_heevd_workspace_bytes(int num_mics, int num_bins);
+
+/* Hermitian eigendecomposition of every bin's CSM, PowerSpectra._get__evd (acoular/spectra.py:351-364:
+ * numpy.linalg.eigh per bin) on the device: csm complex128 [B][M][M] (read only) -> eigval float64 [B][M]
+ * ascending, eigvec complex128 [B][M][M] row-major with the eigenvectors in the columns (numpy's layout;
+ * each column may differ from LAPACK's by a unit phase factor).  Householder tridiagonalisation, implicit QL
+ * with Wilkinson shifts, back-transformation, all in FP64.  info int [B] (may be NULL): 1 where a QL iteration
+ * did not converge in 60 steps.  M <= 4096. */
+int acb_heevd_f64(const void *csm, int num_bins, int num_mics, double *eigval, void *eigvec, int *info,
+                  void *workspace, size_t workspace_bytes, void *stream);
+
 /* Workspace (device bytes) of acb_cleansc_f64 for num_bins bins (n_iter 0 = 2 num_mics iterations). */
 size_t acb_cleansc_workspace_bytes(int num_mics, int64_t num_grid, int num_bins, int n_iter);
 

@@ -93,3 +93,48 @@ def test_beamformer_eig_class_end_to_end(golden):
     assert mu.na == 3 and mu.r_diag is False
     res = np.array(mu.result[bins[0]:bins[-1] + 1])
     assert np.isfinite(res).all() and (res > 0).all()
+
+
+@pytest.mark.parametrize('M', [1, 2, 5, 8, 33, 64, 256, 300])
+def test_heevd_against_lapack(M):
+    """acb_heevd_f64 (Householder tridiagonalisation, implicit QL, back-transformation) on CSM-like matrices:
+    eigenvalues ascending within 1e-12 of numpy's (relative to the largest), residual |A V - V diag(w)| and
+    |V^H V - I| within 1e-12; a zero, an identity and a rank-1 matrix among them."""
+    from acoular_b200 import device as D
+    rng = np.random.RandomState(M)
+    mats = []
+    for _ in range(3):
+        X = rng.randn(2 * M, M) + 1j * rng.randn(2 * M, M)
+        A = X.conj().T @ X / (2 * M)
+        a = np.exp(-1j * rng.uniform(0, 6, M)) / rng.uniform(0.5, 2.0, M)
+        mats.append(A + 40.0 * np.outer(a, a.conj()))
+    a = np.exp(1j * rng.uniform(0, 6, M))
+    mats += [np.zeros((M, M), complex), np.eye(M, dtype=complex), np.outer(a, a.conj())]
+    C = np.stack(mats)
+    w, V, info = D.heevd_f64(_dev(C))
+    w, V = w.cpu().numpy(), V.cpu().numpy()
+    assert not int(info.max())
+    for A, wb, Vb in zip(C, w, V):
+        wr = np.linalg.eigvalsh(A)
+        scale = max(np.abs(wr).max(), 1e-300)
+        assert np.all(np.diff(wb) >= 0)
+        assert np.abs(wb - wr).max() <= 1e-12 * scale
+        assert np.abs(A @ Vb - Vb * wb).max() <= 1e-12 * max(scale, 1.0)
+        assert np.abs(Vb.conj().T @ Vb - np.eye(M)).max() <= 1e-12
+
+
+def test_power_spectra_evd_device_matches_host(golden):
+    """PowerSpectra.evd_device (the device eigendecomposition) against the host LAPACK one of the same CSM:
+    eigenvalues within 1e-12 of max, and a well-separated largest component's eigenvector up to its phase."""
+    import acoular_b200 as ac
+    s = golden('small_kat.npz')
+    ps = ac.PowerSpectra(source=ac.TimeSamples(data=s['data'], sample_freq=float(s['fs'])), block_size=128,
+                         window='Hanning', overlap='50%')
+    ev, evec = ps.evd_device
+    ev, evec = ev.cpu().numpy(), evec.cpu().numpy()
+    wr, vr = ps.eigvals, ps.eigvecs
+    for b in range(ev.shape[0]):
+        assert np.abs(ev[b] - wr[b]).max() <= 1e-12 * max(np.abs(wr[b]).max(), 1e-300)
+        if wr[b, -1] > 1e3 * max(wr[b, -2], 1e-300):
+            ph = np.vdot(vr[b][:, -1], evec[b][:, -1])
+            assert abs(abs(ph) - 1.0) <= 1e-9
