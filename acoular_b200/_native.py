@@ -21,7 +21,7 @@ STATUS_NAMES = {0: 'ok', 1: 'ACB_ERR_SHAPE', 2: 'ACB_ERR_ARG', 3: 'ACB_ERR_CUDA'
 STEER_CODES = {'classic': 1, 'inverse': 2, 'true level': 3, 'true location': 4}
 C128, C64 = 0, 1
 CSM_TC_TF32, CSM_TC_BF16X3 = 2, 3     # tensor-core CSM forms (complex128 csm_upper)
-TC_PRECISIONS = {'bf16x3': 0, 'tf32': 1}
+TC_PRECISIONS = {'bf16x3': 0, 'tf32': 1, 'fp16': 2}
 F32, F64 = 0, 1
 
 

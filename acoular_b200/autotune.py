@@ -139,7 +139,7 @@ def _time(mi, precision: str, tuning, reps: int) -> float:
     return float(np.median(ts))
 
 
-def tune(precisions=('bf16x3', 'tf32'), mic_buckets=MIC_BUCKETS, item_buckets=('tiny', 'few', 'mid', 'many'),
+def tune(precisions=('bf16x3', 'tf32', 'fp16'), mic_buckets=MIC_BUCKETS, item_buckets=('tiny', 'few', 'mid', 'many'),
          reps: int = 5, out: Path | str | None = TABLE_PATH, log=print) -> dict:
     """Time every candidate per shape class on cuda:0; write and return the table."""
     import torch

@@ -32,6 +32,7 @@
 // Every mbarrier wait is bounded (globaltimer); on timeout the CTA raises an error word and exits
 // its loops without further work.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -176,34 +177,91 @@ __host__ __device__ constexpr int tile_index(int C, int i, int j) { return i * C
 // R' rows and columns, and the rows past the grid are never written, so neither needs masking.
 constexpr float TC_FAR = 1e18f;
 
-template <bool TF32>
-__global__ void __launch_bounds__(256) tc_prep_kernel(const double2 *__restrict__ csm, int M, int C, int r_diag,
-                                                      int64_t bin_stride, __nv_bfloat16 *__restrict__ rh,
-                                                      __nv_bfloat16 *__restrict__ rl)
+// Operand precisions of the tensor-core form (the values of acb_tc_precision).
+constexpr int TC_SPLIT = 0;   // split-BF16 hi/lo, three products
+constexpr int TC_TF = 1;      // FP32 rounded to TF32
+constexpr int TC_HALF = 2;    // FP16, R' scaled per bin by a power of two
+
+// FP16 operands: the R' tiles of a bin are scaled by 2^e with e = 15 - ceil-exponent of the bin's
+// largest |R'| entry, so that every entry lies below 2^15 (FP16 holds up to 65504) and the bin keeps
+// FP16's full 11-bit precision down to 2^-14 of that scale; the map sums are scaled back by 2^-e.
+// The largest entry of each bin is found first (tc_binmax_kernel) and kept as FP64 bits in the
+// workspace half that the FP16 tiles leave unused.
+__device__ __forceinline__ int tc_half_shift(const unsigned long long *bmax, int bin)
 {
-    int t = blockIdx.x, i = 0;
+    const double mx = __longlong_as_double((long long)bmax[bin]);
+    int ex = 0;
+    if (mx > 0.0) frexp(mx, &ex);   // mx < 2^ex
+    return mx > 0.0 ? 15 - ex : 0;
+}
+
+// Tile (i, j >= i) of the CTA's blockIdx.x in the upper-triangular tile order of C chunks.
+__device__ __forceinline__ void tc_tile_of_block(int C, int &i, int &j)
+{
+    int t = blockIdx.x;
+    i = 0;
     while (t >= C - i) {
         t -= C - i;
         ++i;
     }
-    const int j = i + t;
+    j = i + t;
+}
+
+// Entry (rr, kk) of R' tile (i, j): row n = 32 j + rr of D (column of R), column k = 32 i + kk.
+__device__ __forceinline__ double tc_rprime(const double2 *Cb, int M, int r_diag, int i, int j, int rr, int kk)
+{
+    const int n = TC_CHUNK * j + rr, k = TC_CHUNK * i + kk;
+    const int a = k >> 1, pa = k & 1, b = n >> 1, pb = n & 1;
+    if (a >= M || b >= M || (r_diag && a == b)) return 0.0;
+    const double2 c = Cb[(int64_t)a * M + b];
+    const double val = (pa == pb) ? c.x : (pa == 0 ? -c.y : c.y);
+    return (j > i) ? 2.0 * val : val;
+}
+
+// Largest |R'| entry of every bin: one CTA per (tile, bin), an atomic max on the FP64 bit pattern
+// (non-negative doubles order like their bits); bmax is zeroed before the launch.
+__global__ void __launch_bounds__(256) tc_binmax_kernel(const double2 *__restrict__ csm, int M, int C, int r_diag,
+                                                        unsigned long long *__restrict__ bmax)
+{
+    int i, j;
+    tc_tile_of_block(C, i, j);
+    const int bin = blockIdx.y;
+    const double2 *Cb = csm + (int64_t)bin * M * M;
+    double m = 0.0;
+    for (int e = threadIdx.x; e < TC_TILE_ELEMS; e += blockDim.x)
+        m = fmax(m, fabs(tc_rprime(Cb, M, r_diag, i, j, e >> 5, e & 31)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double wm[8];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wm[w]);
+        if (m > 0.0) atomicMax(&bmax[bin], (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(256) tc_prep_kernel(const double2 *__restrict__ csm, int M, int C, int r_diag,
+                                                      int64_t bin_stride, __nv_bfloat16 *__restrict__ rh,
+                                                      __nv_bfloat16 *__restrict__ rl)
+{
+    int i, j;
+    tc_tile_of_block(C, i, j);
     const int bin = blockIdx.y;
     const double2 *Cb = csm + (int64_t)bin * M * M;
     __nv_bfloat16 *th = rh + (int64_t)bin * bin_stride + (int64_t)tile_index(C, i, j) * TC_TILE_ELEMS;
     __nv_bfloat16 *tl = rl + (int64_t)bin * bin_stride + (int64_t)tile_index(C, i, j) * TC_TILE_ELEMS;
-    const double factor = (j > i) ? 2.0 : 1.0;
+    const int shift = PREC == TC_HALF ? tc_half_shift(reinterpret_cast<const unsigned long long *>(rl), bin) : 0;
     for (int e = threadIdx.x; e < TC_TILE_ELEMS; e += blockDim.x) {
         const int rr = e >> 5, kk = e & 31;
-        const int n = TC_CHUNK * j + rr, k = TC_CHUNK * i + kk;
-        const int a = k >> 1, pa = k & 1, b = n >> 1, pb = n & 1;
-        double val = 0.0;
-        if (a < M && b < M && !(r_diag && a == b)) {
-            const double2 c = Cb[(int64_t)a * M + b];
-            val = (pa == pb) ? c.x : (pa == 0 ? -c.y : c.y);
-            val *= factor;
+        const double val = tc_rprime(Cb, M, r_diag, i, j, rr, kk);
+        if (PREC == TC_HALF) {
+            reinterpret_cast<__half *>(th)[tile_off(rr, kk)] = __double2half(ldexp(val, shift));
+            continue;
         }
         const float vf = (float)val;
-        if (TF32) {
+        if (PREC == TC_TF) {
             // FP32 tiles of 4 KB: the whole workspace (hi and lo halves) holds them, 2 x bin_stride
             // bf16 elements per bin
             uint32_t *t32 = reinterpret_cast<uint32_t *>(rh + 2 * (int64_t)bin * bin_stride) +
@@ -232,7 +290,7 @@ struct TcSmem {
     __host__ __device__ static constexpr int red_off(int ns, int Mp) { return mic_off(ns) + Mp * 16; }
     // per-item normalisation partial sums, double-buffered by item parity: [2][parts][128]
     __host__ __device__ static constexpr int bar_off(int ns, int Mp) { return red_off(ns, Mp) + 2 * TC_PARTS * TC_ROWS * 8; }
-    __host__ __device__ static constexpr int nbars() { return 2 * TC_ASTAGES_MAX + 3 * TC_NB + 2 + 2; }
+    __host__ __device__ static constexpr int nbars() { return 2 * TC_ASTAGES_MAX + 3 * TC_NB + 4 + 2; }
     __host__ __device__ static constexpr int total(int ns, int Mp) { return bar_off(ns, Mp) + nbars() * 8 + 16; }
 };
 
@@ -270,9 +328,13 @@ __device__ __forceinline__ void finish_point(const TcInst &a, double scalar, dou
 
 // Persistent kernel: one CTA per SM walks the batch's work items (instance, bin, 128-point tile)
 // blockIdx.x, +gridDim.x, ...; the step pipeline runs on across item and instance boundaries.
-template <int ST, bool TF32>
+template <int ST, int PREC>
 __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_constant__ TcBatch b, int *err)
 {
+    constexpr bool TF32 = PREC == TC_TF, HALF = PREC == TC_HALF, SPLIT = PREC == TC_SPLIT;
+    // R' tile ring: 32 split-BF16 pairs (hi and lo halves of the ring region), 32 FP32 tiles, or
+    // 64 FP16 tiles in the same 128 KB; FP16 ring slot s sits at b_base + s * 2 KB
+    constexpr int RING = HALF ? 2 * TC_RING : TC_RING;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // operand tiles start on a 1 KB boundary (the launch reserves 1 KB of slack for this)
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -287,8 +349,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     uint64_t *done = full_b + TC_NB;                  // [8]  MMAs of step T complete
     uint64_t *tfree = done + TC_NB;                   // [8]  epilogue has read all columns of window W
     uint64_t *s_ready = tfree + TC_NB;                // [2]  synthesis sums S of item parity written
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(s_ready + 2 + 2);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(s_ready + 2 + 3);
+    // [2] epilogue has read the sums S of item parity: an item can have fewer steps than the A ring
+    // has stages, so the synthesis warps may finish item li + 2 before the epilogue reaches item li
+    uint64_t *s_free = s_ready + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(s_free + 2);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(s_free + 3);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t nmine = b.nitems > blockIdx.x ? (b.nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
@@ -306,6 +371,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
         for (int s = 0; s < TC_NB; ++s) tc::mbar_init(&tfree[s], TC_EPI_THREADS);
         tc::mbar_init(&s_ready[0], TC_SYNTH_THREADS);
         tc::mbar_init(&s_ready[1], TC_SYNTH_THREADS);
+        tc::mbar_init(&s_free[0], TC_EPI_THREADS);
+        tc::mbar_init(&s_free[1], TC_EPI_THREADS);
         *abort_flag = 0;
         tc::fence_mbar_init();
     }
@@ -322,7 +389,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     if (warp == TC_WARP_PRODUCER) {
         // ---------------- producer: R' tiles of every step into the tile ring ----------------
         // Step T takes n consecutive ring tiles starting at the running tile counter U; tile U
-        // reuses slot U % TC_RING, free once the step that held tile U - TC_RING is complete.
+        // reuses slot U % RING, free once the step that held tile U - RING is complete.
         if (lane == 0) {
             uint32_t ustart[TC_NB];   // first ring tile of the last TC_NB steps
             uint32_t U = 0;
@@ -334,17 +401,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 const TcItem it = decode_item(in, item);
                 const int C = in.C, pw = in.pw;
                 const int64_t bin = it.bin;
-                const __nv_bfloat16 *bh = in.rh + (TF32 ? 2 : 1) * bin * in.bin_stride;
+                const __nv_bfloat16 *bh = in.rh + (TF32 ? 2 : 1) * bin * in.bin_stride;   // FP16: halves
                 const __nv_bfloat16 *bl = in.rl + bin * in.bin_stride;
                 for (int pp = it.pa; pp < it.pz && ok; ++pp) {
                     const int jb = pp * pw, je = min(C, jb + pw);
                     for (int i = 0; i < je && ok; ++i, ++T) {
                         const int j0 = max(i, jb), n = je - j0;
                         // step barriers form a ring of TC_NB: step T - TC_NB must be complete; ring
-                        // slots: every step holding a tile <= U + n - 1 - TC_RING must be complete
+                        // slots: every step holding a tile <= U + n - 1 - RING must be complete
                         while (ok && (freed < T - TC_NB ||
                                       (freed + 1 < T &&
-                                       (int)(ustart[(freed + 1) & (TC_NB - 1)] - (U + n - 1 - TC_RING)) <= 0))) {
+                                       (int)(ustart[(freed + 1) & (TC_NB - 1)] - (U + n - 1 - RING)) <= 0))) {
                             ok = tc::mbar_wait(&done[(freed + 1) & (TC_NB - 1)], (uint32_t)(((freed + 1) / TC_NB) & 1),
                                                abort_flag, b.wait_limit_ns);
                             if (ok) ++freed;
@@ -352,14 +419,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         if (!ok) break;
                         ustart[T & (TC_NB - 1)] = U;
                         uint64_t *fb = &full_b[T & (TC_NB - 1)];
-                        tc::mbar_arrive_expect_tx(fb, 2u * n * TC_TILE_BYTES);   // hi + lo, or one FP32 tile
+                        tc::mbar_arrive_expect_tx(fb, (HALF ? 1u : 2u) * n * TC_TILE_BYTES);   // hi + lo, FP32, FP16
                         const int64_t src = (int64_t)tile_index(C, i, j0) * TC_TILE_ELEMS;
                         int j = 0;
                         while (j < n) {   // contiguous runs of ring slots
-                            const int slot = (int)((U + j) & (TC_RING - 1));
-                            const int run = min(n - j, TC_RING - slot);
+                            const int slot = (int)((U + j) & (RING - 1));
+                            const int run = min(n - j, RING - slot);
                             const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
-                            if (TF32) {   // FP32 tiles of 4 KB, ring slot s at b_base + s * 4 KB
+                            if (HALF) {
+                                tc::bulk_g2s(smem + TcSmem::b_base(NST) + slot * TC_TILE_BYTES,
+                                             bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                            } else if (TF32) {   // FP32 tiles of 4 KB, ring slot s at b_base + s * 4 KB
                                 tc::bulk_g2s(smem + TcSmem::b_base(NST) + slot * 2 * TC_TILE_BYTES,
                                              reinterpret_cast<const uint32_t *>(bh) + src + (int64_t)j * TC_TILE_ELEMS,
                                              2 * bytes, fb);
@@ -398,7 +468,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             constexpr uint32_t A_STEP = TC_A_BYTES >> 4;          // next (stage, hi|lo) block
             constexpr uint32_t T_STEP = (TF32 ? 2 : 1) * (TC_TILE_BYTES >> 4);   // next ring tile
             constexpr uint32_t LO_B = (TC_RING * TC_TILE_BYTES) >> 4;
-            const uint32_t idesc0 = tc::idesc_m128(TF32 ? 2 : 1, 0);
+            // operand format: 0 = FP16, 1 = BF16 (kind::f16), 2 = TF32 (kind::tf32)
+            const uint32_t idesc0 = tc::idesc_m128(TF32 ? 2 : (HALF ? 0 : 1), 0);
             int sa = 0, ua = 0;     // A stage and its phase parity
             int sb = 0, ub = 0;     // step barrier slot and parity
             uint32_t slot0 = 0;     // ring slot of the step's first tile
@@ -436,14 +507,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         const int j0 = max(i, jb), n = je - j0;
                         const uint32_t dcol = wcol + (uint32_t)(TC_CHUNK * (j0 - jb));
                         // split the step's n tiles into runs of <= 8 (N <= 256) that do not wrap
-                        const int run0 = min(min(n, 8), (int)(TC_RING - slot0));
-                        const uint32_t slot1 = (slot0 + run0) & (TC_RING - 1);
+                        const int run0 = min(min(n, 8), (int)(RING - slot0));
+                        const uint32_t slot1 = (slot0 + run0) & (RING - 1);
                         const int rest = n - run0;
-                        const int run1 = min(min(rest, 8), (int)(TC_RING - slot1));
-                        const uint32_t slot2 = (slot1 + run1) & (TC_RING - 1);
+                        const int run1 = min(min(rest, 8), (int)(RING - slot1));
+                        const uint32_t slot2 = (slot1 + run1) & (RING - 1);
                         const int run2 = rest - run1;   // at most one more run (n <= 16)
-                        // BF16: K steps of 16 (2) x products hi*hi, hi*lo, lo*hi; TF32: K steps of 8 (4) x 1
-                        constexpr int KS = TF32 ? 4 : 2, NPROD = TF32 ? 1 : 3;
+                        // BF16: K steps of 16 (2) x products hi*hi, hi*lo, lo*hi; TF32: K steps of 8 (4) x 1;
+                        // FP16: K steps of 16 (2) x 1
+                        constexpr int KS = TF32 ? 4 : 2, NPROD = SPLIT ? 3 : 1;
 #pragma unroll
                         for (int ks = 0; ks < KS; ++ks) {
 #pragma unroll
@@ -474,7 +546,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         tc::mma_commit(&done[sb]);
                         lastb = sb;
                         lastu = ub;
-                        slot0 = (slot0 + (uint32_t)n) & (TC_RING - 1);
+                        slot0 = (slot0 + (uint32_t)n) & (RING - 1);
                         if (++sa == NST) { sa = 0; ua ^= 1; }
                         if (++sb == TC_NB) { sb = 0; ub ^= 1; }
                     }
@@ -536,8 +608,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                                 part = fmaf(d[c4 * 4 + 3], v.w, part);
                             }
                         }
+                        if (HALF) {
+                            // FP16 row: 4 core-matrix columns of 4 (re, im) pairs, 128 bytes apart
 #pragma unroll
-                        for (int grp = 0; grp < (TF32 ? 0 : 4); ++grp) {
+                            for (int grp = 0; grp < 4; ++grp) {
+                                const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
+                                const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w};
+#pragma unroll
+                                for (int e = 0; e < 4; ++e) {
+                                    const float2 v = __half22float2(*reinterpret_cast<const __half2 *>(&hv[e]));
+                                    part = fmaf(d[grp * 8 + 2 * e], v.x, part);
+                                    part = fmaf(d[grp * 8 + 2 * e + 1], v.y, part);
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int grp = 0; grp < (SPLIT ? 4 : 0); ++grp) {
                             const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
                             const uint4 lw = *reinterpret_cast<const uint4 *>(alo + grp * 128);
                             const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w}, lv[4] = {lw.x, lw.y, lw.z, lw.w};
@@ -560,6 +646,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 tc::mbar_arrive(&tfree[W & (TC_NB - 1)]);
             }
             if (!ok) break;
+            if (HALF) {
+                // undo the bin's R' scale; an FP16 steering value out of range (|w| >= 65520) shows as a
+                // non-finite sum and raises bit 2 of the error word
+                acc = ldexp(acc, -tc_half_shift(reinterpret_cast<const unsigned long long *>(in.rl), bin));
+                if (g < in.G && !isfinite(acc) && err) atomicOr(err, 2);
+            }
             // normalisation sums of this item from the synthesis warps
             ok = __all_sync(0xffffffffu, tc::mbar_wait(&s_ready[li & 1], (uint32_t)((li >> 1) & 1), abort_flag,
                                                        b.wait_limit_ns));
@@ -568,6 +660,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             double S = 0.0;
 #pragma unroll
             for (int pp = 0; pp < TC_PARTS; ++pp) S += rs[pp * TC_ROWS + row];
+            tc::mbar_arrive(&s_free[li & 1]);
             if (in.splits > 1) {
                 // publish this group's partial sums; the last group of the (bin, tile) to finish
                 // adds all groups' partials in group order and writes the map
@@ -675,9 +768,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         const uint64_t r = tc::f2_mul(r2, y);
                         // xn = -(k r) reduced: cos(xn) = Re h / w and sin(xn) = Im h / w
                         float xa, xb;
-                        if (TF32) {
-                            // TF32 keeps 11 significant bits: -k r in FP32 (k as a float-float) feeds the
-                            // hardware sincos directly, which reduces the argument by whole turns
+                        if (!SPLIT) {
+                            // TF32 and FP16 keep 11 significant bits: -k r in FP32 (k as a float-float) feeds
+                            // the hardware sincos directly, which reduces the argument by whole turns
                             tc::f2_split(tc::f2_fma(NKL, r, tc::f2_mul(NKH, r)), xa, xb);
                         } else {
                             // k r as an exact float-float product, reduced by the 3-term 2*pi
@@ -720,6 +813,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                                 lw[e] = tf32_bits(vi[h]);
                                 continue;
                             }
+                            if (HALF) {   // FP16 pair (re, im), one packed conversion
+                                const __half2 f2h = __floats2half2_rn(vr[h], vi[h]);
+                                hw[e] = *reinterpret_cast<const uint32_t *>(&f2h);
+                                continue;
+                            }
                             // split-BF16: hi = bf16(x) (packed pair conversion), lo = bf16(x - hi)
                             const __nv_bfloat162 h2 = __floats2bfloat162_rn(vr[h], vi[h]);
                             hw[e] = *reinterpret_cast<const uint32_t *>(&h2);
@@ -737,8 +835,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                     } else {
                         *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 0) + a_off_row) =
                             make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                        *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
-                            make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                        if (SPLIT)
+                            *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
+                                make_uint4(lw[0], lw[1], lw[2], lw[3]);
                     }
                     if (ST >= 2 && t >= jb) {   // each mic's term once, in its own pass
                         float sa2, sb2;
@@ -751,6 +850,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 }
             }
             if (!ok) break;
+            // the slot of item li - 2 must have been read (one phase of s_free per item of that parity)
+            if (li >= 2) {
+                ok = __all_sync(0xffffffffu, tc::mbar_wait(&s_free[li & 1], (uint32_t)(((li >> 1) - 1) & 1),
+                                                           abort_flag, b.wait_limit_ns));
+                if (!ok) break;
+            }
             red[((li & 1) * TC_PARTS + p) * TC_ROWS + row] = S;
             tc::mbar_arrive(&s_ready[li & 1]);
         }
@@ -883,7 +988,22 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
                 return ACB_ERR_CUDA;
             }
         }
-        auto prep = precision == ACB_TC_TF32 ? tc_prep_kernel<true> : tc_prep_kernel<false>;
+        if (precision == ACB_TC_FP16) {
+            // the bins' largest |R'| entries, for the FP16 scale, in the workspace half the tiles leave free
+            unsigned long long *bmax = reinterpret_cast<unsigned long long *>(const_cast<__nv_bfloat16 *>(in.rl));
+            const cudaError_t e = cudaMemsetAsync(bmax, 0, (size_t)in.nbins * sizeof(unsigned long long), s);
+            if (e != cudaSuccess) {
+                set_cuda_error(e);
+                return ACB_ERR_CUDA;
+            }
+            tc_binmax_kernel<<<dim3(tri_tiles(in.C), in.nbins), 256, 0, s>>>(
+                reinterpret_cast<const double2 *>(csms[i]), in.M, in.C, params[i]->r_diag, bmax);
+            const int st = check_launch();
+            if (st) return st;
+        }
+        auto prep = precision == ACB_TC_TF32   ? tc_prep_kernel<TC_TF>
+                    : precision == ACB_TC_FP16 ? tc_prep_kernel<TC_HALF>
+                                               : tc_prep_kernel<TC_SPLIT>;
         prep<<<dim3(tri_tiles(in.C), in.nbins), 256, 0, s>>>(reinterpret_cast<const double2 *>(csms[i]), in.M, in.C,
                                                             params[i]->r_diag, in.bin_stride,
                                                             const_cast<__nv_bfloat16 *>(in.rh),
@@ -908,11 +1028,13 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
     // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)
     if (smem < 116 * 1024) smem = 116 * 1024;
     const dim3 grid((unsigned)(bt.nitems < nsm ? bt.nitems : nsm));
-    const bool tf = precision == ACB_TC_TF32;
-    auto kern = steer_type == 1 ? (tf ? map_tc_kernel<1, true> : map_tc_kernel<1, false>)
-                : steer_type == 2 ? (tf ? map_tc_kernel<2, true> : map_tc_kernel<2, false>)
-                : steer_type == 3 ? (tf ? map_tc_kernel<3, true> : map_tc_kernel<3, false>)
-                                  : (tf ? map_tc_kernel<4, true> : map_tc_kernel<4, false>);
+    using KernT = void (*)(const TcBatch, int *);
+    static const KernT kernels[4][3] = {
+        {map_tc_kernel<1, TC_SPLIT>, map_tc_kernel<1, TC_TF>, map_tc_kernel<1, TC_HALF>},
+        {map_tc_kernel<2, TC_SPLIT>, map_tc_kernel<2, TC_TF>, map_tc_kernel<2, TC_HALF>},
+        {map_tc_kernel<3, TC_SPLIT>, map_tc_kernel<3, TC_TF>, map_tc_kernel<3, TC_HALF>},
+        {map_tc_kernel<4, TC_SPLIT>, map_tc_kernel<4, TC_TF>, map_tc_kernel<4, TC_HALF>}};
+    const KernT kern = kernels[steer_type - 1][precision];
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     kern<<<grid, TC_THREADS, smem, s>>>(bt, error_word);
     return check_launch();
@@ -943,7 +1065,7 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
                int *error_word, void *stream)
 {
     if (!p) return ACB_ERR_ARG;
-    if (precision != ACB_TC_BF16X3 && precision != ACB_TC_TF32) return ACB_ERR_UNSUPPORTED;
+    if (precision != ACB_TC_BF16X3 && precision != ACB_TC_TF32 && precision != ACB_TC_FP16) return ACB_ERR_UNSUPPORTED;
     TcBatch bt;
     bt.n_inst = 1;
     int st = tc_fill_inst(p, csm, wavenumber, mpos, gpos, out_map, out_steer_norm,
@@ -974,7 +1096,7 @@ int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num
 {
     if (!params || !io) return ACB_ERR_ARG;
     if (num_instances <= 0 || num_instances > TC_MAX_INST) return ACB_ERR_SHAPE;
-    if (precision != ACB_TC_BF16X3 && precision != ACB_TC_TF32) return ACB_ERR_UNSUPPORTED;
+    if (precision != ACB_TC_BF16X3 && precision != ACB_TC_TF32 && precision != ACB_TC_FP16) return ACB_ERR_UNSUPPORTED;
     const size_t need = acb_map_tc_batch_workspace_bytes(params, num_instances, precision);
     if (need == 0) return ACB_ERR_SHAPE;
     if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;

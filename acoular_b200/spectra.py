@@ -306,6 +306,8 @@ class PowerSpectraImport(PowerSpectra):
     def __init__(self, csm=None, frequencies=None, device=None):
         object.__setattr__(self, 'block_size', 1024)
         super().__init__(source=None, device=device)
+        # all lines of an imported CSM count: first index 0, no last index (acoular/spectra.py:667-668)
+        self._ind_low, self._ind_high = 0, None
         self._import_csm = None
         self._frequencies = None
         self.set_csm(csm, frequencies)

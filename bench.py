@@ -34,7 +34,10 @@ METRIC = 'map grid-pts*bins/s (CSM + map, 256 mics, 401x401 grid, 513 bins)'
 UNIT = 'grid-pts*bins/s'
 # DRAM bytes of one tensor-core map launch per bin of the 256-mic workload (ncu capture of 4 bins:
 # dram__bytes_read.sum + dram__bytes_write.sum, divided by 4)
-TC_TRAFFIC_PER_BIN = 1.54e6
+TC_TRAFFIC_PER_BIN = {'tf32': 1.54e6, 'bf16x3': 1.54e6}
+TC_PREC_INDEX = {'bf16x3': 0, 'tf32': 1, 'fp16': 2}
+TC_DTYPE = {'tf32': 'tf32 / f32 accum', 'bf16x3': 'bf16x3 (split) / f32 accum',
+            'fp16': 'fp16 (R\' scaled per bin) / f32 accum'}
 
 
 def parse():
@@ -51,7 +54,7 @@ def parse():
     ap.add_argument('--workload', default='precision256',
                     choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig', 'damas',
                              'cleansc', 'stream'])
-    ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32'])
+    ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32', 'fp16'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     ap.add_argument('--no-extra', action='store_true',
                     help='skip the other configurations\' blocks of the default line (profiling runs)')
@@ -532,7 +535,7 @@ def precision_matrix_block(csm64, kvec, mpos, gpos, acc_bins):
             f64_ms, ref = timed(lambda: D.map_f64(cs, ks, mpos, gpos, st, rd, norm))
             ref = ref.cpu().numpy()
             f64_rate = len(acc_bins) * G / (f64_ms / 1e3)
-            for pr in ('tf32', 'bf16x3'):
+            for pr in ('tf32', 'bf16x3', 'fp16'):
                 tc_ms, _ = timed(lambda: D.map_tc(csm64, kvec, mpos, gpos, st, rd, norm, out=o, precision=pr))
                 rate = nb * G / (tc_ms / 1e3)
                 entries[f'{st}|r_diag={rd}|{pr}'] = dict(_err_vs(o[sel].cpu().numpy(), ref), tc_rate=rate,
@@ -1128,7 +1131,7 @@ def main():
 
     if form != 'f64':
         out2 = torch.empty_like(out)
-        for pr in ('bf16x3', 'tf32'):
+        for pr in ('bf16x3', 'tf32', 'fp16'):
             o = out if pr == prec else out2
             t_ms, _ = timed(lambda: D.map_tc(c_all, kvec, mpos, gpos, args.steer, True, norm, out=o, precision=pr))
             forms[f'tc_{pr}'] = {'rate': units / (t_ms / 1e3), 'map_ms': t_ms, 'tc_over_f64':
@@ -1154,17 +1157,18 @@ def main():
         roof = {'bound': 'fp64', 'achieved': achieved_tf, 'peak': gp['fp64_tflops'], 'unit': 'TFLOP/s',
                 'frac': achieved_tf / gp['fp64_tflops'], 'traffic': None, 'kernel': 'map_plain_kernel',
                 'peak_kind': 'DGEMM measured in this run'}
-    elif prec == 'tf32':
-        # denominator: the measured sustained BF16 rate of the peak file (the conservative one: dense TF32
-        # runs at half the BF16 rate); the cuBLAS TF32 GEMM measured in this run is given beside it
-        roof = {'bound': 'tensor', 'achieved': achieved_tf, 'peak': pk['bf16_tflops_sustained'], 'unit': 'TFLOP/s',
-                'frac': achieved_tf / pk['bf16_tflops_sustained'], 'traffic': TC_TRAFFIC_PER_BIN * nbins,
-                'kernel': 'map_tc_kernel<3,true>', 'peak_kind': f"bf16 sustained ({pk['source']})",
-                'frac_of_tf32_gemm_here': achieved_tf / gp['tf32_tflops']}
     else:
+        # denominator: the measured sustained BF16 rate of the peak file (dense FP16 runs at the BF16 rate,
+        # dense TF32 at half of it, so for TF32 it is the conservative one; the cuBLAS TF32 GEMM measured
+        # in this run is given beside it)
+        steer_idx = STEER_TYPES.index(args.steer) + 1
+        tpb = TC_TRAFFIC_PER_BIN.get(prec)
         roof = {'bound': 'tensor', 'achieved': achieved_tf, 'peak': pk['bf16_tflops_sustained'], 'unit': 'TFLOP/s',
-                'frac': achieved_tf / pk['bf16_tflops_sustained'], 'traffic': TC_TRAFFIC_PER_BIN * nbins,
-                'kernel': 'map_tc_kernel<3,false>', 'peak_kind': f"bf16 sustained ({pk['source']})"}
+                'frac': achieved_tf / pk['bf16_tflops_sustained'], 'traffic': None if tpb is None else tpb * nbins,
+                'kernel': f'map_tc_kernel<{steer_idx},{TC_PREC_INDEX[prec]}>',
+                'peak_kind': f"bf16 sustained ({pk['source']})"}
+        if prec == 'tf32':
+            roof['frac_of_tf32_gemm_here'] = achieved_tf / gp['tf32_tflops']
     if roof['traffic'] is not None:
         roof['traffic_note'] = ('DRAM bytes per launch: ncu dram__bytes_read+write of a 4-bin capture, scaled by '
                                 'bins (R\' tiles per bin are the traffic; the grid and output add 8 B per point)')
@@ -1213,8 +1217,7 @@ def main():
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': ws, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
                 'vs_baseline': None,
-                'dtype': 'f64' if form == 'f64' else ('tf32 / f32 accum' if prec == 'tf32' else
-                                                       'bf16x3 (split) / f32 accum'),
+                'dtype': 'f64' if form == 'f64' else TC_DTYPE[prec],
                 'data': 'synthetic (seeded monopoles, GPU-generated)',
                 'config': {'workload': wl.name, 'mics': M, 'grid_points': G, 'bins': nbins, 'block_size': N,
                            'windows': K, 'steer_type': args.steer, 'r_diag': True, 'form': form, 'csm': csm_prec,

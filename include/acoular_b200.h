@@ -170,7 +170,10 @@ int acb_beamformer_freq_f64(const acb_map_params *p, const void *csm, double wav
 /* Tensor-core operand precisions. */
 enum acb_tc_precision {
     ACB_TC_BF16X3 = 0,  /* split-BF16 hi/lo operands, 3 products, FP32 accumulation (~1e-5)      */
-    ACB_TC_TF32 = 1     /* FP32 operands rounded to TF32, 1 product, FP32 accumulation (~1e-4)  */
+    ACB_TC_TF32 = 1,    /* FP32 operands rounded to TF32, 1 product, FP32 accumulation (~1e-4)  */
+    ACB_TC_FP16 = 2     /* FP16 operands (R' scaled per bin by a power of two), 1 product, FP32
+                           accumulation (~1e-4; steering weights |w| < 65504, i.e. distances
+                           below 65 km for 'inverse' and above 15 um for the 1/r types)        */
 };
 
 /* Bytes of workspace acb_map_tc needs (the per-bin split-BF16 copy of the real-embedded CSM). */
@@ -187,13 +190,17 @@ uint64_t acb_tc_set_wait_limit_ns(uint64_t limit_ns);
 /* Tensor-core form of the same map (acoular/fastFuncs.py:217-311 semantics, same arguments and
  * outputs as acb_map_f64): the quadratic form h^H C h is evaluated as the real quadratic form
  * v^T R v of the 2M-dimensional real embedding, R = [[Re C, -Im C], [Im C, Re C]], on tcgen05
- * tensor cores with split-BF16 operands (hi*hi + hi*lo + lo*hi) and FP32 accumulation in TMEM.
- * Steering vectors are synthesised per 128-grid-point tile in shared memory (float32 phase k*r as
- * the reference rounds it, FP64 range reduction); distances, the normalisation sums and the final
- * normalisation are FP64.  num_mics <= 2048; above 256 mics the accumulator is computed in column
- * passes of 512 (steering chunks before a pass are synthesised again).  glibc_faithful is ignored.
+ * tensor cores with FP32 accumulation in TMEM; `precision` (acb_tc_precision) picks the operands:
+ * split-BF16 (hi*hi + hi*lo + lo*hi), TF32 or FP16.  Steering vectors are synthesised per
+ * 128-grid-point tile in shared memory: FP32 distances, the phase k*r with k as a float-float
+ * (reduced by a three-term 2*pi for split-BF16), hardware sincos.  The per-point partial sums, the
+ * normalisation sums and the final normalisation are FP64.  num_mics <= 2048; above 256 mics the
+ * accumulator is computed in column passes of 512 (steering chunks before a pass are synthesised
+ * again).  glibc_faithful is ignored.
  * workspace: >= acb_map_tc_workspace_bytes(num_mics, num_bins, precision) bytes.
- * error_word: int32 on the device or NULL; bit 0 is set if a bounded device-side wait gave up. */
+ * error_word: int32 on the device or NULL; bit 0 is set if a bounded device-side wait gave up,
+ * bit 1 (value 2) if an FP16 map value came out non-finite (a steering weight out of FP16 range,
+ * or a non-finite CSM entry). */
 int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const double *wavenumber,
                const double *mpos, const double *gpos, double *out_map, double *out_steer_norm,
                void *workspace, size_t workspace_bytes, int *error_word, void *stream);

@@ -115,6 +115,31 @@ def test_tc_persistent_many_items_per_cta(M, G, nb):
         assert rel(got[b], ref[b]) <= TOL
 
 
+@pytest.mark.parametrize('precision', ['tf32', 'bf16x3', 'fp16'])
+@pytest.mark.parametrize('M', [16, 32])
+def test_tc_short_items_many_per_cta(M, precision):
+    """Items of one or two steps (<= 32 mics), many per CTA: the steering warps run more than an item
+    ahead of the epilogue, and the per-item normalisation sums must still reach the right item."""
+    from acoular_b200 import device as D
+    dev = torch.device('cuda')
+    nb = 4
+    mpos, gpos, freqs, csm = _case(M, 40000, seed=M + 1, nb=nb)
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    for steer in ('true level', 'inverse'):
+        ref = O.beamformer_calc(csm, freqs, range(nb), r0, rm, 343.0, steer, True)
+        for tuning in ('auto', None):
+            out = D.map_tc(torch.as_tensor(csm, device=dev), torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
+                           torch.as_tensor(mpos, device=dev), torch.as_tensor(gpos, device=dev), steer, True,
+                           O.sig_loss_norm(True, M), clip_negative=True, precision=precision, error_word=err,
+                           tuning=tuning)
+            torch.cuda.synchronize()
+            assert int(err.item()) == 0
+            got = out.cpu().numpy()
+            for b in range(nb):
+                assert rel(got[b], ref[b]) <= TOL, (steer, tuning, b, rel(got[b], ref[b]))
+
+
 def _instances(specs, seed=0):
     """Uneven instances (M, G, bins) with random geometry and CSMs, as device tensors."""
     from acoular_b200 import device as D
@@ -132,10 +157,13 @@ def _instances(specs, seed=0):
 def test_tc_batch_uneven_instances_equal_alone():
     """Each instance's map is the same in the batched launch as alone, and matches the oracle."""
     from acoular_b200 import device as D
-    specs = [(32, 441, 3), (64, 2000, 2), (128, 700, 4), (256, 300, 2), (300, 150, 2), (37, 90001, 1)]
+    specs = [(32, 441, 3), (64, 2000, 2), (128, 700, 4), (256, 300, 2), (300, 150, 2), (37, 90001, 1),
+             (32, 40000, 4), (16, 20000, 3)]
     inst = _instances(specs)
-    D.map_tc_batch([i for i, _ in inst])
+    err = torch.zeros(1, dtype=torch.int32, device=inst[0][0].csm.device)
+    D.map_tc_batch([i for i, _ in inst], error_word=err)
     torch.cuda.synchronize()
+    assert int(err.item()) == 0
     for it, (mpos, gpos, freqs, csm) in inst:
         alone = D.map_tc(it.csm, it.wavenumbers, it.mpos, it.gpos, 'true level', True, it.norm).cpu().numpy()
         got = it.out.cpu().numpy()
@@ -166,17 +194,55 @@ def test_tc_batch_graph_capture_replay():
         assert torch.equal(it.out, r)
 
 
+@pytest.mark.parametrize('precision', ['tf32', 'fp16'])
 @pytest.mark.parametrize('M,G', [(16, 128), (64, 257), (256, 200), (300, 150)])
 @pytest.mark.parametrize('steer', STEERS)
-def test_tf32_form_vs_oracle(M, G, steer):
-    """The FP32/TF32 operand form: one TF32 product, FP32 accumulation; <= 1e-3 of max."""
+def test_tf32_form_vs_oracle(M, G, steer, precision):
+    """The single-product operand forms (FP32 rounded to TF32; FP16 with R' scaled per bin), FP32
+    accumulation; <= 1e-3 of max."""
     mpos, gpos, freqs, csm = _case(M, G, seed=M + 3 * G)
     r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
     for r_diag in (False, True):
         ref = O.beamformer_calc(csm, freqs, range(len(freqs)), r0, rm, 343.0, steer, r_diag)
-        got = _tc(csm, freqs, mpos, gpos, steer, r_diag, precision='tf32')
+        got = _tc(csm, freqs, mpos, gpos, steer, r_diag, precision=precision)
         for b in range(len(freqs)):
             assert rel(got[b], ref[b]) <= TOL, (b, rel(got[b], ref[b]))
+
+
+@pytest.mark.parametrize('scale', [1e-30, 1e-8, 1.0, 1e12, 1e40])
+def test_fp16_form_per_bin_scale(scale):
+    """FP16 operands keep their precision whatever the CSM's magnitude: each bin's R' is scaled by a
+    power of two, here with bins 1e6 apart inside one call and the whole CSM from 1e-30 to 1e40."""
+    mpos, gpos, freqs, csm = _case(64, 500, seed=7)
+    csm = csm * (scale * np.array([1.0, 1e6, 1e-6])[:, None, None])
+    r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
+    for steer in ('true level', 'classic'):
+        ref = O.beamformer_calc(csm, freqs, range(len(freqs)), r0, rm, 343.0, steer, True)
+        got = _tc(csm, freqs, mpos, gpos, steer, True, precision='fp16')
+        for b in range(len(freqs)):
+            assert rel(got[b], ref[b]) <= TOL, (b, rel(got[b], ref[b]))
+
+
+def test_fp16_form_range_error_bit():
+    """'inverse' steering weights are the distances themselves: grid points 1e5 m away give FP16
+    operands above 65504, which the launch reports in bit 1 of the error word (the map holds
+    non-finite values there) instead of returning a wrong finite map."""
+    from acoular_b200 import device as D
+    dev = torch.device('cuda')
+    mpos, gpos, freqs, csm = _case(32, 300, seed=8)
+    far = gpos.copy()
+    far[2] = -1e5
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    args = (torch.as_tensor(csm, device=dev), torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
+            torch.as_tensor(mpos, device=dev))
+    D.map_tc(*args, torch.as_tensor(gpos, device=dev), 'inverse', True, 1.0, precision='fp16', error_word=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    out = D.map_tc(*args, torch.as_tensor(far, device=dev), 'inverse', True, 1.0, precision='fp16',
+                   error_word=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) & 2
+    assert not np.isfinite(out.cpu().numpy()).all()
 
 
 @pytest.mark.parametrize('M,G,steer', [(40, 700, 'true level'), (256, 300, 'true location'), (600, 260, 'inverse'),
@@ -251,7 +317,7 @@ def precision256_reduced():
     return wl.mics.pos, grid.pos, freqs, csm.cpu().numpy()
 
 
-@pytest.mark.parametrize('precision', ['tf32', 'bf16x3'])
+@pytest.mark.parametrize('precision', ['tf32', 'bf16x3', 'fp16'])
 @pytest.mark.parametrize('steer', STEERS)
 def test_precision_matrix_256mic_reduced_grid(precision256_reduced, steer, precision):
     """The precision matrix of the 256-mic workload at a reduced size: each steering type x r_diag x

@@ -2,8 +2,8 @@
 
 Every mbarrier wait of map_tc_kernel gives up after a limit (acb_tc_set_wait_limit_ns, 0.5 s by
 default), raises the launch's error word, lets the CTA's own bulk copies and MMAs finish, frees its
-tensor memory and returns.  Here the limit is set to 2 microseconds, shorter than the first steering
-synthesis and MMA of an item, so waits run out on a normal input (no fault, no trap, nothing that
+tensor memory and returns.  Here the limit is set to 100 ns, far shorter than the bulk copies, steering
+synthesis and MMAs that the pipeline's waits cover, so waits run out on a normal input (no fault, no trap, nothing that
 never finishes); the test checks that the error word reports it, that the context stays usable, and
 that the next launch at the default limit, which must allocate the tensor memory again, gives the
 oracle's map with a clear error word.
@@ -23,7 +23,7 @@ def test_tc_wait_timeout_reports_and_recovers():
     from acoular_b200 import device as D
     dev = torch.device('cuda')
     L = N.lib()
-    M, G, nb = 128, 20000, 4
+    M, G, nb = 256, 40000, 4
     rng = np.random.RandomState(5)
     mpos = np.vstack([rng.uniform(-0.5, 0.5, (2, M)), np.zeros((1, M))])
     gpos = np.vstack([rng.uniform(-0.4, 0.4, (2, G)), np.full((1, G), -0.7)])
@@ -44,7 +44,7 @@ def test_tc_wait_timeout_reports_and_recovers():
 
     run()                                         # at the default limit: no timeout
     assert int(err.item()) == 0
-    prev = L.acb_tc_set_wait_limit_ns(2000)
+    prev = L.acb_tc_set_wait_limit_ns(100)
     try:
         flags = [run()[1] for _ in range(3)]
     finally:
