@@ -164,6 +164,11 @@ __device__ __forceinline__ int find_inst(const TcBatch &b, int64_t item)
 }
 
 constexpr int TC_NB = 8;       // chunk barrier ring (full_b / done); the producer runs <= 7 chunks ahead
+// The epilogue waits on every step's `done` barrier in turn; the MMAs of step T + TC_NB complete the
+// same barrier slot again.  They need the A stage of step T + TC_NB, which the epilogue frees at step
+// T + TC_NB - stages, so with at most TC_NB A stages the epilogue has always seen step T first (more
+// stages would let a slot run two phases ahead of its waiter and the parity wait would never pass).
+static_assert(TC_ASTAGES_MAX <= TC_NB, "A ring deeper than the step barrier ring");
 
 __host__ __device__ constexpr int tri_tiles(int C) { return C * (C + 1) / 2; }
 // index of tile (i, j >= i) in the row-major upper-triangular tile order
