@@ -119,6 +119,7 @@ struct TcInst {
     uint8_t sp0[TC_MAX_SPLIT + 1];  // pass group s covers passes [sp0[s], sp0[s+1])
     double2 *part;             // [nbins * ntiles][splits][128] partial (B, S) when splits > 1
     int *cnt;                  // [nbins * ntiles][4] finished groups per epilogue warp (zeroed per launch)
+    int small;                 // every item number of the batch < 2^31: item decoding in 32-bit arithmetic
 };
 
 // Position of a work item inside its instance: items run (bin, tile, group) with the group fastest.
@@ -131,11 +132,21 @@ struct TcItem {
 __device__ __forceinline__ TcItem decode_item(const TcInst &in, int64_t item)
 {
     TcItem t;
-    const int64_t local = item - in.item_off;
-    t.split = (int)(local % in.splits);
-    t.base = local / in.splits;
-    t.bin = (int)(t.base / in.ntiles);
-    t.tile = t.base % in.ntiles;
+    if (in.small) {
+        // 32-bit division: the decode sits on the single-thread MMA issuer's path once per item
+        const uint32_t local = (uint32_t)(item - in.item_off), sp = (uint32_t)in.splits, nt = (uint32_t)in.ntiles;
+        const uint32_t base = local / sp;
+        t.split = (int)(local - base * sp);
+        t.base = base;
+        t.bin = (int)(base / nt);
+        t.tile = base - (uint32_t)t.bin * nt;
+    } else {
+        const int64_t local = item - in.item_off;
+        t.split = (int)(local % in.splits);
+        t.base = local / in.splits;
+        t.bin = (int)(t.base / in.ntiles);
+        t.tile = t.base % in.ntiles;
+    }
     t.pa = in.sp0[t.split];
     t.pz = in.sp0[t.split + 1];
     return t;
@@ -299,14 +310,19 @@ struct TcSmem {
     __host__ __device__ static constexpr int total(int ns, int Mp) { return bar_off(ns, Mp) + nbars() * 8 + 16; }
 };
 
+// Reference distance of grid point g (loaded at an item's start, so the epilogue does not wait for
+// the grid positions after the item's last step).
+__device__ __forceinline__ double ref_distance(const TcInst &a, int64_t g)
+{
+    if (a.ref_mode == 1 || g >= a.G) return a.ref_dist;
+    return dist3(a.gpos[g], a.gpos[a.G + g], a.gpos[2 * a.G + g], a.ref0, a.ref1, a.ref2);
+}
+
 // Normalisation of the steering type (acoular/fastFuncs.py:293-310) and clipping.
 template <int ST>
-__device__ __forceinline__ void finish_point(const TcInst &a, double scalar, double S, double gx, double gy, double gz,
-                                             int bin, int64_t g, double *out_map, double *out_norm)
+__device__ __forceinline__ void finish_point(const TcInst &a, double scalar, double S, double r0, int bin, int64_t g,
+                                             double *out_map, double *out_norm)
 {
-    double r0;
-    if (a.ref_mode == 1) r0 = a.ref_dist;
-    else r0 = dist3(gx, gy, gz, a.ref0, a.ref1, a.ref2);
     const double Md = (double)a.M;
     double res, ns;
     if (ST == 1) {
@@ -586,6 +602,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             }
             const int bin = it.bin;
             const int64_t g = it.tile * TC_ROWS + row;
+            // (split BF16 has no registers to spare across the steps: it loads them after the last one)
+            const double r0 = SPLIT ? 0.0 : ref_distance(in, g);
             double acc = 0.0;
             for (int pp = it.pa; pp < it.pz && ok; ++pp, ++W) {
                 const int jb = pp * pw, je = min(C, jb + pw);
@@ -687,9 +705,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                     S += v.y;
                 }
             }
-            if (g < in.G)
-                finish_point<ST>(in, acc, S, in.gpos[g], in.gpos[in.G + g], in.gpos[2 * in.G + g], bin, g, in.out,
-                                 in.out_norm);
+            if (g < in.G) finish_point<ST>(in, acc, S, SPLIT ? ref_distance(in, g) : r0, bin, g, in.out, in.out_norm);
         }
     } else if (tc_synth_index(warp) >= 0) {
         // ---------------- steering synthesis (16 warps off scheduler 1) ----------------
@@ -705,10 +721,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
         const uint64_t NHALF = tc::f2_splat(-0.5f), THALF = tc::f2_splat(1.5f);
         int T = 0, sa = 0, ua = 0, cur_inst = -1;
         bool ok = true;
+        // the grid point and wave number of an item are loaded one item ahead, so that their global-memory
+        // latency overlaps the previous item's steps (at the item's start for split BF16, whose
+        // synthesis has no registers to spare)
+        float nx = -TC_FAR, ny = -TC_FAR, nz = -TC_FAR;
+        double nk = 0.0;
+        auto fetch = [&](int64_t lj) {
+            const int64_t itm = blockIdx.x + lj * gridDim.x;
+            const TcInst &ij = b.inst[find_inst(b, itm)];
+            const TcItem tj = decode_item(ij, itm);
+            const int64_t gj = tj.tile * TC_ROWS + row;
+            nx = ny = nz = -TC_FAR;
+            if (gj < ij.G) {
+                nx = (float)ij.gpos[gj];
+                ny = (float)ij.gpos[ij.G + gj];
+                nz = (float)ij.gpos[2 * ij.G + gj];
+            }
+            nk = ij.k[tj.bin];
+        };
+        if (!SPLIT && nmine > 0) fetch(0);
         for (int64_t li = 0; li < nmine && ok; ++li) {
             const int64_t item = blockIdx.x + li * gridDim.x;
             const int ii = find_inst(b, item);
             const TcInst &in = b.inst[ii];
+            if (SPLIT) fetch(li);
+            const float gxf = nx, gyf = ny, gzf = nz;
+            const double k = nk;
+            if (!SPLIT && li + 1 < nmine) fetch(li + 1);
             if (ii != cur_inst) {
                 // new instance: every synthesis thread is past the previous item, reload the mics
                 asm volatile("bar.sync 2, %0;" ::"r"(TC_SYNTH_THREADS) : "memory");
@@ -731,17 +770,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             }
             const TcItem it = decode_item(in, item);
             const int C = in.C, pw = in.pw;
-            const int bin = it.bin;
-            const int64_t g = it.tile * TC_ROWS + row;
-            const bool gvalid = g < in.G;
-            float gxf = -TC_FAR, gyf = -TC_FAR, gzf = -TC_FAR;
-            if (gvalid) {
-                gxf = (float)in.gpos[g];
-                gyf = (float)in.gpos[in.G + g];
-                gzf = (float)in.gpos[2 * in.G + g];
-            }
             const uint64_t GX = tc::f2_splat(gxf), GY = tc::f2_splat(gyf), GZ = tc::f2_splat(gzf);
-            const double k = in.k[bin];
             const float khi = (float)k, klo = (float)(k - (double)khi);
             const uint64_t KH = tc::f2_splat(khi), KL = tc::f2_splat(klo);
             const uint64_t NKH = tc::f2_splat(-khi), NKL = tc::f2_splat(-klo);
@@ -916,6 +945,7 @@ static int tc_fill_inst(const acb_map_params *p, const void *csm, const double *
     in.sp0[1] = (uint8_t)in.P;
     in.part = nullptr;
     in.cnt = nullptr;
+    in.small = 0;   // set once the batch's item count is known
     return ACB_OK;
 }
 
@@ -1079,6 +1109,7 @@ int acb_map_tc(const acb_map_params *p, int precision, const void *csm, const do
     const size_t need = acb_map_tc_workspace_bytes(p->num_mics, p->num_bins, precision);
     if (!workspace || workspace_bytes < need) return ACB_ERR_WORKSPACE;
     bt.nitems = bt.inst[0].ntiles * bt.inst[0].nbins;
+    bt.inst[0].small = bt.nitems < (int64_t(1) << 31);
     const acb_map_params *pp[1] = {p};
     const void *cc[1] = {csm};
     return tc_launch(bt, pp, cc, p->steer_type, precision, error_word, as_stream(stream));
@@ -1131,6 +1162,7 @@ int acb_map_tc_batch(const acb_map_params *params, const acb_map_io *io, int num
         cc[i] = io[i].csm;
     }
     bt.nitems = items;
+    for (int i = 0; i < num_instances; ++i) bt.inst[i].small = items < (int64_t(1) << 31);
     return tc_launch(bt, pp, cc, steer, precision, error_word, as_stream(stream));
 }
 

@@ -642,6 +642,9 @@ def run_eig(args):
     x = workloads.monopole_time_data_torch(wl, device=dev)
     csm = D.calc_csm(x, N, 'Hanning', '50%', 'complex128')
     del x
+    if args.bins:   # profiling: the first bins only
+        F = min(F, args.bins)
+        csm = csm[:F].contiguous()
     freqs = np.abs(np.fft.fftfreq(N, 1 / wl.fs)[:F])
     k = torch.as_tensor(2 * np.pi * freqs / wl.c, device=dev)
     mpos, gpos = torch.as_tensor(wl.mics.pos, device=dev), torch.as_tensor(wl.grid.pos, device=dev)
@@ -682,7 +685,8 @@ def run_eig(args):
     # end to end against the oracle (numpy eigh + the reference's eigen kernel) on 2 bins
     r0, rm = O.apparent_r(wl.grid.pos), O.apparent_r(wl.grid.pos, wl.mics.pos)
     errs = []
-    for b in (100, 400):
+    check_bins = [b for b in (100, 400) if b < F] or [F - 1]
+    for b in check_bins:
         c_h = csm[b].cpu().numpy()
         w, v = np.linalg.eigh(c_h)
         ref = O.beamformer_freq_eig('true level', True, norm, r0, rm, 2 * np.pi * freqs[b] / wl.c, w[M - 1:],
@@ -697,7 +701,7 @@ def run_eig(args):
            'csm': 'complex128, computed once'},
           eigh_ms_per_step=float(np.mean(ev_ms)), map_ms_per_step=float(np.mean(map_ms)),
           map_rate=G * F / (float(np.mean(map_ms)) / 1e3), map_tflops_algorithmic=flops / (np.mean(map_ms) / 1e3) / 1e12,
-          accuracy={'vs': 'oracle (numpy eigh + the reference eigen kernel restated)', 'bins': [100, 400],
+          accuracy={'vs': 'oracle (numpy eigh + the reference eigen kernel restated)', 'bins': check_bins,
                     'max_rel_err': max(errs)},
           gpu_launches_per_step='eigendecomposition (heevd_tridiag, heevd_tql, heevd_back kernels) + 1 map_eig_kernel',
           clocks=clk.summary(),
@@ -1044,7 +1048,9 @@ def main():
     K = D.num_windows(wl.num_samples, N, 2)
     prec = args.tc_precision
     # the CSM in the same form as the map: FP64 Gram for the FP64 form, tensor-core Gram otherwise
-    csm_prec = 'complex128' if form == 'f64' else f'tc_{prec}'
+    # the tensor-core CSM has TF32 and split-BF16 forms; the FP16 map takes the TF32 CSM
+    csm_tc = 'tf32' if prec == 'fp16' else prec
+    csm_prec = 'complex128' if form == 'f64' else f'tc_{csm_tc}'
     ws_bytes = NAT.lib().acb_csm_workspace_bytes(M, F, K, D.CSM_PRECISIONS[csm_prec])
     workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     csm_up = torch.zeros((F, M, M), dtype=torch.complex128, device=dev)
@@ -1183,7 +1189,7 @@ def main():
         times = []
         for i in range(2 + max(1, min(args.steps, 3))):
             ps = ac.PowerSpectra(source=ts, block_size=N, window='Hanning', overlap='50%',
-                                 form='f64' if form == 'f64' else 'tc', tc_precision=prec)
+                                 form='f64' if form == 'f64' else 'tc', tc_precision=csm_tc)
             st = ac.SteeringVector(grid=wl.grid, mics=wl.mics, steer_type=args.steer)
             bb = ac.BeamformerBase(freq_data=ps, steer=st, r_diag=True, form=form, tc_precision=prec)
             torch.cuda.synchronize()
