@@ -180,6 +180,8 @@ constexpr int TC_NB = 8;       // chunk barrier ring (full_b / done); the produc
 // T + TC_NB - stages, so with at most TC_NB A stages the epilogue has always seen step T first (more
 // stages would let a slot run two phases ahead of its waiter and the parity wait would never pass).
 static_assert(TC_ASTAGES_MAX <= TC_NB, "A ring deeper than the step barrier ring");
+// (with two chunks per stage, the FP16 form, the bound is on chunks: 2 x stages <= TC_NB; the host
+// caps its stages at TC_NB / 2)
 
 __host__ __device__ constexpr int tri_tiles(int C) { return C * (C + 1) / 2; }
 // index of tile (i, j >= i) in the row-major upper-triangular tile order
@@ -356,6 +358,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     // R' tile ring: 32 split-BF16 pairs (hi and lo halves of the ring region), 32 FP32 tiles, or
     // 64 FP16 tiles in the same 128 KB; FP16 ring slot s sits at b_base + s * 2 KB
     constexpr int RING = HALF ? 2 * TC_RING : TC_RING;
+    // chunks per A stage: an FP16 chunk fills half a stage (8 KB), so a stage carries two and the
+    // steering -> MMA -> epilogue handshakes run once per chunk pair (a pass's chunks pair up from its
+    // first; an odd last chunk has its stage alone)
+    constexpr int CPS = HALF ? 2 : 1;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // operand tiles start on a 1 KB boundary (the launch reserves 1 KB of slack for this)
     uint8_t *smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -521,8 +527,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                                            abort_flag, b.wait_limit_ns);
                     const uint32_t wcol = taddr + (uint32_t)(((W - w_start) % wpt) * width);
                     for (int i = 0; i < je && ok; ++i) {
-                        ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, b.wait_limit_ns) &&
-                             tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, b.wait_limit_ns);
+                        if (i % CPS == 0) ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, b.wait_limit_ns);
+                        ok = ok && tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, b.wait_limit_ns);
                         if (!ok) break;
                         tc::tc_fence_after();
                         const int j0 = max(i, jb), n = je - j0;
@@ -541,7 +547,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         for (int ks = 0; ks < KS; ++ks) {
 #pragma unroll
                             for (int prod = 0; prod < NPROD; ++prod) {
-                                const uint64_t ad = a_base + (uint64_t)((sa * 2 + (prod == 2)) * A_STEP + ks * 16);
+                                // A: split-BF16 hi (lo for the third product), FP32, or FP16 chunk i % 2 of the stage
+                                const uint64_t ad =
+                                    a_base + (uint64_t)((sa * 2 + (HALF ? (i & 1) : (prod == 2))) * A_STEP + ks * 16);
                                 const uint64_t bd = b_base + (uint64_t)((prod == 1 ? LO_B : 0u) + ks * 16);
                                 const uint32_t accum = (i == 0 && ks == 0 && prod == 0) ? 0u : 1u;
                                 const uint32_t n0 = idesc0 | ((uint32_t)(run0 * 4) << 17);
@@ -568,7 +576,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         lastb = sb;
                         lastu = ub;
                         slot0 = (slot0 + (uint32_t)n) & (RING - 1);
-                        if (++sa == NST) { sa = 0; ua ^= 1; }
+                        if (i % CPS == CPS - 1 || i == je - 1) {
+                            if (++sa == NST) { sa = 0; ua ^= 1; }
+                        }
                         if (++sb == TC_NB) { sb = 0; ub ^= 1; }
                     }
                 }
@@ -616,8 +626,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         tc::tc_fence_after();
                         float d[TC_CHUNK];
                         tc::tmem_ld_x32(wcol + (uint32_t)(TC_CHUNK * (i - jb)), d);
-                        const uint8_t *ahi = smem + TcSmem::a_off(sa, 0) + a_row;
-                        const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;
+                        const uint8_t *ahi = smem + TcSmem::a_off(sa, HALF ? (i & 1) : 0) + a_row;
+                        const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;   // split BF16 only
                         float part = 0.f;
                         if (TF32) {
                             // FP32 row: 8 core-matrix columns of 4 values, 128 bytes apart
@@ -662,8 +672,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         acc += (double)part;
                         tc::tc_fence_before();
                     }
-                    tc::mbar_arrive(&afree[sa]);
-                    if (++sa == NST) sa = 0;
+                    if (i % CPS == CPS - 1 || i == je - 1) {
+                        tc::mbar_arrive(&afree[sa]);
+                        if (++sa == NST) sa = 0;
+                    }
                 }
                 if (!ok) break;
                 tc::mbar_arrive(&tfree[W & (TC_NB - 1)]);
@@ -777,106 +789,115 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             double S = 0.0;
             for (int pp = it.pa; pp < it.pz && ok; ++pp) {
                 const int jb = pp * pw, je = min(C, jb + pw);
-                for (int t = 0; t < je; ++t, ++T) {
+                // T counts A stages: each holds CPS chunks t0 .. t0 + CPS - 1 of the pass
+                for (int t0 = 0; t0 < je; t0 += CPS, ++T) {
                     if (T >= NST) {
-                        // the A stage is free once the epilogue of step T - NST has released it
+                        // the A stage is free once the epilogue has released stage T - NST
                         ok = __all_sync(0xffffffffu, tc::mbar_wait(&afree[sa], (uint32_t)(ua ^ 1), abort_flag,
                                                                    b.wait_limit_ns));
                         if (!ok) break;
                     }
-                    uint64_t s2 = 0;   // packed normalisation partial sums (0.0f, 0.0f)
-                    uint32_t hw[4], lw[4];
 #pragma unroll
-                    for (int e2 = 0; e2 < 2; ++e2) {
-                        const int j = t * (TC_MPC / 2) + p * 2 + e2;   // mics 2j, 2j+1
-                        const float4 pa = mp4[2 * j], pb = mp4[2 * j + 1];
-                        const uint64_t dx = tc::f2_sub(GX, tc::f2(pa.x, pa.y));
-                        const uint64_t dy = tc::f2_sub(GY, tc::f2(pa.z, pa.w));
-                        const uint64_t dz = tc::f2_sub(GZ, tc::f2(pb.x, pb.y));
-                        const uint64_t r2 = tc::f2_fma(dz, dz, tc::f2_fma(dy, dy, tc::f2_mul(dx, dx)));
-                        float r2a, r2b;
-                        tc::f2_split(r2, r2a, r2b);
-                        // 1/r: hardware rsqrt (~2^-22 relative) and one Newton step y *= 1.5 - 0.5 r^2 y^2
-                        uint64_t y = tc::f2(tc::rsqrt_approx(r2a), tc::rsqrt_approx(r2b));
-                        y = tc::f2_mul(y, tc::f2_fma(tc::f2_mul(tc::f2_mul(r2, y), y), NHALF, THALF));
-                        const uint64_t r = tc::f2_mul(r2, y);
-                        // xn = -(k r) reduced: cos(xn) = Re h / w and sin(xn) = Im h / w
-                        float xa, xb;
-                        if (!SPLIT) {
-                            // TF32 and FP16 keep 11 significant bits: -k r in FP32 (k as a float-float) feeds
-                            // the hardware sincos directly, which reduces the argument by whole turns
-                            tc::f2_split(tc::f2_fma(NKL, r, tc::f2_mul(NKH, r)), xa, xb);
-                        } else {
-                            // k r as an exact float-float product, reduced by the 3-term 2*pi
-                            const uint64_t ph = tc::f2_mul(KH, r);
-                            const uint64_t pl = tc::f2_fma(KL, r, tc::f2_fma(KH, r, tc::f2_mul(NKH, r)));
-                            const uint64_t MAG = tc::f2_splat(12582912.f);
-                            const uint64_t nnq = tc::f2_sub(MAG, tc::f2_fma(ph, tc::f2_splat(TC_INV2PI), MAG));
-                            uint64_t x = tc::f2_fma(nnq, tc::f2_splat(TC_P2A), ph);
-                            x = tc::f2_fma(nnq, tc::f2_splat(TC_P2B), x);
-                            x = tc::f2_fma(nnq, tc::f2_splat(TC_P2C), x);
-                            tc::f2_split(tc::f2_add(x, pl), xa, xb);
-                            xa = -xa;
-                            xb = -xb;
-                        }
-                        float sa_, ca_, sb_, cb_;
-                        tc::sincos_approx(xa, sa_, ca_);
-                        tc::sincos_approx(xb, sb_, cb_);
-                        uint64_t vre = tc::f2(ca_, cb_), vim = tc::f2(sa_, sb_);
-                        // steering weight: 1, r (inverse, times the mics' table weights: 0 for padding)
-                        // or 1/r (true level / location)
-                        if (ST == 2) {
-                            const uint64_t wt = tc::f2(pb.z, pb.w);
-                            const uint64_t w = tc::f2_mul(r, wt);
-                            s2 = tc::f2_fma(r2, wt, s2);
-                            vre = tc::f2_mul(vre, w);
-                            vim = tc::f2_mul(vim, w);
-                        } else if (ST >= 3) {
-                            s2 = tc::f2_fma(y, y, s2);
-                            vre = tc::f2_mul(vre, y);
-                            vim = tc::f2_mul(vim, y);
-                        }
-                        float vr[2], vi[2];
-                        tc::f2_split(vre, vr[0], vr[1]);
-                        tc::f2_split(vim, vi[0], vi[1]);
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int e = 2 * e2 + h;
-                            if (TF32) {   // FP32 operand rounded to TF32: (re, im) of mic e in hw[e], lw[e]
-                                hw[e] = tf32_bits(vr[h]);
-                                lw[e] = tf32_bits(vi[h]);
-                                continue;
+                    for (int c = 0; c < CPS; ++c) {
+                        // a pass's odd last chunk: the second slot repeats the first chunk's arithmetic (so both
+                        // slots' instructions interleave) and stores nothing
+                        const bool live = c == 0 || t0 + c < je;
+                        const int t = live ? t0 + c : t0;
+                        uint64_t s2 = 0;   // packed normalisation partial sums (0.0f, 0.0f)
+                        uint32_t hw[4], lw[4];
+    #pragma unroll
+                        for (int e2 = 0; e2 < 2; ++e2) {
+                            const int j = t * (TC_MPC / 2) + p * 2 + e2;   // mics 2j, 2j+1
+                            const float4 pa = mp4[2 * j], pb = mp4[2 * j + 1];
+                            const uint64_t dx = tc::f2_sub(GX, tc::f2(pa.x, pa.y));
+                            const uint64_t dy = tc::f2_sub(GY, tc::f2(pa.z, pa.w));
+                            const uint64_t dz = tc::f2_sub(GZ, tc::f2(pb.x, pb.y));
+                            const uint64_t r2 = tc::f2_fma(dz, dz, tc::f2_fma(dy, dy, tc::f2_mul(dx, dx)));
+                            float r2a, r2b;
+                            tc::f2_split(r2, r2a, r2b);
+                            // 1/r: hardware rsqrt (~2^-22 relative) and one Newton step y *= 1.5 - 0.5 r^2 y^2
+                            uint64_t y = tc::f2(tc::rsqrt_approx(r2a), tc::rsqrt_approx(r2b));
+                            y = tc::f2_mul(y, tc::f2_fma(tc::f2_mul(tc::f2_mul(r2, y), y), NHALF, THALF));
+                            const uint64_t r = tc::f2_mul(r2, y);
+                            // xn = -(k r) reduced: cos(xn) = Re h / w and sin(xn) = Im h / w
+                            float xa, xb;
+                            if (!SPLIT) {
+                                // TF32 and FP16 keep 11 significant bits: -k r in FP32 (k as a float-float) feeds
+                                // the hardware sincos directly, which reduces the argument by whole turns
+                                tc::f2_split(tc::f2_fma(NKL, r, tc::f2_mul(NKH, r)), xa, xb);
+                            } else {
+                                // k r as an exact float-float product, reduced by the 3-term 2*pi
+                                const uint64_t ph = tc::f2_mul(KH, r);
+                                const uint64_t pl = tc::f2_fma(KL, r, tc::f2_fma(KH, r, tc::f2_mul(NKH, r)));
+                                const uint64_t MAG = tc::f2_splat(12582912.f);
+                                const uint64_t nnq = tc::f2_sub(MAG, tc::f2_fma(ph, tc::f2_splat(TC_INV2PI), MAG));
+                                uint64_t x = tc::f2_fma(nnq, tc::f2_splat(TC_P2A), ph);
+                                x = tc::f2_fma(nnq, tc::f2_splat(TC_P2B), x);
+                                x = tc::f2_fma(nnq, tc::f2_splat(TC_P2C), x);
+                                tc::f2_split(tc::f2_add(x, pl), xa, xb);
+                                xa = -xa;
+                                xb = -xb;
                             }
-                            if (HALF) {   // FP16 pair (re, im), one packed conversion
-                                const __half2 f2h = __floats2half2_rn(vr[h], vi[h]);
-                                hw[e] = *reinterpret_cast<const uint32_t *>(&f2h);
-                                continue;
+                            float sa_, ca_, sb_, cb_;
+                            tc::sincos_approx(xa, sa_, ca_);
+                            tc::sincos_approx(xb, sb_, cb_);
+                            uint64_t vre = tc::f2(ca_, cb_), vim = tc::f2(sa_, sb_);
+                            // steering weight: 1, r (inverse, times the mics' table weights: 0 for padding)
+                            // or 1/r (true level / location)
+                            if (ST == 2) {
+                                const uint64_t wt = tc::f2(pb.z, pb.w);
+                                const uint64_t w = tc::f2_mul(r, wt);
+                                s2 = tc::f2_fma(r2, wt, s2);
+                                vre = tc::f2_mul(vre, w);
+                                vim = tc::f2_mul(vim, w);
+                            } else if (ST >= 3) {
+                                s2 = tc::f2_fma(y, y, s2);
+                                vre = tc::f2_mul(vre, y);
+                                vim = tc::f2_mul(vim, y);
                             }
-                            // split-BF16: hi = bf16(x) (packed pair conversion), lo = bf16(x - hi)
-                            const __nv_bfloat162 h2 = __floats2bfloat162_rn(vr[h], vi[h]);
-                            hw[e] = *reinterpret_cast<const uint32_t *>(&h2);
-                            const float lr = vr[h] - __uint_as_float(hw[e] << 16);
-                            const float li_ = vi[h] - __uint_as_float(hw[e] & 0xFFFF0000u);
-                            const __nv_bfloat162 l2 = __floats2bfloat162_rn(lr, li_);
-                            lw[e] = *reinterpret_cast<const uint32_t *>(&l2);
+                            float vr[2], vi[2];
+                            tc::f2_split(vre, vr[0], vr[1]);
+                            tc::f2_split(vim, vi[0], vi[1]);
+    #pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                const int e = 2 * e2 + h;
+                                if (TF32) {   // FP32 operand rounded to TF32: (re, im) of mic e in hw[e], lw[e]
+                                    hw[e] = tf32_bits(vr[h]);
+                                    lw[e] = tf32_bits(vi[h]);
+                                    continue;
+                                }
+                                if (HALF) {   // FP16 pair (re, im), one packed conversion
+                                    const __half2 f2h = __floats2half2_rn(vr[h], vi[h]);
+                                    hw[e] = *reinterpret_cast<const uint32_t *>(&f2h);
+                                    continue;
+                                }
+                                // split-BF16: hi = bf16(x) (packed pair conversion), lo = bf16(x - hi)
+                                const __nv_bfloat162 h2 = __floats2bfloat162_rn(vr[h], vi[h]);
+                                hw[e] = *reinterpret_cast<const uint32_t *>(&h2);
+                                const float lr = vr[h] - __uint_as_float(hw[e] << 16);
+                                const float li_ = vi[h] - __uint_as_float(hw[e] & 0xFFFF0000u);
+                                const __nv_bfloat162 l2 = __floats2bfloat162_rn(lr, li_);
+                                lw[e] = *reinterpret_cast<const uint32_t *>(&l2);
+                            }
                         }
-                    }
-                    if (TF32) {
-                        // components 8p..8p+7 = core-matrix columns 2p, 2p+1 of the FP32 row
-                        uint8_t *a32 = smem + TcSmem::a_off(sa, 0) + ((row >> 3) << 10) + ((row & 7) << 4) + p * 256;
-                        *reinterpret_cast<uint4 *>(a32) = make_uint4(hw[0], lw[0], hw[1], lw[1]);
-                        *reinterpret_cast<uint4 *>(a32 + 128) = make_uint4(hw[2], lw[2], hw[3], lw[3]);
-                    } else {
-                        *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 0) + a_off_row) =
-                            make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                        if (SPLIT)
-                            *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
-                                make_uint4(lw[0], lw[1], lw[2], lw[3]);
-                    }
-                    if (ST >= 2 && t >= jb) {   // each mic's term once, in its own pass
-                        float sa2, sb2;
-                        tc::f2_split(s2, sa2, sb2);
-                        S += (double)(sa2 + sb2);
+                        if (TF32) {
+                            // components 8p..8p+7 = core-matrix columns 2p, 2p+1 of the FP32 row
+                            uint8_t *a32 = smem + TcSmem::a_off(sa, 0) + ((row >> 3) << 10) + ((row & 7) << 4) + p * 256;
+                            *reinterpret_cast<uint4 *>(a32) = make_uint4(hw[0], lw[0], hw[1], lw[1]);
+                            *reinterpret_cast<uint4 *>(a32 + 128) = make_uint4(hw[2], lw[2], hw[3], lw[3]);
+                        } else if (live) {
+                            // FP16: chunk c of the stage in slot c; split BF16: hi and lo halves
+                            *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, HALF ? c : 0) + a_off_row) =
+                                make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                            if (SPLIT)
+                                *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
+                                    make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                        }
+                        if (ST >= 2 && live && t >= jb) {   // each mic's term once, in its own pass
+                            float sa2, sb2;
+                            tc::f2_split(s2, sa2, sb2);
+                            S += (double)(sa2 + sb2);
+                        }
                     }
                     tc::fence_proxy_async_smem();
                     tc::mbar_arrive(&full_a[sa]);
@@ -1057,7 +1078,9 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
     // the deepest A ring that fits beside this batch's mic table (+1 KB of alignment slack)
     int ns = TC_ASTAGES_MAX;
     while (ns > TC_ASTAGES_MIN && TcSmem::total(ns, mp_max) + 1024 > smem_max) --ns;
-    bt.nstages = ns;
+    // an FP16 stage carries two chunks; chunks in flight (stages x chunks per stage) stay within the
+    // step barrier ring
+    bt.nstages = precision == ACB_TC_FP16 ? min(ns, TC_NB / 2) : ns;
     int smem = TcSmem::total(ns, mp_max) + 1024;
     // each CTA takes all 512 TMEM columns and must be alone on its SM: size the shared memory so
     // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)

@@ -34,7 +34,10 @@ METRIC = 'map grid-pts*bins/s (CSM + map, 256 mics, 401x401 grid, 513 bins)'
 UNIT = 'grid-pts*bins/s'
 # DRAM bytes of one tensor-core map launch per bin of the 256-mic workload (ncu capture of 4 bins:
 # dram__bytes_read.sum + dram__bytes_write.sum, divided by 4)
-TC_TRAFFIC_PER_BIN = {'tf32': 1.54e6, 'bf16x3': 1.54e6}
+# DRAM bytes (read + write) of one tensor-core map launch per bin of the 256-mic workload: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of the whole 513-bin launch, divided by 513 (writes still
+# in L2 at the kernel's end not counted); split BF16 reads the same R' bytes as TF32
+TC_TRAFFIC_PER_BIN = {'fp16': 762.7e6 / 513, 'tf32': 913.5e6 / 513, 'bf16x3': 913.5e6 / 513}
 TC_PREC_INDEX = {'bf16x3': 0, 'tf32': 1, 'fp16': 2}
 TC_DTYPE = {'tf32': 'tf32 / f32 accum', 'bf16x3': 'bf16x3 (split) / f32 accum',
             'fp16': 'fp16 (R\' scaled per bin) / f32 accum'}
@@ -1102,7 +1105,9 @@ def main():
 
     # the forms side by side on the same CSM: both tensor-core precisions over all bins, and the plain
     # FP64 form on a spread of 6 bins (its rate per grid-pt x bin does not depend on the bin)
-    acc_bins = np.unique(np.linspace(2, nbins - 1, 6).round().astype(int))
+    acc_bins = np.unique(np.linspace(min(2, nbins - 1), nbins - 1, 6).round().astype(int))
+    if acc_bins.min() < 0 or acc_bins.max() >= nbins:   # checked on the host, before any device indexing
+        raise ValueError(f'accuracy bins {acc_bins.tolist()} outside the {nbins} map bins')
     sel = torch.as_tensor(acc_bins, device=dev)
     accuracy, forms = None, {}
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -1176,8 +1181,9 @@ def main():
         if prec == 'tf32':
             roof['frac_of_tf32_gemm_here'] = achieved_tf / gp['tf32_tflops']
     if roof['traffic'] is not None:
-        roof['traffic_note'] = ('DRAM bytes per launch: ncu dram__bytes_read+write of a 4-bin capture, scaled by '
-                                'bins (R\' tiles per bin are the traffic; the grid and output add 8 B per point)')
+        roof['traffic_note'] = ('DRAM bytes per launch: ncu dram__bytes_read+write of the whole 513-bin launch '
+                                '(per-bin figure x bins); algorithmic bytes: the map written once plus each bin\'s R\' '
+                                'tiles read once')
 
     # end to end through the public API (pinned host samples -> host result)
     e2e = None
