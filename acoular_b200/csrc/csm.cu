@@ -177,6 +177,184 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
 }
 
 // ------------------------------------------------------------------------------------------------
+// Tensor-core operand tiles straight from the samples, four windows per CTA (fft4_tc_kernel).
+// The tile layout is K-major: a 16-byte core-matrix row holds 4 consecutive windows (TF32) or 8
+// (BF16) of one spectrum component, so a CTA that transforms 4 consecutive windows of `mpb` mics
+// stores whole 16-byte rows (TF32) or half rows (BF16) instead of one 4-byte value per window.
+// The transform runs in FP32 (the operands are rounded to TF32 or split into BF16 hi + lo right
+// after it, so FP64 arithmetic buys nothing): complex points are 8 bytes, half the shared-memory
+// traffic of the FP64 transform.  Padded windows (>= the chunk's count, up to 32 KC) and padded
+// mics (up to 16 R) are written as zeros, so the operand buffer needs no clearing beforehand.
+// ------------------------------------------------------------------------------------------------
+// Shared-memory slot of point j: one padding slot per 16 points (8-byte points), so that the passes'
+// strided accesses spread over the banks.
+__device__ __forceinline__ int zpf(int j) { return j + (j >> 4); }
+__host__ __device__ constexpr int fft_stride_f(int H) { return H + (H >> 4) + 1; }
+
+// s (1..3) consecutive radix-2 DIT stages on a bit-reversed FP32 sequence (see fft_pass); the
+// twiddles W_N^e come from a shared-memory FP32 copy of the table.
+template <int S>
+__device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int L1, int task, int N, const float2 *__restrict__ twf)
+{
+    const int half1 = L1 >> 1;
+    const int Ls = L1 << (S - 1);
+    const int grp = task / half1, pos = task % half1;
+    const int base = grp * Ls + pos;
+    float2 v[1 << S];
+#pragma unroll
+    for (int t = 0; t < (1 << S); ++t) v[t] = z[zpf(base + t * half1)];
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+        const int L = L1 << q, hf = L >> 1;
+        const int stride = N / L;
+#pragma unroll
+        for (int t = 0; t < (1 << S); ++t) {
+            if (t & (1 << q)) continue;
+            const int i0 = base + t * half1;
+            const float2 w = twf[(i0 % hf) * stride];
+            const float2 b = v[t + (1 << q)];
+            const float br = b.x * w.x - b.y * w.y;
+            const float bi = b.x * w.y + b.y * w.x;
+            const float2 a = v[t];
+            v[t] = make_float2(a.x + br, a.y + bi);
+            v[t + (1 << q)] = make_float2(a.x - br, a.y - bi);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < (1 << S); ++t) z[zpf(base + t * half1)] = v[t];
+}
+
+constexpr int FFT4_WIN = 4;   // windows per CTA
+
+template <typename TS, int OUT>
+__global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ samples, int M, int N, int hop, int64_t w0,
+                                                      int64_t nw, int mpb, const double *__restrict__ window,
+                                                      const double2 *__restrict__ tw, int bin_lo, int nbins,
+                                                      void *__restrict__ out, int R, int KC, int64_t lo_elems)
+{
+    extern __shared__ __align__(16) uint8_t fsm[];
+    const int H = N >> 1;
+    const int st = fft_stride_f(H);
+    float2 *zs = reinterpret_cast<float2 *>(fsm);                 // [FFT4_WIN][mpb][st]
+    float2 *twf = zs + FFT4_WIN * mpb * st;                       // [H]
+    float *wf = reinterpret_cast<float *>(twf + H);               // [N]
+    int logH = 0;
+    while ((1 << logH) < H) ++logH;
+    const int wg = blockIdx.y;                                     // windows 4 wg .. 4 wg + 3 of the chunk
+    const int m0 = blockIdx.x * mpb;
+    for (int i = threadIdx.x; i < H; i += blockDim.x) {
+        const double2 t = tw[i];
+        twf[i] = make_float2((float)t.x, (float)t.y);
+    }
+    for (int i = threadIdx.x; i < N; i += blockDim.x) wf[i] = (float)window[i];
+    __syncthreads();
+
+    // load + window + bit-reversed placement; windows past the chunk and padding mics are zeros
+    for (int idx = threadIdx.x; idx < FFT4_WIN * H * mpb; idx += blockDim.x) {
+        const int ml = idx % mpb;
+        const int j = (idx / mpb) % H;
+        const int wi = idx / (mpb * H);
+        const int64_t w = (int64_t)wg * FFT4_WIN + wi;
+        const int m = m0 + ml;
+        float2 v = make_float2(0.f, 0.f);
+        if (w < nw && m < M) {
+            const TS *src = samples + ((w0 + w) * (int64_t)hop + 2 * j) * M + m;
+            v = make_float2((float)src[0] * wf[2 * j], (float)src[M] * wf[2 * j + 1]);
+        }
+        const int jr = logH ? (int)(__brev((unsigned)j) >> (32 - logH)) : 0;
+        zs[(wi * mpb + ml) * st + zpf(jr)] = v;
+    }
+    __syncthreads();
+
+    // radix-2 DIT stages, up to three per pass, over all 4 mpb sequences
+    const int nseq = FFT4_WIN * mpb;
+    for (int sg = 0; sg < logH;) {
+        const int S = logH - sg >= 3 ? 3 : logH - sg;
+        const int L1 = 2 << sg;
+        const int ntask = H >> S;
+        for (int idx = threadIdx.x; idx < nseq * ntask; idx += blockDim.x) {
+            const int q = idx / ntask;
+            const int task = idx - q * ntask;
+            if (S == 3) fft_pass_f<3>(zs + q * st, L1, task, N, twf);
+            else if (S == 2) fft_pass_f<2>(zs + q * st, L1, task, N, twf);
+            else fft_pass_f<1>(zs + q * st, L1, task, N, twf);
+        }
+        __syncthreads();
+        sg += S;
+    }
+
+    // real split of each bin for the 4 windows, then one store per tile row (Re row 2m, Im row 2m+1)
+    const int col0 = (wg * FFT4_WIN) & 31;
+    const int64_t kc = (wg * FFT4_WIN) >> 5;
+    for (int idx = threadIdx.x; idx < nbins * mpb; idx += blockDim.x) {
+        const int ml = idx % mpb;
+        const int b = idx / mpb;
+        const int k = bin_lo + b;
+        const int kh = k % H, kc2 = (H - kh) % H;
+        const float2 wk = k < H ? twf[k] : make_float2(-1.f, 0.f);
+        float xr[FFT4_WIN], xi[FFT4_WIN];
+#pragma unroll
+        for (int wi = 0; wi < FFT4_WIN; ++wi) {
+            const float2 *z = zs + (wi * mpb + ml) * st;
+            const float2 zk = z[zpf(kh)], zc = z[zpf(kc2)];
+            const float er = 0.5f * (zk.x + zc.x), ei = 0.5f * (zk.y - zc.y);
+            const float orr = 0.5f * (zk.y + zc.y), oi = -0.5f * (zk.x - zc.x);
+            xr[wi] = er + (wk.x * orr - wk.y * oi);
+            xi[wi] = ei + (wk.x * oi + wk.y * orr);
+        }
+        const int m = m0 + ml;                                    // padded mics carry zeros
+        const int rowc = 2 * m;
+        const int64_t tile = ((int64_t)b * KC + kc) * R + (rowc >> 5);
+        const int r0 = rowc & 31;
+        if (OUT == OUT_TF32) {
+            uint32_t *t = reinterpret_cast<uint32_t *>(out) + tile * 1024;
+            *reinterpret_cast<uint4 *>(t + tile_off_tf32(r0, col0)) =
+                make_uint4(tf32_bits(xr[0]), tf32_bits(xr[1]), tf32_bits(xr[2]), tf32_bits(xr[3]));
+            *reinterpret_cast<uint4 *>(t + tile_off_tf32(r0 + 1, col0)) =
+                make_uint4(tf32_bits(xi[0]), tf32_bits(xi[1]), tf32_bits(xi[2]), tf32_bits(xi[3]));
+        } else {
+            __nv_bfloat16 *t = reinterpret_cast<__nv_bfloat16 *>(out) + tile * 1024;
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {   // Re row, Im row
+                const float *x = part ? xi : xr;
+                uint32_t hv[2], lv[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const __nv_bfloat162 hi = __floats2bfloat162_rn(x[2 * h], x[2 * h + 1]);
+                    const float2 hf = __bfloat1622float2(hi);
+                    const __nv_bfloat162 lo = __floats2bfloat162_rn(x[2 * h] - hf.x, x[2 * h + 1] - hf.y);
+                    hv[h] = *reinterpret_cast<const uint32_t *>(&hi);
+                    lv[h] = *reinterpret_cast<const uint32_t *>(&lo);
+                }
+                const int o = tile_off(r0 + part, col0);
+                *reinterpret_cast<uint2 *>(t + o) = make_uint2(hv[0], hv[1]);
+                *reinterpret_cast<uint2 *>(t + lo_elems + o) = make_uint2(lv[0], lv[1]);
+            }
+        }
+    }
+}
+
+// Mics per CTA of fft4_tc_kernel: about 72 KB of FP32 sequences (2 to 3 CTAs per SM), power of two
+// <= 16 (so that the 16 R padded mics split evenly); 0 if even one mic's 4 windows do not fit.
+static int fft4_mics_per_block(int N)
+{
+    const size_t per_mic = (size_t)FFT4_WIN * fft_stride_f(N / 2) * sizeof(float2);
+    const size_t tables = (size_t)(N / 2) * sizeof(float2) + (size_t)N * sizeof(float);
+    if (per_mic + tables > 200 * 1024) return 0;
+    int mpb = 16;
+    while (mpb > 1 && (size_t)mpb * per_mic > 72 * 1024) mpb >>= 1;
+    return mpb;
+}
+
+bool fft_tiles_written_whole(int block_size) { return fft4_mics_per_block(block_size) > 0; }
+
+static size_t fft4_smem_bytes(int N, int mpb)
+{
+    return (size_t)FFT4_WIN * mpb * fft_stride_f(N / 2) * sizeof(float2) + (size_t)(N / 2) * sizeof(float2) +
+           (size_t)N * sizeof(float);
+}
+
+// ------------------------------------------------------------------------------------------------
 // Large blocks (N > 16384): one mic's N/2-point sequence no longer fits a CTA's shared memory.  It is
 // split by decimation in time into D = N / 16384 interleaved sub-sequences z[d + D i] of 8192 points:
 // fft_sub_kernel transforms each one in shared memory with the passes above (sub-spectra Y_d to a
@@ -461,6 +639,30 @@ int fft_launch(const void *samples, int sample_dtype, int out_form, int num_mics
                                                                 num_bins, tw, out, R, KC, lo_elems); break;
         }
         return check_launch();
+    }
+    if (out_form >= OUT_TF32) {
+        const int mpb4 = fft4_mics_per_block(block_size);
+        if (mpb4 > 0) {
+            // every tile row (16 R padded mics) and column (32 KC padded windows) is written
+            const dim3 g4((unsigned)(R * 16 / mpb4), (unsigned)(KC * 32 / FFT4_WIN));
+            const size_t smem4 = fft4_smem_bytes(block_size, mpb4);
+#define ACB_FFT4_LAUNCH(TS, OF)                                                                                     \
+    do {                                                                                                            \
+        auto kern = fft4_tc_kernel<TS, OF>;                                                                         \
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem4);                        \
+        kern<<<g4, 256, smem4, s>>>(reinterpret_cast<const TS *>(samples), num_mics, block_size, hop, first_window,  \
+                                    num_windows, mpb4, window, tw, bin_lo, num_bins, out, R, KC, lo_elems);        \
+    } while (0)
+            if (sample_dtype == ACB_F32) {
+                if (out_form == OUT_TF32) ACB_FFT4_LAUNCH(float, OUT_TF32);
+                else ACB_FFT4_LAUNCH(float, OUT_BF16);
+            } else {
+                if (out_form == OUT_TF32) ACB_FFT4_LAUNCH(double, OUT_TF32);
+                else ACB_FFT4_LAUNCH(double, OUT_BF16);
+            }
+#undef ACB_FFT4_LAUNCH
+            return check_launch();
+        }
     }
     const int mpb = fft_mics_per_block(block_size);
     const dim3 g1((num_mics + mpb - 1) / mpb, (unsigned)num_windows);

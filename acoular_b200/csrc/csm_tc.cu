@@ -260,11 +260,13 @@ int csm_tc_accumulate(const void *samples, int sample_dtype, int num_mics, int b
     const int R = csm_tc_row_tiles(num_mics);
     const int KC = (int)((num_windows + 31) / 32);
     const size_t ops_bytes = csm_tc_workspace_bytes(num_mics, num_bins, num_windows);
-    // padded windows and padded mics must read as zero
-    cudaError_t e = cudaMemsetAsync(workspace, 0, ops_bytes, s);
-    if (e != cudaSuccess) {
-        set_cuda_error(e);
-        return ACB_ERR_CUDA;
+    // padded windows and padded mics must read as zero (the four-window transform writes them itself)
+    if (!fft_tiles_written_whole(block_size)) {
+        const cudaError_t e = cudaMemsetAsync(workspace, 0, ops_bytes, s);
+        if (e != cudaSuccess) {
+            set_cuda_error(e);
+            return ACB_ERR_CUDA;
+        }
     }
     const int64_t lo_elems = (int64_t)num_bins * KC * R * 1024;   // BF16: lo tiles after the hi tiles
     int st = fft_launch(samples, sample_dtype, tf32 ? 2 : 3, num_mics, block_size, hop, first_window, num_windows,

@@ -27,7 +27,8 @@ def _samples(S, M, dtype, seed):
 @pytest.mark.parametrize('precision', ['tc_tf32', 'tc_bf16x3'])
 @pytest.mark.parametrize('M,N,S,dtype', [(8, 128, 4000, torch.float64), (40, 256, 9000, torch.float32),
                                          (64, 1024, 51200, torch.float32), (130, 512, 20000, torch.float64),
-                                         (256, 1024, 40000, torch.float32)])
+                                         (256, 1024, 40000, torch.float32), (20, 4096, 40000, torch.float32),
+                                         (9, 8192, 60000, torch.float64), (6, 16384, 70000, torch.float32)])
 def test_tc_csm_vs_f64(precision, M, N, S, dtype):
     from acoular_b200 import device as D
     x = _samples(S, M, dtype, seed=M + N)
