@@ -44,28 +44,28 @@ __device__ __forceinline__ int zp(int j) { return j + (j >> 3); }
 // padded length of one mic's sequence of H points (an odd number of 16-byte slots past the padding)
 __host__ __device__ constexpr int fft_stride(int H) { return H + (H >> 3) + 1; }
 
-// s (1..3) consecutive radix-2 DIT stages of lengths L1, 2 L1, .., on a bit-reversed sequence z of
-// H points (one mic).  Task `task` in [0, H / 2^s) owns points base + t * L1/2, t = 0 .. 2^s - 1.
+// s (1..3) consecutive radix-2 DIT stages of lengths L1 = 2^(sg + 1), 2 L1, .., on a bit-reversed
+// sequence z of H points (one mic).  Task `task` in [0, H / 2^s) owns points base + t * L1/2,
+// t = 0 .. 2^s - 1.  All lengths are powers of two (logN = log2 N): shifts and masks index the
+// points and the twiddles W_N^e.
 template <int S>
-__device__ __forceinline__ void fft_pass(double2 *__restrict__ z, int L1, int task, int N,
+__device__ __forceinline__ void fft_pass(double2 *__restrict__ z, int sg, int task, int logN,
                                          const double2 *__restrict__ tw)
 {
-    const int half1 = L1 >> 1;
-    const int Ls = L1 << (S - 1);            // length of the last stage of the pass
-    const int grp = task / half1, pos = task % half1;
-    const int base = grp * Ls + pos;
+    const int half1 = 1 << sg;
+    const int base = ((task >> sg) << (sg + S)) + (task & (half1 - 1));   // the pass spans 2^(sg + S) points
     double2 v[1 << S];
 #pragma unroll
     for (int t = 0; t < (1 << S); ++t) v[t] = z[zp(base + t * half1)];
 #pragma unroll
     for (int q = 0; q < S; ++q) {
-        const int L = L1 << q, hf = L >> 1;
-        const int stride = N / L;
+        const int hf = half1 << q;                       // half the stage length L = 2^(sg + 1 + q)
+        const int shift = logN - (sg + 1 + q);           // W_L^i = W_N^(i N / L)
 #pragma unroll
         for (int t = 0; t < (1 << S); ++t) {
             if (t & (1 << q)) continue;
             const int i0 = base + t * half1;
-            const double2 w = __ldg(tw + (i0 % hf) * stride);
+            const double2 w = __ldg(tw + ((i0 & (hf - 1)) << shift));
             const double2 b = v[t + (1 << q)];
             const double br = b.x * w.x - b.y * w.y;
             const double bi = b.x * w.y + b.y * w.x;
@@ -145,14 +145,13 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
     // radix-2 DIT stages, up to three per pass
     for (int st = 0; st < logH;) {
         const int S = logH - st >= 3 ? 3 : logH - st;
-        const int L1 = 2 << st;
-        const int ntask = H >> S;
-        for (int idx = threadIdx.x; idx < nm * ntask; idx += blockDim.x) {
-            const int ml = idx / ntask;
-            const int task = idx - ml * ntask;
-            if (S == 3) fft_pass<3>(zs + ml * fft_stride(H), L1, task, N, tw);
-            else if (S == 2) fft_pass<2>(zs + ml * fft_stride(H), L1, task, N, tw);
-            else fft_pass<1>(zs + ml * fft_stride(H), L1, task, N, tw);
+        const int logT = logH - S;   // H / 2^S tasks per mic
+        for (int idx = threadIdx.x; idx < nm << logT; idx += blockDim.x) {
+            const int ml = idx >> logT;
+            const int task = idx & ((1 << logT) - 1);
+            if (S == 3) fft_pass<3>(zs + ml * fft_stride(H), st, task, logH + 1, tw);
+            else if (S == 2) fft_pass<2>(zs + ml * fft_stride(H), st, task, logH + 1, tw);
+            else fft_pass<1>(zs + ml * fft_stride(H), st, task, logH + 1, tw);
         }
         __syncthreads();
         st += S;
@@ -191,27 +190,27 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
 __device__ __forceinline__ int zpf(int j) { return j + (j >> 4); }
 __host__ __device__ constexpr int fft_stride_f(int H) { return H + (H >> 4) + 1; }
 
-// s (1..3) consecutive radix-2 DIT stages on a bit-reversed FP32 sequence (see fft_pass); the
-// twiddles W_N^e come from a shared-memory FP32 copy of the table.
+// s (1..3) consecutive radix-2 DIT stages, the first of length 2^(sg + 1), on a bit-reversed FP32
+// sequence (see fft_pass); the twiddles W_N^e come from a shared-memory FP32 copy of the table.  All
+// lengths are powers of two, so the index arithmetic is shifts and masks (logN = log2 N).
 template <int S>
-__device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int L1, int task, int N, const float2 *__restrict__ twf)
+__device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int sg, int task, int logN,
+                                           const float2 *__restrict__ twf)
 {
-    const int half1 = L1 >> 1;
-    const int Ls = L1 << (S - 1);
-    const int grp = task / half1, pos = task % half1;
-    const int base = grp * Ls + pos;
+    const int half1 = 1 << sg;
+    const int base = ((task >> sg) << (sg + S)) + (task & (half1 - 1));
     float2 v[1 << S];
 #pragma unroll
     for (int t = 0; t < (1 << S); ++t) v[t] = z[zpf(base + t * half1)];
 #pragma unroll
     for (int q = 0; q < S; ++q) {
-        const int L = L1 << q, hf = L >> 1;
-        const int stride = N / L;
+        const int hf = half1 << q;                       // half the stage length L = 2^(sg + 1 + q)
+        const int shift = logN - (sg + 1 + q);           // W_L^i = W_N^(i N / L)
 #pragma unroll
         for (int t = 0; t < (1 << S); ++t) {
             if (t & (1 << q)) continue;
             const int i0 = base + t * half1;
-            const float2 w = twf[(i0 % hf) * stride];
+            const float2 w = twf[(i0 & (hf - 1)) << shift];
             const float2 b = v[t + (1 << q)];
             const float br = b.x * w.x - b.y * w.y;
             const float bi = b.x * w.y + b.y * w.x;
@@ -238,8 +237,9 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
     float2 *zs = reinterpret_cast<float2 *>(fsm);                 // [FFT4_WIN][mpb][st]
     float2 *twf = zs + FFT4_WIN * mpb * st;                       // [H]
     float *wf = reinterpret_cast<float *>(twf + H);               // [N]
-    int logH = 0;
+    int logH = 0, logP = 0;
     while ((1 << logH) < H) ++logH;
+    while ((1 << logP) < mpb) ++logP;                              // mpb is a power of two
     const int wg = blockIdx.y;                                     // windows 4 wg .. 4 wg + 3 of the chunk
     const int m0 = blockIdx.x * mpb;
     for (int i = threadIdx.x; i < H; i += blockDim.x) {
@@ -251,9 +251,9 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
 
     // load + window + bit-reversed placement; windows past the chunk and padding mics are zeros
     for (int idx = threadIdx.x; idx < FFT4_WIN * H * mpb; idx += blockDim.x) {
-        const int ml = idx % mpb;
-        const int j = (idx / mpb) % H;
-        const int wi = idx / (mpb * H);
+        const int ml = idx & (mpb - 1);
+        const int j = (idx >> logP) & (H - 1);
+        const int wi = idx >> (logP + logH);
         const int64_t w = (int64_t)wg * FFT4_WIN + wi;
         const int m = m0 + ml;
         float2 v = make_float2(0.f, 0.f);
@@ -270,14 +270,13 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
     const int nseq = FFT4_WIN * mpb;
     for (int sg = 0; sg < logH;) {
         const int S = logH - sg >= 3 ? 3 : logH - sg;
-        const int L1 = 2 << sg;
-        const int ntask = H >> S;
-        for (int idx = threadIdx.x; idx < nseq * ntask; idx += blockDim.x) {
-            const int q = idx / ntask;
-            const int task = idx - q * ntask;
-            if (S == 3) fft_pass_f<3>(zs + q * st, L1, task, N, twf);
-            else if (S == 2) fft_pass_f<2>(zs + q * st, L1, task, N, twf);
-            else fft_pass_f<1>(zs + q * st, L1, task, N, twf);
+        const int logT = logH - S;                                 // H / 2^S tasks per sequence
+        for (int idx = threadIdx.x; idx < nseq << logT; idx += blockDim.x) {
+            const int q = idx >> logT;
+            const int task = idx & ((1 << logT) - 1);
+            if (S == 3) fft_pass_f<3>(zs + q * st, sg, task, logH + 1, twf);
+            else if (S == 2) fft_pass_f<2>(zs + q * st, sg, task, logH + 1, twf);
+            else fft_pass_f<1>(zs + q * st, sg, task, logH + 1, twf);
         }
         __syncthreads();
         sg += S;
@@ -287,10 +286,10 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
     const int col0 = (wg * FFT4_WIN) & 31;
     const int64_t kc = (wg * FFT4_WIN) >> 5;
     for (int idx = threadIdx.x; idx < nbins * mpb; idx += blockDim.x) {
-        const int ml = idx % mpb;
-        const int b = idx / mpb;
+        const int ml = idx & (mpb - 1);
+        const int b = idx >> logP;
         const int k = bin_lo + b;
-        const int kh = k % H, kc2 = (H - kh) % H;
+        const int kh = k & (H - 1), kc2 = (H - kh) & (H - 1);
         const float2 wk = k < H ? twf[k] : make_float2(-1.f, 0.f);
         float xr[FFT4_WIN], xi[FFT4_WIN];
 #pragma unroll
@@ -389,14 +388,15 @@ __global__ void __launch_bounds__(256) fft_sub_kernel(const TS *__restrict__ sam
         zs[zp((int)(__brev((unsigned)i) >> (32 - logHs)))] = make_double2(x0, x1);
     }
     __syncthreads();
+    int logN = 0;
+    while ((1 << logN) < N) ++logN;
     for (int st = 0; st < logHs;) {
         const int S = logHs - st >= 3 ? 3 : logHs - st;
-        const int L1 = 2 << st;
         const int ntask = FFT_SUB_H >> S;
         for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-            if (S == 3) fft_pass<3>(zs, L1, task, N, tw);
-            else if (S == 2) fft_pass<2>(zs, L1, task, N, tw);
-            else fft_pass<1>(zs, L1, task, N, tw);
+            if (S == 3) fft_pass<3>(zs, st, task, logN, tw);
+            else if (S == 2) fft_pass<2>(zs, st, task, logN, tw);
+            else fft_pass<1>(zs, st, task, logN, tw);
         }
         __syncthreads();
         st += S;

@@ -180,8 +180,6 @@ constexpr int TC_NB = 8;       // chunk barrier ring (full_b / done); the produc
 // T + TC_NB - stages, so with at most TC_NB A stages the epilogue has always seen step T first (more
 // stages would let a slot run two phases ahead of its waiter and the parity wait would never pass).
 static_assert(TC_ASTAGES_MAX <= TC_NB, "A ring deeper than the step barrier ring");
-// (with two chunks per stage, the FP16 form, the bound is on chunks: 2 x stages <= TC_NB; the host
-// caps its stages at TC_NB / 2)
 
 __host__ __device__ constexpr int tri_tiles(int C) { return C * (C + 1) / 2; }
 // index of tile (i, j >= i) in the row-major upper-triangular tile order
@@ -358,9 +356,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     // R' tile ring: 32 split-BF16 pairs (hi and lo halves of the ring region), 32 FP32 tiles, or
     // 64 FP16 tiles in the same 128 KB; FP16 ring slot s sits at b_base + s * 2 KB
     constexpr int RING = HALF ? 2 * TC_RING : TC_RING;
-    // chunks per A stage: an FP16 chunk fills half a stage (8 KB), so a stage carries two and the
-    // steering -> MMA -> epilogue handshakes run once per chunk pair (a pass's chunks pair up from its
-    // first; an odd last chunk has its stage alone)
+    // chunks per step: an FP16 chunk fills half an A stage (8 KB), so a stage carries two, and a step
+    // (one A stage, one R' tile barrier, one MMA commit) covers a chunk pair: the steering -> MMA ->
+    // epilogue hand-offs run once per pair (a pass's chunks pair up from its first; an odd last chunk
+    // is a step alone)
     constexpr int CPS = HALF ? 2 : 1;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // operand tiles start on a 1 KB boundary (the launch reserves 1 KB of slack for this)
@@ -415,8 +414,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
     // when i >= 16p; those steps also carry chunk i's dot product and normalisation sum.
     if (warp == TC_WARP_PRODUCER) {
         // ---------------- producer: R' tiles of every step into the tile ring ----------------
-        // Step T takes n consecutive ring tiles starting at the running tile counter U; tile U
-        // reuses slot U % RING, free once the step that held tile U - RING is complete.
+        // Step T (the CPS chunks of one A stage) takes n consecutive ring tiles starting at the running
+        // tile counter U; tile U reuses slot U % RING, free once the step that held tile U - RING is
+        // complete.
         if (lane == 0) {
             uint32_t ustart[TC_NB];   // first ring tile of the last TC_NB steps
             uint32_t U = 0;
@@ -432,8 +432,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                 const __nv_bfloat16 *bl = in.rl + bin * in.bin_stride;
                 for (int pp = it.pa; pp < it.pz && ok; ++pp) {
                     const int jb = pp * pw, je = min(C, jb + pw);
-                    for (int i = 0; i < je && ok; ++i, ++T) {
-                        const int j0 = max(i, jb), n = je - j0;
+                    for (int i0 = 0; i0 < je && ok; i0 += CPS, ++T) {
+                        const int i1 = min(je, i0 + CPS);
+                        int n = 0;   // the step's tiles: chunk i feeds columns j >= max(i, jb)
+                        for (int i = i0; i < i1; ++i) n += je - max(i, jb);
                         // step barriers form a ring of TC_NB: step T - TC_NB must be complete; ring
                         // slots: every step holding a tile <= U + n - 1 - RING must be complete
                         while (ok && (freed < T - TC_NB ||
@@ -447,28 +449,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         ustart[T & (TC_NB - 1)] = U;
                         uint64_t *fb = &full_b[T & (TC_NB - 1)];
                         tc::mbar_arrive_expect_tx(fb, (HALF ? 1u : 2u) * n * TC_TILE_BYTES);   // hi + lo, FP32, FP16
-                        const int64_t src = (int64_t)tile_index(C, i, j0) * TC_TILE_ELEMS;
-                        int j = 0;
-                        while (j < n) {   // contiguous runs of ring slots
-                            const int slot = (int)((U + j) & (RING - 1));
-                            const int run = min(n - j, RING - slot);
-                            const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
-                            if (HALF) {
-                                tc::bulk_g2s(smem + TcSmem::b_base(NST) + slot * TC_TILE_BYTES,
-                                             bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
-                            } else if (TF32) {   // FP32 tiles of 4 KB, ring slot s at b_base + s * 4 KB
-                                tc::bulk_g2s(smem + TcSmem::b_base(NST) + slot * 2 * TC_TILE_BYTES,
-                                             reinterpret_cast<const uint32_t *>(bh) + src + (int64_t)j * TC_TILE_ELEMS,
-                                             2 * bytes, fb);
-                            } else {
-                                tc::bulk_g2s(smem + TcSmem::b_off(NST, slot, 0), bh + src + (int64_t)j * TC_TILE_ELEMS, bytes,
-                                             fb);
-                                tc::bulk_g2s(smem + TcSmem::b_off(NST, slot, 1), bl + src + (int64_t)j * TC_TILE_ELEMS, bytes,
-                                             fb);
+                        for (int i = i0; i < i1; ++i) {
+                            const int j0 = max(i, jb), nc = je - j0;
+                            const int64_t src = (int64_t)tile_index(C, i, j0) * TC_TILE_ELEMS;
+                            int j = 0;
+                            while (j < nc) {   // contiguous runs of ring slots
+                                const int slot = (int)((U + j) & (RING - 1));
+                                const int run = min(nc - j, RING - slot);
+                                const uint32_t bytes = (uint32_t)run * TC_TILE_BYTES;
+                                if (HALF) {
+                                    tc::bulk_g2s(smem + TcSmem::b_base(NST) + slot * TC_TILE_BYTES,
+                                                 bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                                } else if (TF32) {   // FP32 tiles of 4 KB, ring slot s at b_base + s * 4 KB
+                                    tc::bulk_g2s(smem + TcSmem::b_base(NST) + slot * 2 * TC_TILE_BYTES,
+                                                 reinterpret_cast<const uint32_t *>(bh) + src +
+                                                     (int64_t)j * TC_TILE_ELEMS,
+                                                 2 * bytes, fb);
+                                } else {
+                                    tc::bulk_g2s(smem + TcSmem::b_off(NST, slot, 0),
+                                                 bh + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                                    tc::bulk_g2s(smem + TcSmem::b_off(NST, slot, 1),
+                                                 bl + src + (int64_t)j * TC_TILE_ELEMS, bytes, fb);
+                                }
+                                j += run;
                             }
-                            j += run;
+                            U += (uint32_t)nc;
                         }
-                        U += (uint32_t)n;
                         lastT = T;
                     }
                 }
@@ -526,59 +532,62 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         ok = tc::mbar_wait(&tfree[(W - wpt) & (TC_NB - 1)], (uint32_t)(((W - wpt) / TC_NB) & 1),
                                            abort_flag, b.wait_limit_ns);
                     const uint32_t wcol = taddr + (uint32_t)(((W - w_start) % wpt) * width);
-                    for (int i = 0; i < je && ok; ++i) {
-                        if (i % CPS == 0) ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, b.wait_limit_ns);
-                        ok = ok && tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, b.wait_limit_ns);
+                    for (int i0 = 0; i0 < je && ok; i0 += CPS) {
+                        ok = tc::mbar_wait(&full_a[sa], (uint32_t)ua, abort_flag, b.wait_limit_ns) &&
+                             tc::mbar_wait(&full_b[sb], (uint32_t)ub, abort_flag, b.wait_limit_ns);
                         if (!ok) break;
                         tc::tc_fence_after();
-                        const int j0 = max(i, jb), n = je - j0;
-                        const uint32_t dcol = wcol + (uint32_t)(TC_CHUNK * (j0 - jb));
-                        // split the step's n tiles into runs of <= 8 (N <= 256) that do not wrap
-                        const int run0 = min(min(n, 8), (int)(RING - slot0));
-                        const uint32_t slot1 = (slot0 + run0) & (RING - 1);
-                        const int rest = n - run0;
-                        const int run1 = min(min(rest, 8), (int)(RING - slot1));
-                        const uint32_t slot2 = (slot1 + run1) & (RING - 1);
-                        const int run2 = rest - run1;   // at most one more run (n <= 16)
-                        // BF16: K steps of 16 (2) x products hi*hi, hi*lo, lo*hi; TF32: K steps of 8 (4) x 1;
-                        // FP16: K steps of 16 (2) x 1
-                        constexpr int KS = TF32 ? 4 : 2, NPROD = SPLIT ? 3 : 1;
+                        for (int i = i0; i < min(je, i0 + CPS); ++i) {
+                            const int j0 = max(i, jb), n = je - j0;
+                            const uint32_t dcol = wcol + (uint32_t)(TC_CHUNK * (j0 - jb));
+                            // split the step's n tiles into runs of <= 8 (N <= 256) that do not wrap
+                            const int run0 = min(min(n, 8), (int)(RING - slot0));
+                            const uint32_t slot1 = (slot0 + run0) & (RING - 1);
+                            const int rest = n - run0;
+                            const int run1 = min(min(rest, 8), (int)(RING - slot1));
+                            const uint32_t slot2 = (slot1 + run1) & (RING - 1);
+                            const int run2 = rest - run1;   // at most one more run (n <= 16)
+                            // BF16: K steps of 16 (2) x products hi*hi, hi*lo, lo*hi; TF32: K steps of 8 (4) x 1;
+                            // FP16: K steps of 16 (2) x 1
+                            constexpr int KS = TF32 ? 4 : 2, NPROD = SPLIT ? 3 : 1;
 #pragma unroll
-                        for (int ks = 0; ks < KS; ++ks) {
+                            for (int ks = 0; ks < KS; ++ks) {
 #pragma unroll
-                            for (int prod = 0; prod < NPROD; ++prod) {
-                                // A: split-BF16 hi (lo for the third product), FP32, or FP16 chunk i % 2 of the stage
-                                const uint64_t ad =
-                                    a_base + (uint64_t)((sa * 2 + (HALF ? (i & 1) : (prod == 2))) * A_STEP + ks * 16);
-                                const uint64_t bd = b_base + (uint64_t)((prod == 1 ? LO_B : 0u) + ks * 16);
-                                const uint32_t accum = (i == 0 && ks == 0 && prod == 0) ? 0u : 1u;
-                                const uint32_t n0 = idesc0 | ((uint32_t)(run0 * 4) << 17);
-                                const uint32_t n1 = idesc0 | ((uint32_t)(run1 * 4) << 17);
-                                const uint32_t n2 = idesc0 | ((uint32_t)(run2 * 4) << 17);
-                                if (TF32) {
-                                    tc::mma_tf32(dcol, ad, bd + slot0 * T_STEP, n0, accum);
-                                    if (run1 > 0)
-                                        tc::mma_tf32(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP, n1, accum);
-                                    if (run2 > 0)
-                                        tc::mma_tf32(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
-                                                     n2, accum);
-                                } else {
-                                    tc::mma_bf16(dcol, ad, bd + slot0 * T_STEP, n0, accum);
-                                    if (run1 > 0)
-                                        tc::mma_bf16(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP, n1, accum);
-                                    if (run2 > 0)
-                                        tc::mma_bf16(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad, bd + slot2 * T_STEP,
-                                                     n2, accum);
+                                for (int prod = 0; prod < NPROD; ++prod) {
+                                    // A: split-BF16 hi (lo for the third product), FP32, or FP16 chunk
+                                    // i - i0 of the stage
+                                    const int ablk = sa * 2 + (HALF ? (i - i0) : (prod == 2));
+                                    const uint64_t ad = a_base + (uint64_t)(ablk * A_STEP + ks * 16);
+                                    const uint64_t bd = b_base + (uint64_t)((prod == 1 ? LO_B : 0u) + ks * 16);
+                                    const uint32_t accum = (i == 0 && ks == 0 && prod == 0) ? 0u : 1u;
+                                    const uint32_t n0 = idesc0 | ((uint32_t)(run0 * 4) << 17);
+                                    const uint32_t n1 = idesc0 | ((uint32_t)(run1 * 4) << 17);
+                                    const uint32_t n2 = idesc0 | ((uint32_t)(run2 * 4) << 17);
+                                    if (TF32) {
+                                        tc::mma_tf32(dcol, ad, bd + slot0 * T_STEP, n0, accum);
+                                        if (run1 > 0)
+                                            tc::mma_tf32(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP, n1,
+                                                        accum);
+                                        if (run2 > 0)
+                                            tc::mma_tf32(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad,
+                                                        bd + slot2 * T_STEP, n2, accum);
+                                    } else {
+                                        tc::mma_bf16(dcol, ad, bd + slot0 * T_STEP, n0, accum);
+                                        if (run1 > 0)
+                                            tc::mma_bf16(dcol + (uint32_t)(run0 * TC_CHUNK), ad, bd + slot1 * T_STEP, n1,
+                                                        accum);
+                                        if (run2 > 0)
+                                            tc::mma_bf16(dcol + (uint32_t)((run0 + run1) * TC_CHUNK), ad,
+                                                        bd + slot2 * T_STEP, n2, accum);
+                                    }
                                 }
                             }
+                            slot0 = (slot0 + (uint32_t)n) & (RING - 1);
                         }
                         tc::mma_commit(&done[sb]);
                         lastb = sb;
                         lastu = ub;
-                        slot0 = (slot0 + (uint32_t)n) & (RING - 1);
-                        if (i % CPS == CPS - 1 || i == je - 1) {
-                            if (++sa == NST) { sa = 0; ua ^= 1; }
-                        }
+                        if (++sa == NST) { sa = 0; ua ^= 1; }
                         if (++sb == TC_NB) { sb = 0; ub ^= 1; }
                     }
                 }
@@ -618,64 +627,72 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             for (int pp = it.pa; pp < it.pz && ok; ++pp, ++W) {
                 const int jb = pp * pw, je = min(C, jb + pw);
                 const uint32_t wcol = lane_addr + (uint32_t)(((W - w_start) % wpt) * width);
-                for (int i = 0; i < je; ++i, ++T) {
+                for (int i0 = 0; i0 < je; i0 += CPS, ++T) {
                     ok = __all_sync(0xffffffffu, tc::mbar_wait(&done[T & (TC_NB - 1)], (uint32_t)((T / TC_NB) & 1),
                                                                abort_flag, b.wait_limit_ns));
                     if (!ok) break;
-                    if (i >= jb) {
-                        tc::tc_fence_after();
-                        float d[TC_CHUNK];
-                        tc::tmem_ld_x32(wcol + (uint32_t)(TC_CHUNK * (i - jb)), d);
-                        const uint8_t *ahi = smem + TcSmem::a_off(sa, HALF ? (i & 1) : 0) + a_row;
-                        const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;   // split BF16 only
-                        float part = 0.f;
-                        if (TF32) {
-                            // FP32 row: 8 core-matrix columns of 4 values, 128 bytes apart
-                            const uint8_t *a32 = smem + TcSmem::a_off(sa, 0) + ((row >> 3) << 10) + ((row & 7) << 4);
+                    for (int i = i0; i < min(je, i0 + CPS); ++i) {
+                        if (i >= jb) {
+                            tc::tc_fence_after();
+                            float d[TC_CHUNK];
+                            tc::tmem_ld_x32(wcol + (uint32_t)(TC_CHUNK * (i - jb)), d);
+                            const uint8_t *ahi = smem + TcSmem::a_off(sa, HALF ? (i - i0) : 0) + a_row;
+                            const uint8_t *alo = smem + TcSmem::a_off(sa, 1) + a_row;   // split BF16 only
+                            float part = 0.f;
+                            // the 11-bit forms dot in packed FP32: (re, im) component pairs, two accumulators
+                            uint64_t pacc[2] = {0, 0};
+                            if (TF32) {
+                                // FP32 row: 8 core-matrix columns of 4 values, 128 bytes apart
+                                const uint8_t *a32 =
+                                    smem + TcSmem::a_off(sa, 0) + ((row >> 3) << 10) + ((row & 7) << 4);
 #pragma unroll
-                            for (int c4 = 0; c4 < 8; ++c4) {
-                                const float4 v = *reinterpret_cast<const float4 *>(a32 + c4 * 128);
-                                part = fmaf(d[c4 * 4 + 0], v.x, part);
-                                part = fmaf(d[c4 * 4 + 1], v.y, part);
-                                part = fmaf(d[c4 * 4 + 2], v.z, part);
-                                part = fmaf(d[c4 * 4 + 3], v.w, part);
-                            }
-                        }
-                        if (HALF) {
-                            // FP16 row: 4 core-matrix columns of 4 (re, im) pairs, 128 bytes apart
-#pragma unroll
-                            for (int grp = 0; grp < 4; ++grp) {
-                                const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
-                                const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w};
-#pragma unroll
-                                for (int e = 0; e < 4; ++e) {
-                                    const float2 v = __half22float2(*reinterpret_cast<const __half2 *>(&hv[e]));
-                                    part = fmaf(d[grp * 8 + 2 * e], v.x, part);
-                                    part = fmaf(d[grp * 8 + 2 * e + 1], v.y, part);
+                                for (int c4 = 0; c4 < 8; ++c4) {
+                                    const float4 v = *reinterpret_cast<const float4 *>(a32 + c4 * 128);
+                                    const float *dc = d + c4 * 4;
+                                    pacc[0] = tc::f2_fma(tc::f2(dc[0], dc[1]), tc::f2(v.x, v.y), pacc[0]);
+                                    pacc[1] = tc::f2_fma(tc::f2(dc[2], dc[3]), tc::f2(v.z, v.w), pacc[1]);
                                 }
                             }
-                        }
+                            if (HALF) {
+                                // FP16 row: 4 core-matrix columns of 4 (re, im) pairs, 128 bytes apart
 #pragma unroll
-                        for (int grp = 0; grp < (SPLIT ? 4 : 0); ++grp) {
-                            const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
-                            const uint4 lw = *reinterpret_cast<const uint4 *>(alo + grp * 128);
-                            const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w}, lv[4] = {lw.x, lw.y, lw.z, lw.w};
+                                for (int grp = 0; grp < 4; ++grp) {
+                                    const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
+                                    const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w};
 #pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const float vr = __uint_as_float(hv[e] << 16) + __uint_as_float(lv[e] << 16);
-                                const float vi =
-                                    __uint_as_float(hv[e] & 0xFFFF0000u) + __uint_as_float(lv[e] & 0xFFFF0000u);
-                                part = fmaf(d[grp * 8 + 2 * e], vr, part);
-                                part = fmaf(d[grp * 8 + 2 * e + 1], vi, part);
+                                    for (int e = 0; e < 4; ++e) {
+                                        const float2 v = __half22float2(*reinterpret_cast<const __half2 *>(&hv[e]));
+                                        pacc[0] = tc::f2_fma(tc::f2(d[grp * 8 + 2 * e], d[grp * 8 + 2 * e + 1]),
+                                                             tc::f2(v.x, v.y), pacc[0]);
+                                    }
+                                }
                             }
+                            if (!SPLIT) {
+                                float p0, p1, p2, p3;
+                                tc::f2_split(pacc[0], p0, p1);
+                                tc::f2_split(pacc[1], p2, p3);
+                                part = (p0 + p1) + (p2 + p3);
+                            }
+#pragma unroll
+                            for (int grp = 0; grp < (SPLIT ? 4 : 0); ++grp) {
+                                const uint4 hw = *reinterpret_cast<const uint4 *>(ahi + grp * 128);
+                                const uint4 lw = *reinterpret_cast<const uint4 *>(alo + grp * 128);
+                                const uint32_t hv[4] = {hw.x, hw.y, hw.z, hw.w}, lv[4] = {lw.x, lw.y, lw.z, lw.w};
+#pragma unroll
+                                for (int e = 0; e < 4; ++e) {
+                                    const float vr = __uint_as_float(hv[e] << 16) + __uint_as_float(lv[e] << 16);
+                                    const float vi =
+                                        __uint_as_float(hv[e] & 0xFFFF0000u) + __uint_as_float(lv[e] & 0xFFFF0000u);
+                                    part = fmaf(d[grp * 8 + 2 * e], vr, part);
+                                    part = fmaf(d[grp * 8 + 2 * e + 1], vi, part);
+                                }
+                            }
+                            acc += (double)part;
+                            tc::tc_fence_before();
                         }
-                        acc += (double)part;
-                        tc::tc_fence_before();
                     }
-                    if (i % CPS == CPS - 1 || i == je - 1) {
-                        tc::mbar_arrive(&afree[sa]);
-                        if (++sa == NST) sa = 0;
-                    }
+                    tc::mbar_arrive(&afree[sa]);
+                    if (++sa == NST) sa = 0;
                 }
                 if (!ok) break;
                 tc::mbar_arrive(&tfree[W & (TC_NB - 1)]);
@@ -789,6 +806,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
             double S = 0.0;
             for (int pp = it.pa; pp < it.pz && ok; ++pp) {
                 const int jb = pp * pw, je = min(C, jb + pw);
+                // packed FP32 running sums of the normalisation terms of 4 consecutive chunks (8 per lane),
+                // added to the FP64 sum per group: passes start at multiples of 4 chunks, so the groups, and
+                // with them the sum's bits, do not depend on the pass width
+                uint64_t s2run = 0;
                 // T counts A stages: each holds CPS chunks t0 .. t0 + CPS - 1 of the pass
                 for (int t0 = 0; t0 < je; t0 += CPS, ++T) {
                     if (T >= NST) {
@@ -805,7 +826,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                         const int t = live ? t0 + c : t0;
                         uint64_t s2 = 0;   // packed normalisation partial sums (0.0f, 0.0f)
                         uint32_t hw[4], lw[4];
-    #pragma unroll
+#pragma unroll
                         for (int e2 = 0; e2 < 2; ++e2) {
                             const int j = t * (TC_MPC / 2) + p * 2 + e2;   // mics 2j, 2j+1
                             const float4 pa = mp4[2 * j], pb = mp4[2 * j + 1];
@@ -815,9 +836,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                             const uint64_t r2 = tc::f2_fma(dz, dz, tc::f2_fma(dy, dy, tc::f2_mul(dx, dx)));
                             float r2a, r2b;
                             tc::f2_split(r2, r2a, r2b);
-                            // 1/r: hardware rsqrt (~2^-22 relative) and one Newton step y *= 1.5 - 0.5 r^2 y^2
+                            // 1/r: hardware rsqrt (~2^-22 relative); split BF16 (16 significant bits) adds one
+                            // Newton step y *= 1.5 - 0.5 r^2 y^2, the 11-bit forms do not need it
                             uint64_t y = tc::f2(tc::rsqrt_approx(r2a), tc::rsqrt_approx(r2b));
-                            y = tc::f2_mul(y, tc::f2_fma(tc::f2_mul(tc::f2_mul(r2, y), y), NHALF, THALF));
+                            if (SPLIT) y = tc::f2_mul(y, tc::f2_fma(tc::f2_mul(tc::f2_mul(r2, y), y), NHALF, THALF));
                             const uint64_t r = tc::f2_mul(r2, y);
                             // xn = -(k r) reduced: cos(xn) = Re h / w and sin(xn) = Im h / w
                             float xa, xb;
@@ -858,7 +880,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                             float vr[2], vi[2];
                             tc::f2_split(vre, vr[0], vr[1]);
                             tc::f2_split(vim, vi[0], vi[1]);
-    #pragma unroll
+#pragma unroll
                             for (int h = 0; h < 2; ++h) {
                                 const int e = 2 * e2 + h;
                                 if (TF32) {   // FP32 operand rounded to TF32: (re, im) of mic e in hw[e], lw[e]
@@ -893,10 +915,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) map_tc_kernel(const __grid_cons
                                 *reinterpret_cast<uint4 *>(smem + TcSmem::a_off(sa, 1) + a_off_row) =
                                     make_uint4(lw[0], lw[1], lw[2], lw[3]);
                         }
-                        if (ST >= 2 && live && t >= jb) {   // each mic's term once, in its own pass
-                            float sa2, sb2;
-                            tc::f2_split(s2, sa2, sb2);
-                            S += (double)(sa2 + sb2);
+                        // each mic's normalisation term once, in its own pass
+                        if (ST >= 2 && live && t >= jb) {
+                            s2run = tc::f2_add(s2run, s2);
+                            if ((t & 3) == 3 || t == je - 1) {
+                                float sa2, sb2;
+                                tc::f2_split(s2run, sa2, sb2);
+                                S += (double)sa2 + (double)sb2;
+                                s2run = 0;
+                            }
                         }
                     }
                     tc::fence_proxy_async_smem();
@@ -1078,9 +1105,7 @@ static int tc_launch(TcBatch &bt, const acb_map_params *const *params, const voi
     // the deepest A ring that fits beside this batch's mic table (+1 KB of alignment slack)
     int ns = TC_ASTAGES_MAX;
     while (ns > TC_ASTAGES_MIN && TcSmem::total(ns, mp_max) + 1024 > smem_max) --ns;
-    // an FP16 stage carries two chunks; chunks in flight (stages x chunks per stage) stay within the
-    // step barrier ring
-    bt.nstages = precision == ACB_TC_FP16 ? min(ns, TC_NB / 2) : ns;
+    bt.nstages = ns;
     int smem = TcSmem::total(ns, mp_max) + 1024;
     // each CTA takes all 512 TMEM columns and must be alone on its SM: size the shared memory so
     // that no second CTA fits (a second one would stall in tcgen05.alloc until the first exits)

@@ -122,6 +122,8 @@ class BeamformerBase:
     """Delay-and-sum beamformer in the frequency domain, computed on the GPU."""
 
     FORMS = ('f64', 'tc')
+    # tensor-core operand forms: split BF16 (~1e-5 of max), TF32 and FP16 (~1e-4; FP16 scales each bin's R')
+    TC_PRECISIONS = ('bf16x3', 'tf32', 'fp16')
 
     def __init__(self, freq_data=None, steer: SteeringVector | None = None, r_diag: bool = True,
                  r_diag_norm: float = 0.0, precision: str = 'float64', cached: bool = False, form: str = 'f64',
@@ -139,6 +141,9 @@ class BeamformerBase:
             msg = f'form must be one of {self.FORMS}, got {form!r}'
             raise ValueError(msg)
         self.form = form
+        if tc_precision not in self.TC_PRECISIONS:
+            msg = f'tc_precision must be one of {self.TC_PRECISIONS}, got {tc_precision!r}'
+            raise ValueError(msg)
         self.tc_precision = tc_precision
         self.glibc_faithful = glibc_faithful
         self.max_bins_per_launch = max_bins_per_launch

@@ -130,6 +130,10 @@ def test_beamformer_settings_and_channel_check():
         ac.SteeringVector(steer_type='foo')
     with pytest.raises(ValueError):
         ac.BeamformerBase(form='gpu')
+    for prec in ('bf16x3', 'tf32', 'fp16'):
+        assert ac.BeamformerBase(form='tc', tc_precision=prec).tc_precision == prec
+    with pytest.raises(ValueError, match='tc_precision'):
+        ac.BeamformerBase(form='tc', tc_precision='fp8')
 
 
 def test_band_indices_match_reference_rule():
