@@ -57,7 +57,9 @@ def parse():
     ap.add_argument('--workload', default='precision256',
                     choices=['precision256', 'batched64', 'large3d', 'serving', 'serving-mixed', 'eig', 'damas',
                              'cleansc', 'stream'])
-    ap.add_argument('--tc-precision', default='tf32', choices=['bf16x3', 'tf32', 'fp16'])
+    # FP16 operands (each bin's R' scaled by a power of two) carry TF32's 11-bit significand at half the MMA
+    # chain and half the tile bytes: the same error as TF32, the fastest form
+    ap.add_argument('--tc-precision', default='fp16', choices=['bf16x3', 'tf32', 'fp16'])
     ap.add_argument('--duration', type=float, default=10.0, help='serving: seconds of offered load')
     ap.add_argument('--no-extra', action='store_true',
                     help='skip the other configurations\' blocks of the default line (profiling runs)')
@@ -198,10 +200,12 @@ CPU_SAMPLE_BINS = (100, 256, 400)
 
 class CpuSample:
     """The CPU oracle (C/OpenMP port of the reference's numba calcCSM and _freqBeamformer_FullCSM) on a
-    bounded sample of the 256-mic workload, on all host threads: one map bin over the full grid (bins
-    rotating through ``CPU_SAMPLE_BINS``) plus one bin's share of the CSM (the Welch accumulation of 65
-    windows over all bins, scaled by K / 65 / F).  ``value`` = grid points / (map time + CSM share) per
-    bin.  The bench line's ``cpu_baseline`` and the ``--impl reference`` arm both use this class."""
+    bounded sample of the 256-mic workload, on all host threads.  One step is one pass over the sample
+    bins ``CPU_SAMPLE_BINS``: per bin the map over the full grid plus one bin's share of the CSM (the Welch
+    accumulation of 65 windows over all bins, scaled by K / 65 / F).  ``value`` = grid points / (map time +
+    CSM share) per bin, averaged over the pass, so every step weighs the bins alike (the C library's
+    cosf/sinf cost grows with the phase argument).  The bench line's ``cpu_baseline`` and the
+    ``--impl reference`` arm both use this class, with one warm-up step each."""
 
     def __init__(self, wl, steer):
         from acoular_b200 import device as D
@@ -221,25 +225,27 @@ class CpuSample:
         self.freqs = O.fftfreq(self.N, wl.fs)
         self.data = rng.randn(64 * (self.N // 2) + self.N, self.M)   # 65 windows; values do not change the cost
         self.norm = O.sig_loss_norm(True, self.M)
-        self.i = 0
         O.beamformer_freq(steer, True, 1.0, self.r0[:64], self.rm[:64], 1.0, self.csm_bin)   # warm the pool
 
     def step(self) -> float:
-        """One bin's map plus one bin's CSM share; returns seconds (the bin's equivalent time)."""
+        """One pass over the sample bins; returns seconds per bin (the bin's equivalent time)."""
         O, wl = self.O, self.wl
-        b = CPU_SAMPLE_BINS[self.i % len(CPU_SAMPLE_BINS)]
-        self.i += 1
-        t0 = time.perf_counter()
-        O.beamformer_freq(self.steer, True, self.norm, self.r0, self.rm, 2 * np.pi * self.freqs[b] / wl.c, self.csm_bin)
-        t1 = time.perf_counter()
-        O.calc_csm(self.data, self.N, 'Hanning', '50%', 'complex128')
-        t2 = time.perf_counter()
-        return (t1 - t0) + (t2 - t1) * (self.K / 65.0) / self.F
+        total = 0.0
+        for b in CPU_SAMPLE_BINS:
+            t0 = time.perf_counter()
+            O.beamformer_freq(self.steer, True, self.norm, self.r0, self.rm, 2 * np.pi * self.freqs[b] / wl.c,
+                              self.csm_bin)
+            t1 = time.perf_counter()
+            O.calc_csm(self.data, self.N, 'Hanning', '50%', 'complex128')
+            t2 = time.perf_counter()
+            total += (t1 - t0) + (t2 - t1) * (self.K / 65.0) / self.F
+        return total / len(CPU_SAMPLE_BINS)
 
     def describe(self, nsteps: int) -> str:
-        return (f'{nsteps} x (map of 1 bin over {self.G} grid points, bins cycling {list(CPU_SAMPLE_BINS)}, + the CSM '
-                f'of 65 windows x all {self.F} bins scaled to one bin\'s share K/65/F, K = {self.K}); C/OpenMP port of '
-                f'the reference numba calcCSM and _freqBeamformer_FullCSM, {self.ncores} threads')
+        return (f'{nsteps} x {len(CPU_SAMPLE_BINS)} bins {list(CPU_SAMPLE_BINS)} (after one warm-up pass), each the map of '
+                f'the bin over {self.G} grid points + the CSM of 65 windows x all {self.F} bins scaled to one bin\'s '
+                f'share K/65/F, K = {self.K}; C/OpenMP port of the reference numba calcCSM and '
+                f'_freqBeamformer_FullCSM, {self.ncores} threads')
 
 
 def run_reference(args, wl):
@@ -249,8 +255,7 @@ def run_reference(args, wl):
     if rank != 0:
         return
     cs = CpuSample(wl, args.steer)
-    for _ in range(args.warmup):
-        cs.step()
+    cs.step()   # one warm-up pass, as cpu_baseline_sample does
     dt = sum(cs.step() for _ in range(args.steps)) / args.steps
     value = cs.G / dt
     line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': ws, 'steps': args.steps,
@@ -265,10 +270,11 @@ def run_reference(args, wl):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_sample(wl, steer, nsteps: int = 6):
+def cpu_baseline_sample(wl, steer, nsteps: int = 2):
     """Oracle timing on the host cores for the bench line's cpu_baseline (rank 0, N=1): the same sample
-    as the reference arm, two passes over the sample bins."""
+    as the reference arm, one warm-up pass and two timed passes over the sample bins."""
     cs = CpuSample(wl, steer)
+    cs.step()
     dt = sum(cs.step() for _ in range(nsteps)) / nsteps
     return {'value': cs.G / dt, 'unit': UNIT, 'cores': cs.ncores, 'kind': 'port', 'sample': cs.describe(nsteps),
             'host': host_info()}
