@@ -154,18 +154,20 @@ def _instances(specs, seed=0):
     return out
 
 
-def test_tc_batch_uneven_instances_equal_alone():
+@pytest.mark.parametrize('precision', ['bf16x3', 'fp16'])
+def test_tc_batch_uneven_instances_equal_alone(precision):
     """Each instance's map is the same in the batched launch as alone, and matches the oracle."""
     from acoular_b200 import device as D
     specs = [(32, 441, 3), (64, 2000, 2), (128, 700, 4), (256, 300, 2), (300, 150, 2), (37, 90001, 1),
              (32, 40000, 4), (16, 20000, 3)]
     inst = _instances(specs)
     err = torch.zeros(1, dtype=torch.int32, device=inst[0][0].csm.device)
-    D.map_tc_batch([i for i, _ in inst], error_word=err)
+    D.map_tc_batch([i for i, _ in inst], precision=precision, error_word=err)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     for it, (mpos, gpos, freqs, csm) in inst:
-        alone = D.map_tc(it.csm, it.wavenumbers, it.mpos, it.gpos, 'true level', True, it.norm).cpu().numpy()
+        alone = D.map_tc(it.csm, it.wavenumbers, it.mpos, it.gpos, 'true level', True, it.norm,
+                         precision=precision).cpu().numpy()
         got = it.out.cpu().numpy()
         assert np.array_equal(got, alone)
         nb = len(freqs)
