@@ -1,5 +1,6 @@
-// Stage B, tensor-core form: the steered-response map as a real GEMM on tcgen05 with split-BF16
-// operands (hi + lo, three products, FP32 accumulation in TMEM).
+// Stage B, tensor-core form: the steered-response map as a real GEMM on tcgen05 with FP32
+// accumulation in TMEM, in one of three operand forms: split BF16 (hi + lo, three products), FP32
+// rounded to TF32, or FP16 with each bin's R' scaled by a power of two.
 //
 // Formulation.  With h_g = (cos phi - i sin phi) * w(r) the steering vector of grid point g and
 // v_g = (Re h_0, Im h_0, Re h_1, Im h_1, ...) in R^{2M}, the map value is
@@ -8,8 +9,8 @@
 // symmetric,  B = sum_j D'_j . v_j  with  D'_j = sum_{i<=j} v_i^T R'_ij,  R'_ij = 2 R_ij (i < j),
 // R'_jj = R_jj.  The kernel runs the K loop over chunks i and for each i issues the MMAs into the
 // accumulator columns of every chunk j >= i; after chunk i the columns of chunk i are final, so
-// the epilogue dots them with v_i while v_i is still in the synthesising thread's registers.
-// Steering vectors are never re-synthesised and about half of the dense GEMM is skipped.
+// the epilogue dots them with v_i while v_i is still in the A stage.  Steering vectors are never
+// re-synthesised and about half of the dense GEMM is skipped.
 //
 // Work item: 128 grid points (UMMA M = 128, one TMEM lane each) x one frequency bin x one group of
 // column passes.  The accumulator columns of an item are covered in passes of `pw` chunks (a
@@ -17,18 +18,21 @@
 // passes of one (bin, tile) are shared among several items whose partial sums (B and the
 // normalisation sum S are both additive over chunks) are combined by the last item to finish, in
 // split order, before the steering-type normalisation.
-//   warp 5      : bulk copies of the R' tiles of chunk i (pre-laid in HBM in the shared-memory
-//                 core-matrix order by tc_prep_kernel) into a 32-tile ring, running ahead of the MMAs
+//
+// Pipeline step: one A stage (16 KB), i.e. one chunk (split BF16, TF32) or two (FP16, 8 KB each).
+// Every role works per step: one steering arrival, one R' tile barrier, one MMA commit, one
+// epilogue wait and release.
+//   warp 5      : bulk copies of the step's R' tiles (pre-laid in HBM in the shared-memory
+//                 core-matrix order by tc_prep_kernel) into a 128 KB tile ring, running ahead
 //   warp 1      : TMEM allocation; one thread issues tcgen05.mma (A = steering chunk, B = R'
-//                 tiles; products hi*hi + hi*lo + lo*hi) and commits to the stage's mbarrier
-//   warps 0,9,2,3: epilogue (TMEM lane quarters 0..3): after the MMAs of chunk i, read its
-//                 accumulator columns from TMEM and dot them with the steering chunk read back
-//                 from the A stage (hi + lo)
-//   16 warps    : steering synthesis of chunk i (four threads per grid point, 4 mics each):
-//                 FP32 distance (Newton rsqrt), the phase k*r as an exact float-float product,
-//                 Cody-Waite reduction by a three-term 2*pi, hardware sincos, bf16 hi/lo split
-//                 into the A stage.  No FP64<->FP32 conversion and no TMEM access sits in the
-//                 per-element path.
+//                 tiles) and commits to the step's mbarrier
+//   warps 0,9,2,3: epilogue (TMEM lane quarters 0..3): after the step's MMAs, read the final
+//                 accumulator columns from TMEM and dot them with the steering chunks read back
+//                 from the A stage
+//   16 warps    : steering synthesis (four threads per grid point, 4 mics of each chunk), packed
+//                 FP32: distance by rsqrt, the phase (k as a float-float; reduced by a three-term
+//                 2*pi for split BF16), hardware sincos, the operand conversion into the A stage.
+//                 No FP64 arithmetic and no TMEM access sits in the per-element path.
 // Every mbarrier wait is bounded (globaltimer); on timeout the CTA raises an error word and exits
 // its loops without further work.
 #include <cuda_bf16.h>
