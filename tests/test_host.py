@@ -199,7 +199,7 @@ def test_committed_tuning_table_is_valid():
     for key, ent in tab['classes'].items():
         prec, mb, ib = key.split(':')
         M = int(mb[1:])
-        assert prec in ('bf16x3', 'tf32') and ib in ('tiny', 'few', 'mid', 'many')
+        assert prec in ('bf16x3', 'tf32', 'fp16') and ib in ('tiny', 'few', 'mid', 'many')
         assert (ent['pass_chunks'], ent['splits']) in A.candidates(M)
         assert ent['ms'] == min(ent['candidates_ms'].values())
 
