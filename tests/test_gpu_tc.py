@@ -104,13 +104,15 @@ def test_tc_error_word_stays_clear():
     assert int(err.item()) == 0
 
 
+@pytest.mark.parametrize('precision', ['bf16x3', 'fp16'])
 @pytest.mark.parametrize('M,G,nb', [(64, 20000, 4), (256, 12000, 3), (40, 50000, 2), (700, 2000, 2)])
-def test_tc_persistent_many_items_per_cta(M, G, nb):
-    """More work items (bin x 128-point tile) than CTAs: the pipeline runs across item boundaries."""
+def test_tc_persistent_many_items_per_cta(M, G, nb, precision):
+    """More work items (bin x 128-point tile) than CTAs: the pipeline runs across item boundaries (FP16:
+    chunk-pair steps, an odd chunk count per pass at 40 and 700 mics)."""
     mpos, gpos, freqs, csm = _case(M, G, seed=M * 3 + nb, nb=nb)
     r0, rm = O.apparent_r(gpos), O.apparent_r(gpos, mpos)
     ref = O.beamformer_calc(csm, freqs, range(nb), r0, rm, 343.0, 'true location', True)
-    got = _tc(csm, freqs, mpos, gpos, 'true location', True)
+    got = _tc(csm, freqs, mpos, gpos, 'true location', True, precision=precision)
     for b in range(nb):
         assert rel(got[b], ref[b]) <= TOL
 
@@ -247,9 +249,10 @@ def test_fp16_form_range_error_bit():
     assert not np.isfinite(out.cpu().numpy()).all()
 
 
+@pytest.mark.parametrize('precision', ['bf16x3', 'fp16'])
 @pytest.mark.parametrize('M,G,steer', [(40, 700, 'true level'), (256, 300, 'true location'), (600, 260, 'inverse'),
                                        (1100, 130, 'classic')])
-def test_tc_tile_width_and_split_agree(M, G, steer):
+def test_tc_tile_width_and_split_agree(M, G, steer, precision):
     """Every (pass width, split) candidate gives the default schedule's map (FP64 partial-sum order
     differs only), and the single-instance entry (acb_map_tc) gives it too."""
     from acoular_b200 import autotune
@@ -259,13 +262,13 @@ def test_tc_tile_width_and_split_agree(M, G, steer):
     args = (torch.as_tensor(csm, device=dev), torch.as_tensor(2 * np.pi * freqs / 343.0, device=dev),
             torch.as_tensor(mpos, device=dev), torch.as_tensor(np.ascontiguousarray(gpos), device=dev), steer, True,
             O.sig_loss_norm(True, M))
-    base = D.map_tc(*args, clip_negative=True, tuning=(16, 1)).cpu().numpy()
-    single = D.map_tc(*args, clip_negative=True, tuning=None).cpu().numpy()
+    base = D.map_tc(*args, clip_negative=True, tuning=(16, 1), precision=precision).cpu().numpy()
+    single = D.map_tc(*args, clip_negative=True, tuning=None, precision=precision).cpu().numpy()
     assert np.array_equal(single, base)
     cands = autotune.candidates(M)
     assert len(cands) >= (3 if M > 64 else 1)
     for pw, sp in cands:
-        got = D.map_tc(*args, clip_negative=True, tuning=(pw, sp)).cpu().numpy()
+        got = D.map_tc(*args, clip_negative=True, tuning=(pw, sp), precision=precision).cpu().numpy()
         assert rel(got, base) <= 1e-12, (pw, sp)
     ref = O.beamformer_calc(csm, freqs, range(len(freqs)), O.apparent_r(gpos), O.apparent_r(gpos, mpos), 343.0, steer,
                             True)
