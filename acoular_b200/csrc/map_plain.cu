@@ -49,13 +49,13 @@ __device__ __forceinline__ double grid_mic_dist(const MapArgs &a, const double *
 
 // Synthesise h for mics [m0, m0+n) of this CTA's 32 grid points into hs[m - m0][lane]; with CUSTOM,
 // copy the caller's steering vectors hv[g][m] instead (custom steering, acoular/fastFuncs.py:414-559).
-template <bool USE_RM, bool CUSTOM = false>
+template <bool USE_RM, bool CUSTOM = false, int NW = kWarps>
 __device__ __forceinline__ void synth_chunk(const MapArgs &a, const double *__restrict__ rm, double k, int64_t g,
                                            bool gvalid, double g0, double g1, double g2, const double *mp, int m0,
                                            int n, double2 *hs, const double2 *__restrict__ hv = nullptr)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = warp; i < n; i += kWarps) {
+    for (int i = warp; i < n; i += NW) {
         double2 h = make_double2(0.0, 0.0);
         if (CUSTOM) {
             if (gvalid) h = __ldg(hv + g * a.M + m0 + i);
@@ -257,10 +257,14 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
 // multicast; one copy per row, completion on the stage's mbarrier); the next chunk is in flight while
 // the warp works on the current one.  Every loaded C value then feeds the 32 grid points of the warp
 // from shared memory instead of a broadcast load through L1/L2 per complex FMA, and the masking of the
-// triangle is confined to the diagonal 8 x 8 block.  Waits are bounded; a CTA that gives up raises the
-// error word, writes NaN and returns after its own copies have landed.
+// triangle is confined to the diagonal 8 x 8 block.  Sixteen warps (four per scheduler, 128 registers
+// each) share the CTA's steering block: the FP64 FMA chains of the 8-row blocks need that many warps
+// to cover their latency at one CTA per SM (8 warps: 19.7 TFLOP/s on the 256-mic workload, 16: 24.7).
+// Waits are bounded; a CTA that gives up raises the error word, writes NaN and returns after its own
+// copies have landed.
 // ------------------------------------------------------------------------------------------------
-constexpr int kCB = 32;                                  // C columns per staged chunk
+constexpr int kSWarps = 16;                              // warps of the staged kernel (4 per scheduler)
+constexpr int kCB = 16;                                  // C columns per staged chunk
 constexpr int kCStageElems = kRowBlock * kCB;            // double2 per (warp, stage)
 constexpr uint64_t kPlainWaitNs = 500ull * 1000 * 1000;  // limit of one wait
 
@@ -269,8 +273,8 @@ struct StagedSmem {
     __host__ __device__ static constexpr size_t mp(int) { return 0; }
     __host__ __device__ static constexpr size_t ha(int M) { return (size_t)((3 * M + 1) & ~1) * 8; }
     __host__ __device__ static constexpr size_t cst(int M) { return ha(M) + (size_t)M * kLanes * 16; }
-    __host__ __device__ static constexpr size_t bars(int M) { return cst(M) + (size_t)kWarps * 2 * kCStageElems * 16; }
-    __host__ __device__ static constexpr size_t total(int M) { return bars(M) + kWarps * 2 * 8 + 16; }
+    __host__ __device__ static constexpr size_t bars(int M) { return cst(M) + (size_t)kSWarps * 2 * kCStageElems * 16; }
+    __host__ __device__ static constexpr size_t total(int M) { return bars(M) + kSWarps * 2 * 8 + 16; }
 };
 
 // the chunk sequence of one warp: its row blocks in snake order, each block's columns [a0, M) in kCB chunks
@@ -282,19 +286,16 @@ struct ChunkCursor {
 __device__ __forceinline__ int warp_block(int warp, int t)
 {
     // t-th row block of `warp` in the snake assignment 0..7, 7..0, 0..7, ...
-    return t * kWarps + ((t & 1) ? (kWarps - 1 - warp) : warp);
+    return t * kSWarps + ((t & 1) ? (kSWarps - 1 - warp) : warp);
 }
 
 template <bool USE_RM, bool CUSTOM>
-__global__ void __launch_bounds__(256, 1) map_plain_staged_kernel(MapArgs a, const double2 *__restrict__ csm,
-                                                                  const double *__restrict__ wavenumber, double k_scalar,
-                                                                  const double *__restrict__ mpos,
-                                                                  const double *__restrict__ gpos,
-                                                                  const double *__restrict__ r0_in,
-                                                                  const double *__restrict__ rm,
-                                                                  double *__restrict__ out_map,
-                                                                  double *__restrict__ out_norm,
-                                                                  const double2 *__restrict__ steer, int *err)
+__global__ void __launch_bounds__(kLanes * kSWarps, 1)
+    map_plain_staged_kernel(MapArgs a, const double2 *__restrict__ csm, const double *__restrict__ wavenumber,
+                            double k_scalar, const double *__restrict__ mpos, const double *__restrict__ gpos,
+                            const double *__restrict__ r0_in, const double *__restrict__ rm,
+                            double *__restrict__ out_map, double *__restrict__ out_norm,
+                            const double2 *__restrict__ steer, int *err)
 {
     extern __shared__ __align__(16) uint8_t smem_b[];
     const int M = a.M;
@@ -302,8 +303,8 @@ __global__ void __launch_bounds__(256, 1) map_plain_staged_kernel(MapArgs a, con
     double2 *ha = reinterpret_cast<double2 *>(smem_b + StagedSmem::ha(M));     // [M][32]
     double2 *cst = reinterpret_cast<double2 *>(smem_b + StagedSmem::cst(M));   // [warp][stage][8][kCB]
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_b + StagedSmem::bars(M));   // [warp][stage]
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + kWarps * 2);
-    __shared__ double red_off[kWarps][kLanes], red_diag[kWarps][kLanes], red_s[kWarps][kLanes];
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + kSWarps * 2);
+    __shared__ double red_off[kSWarps][kLanes], red_diag[kSWarps][kLanes], red_s[kSWarps][kLanes];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int bin = blockIdx.y;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(256, 1) map_plain_staged_kernel(MapArgs a, con
     const double2 *hv = CUSTOM ? steer + (int64_t)bin * a.G * M : nullptr;
 
     if (threadIdx.x == 0) {
-        for (int i = 0; i < kWarps * 2; ++i) tc::mbar_init(&bars[i], 1);
+        for (int i = 0; i < kSWarps * 2; ++i) tc::mbar_init(&bars[i], 1);
         *abort_flag = 0;
         tc::fence_mbar_init();
     }
@@ -366,17 +367,17 @@ __global__ void __launch_bounds__(256, 1) map_plain_staged_kernel(MapArgs a, con
     double s_part = 0.0;
     if (CUSTOM) {
         if (gvalid)
-            for (int m = warp; m < M; m += kWarps) {
+            for (int m = warp; m < M; m += kSWarps) {
                 const double2 h = __ldg(hv + g * M + m);
                 s_part += h.x * h.x + h.y * h.y;
             }
     } else if (gvalid && a.steer_type >= 2) {
-        for (int m = warp; m < M; m += kWarps) {
+        for (int m = warp; m < M; m += kSWarps) {
             const double r = grid_mic_dist<USE_RM>(a, rm, g, m, g0, g1, g2, mp);
             s_part += (a.steer_type == 2) ? r * r : 1.0 / (r * r);
         }
     }
-    synth_chunk<USE_RM, CUSTOM>(a, rm, k, g, gvalid, g0, g1, g2, mp, 0, M, ha, hv);
+    synth_chunk<USE_RM, CUSTOM, kSWarps>(a, rm, k, g, gvalid, g0, g1, g2, mp, 0, M, ha, hv);
     __syncthreads();
 
     double off = 0.0, dsum = 0.0;
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(256, 1) map_plain_staged_kernel(MapArgs a, con
     if (warp == 0 && gvalid) {
         double o = 0.0, d = 0.0, S = 0.0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
+        for (int w = 0; w < kSWarps; ++w) {
             o += red_off[w][lane];
             d += red_diag[w][lane];
             S += red_s[w][lane];
@@ -648,9 +649,9 @@ static int launch_plain(const MapArgs &a, int nbins, const void *csm, const doub
         auto kern = map_plain_staged_kernel<USE_RM, CUSTOM>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const dim3 grid((unsigned)((a.G + kLanes - 1) / kLanes), nbins);
-        kern<<<grid, kLanes * kWarps, smem, s>>>(a, reinterpret_cast<const double2 *>(csm), k, k_scalar, mpos, gpos,
-                                                r0, rm, out_map, out_norm, reinterpret_cast<const double2 *>(steer),
-                                                err);
+        kern<<<grid, kLanes * kSWarps, smem, s>>>(a, reinterpret_cast<const double2 *>(csm), k, k_scalar, mpos, gpos,
+                                                 r0, rm, out_map, out_norm, reinterpret_cast<const double2 *>(steer),
+                                                 err);
         return check_launch();
     }
     const int mc = a.M <= 256 ? a.M : 128;
