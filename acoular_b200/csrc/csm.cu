@@ -191,11 +191,13 @@ __device__ __forceinline__ int zpf(int j) { return j + (j >> 4); }
 __host__ __device__ constexpr int fft_stride_f(int H) { return H + (H >> 4) + 1; }
 
 // s (1..3) consecutive radix-2 DIT stages, the first of length 2^(sg + 1), on a bit-reversed FP32
-// sequence (see fft_pass); the twiddles W_N^e come from a shared-memory FP32 copy of the table.  All
-// lengths are powers of two, so the index arithmetic is shifts and masks (logN = log2 N).
+// sequence (see fft_pass).  The twiddles come from a shared-memory table in stage order: the stage of
+// length L = 2 hf reads W_L^i (i < hf) at tws[hf + i], so consecutive threads read consecutive
+// entries (the natural-order table read with the stride N / L put up to 16 threads on one bank).  The
+// entries are the FP32 roundings of the same W_N^e as the natural-order table.  All lengths are powers
+// of two, so the index arithmetic is shifts and masks.
 template <int S>
-__device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int sg, int task, int logN,
-                                           const float2 *__restrict__ twf)
+__device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int sg, int task, const float2 *__restrict__ tws)
 {
     const int half1 = 1 << sg;
     const int base = ((task >> sg) << (sg + S)) + (task & (half1 - 1));
@@ -205,12 +207,11 @@ __device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int sg, int t
 #pragma unroll
     for (int q = 0; q < S; ++q) {
         const int hf = half1 << q;                       // half the stage length L = 2^(sg + 1 + q)
-        const int shift = logN - (sg + 1 + q);           // W_L^i = W_N^(i N / L)
 #pragma unroll
         for (int t = 0; t < (1 << S); ++t) {
             if (t & (1 << q)) continue;
             const int i0 = base + t * half1;
-            const float2 w = twf[(i0 & (hf - 1)) << shift];
+            const float2 w = tws[hf + (i0 & (hf - 1))];
             const float2 b = v[t + (1 << q)];
             const float br = b.x * w.x - b.y * w.y;
             const float bi = b.x * w.y + b.y * w.x;
@@ -225,9 +226,79 @@ __device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int sg, int t
 
 constexpr int FFT4_WIN = 4;   // windows per CTA
 
+// V consecutive samples of one row, as float (V = 1, 2 or 4; the address is aligned to the vector)
+template <int V>
+__device__ __forceinline__ void ld_row(const float *__restrict__ p, float (&x)[V])
+{
+    if (V == 4) {
+        const float4 u = __ldg(reinterpret_cast<const float4 *>(p));
+        x[0] = u.x;
+        x[1] = u.y;
+        x[2] = u.z;
+        x[3] = u.w;
+    } else if (V == 2) {
+        const float2 u = __ldg(reinterpret_cast<const float2 *>(p));
+        x[0] = u.x;
+        x[1] = u.y;
+    } else {
+        x[0] = __ldg(p);
+    }
+}
+template <int V>
+__device__ __forceinline__ void ld_row(const double *__restrict__ p, float (&x)[V])
+{
+    if (V == 1) {
+        x[0] = (float)__ldg(p);
+    } else {
+#pragma unroll
+        for (int e = 0; e < V; e += 2) {
+            const double2 u = __ldg(reinterpret_cast<const double2 *>(p + e));
+            x[e] = (float)u.x;
+            x[e + 1] = (float)u.y;
+        }
+    }
+}
+
+// Load, window and bit-reversed placement of the CTA's 4 windows x mpb mics: one thread per (window,
+// group of V mics, point j), j fastest, so that a warp's stores into the bit-reversed slots of one
+// sequence spread over the banks, and each thread loads rows 2j and 2j + 1 as one vector of V mics.
+// Windows past the chunk and padding mics are zeros (M % V == 0: a group is all in or all out).
+template <typename TS, int V>
+__device__ __forceinline__ void fft4_load(const TS *__restrict__ samples, int M, int hop, int64_t w0, int64_t nw,
+                                          int wg, int m0, int mpb, int H, int logH, int st,
+                                          const float *__restrict__ wf, float2 *__restrict__ zs)
+{
+    constexpr int logV = V == 4 ? 2 : (V == 2 ? 1 : 0);
+    int logG = 0;
+    while ((V << logG) < mpb) ++logG;                          // mpb / V groups
+    const int total = FFT4_WIN * H << logG;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int j = idx & (H - 1);
+        const int mg = (idx >> logH) & ((1 << logG) - 1);
+        const int wi = idx >> (logH + logG);
+        const int64_t w = (int64_t)wg * FFT4_WIN + wi;
+        const int m = m0 + (mg << logV);
+        float x0[V], x1[V];
+        if (w < nw && m < M) {
+            const TS *src = samples + ((w0 + w) * (int64_t)hop + 2 * j) * M + m;
+            ld_row<V>(src, x0);
+            ld_row<V>(src + M, x1);
+        } else {
+#pragma unroll
+            for (int e = 0; e < V; ++e) x0[e] = x1[e] = 0.f;
+        }
+        const float a0 = wf[2 * j], a1 = wf[2 * j + 1];
+        const int jr = logH ? (int)(__brev((unsigned)j) >> (32 - logH)) : 0;
+        float2 *z = zs + (wi * mpb + (mg << logV)) * st + zpf(jr);
+#pragma unroll
+        for (int e = 0; e < V; ++e) z[e * st] = make_float2(x0[e] * a0, x1[e] * a1);
+    }
+}
+
 template <typename TS, int OUT>
 __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ samples, int M, int N, int hop, int64_t w0,
-                                                      int64_t nw, int mpb, const double *__restrict__ window,
+                                                      int64_t nw, int mpb, int vw, const double *__restrict__ window,
                                                       const double2 *__restrict__ tw, int bin_lo, int nbins,
                                                       void *__restrict__ out, int R, int KC, int64_t lo_elems)
 {
@@ -235,35 +306,25 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
     const int H = N >> 1;
     const int st = fft_stride_f(H);
     float2 *zs = reinterpret_cast<float2 *>(fsm);                 // [FFT4_WIN][mpb][st]
-    float2 *twf = zs + FFT4_WIN * mpb * st;                       // [H]
-    float *wf = reinterpret_cast<float *>(twf + H);               // [N]
+    float2 *tws = zs + FFT4_WIN * mpb * st;                       // [H] twiddles in stage order (fft_pass_f)
+    float *wf = reinterpret_cast<float *>(tws + H);               // [N]
     int logH = 0, logP = 0;
     while ((1 << logH) < H) ++logH;
     while ((1 << logP) < mpb) ++logP;                              // mpb is a power of two
     const int wg = blockIdx.y;                                     // windows 4 wg .. 4 wg + 3 of the chunk
     const int m0 = blockIdx.x * mpb;
-    for (int i = threadIdx.x; i < H; i += blockDim.x) {
-        const double2 t = tw[i];
-        twf[i] = make_float2((float)t.x, (float)t.y);
+    for (int i = threadIdx.x + 1; i < H; i += blockDim.x) {
+        // i = hf + r, hf the largest power of two <= i: W_{2 hf}^r = W_N^(r H / hf), N = 2 H
+        const int lhf = 31 - __clz(i);
+        const double2 u = tw[(i - (1 << lhf)) << (logH - lhf)];
+        tws[i] = make_float2((float)u.x, (float)u.y);
     }
     for (int i = threadIdx.x; i < N; i += blockDim.x) wf[i] = (float)window[i];
     __syncthreads();
 
-    // load + window + bit-reversed placement; windows past the chunk and padding mics are zeros
-    for (int idx = threadIdx.x; idx < FFT4_WIN * H * mpb; idx += blockDim.x) {
-        const int ml = idx & (mpb - 1);
-        const int j = (idx >> logP) & (H - 1);
-        const int wi = idx >> (logP + logH);
-        const int64_t w = (int64_t)wg * FFT4_WIN + wi;
-        const int m = m0 + ml;
-        float2 v = make_float2(0.f, 0.f);
-        if (w < nw && m < M) {
-            const TS *src = samples + ((w0 + w) * (int64_t)hop + 2 * j) * M + m;
-            v = make_float2((float)src[0] * wf[2 * j], (float)src[M] * wf[2 * j + 1]);
-        }
-        const int jr = logH ? (int)(__brev((unsigned)j) >> (32 - logH)) : 0;
-        zs[(wi * mpb + ml) * st + zpf(jr)] = v;
-    }
+    if (vw == 4) fft4_load<TS, 4>(samples, M, hop, w0, nw, wg, m0, mpb, H, logH, st, wf, zs);
+    else if (vw == 2) fft4_load<TS, 2>(samples, M, hop, w0, nw, wg, m0, mpb, H, logH, st, wf, zs);
+    else fft4_load<TS, 1>(samples, M, hop, w0, nw, wg, m0, mpb, H, logH, st, wf, zs);
     __syncthreads();
 
     // radix-2 DIT stages, up to three per pass, over all 4 mpb sequences
@@ -274,9 +335,9 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
         for (int idx = threadIdx.x; idx < nseq << logT; idx += blockDim.x) {
             const int q = idx >> logT;
             const int task = idx & ((1 << logT) - 1);
-            if (S == 3) fft_pass_f<3>(zs + q * st, sg, task, logH + 1, twf);
-            else if (S == 2) fft_pass_f<2>(zs + q * st, sg, task, logH + 1, twf);
-            else fft_pass_f<1>(zs + q * st, sg, task, logH + 1, twf);
+            if (S == 3) fft_pass_f<3>(zs + q * st, sg, task, tws);
+            else if (S == 2) fft_pass_f<2>(zs + q * st, sg, task, tws);
+            else fft_pass_f<1>(zs + q * st, sg, task, tws);
         }
         __syncthreads();
         sg += S;
@@ -290,7 +351,11 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
         const int b = idx >> logP;
         const int k = bin_lo + b;
         const int kh = k & (H - 1), kc2 = (H - kh) & (H - 1);
-        const float2 wk = k < H ? twf[k] : make_float2(-1.f, 0.f);
+        float2 wk = make_float2(-1.f, 0.f);
+        if (k < H) {
+            const double2 t = __ldg(tw + k);
+            wk = make_float2((float)t.x, (float)t.y);
+        }
         float xr[FFT4_WIN], xi[FFT4_WIN];
 #pragma unroll
         for (int wi = 0; wi < FFT4_WIN; ++wi) {
@@ -646,12 +711,18 @@ int fft_launch(const void *samples, int sample_dtype, int out_form, int num_mics
             // every tile row (16 R padded mics) and column (32 KC padded windows) is written
             const dim3 g4((unsigned)(R * 16 / mpb4), (unsigned)(KC * 32 / FFT4_WIN));
             const size_t smem4 = fft4_smem_bytes(block_size, mpb4);
+            // vector width of the sample loads: V mics of a row at once where M and the base allow it
+            const size_t es = sample_dtype == ACB_F32 ? 4 : 8;
+            int vw = 1;
+            for (int v = 4; v >= 2 && vw == 1; v >>= 1)
+                if (v <= mpb4 && num_mics % v == 0 && reinterpret_cast<uintptr_t>(samples) % (v * es < 16 ? v * es : 16) == 0)
+                    vw = v;
 #define ACB_FFT4_LAUNCH(TS, OF)                                                                                     \
     do {                                                                                                            \
         auto kern = fft4_tc_kernel<TS, OF>;                                                                         \
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem4);                        \
         kern<<<g4, 256, smem4, s>>>(reinterpret_cast<const TS *>(samples), num_mics, block_size, hop, first_window,  \
-                                    num_windows, mpb4, window, tw, bin_lo, num_bins, out, R, KC, lo_elems);        \
+                                    num_windows, mpb4, vw, window, tw, bin_lo, num_bins, out, R, KC, lo_elems);    \
     } while (0)
             if (sample_dtype == ACB_F32) {
                 if (out_form == OUT_TF32) ACB_FFT4_LAUNCH(float, OUT_TF32);
