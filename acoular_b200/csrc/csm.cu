@@ -188,7 +188,14 @@ __global__ void __launch_bounds__(256) fft_window_kernel(const TS *__restrict__ 
 // Shared-memory slot of point j: one padding slot per 16 points (8-byte points), so that the passes'
 // strided accesses spread over the banks.
 __device__ __forceinline__ int zpf(int j) { return j + (j >> 4); }
-__host__ __device__ constexpr int fft_stride_f(int H) { return H + (H >> 4) + 1; }
+// Padded length of one sequence: at least H + H/16 slots and congruent to 32 / mpb modulo 16.  In the real
+// split a warp reads Z[k] of mpb mics x 32 / mpb consecutive bins; with that stride the mics' slots fall
+// on different bank pairs (with the stride 1 modulo 16 of a first version, 4 mics x 8 bins put up to 4
+// threads on one bank pair).
+__host__ __device__ constexpr int fft_stride_f(int H, int mpb)
+{
+    return H + (H >> 4) + ((((32 / mpb) & 15) - (H + (H >> 4))) & 15);
+}
 
 // s (1..3) consecutive radix-2 DIT stages, the first of length 2^(sg + 1), on a bit-reversed FP32
 // sequence (see fft_pass).  The twiddles come from a shared-memory table in stage order: the stage of
@@ -304,7 +311,7 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
 {
     extern __shared__ __align__(16) uint8_t fsm[];
     const int H = N >> 1;
-    const int st = fft_stride_f(H);
+    const int st = fft_stride_f(H, mpb);
     float2 *zs = reinterpret_cast<float2 *>(fsm);                 // [FFT4_WIN][mpb][st]
     float2 *tws = zs + FFT4_WIN * mpb * st;                       // [H] twiddles in stage order (fft_pass_f)
     float *wf = reinterpret_cast<float *>(tws + H);               // [N]
@@ -402,11 +409,10 @@ __global__ void __launch_bounds__(256) fft4_tc_kernel(const TS *__restrict__ sam
 // <= 16 (so that the 16 R padded mics split evenly); 0 if even one mic's 4 windows do not fit.
 static int fft4_mics_per_block(int N)
 {
-    const size_t per_mic = (size_t)FFT4_WIN * fft_stride_f(N / 2) * sizeof(float2);
     const size_t tables = (size_t)(N / 2) * sizeof(float2) + (size_t)N * sizeof(float);
-    if (per_mic + tables > 200 * 1024) return 0;
+    if ((size_t)FFT4_WIN * fft_stride_f(N / 2, 1) * sizeof(float2) + tables >= 200 * 1024) return 0;
     int mpb = 16;
-    while (mpb > 1 && (size_t)mpb * per_mic > 72 * 1024) mpb >>= 1;
+    while (mpb > 1 && (size_t)mpb * FFT4_WIN * fft_stride_f(N / 2, mpb) * sizeof(float2) > 72 * 1024) mpb >>= 1;
     return mpb;
 }
 
@@ -414,7 +420,7 @@ bool fft_tiles_written_whole(int block_size) { return fft4_mics_per_block(block_
 
 static size_t fft4_smem_bytes(int N, int mpb)
 {
-    return (size_t)FFT4_WIN * mpb * fft_stride_f(N / 2) * sizeof(float2) + (size_t)(N / 2) * sizeof(float2) +
+    return (size_t)FFT4_WIN * mpb * fft_stride_f(N / 2, mpb) * sizeof(float2) + (size_t)(N / 2) * sizeof(float2) +
            (size_t)N * sizeof(float);
 }
 
