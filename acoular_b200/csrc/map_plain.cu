@@ -47,6 +47,25 @@ __device__ __forceinline__ double grid_mic_dist(const MapArgs &a, const double *
     return dist3(g0, g1, g2, mp[m], mp[a.M + m], mp[2 * a.M + m]);
 }
 
+// Steering value of a grid point and a mic at distance r (acoular/fastFuncs.py:258-273): the phase
+// rounded to float32, cos - i sin of it as the C library's float32 functions give them, then the
+// weight r (inverse) or 1/r (true level, true location).
+__device__ __forceinline__ double2 steer_value(const MapArgs &a, double k, double r)
+{
+    const float arg = __double2float_rn(__dmul_rn(k, r));
+    float c, s;
+    sincos_f32_arg(arg, a.table, a.table_mask, a.faithful != 0, c, s);
+    double2 h = make_double2((double)c, -(double)s);
+    if (a.steer_type == 2) {
+        h.x = __dmul_rn(h.x, r);
+        h.y = __dmul_rn(h.y, r);
+    } else if (a.steer_type >= 3) {
+        h.x = __ddiv_rn(h.x, r);
+        h.y = __ddiv_rn(h.y, r);
+    }
+    return h;
+}
+
 // Synthesise h for mics [m0, m0+n) of this CTA's 32 grid points into hs[m - m0][lane]; with CUSTOM,
 // copy the caller's steering vectors hv[g][m] instead (custom steering, acoular/fastFuncs.py:414-559).
 template <bool USE_RM, bool CUSTOM = false, int NW = kWarps>
@@ -60,18 +79,7 @@ __device__ __forceinline__ void synth_chunk(const MapArgs &a, const double *__re
         if (CUSTOM) {
             if (gvalid) h = __ldg(hv + g * a.M + m0 + i);
         } else if (gvalid) {
-            const double r = grid_mic_dist<USE_RM>(a, rm, g, m0 + i, g0, g1, g2, mp);
-            const float arg = __double2float_rn(__dmul_rn(k, r));
-            float c, s;
-            sincos_f32_arg(arg, a.table, a.table_mask, a.faithful != 0, c, s);
-            h = make_double2((double)c, -(double)s);
-            if (a.steer_type == 2) {
-                h.x = __dmul_rn(h.x, r);
-                h.y = __dmul_rn(h.y, r);
-            } else if (a.steer_type >= 3) {
-                h.x = __ddiv_rn(h.x, r);
-                h.y = __ddiv_rn(h.y, r);
-            }
+            h = steer_value(a, k, grid_mic_dist<USE_RM>(a, rm, g, m0 + i, g0, g1, g2, mp));
         }
         hs[i * kLanes + lane] = h;
     }
@@ -612,6 +620,81 @@ __global__ void __launch_bounds__(256) map_eig_kernel(MapArgs a, int E, const do
     }
 }
 
+// Eigenvalue form for a few components (E <= kEigSmall, e.g. BeamformerEig's default n = -1 and each
+// CLEAN-SC iteration's single component): one thread per grid point walks the mics in order,
+// synthesises each steering value once and accumulates the E projections and the normalisation sum in
+// registers.  Without shared memory a CTA of 4 warps holds no resources but registers, so many warps
+// per SM hide the latency of the FP64 synthesis and of the exception-table probes; the shared-memory
+// form above (one CTA of 8 warps per SM) serves larger E, where the projections outnumber the
+// registers.  Each component's mic sum runs in the reference's order.
+constexpr int kEigSmall = 4;
+constexpr int kEigSmallThreads = 128;
+
+template <bool USE_RM, bool CUSTOM, int EMAX>
+__global__ void __launch_bounds__(kEigSmallThreads)
+    map_eig_small_kernel(MapArgs a, int E, const double *__restrict__ eigval, const double2 *__restrict__ eigvec,
+                         const double *__restrict__ wavenumber, double k_scalar, const double *__restrict__ mpos,
+                         const double *__restrict__ gpos, const double *__restrict__ r0_in,
+                         const double *__restrict__ rm, double *__restrict__ out_map, double *__restrict__ out_norm,
+                         const double2 *__restrict__ steer, const int *__restrict__ active)
+{
+    const int bin = blockIdx.y;
+    if (active && !active[bin]) return;   // a bin whose iteration has stopped (CLEAN-SC)
+    const int64_t g = (int64_t)blockIdx.x * kEigSmallThreads + threadIdx.x;
+    if (g >= a.G) return;
+    const int M = a.M;
+    const double k = wavenumber ? wavenumber[bin] : k_scalar;
+    const double *lam = eigval + (int64_t)bin * E;
+    const double2 *V = eigvec + (int64_t)bin * M * E;
+    const double2 *hv = CUSTOM ? steer + ((int64_t)bin * a.G + g) * M : nullptr;
+    double g0 = 0, g1 = 0, g2 = 0;
+    if (!USE_RM && !CUSTOM) {
+        g0 = gpos[g];
+        g1 = gpos[a.G + g];
+        g2 = gpos[2 * a.G + g];
+    }
+    double fr[EMAX], fi[EMAX], dg[EMAX];
+#pragma unroll
+    for (int j = 0; j < EMAX; ++j) fr[j] = fi[j] = dg[j] = 0.0;
+    double S = 0.0;
+    for (int m = 0; m < M; ++m) {
+        double2 h;
+        if (CUSTOM) {
+            h = __ldg(hv + m);
+            S += h.x * h.x + h.y * h.y;
+        } else {
+            const double r = USE_RM ? __ldg(rm + g * M + m)
+                                    : dist3(g0, g1, g2, __ldg(mpos + m), __ldg(mpos + M + m), __ldg(mpos + 2 * M + m));
+            h = steer_value(a, k, r);
+            if (a.steer_type >= 2) S += (a.steer_type == 2) ? r * r : 1.0 / (r * r);
+        }
+        const double2 *vrow = V + (int64_t)m * E;
+#pragma unroll
+        for (int j = 0; j < EMAX; ++j) {
+            if (j >= E) break;
+            const double2 v = __ldg(vrow + j);
+            // temp1 = conj(V[m][e]) * h[m]
+            const double tr = v.x * h.x + v.y * h.y, ti = v.x * h.y - v.y * h.x;
+            fr[j] += tr;
+            fi[j] += ti;
+            if (a.r_diag) dg[j] += tr * tr + ti * ti;
+        }
+    }
+    double scal = 0.0;
+#pragma unroll
+    for (int j = 0; j < EMAX; ++j) {
+        if (j >= E) break;
+        const double full = fr[j] * fr[j] + fi[j] * fi[j];
+        scal += (a.r_diag ? full - dg[j] : full) * lam[j];
+    }
+    double r0 = 0.0;
+    if (CUSTOM) r0 = 0.0;
+    else if (a.ref_mode == 1) r0 = a.ref_dist;
+    else if (USE_RM) r0 = r0_in[g];
+    else r0 = dist3(g0, g1, g2, a.ref0, a.ref1, a.ref2);
+    finish_plain(a, scal, S, r0, bin, g, out_map, out_norm);
+}
+
 static int make_args(const acb_map_params *p, MapArgs &a)
 {
     if (!p) return ACB_ERR_ARG;
@@ -671,6 +754,14 @@ static int launch_eig(const MapArgs &a, int nbins, int E, const double *eigval, 
                       double *out_map, double *out_norm, cudaStream_t s, const void *steer = nullptr,
                       const int *active = nullptr)
 {
+    if (E <= kEigSmall) {
+        const dim3 grid((unsigned)((a.G + kEigSmallThreads - 1) / kEigSmallThreads), nbins);
+        auto kern = E == 1 ? map_eig_small_kernel<USE_RM, CUSTOM, 1> : map_eig_small_kernel<USE_RM, CUSTOM, kEigSmall>;
+        kern<<<grid, kEigSmallThreads, 0, s>>>(a, E, eigval, reinterpret_cast<const double2 *>(eigvec), k, k_scalar,
+                                               mpos, gpos, r0, rm, out_map, out_norm,
+                                               reinterpret_cast<const double2 *>(steer), active);
+        return check_launch();
+    }
     const int mc = a.M <= 256 ? a.M : 128;
     const size_t smem = (size_t)(((3 * a.M + 1) & ~1) * sizeof(double)) + (size_t)mc * kLanes * sizeof(double2);
     auto kern = map_eig_kernel<USE_RM, CUSTOM>;
