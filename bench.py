@@ -712,7 +712,7 @@ def run_eig(args):
           map_rate=G * F / (float(np.mean(map_ms)) / 1e3), map_tflops_algorithmic=flops / (np.mean(map_ms) / 1e3) / 1e12,
           accuracy={'vs': 'oracle (numpy eigh + the reference eigen kernel restated)', 'bins': check_bins,
                     'max_rel_err': max(errs)},
-          gpu_launches_per_step='eigendecomposition (heevd_tridiag, heevd_tql, heevd_back kernels) + 1 map_eig_kernel',
+          gpu_launches_per_step='eigendecomposition (heevd_tridiag, heevd_tql, heevd_back kernels) + 1 map_eig_small_kernel',
           clocks=clk.summary(),
           dtype='f64')
 
@@ -914,7 +914,7 @@ def run_cleansc(args):
           cpu_baseline={'value': 1.0 / cpu_s, 'unit': 'bins/s', 'cores': O.num_threads(), 'kind': 'port',
                         'sample': f'1 bin (bin {b0}): map + CLEAN-SC iterations'},
           gpu_launches=f'{2 + 2 * J - 1} per step (init, map_plain_kernel, {J} cleansc_step_kernel, '
-                       f'{J - 1} map_eig_kernel; stopped bins return at once)',
+                       f'{J - 1} map_eig_small_kernel; stopped bins return at once)',
           clocks=clk.summary(), dtype='f64')
 
 
