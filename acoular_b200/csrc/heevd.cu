@@ -244,15 +244,31 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tql_kernel(const double *__r
             __syncthreads();   // every thread has read the control words before thread 0 writes them again
             if (done) break;
             ++iter;
-            // apply the rotations in the order they were formed to every row k of Z
+            // apply the rotations in the order they were formed to every row k of Z.  Rotation i reads entry i
+            // and writes entry i + 1 of the row, so every entry is read before it is written: the reads of 8
+            // rotations are issued together, ahead of their writes, and their latency is paid once per 8
+            // (one read at a time waited for the previous write, about one L2 round trip per rotation)
             for (int k = tid; k < M; k += kEvThreads) {
-                double carry = Z[(int64_t)m * M + k];
-                for (int i = m - 1; i >= stop; --i) {
-                    const double zi = Z[(int64_t)i * M + k];
-                    Z[(int64_t)(i + 1) * M + k] = sn[i] * zi + cs[i] * carry;
+                double *zk = Z + k;   // entry i of row k at zk[i * M]
+                double carry = zk[(int64_t)m * M];
+                int i = m - 1;
+                for (; i - 7 >= stop; i -= 8) {
+                    double zv[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) zv[j] = zk[(int64_t)(i - j) * M];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int ii = i - j;
+                        zk[(int64_t)(ii + 1) * M] = sn[ii] * zv[j] + cs[ii] * carry;
+                        carry = cs[ii] * zv[j] - sn[ii] * carry;
+                    }
+                }
+                for (; i >= stop; --i) {
+                    const double zi = zk[(int64_t)i * M];
+                    zk[(int64_t)(i + 1) * M] = sn[i] * zi + cs[i] * carry;
                     carry = cs[i] * zi - sn[i] * carry;
                 }
-                Z[(int64_t)stop * M + k] = carry;
+                zk[(int64_t)stop * M] = carry;
             }
             __syncthreads();
         }
