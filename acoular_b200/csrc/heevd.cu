@@ -25,6 +25,9 @@ namespace acb {
 
 constexpr int kEvThreads = 256;
 constexpr int kEvWarps = kEvThreads / 32;
+// the QL kernel's CTA: 128 threads, so that every matrix of a 513-bin request has its CTA resident at once
+// (the sweeps are one thread's serial recurrence, so a matrix takes the same time in any wave)
+constexpr int kQlThreads = 128;
 constexpr int kQlMaxIter = 60;   // QL iterations per eigenvalue before giving up (info = 1)
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
@@ -169,7 +172,7 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tridiag_kernel(double2 *__re
 // d, e (B, M) -> eigenvalues w (B, M) ascending, Z (B, M, M) column-major (column j = eigenvector of the
 // unsorted eigenvalue j), perm (B, M): sorted position q holds unsorted index perm[q]; info[b] = 1 if a QL
 // iteration did not converge.
-__global__ void __launch_bounds__(kEvThreads) heevd_tql_kernel(const double *__restrict__ dall,
+__global__ void __launch_bounds__(kQlThreads) heevd_tql_kernel(const double *__restrict__ dall,
                                                                const double *__restrict__ eall, int M,
                                                                double *__restrict__ wall, double *__restrict__ Zall,
                                                                int *__restrict__ permall, int *__restrict__ info)
@@ -183,11 +186,11 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tql_kernel(const double *__r
     const int b = blockIdx.x;
     const int tid = threadIdx.x;
     double *Z = Zall + (int64_t)b * M * M;
-    for (int k = tid; k < M; k += kEvThreads) {
+    for (int k = tid; k < M; k += kQlThreads) {
         d[k] = dall[(int64_t)b * M + k];
         e[k] = eall[(int64_t)b * M + k];
     }
-    for (int64_t idx = tid; idx < (int64_t)M * M; idx += kEvThreads) Z[idx] = (idx / M == idx % M) ? 1.0 : 0.0;
+    for (int64_t idx = tid; idx < (int64_t)M * M; idx += kQlThreads) Z[idx] = (idx / M == idx % M) ? 1.0 : 0.0;
     if (tid == 0) s_fail = 0;
     __syncthreads();
     const double eps = 2.220446049250313e-16;
@@ -220,8 +223,9 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tql_kernel(const double *__r
                             restart = true;
                             break;
                         }
-                        s = f / r;
-                        c = g / r;
+                        const double rinv = 1.0 / r;   // one division for both ratios
+                        s = f * rinv;
+                        c = g * rinv;
                         g = d[i + 1] - p;
                         r = (d[i] - g) * s + 2.0 * c * bb;
                         p = s * r;
@@ -248,7 +252,7 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tql_kernel(const double *__r
             // and writes entry i + 1 of the row, so every entry is read before it is written: the reads of 8
             // rotations are issued together, ahead of their writes, and their latency is paid once per 8
             // (one read at a time waited for the previous write, about one L2 round trip per rotation)
-            for (int k = tid; k < M; k += kEvThreads) {
+            for (int k = tid; k < M; k += kQlThreads) {
                 double *zk = Z + k;   // entry i of row k at zk[i * M]
                 double carry = zk[(int64_t)m * M];
                 int i = m - 1;
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tql_kernel(const double *__r
         }
     }
     // ascending order, ties by index (as a stable sort)
-    for (int k = tid; k < M; k += kEvThreads) {
+    for (int k = tid; k < M; k += kQlThreads) {
         const double dk = d[k];
         int rank = 0;
         for (int j = 0; j < M; ++j) rank += (d[j] < dk) || (d[j] == dk && j < k);
@@ -424,7 +428,7 @@ int acb_heevd_f64(const void *csm, int num_bins, int num_mics, double *eigval, v
     heevd_tridiag_kernel<<<B, kEvThreads, sm1, s>>>(A, M, d, e, tau, vh);
     int st = check_launch();
     if (st) return st;
-    heevd_tql_kernel<<<B, kEvThreads, sm2, s>>>(d, e, M, eigval, Z, perm, info);
+    heevd_tql_kernel<<<B, kQlThreads, sm2, s>>>(d, e, M, eigval, Z, perm, info);
     st = check_launch();
     if (st) return st;
     const size_t smem = ((size_t)M * W + M + W) * sizeof(double2);

@@ -502,7 +502,7 @@ def damas_gauss_seidel(psf: torch.Tensor, dirty_map: torch.Tensor, n_iter: int, 
 # ------------------------------------------------------------------------------------------------
 # CLEAN-SC
 # ------------------------------------------------------------------------------------------------
-def heevd_f64(csm: torch.Tensor, chunk_bytes: int = 1 << 30):
+def heevd_f64(csm: torch.Tensor, chunk_bytes: int = 4 << 30):
     """Hermitian eigendecomposition of every bin: csm (B, M, M) complex128 on the device ->
     (eigvals (B, M) float64 ascending, eigvecs (B, M, M) complex128, eigenvectors in the columns, info (B,)
     int32), the layout numpy.linalg.eigh returns; bins in chunks whose workspace fits ``chunk_bytes``."""
