@@ -11,8 +11,9 @@
 //                          sweep's plane rotations from d and e; all threads then apply them to their rows of
 //                          Z (no barrier per rotation).  Then the ascending order of the eigenvalues.
 //   heevd_back_kernel    : eigenvectors of A, V = Q Z = H_0 H_1 ... H_{M-2} Z, for a slab of columns held in
-//                          shared memory, reflectors applied from the last; columns written in ascending
-//                          eigenvalue order.
+//                          shared memory, reflectors applied from the last; each warp owns columns of the
+//                          slab, so the reflectors need no barrier; columns written in ascending eigenvalue
+//                          order.
 // All arithmetic is FP64.  The eigenvectors differ from LAPACK's by a phase per column (any unit factor is an
 // eigenvector); the eigenvalue beamformers use them only through |v^H h|.
 #include <cuda_runtime.h>
@@ -288,8 +289,12 @@ __global__ void __launch_bounds__(kQlThreads) heevd_tql_kernel(const double *__r
     if (tid == 0 && info) info[b] = s_fail;
 }
 
-// V = Q Z for the output columns [c0, c0 + W) of one matrix: the slab in shared memory, reflectors from the last.
-// V (B, M, M) complex128 row-major, columns = eigenvectors in ascending order.
+// V = Q Z for the output columns [c0, c0 + W) of one matrix, reflectors applied from the last.  The slab
+// sits in shared memory column by column (stride M + 1), and warp w owns the slab's columns w, w + 8, ..:
+// for each reflector a warp forms tau v^H S[:, j] over its own columns (lanes along the rows, a shuffle
+// reduction) and updates them, so no barrier separates the reflectors.  The reflector's entries are read
+// by all warps from L1.  V (B, M, M) complex128 row-major, columns = eigenvectors in ascending order.
+template <int CPW>
 __global__ void __launch_bounds__(kEvThreads) heevd_back_kernel(const double2 *__restrict__ vhall,
                                                                 const double2 *__restrict__ tauall,
                                                                 const double *__restrict__ Zall,
@@ -297,9 +302,8 @@ __global__ void __launch_bounds__(kEvThreads) heevd_back_kernel(const double2 *_
                                                                 double2 *__restrict__ Vall)
 {
     extern __shared__ double2 bk_sm[];
-    double2 *S = bk_sm;                    // [M][W]
-    double2 *vb = bk_sm + (size_t)M * W;   // [M] current reflector
-    double2 *sc = vb + M;                  // [W] tau * (v^H S[:, j])
+    const int Mp = M + 1;
+    double2 *S = bk_sm;                    // [W][Mp]: entry r of slab column j at S[j * Mp + r]
     const int b = blockIdx.x;
     const int c0 = blockIdx.y * W;
     const int nw = min(W, M - c0);
@@ -308,44 +312,56 @@ __global__ void __launch_bounds__(kEvThreads) heevd_back_kernel(const double2 *_
     const double2 *tau = tauall + (int64_t)b * M;
     const double *Z = Zall + (int64_t)b * M * M;
     const int *perm = permall + (int64_t)b * M;
-    for (int idx = tid; idx < M * W; idx += kEvThreads) {
-        const int r = idx / W, j = idx % W;
-        S[idx] = make_double2(j < nw ? Z[(int64_t)perm[c0 + j] * M + r] : 0.0, 0.0);
+    for (int j = warp; j < nw; j += kEvWarps) {
+        const double *zc = Z + (int64_t)perm[c0 + j] * M;   // column-major Z: eigenvector of T
+        for (int r = lane; r < M; r += 32) S[j * Mp + r] = make_double2(zc[r], 0.0);
     }
-    __syncthreads();
-    for (int i = M - 2; i >= 0; --i) {
-        const double2 t = tau[i];
+    // this warp's columns (j < nw)
+    int nq = 0;
+    while (nq < CPW && warp + kEvWarps * nq < nw) ++nq;
+    for (int i = M - 2; i >= 0 && nq > 0; --i) {
+        const double2 t = __ldg(tau + i);
         if (t.x == 0.0 && t.y == 0.0) continue;
-        for (int r = i + 1 + tid; r < M; r += kEvThreads) vb[r] = vh[(int64_t)i * M + r];
-        __syncthreads();
-        // s_j = tau * sum_r conj(v_r) S[r][j]: a warp per column, lanes along the rows
-        for (int j = warp; j < nw; j += kEvWarps) {
-            double ar = 0.0, ai = 0.0;
-            for (int r = i + 1 + lane; r < M; r += 32) {
-                const double2 x = cmulc(vb[r], S[r * W + j]);
-                ar += x.x;
-                ai += x.y;
+        const double2 *v = vh + (int64_t)i * M;
+        double ar[CPW], ai[CPW];
+#pragma unroll
+        for (int q = 0; q < CPW; ++q) ar[q] = ai[q] = 0.0;
+        for (int r = i + 1 + lane; r < M; r += 32) {
+            const double2 vr = __ldg(v + r);
+#pragma unroll
+            for (int q = 0; q < CPW; ++q) {
+                if (q >= nq) break;
+                const double2 x = cmulc(vr, S[(warp + kEvWarps * q) * Mp + r]);
+                ar[q] += x.x;
+                ai[q] += x.y;
             }
+        }
+        double2 sc[CPW];
+#pragma unroll
+        for (int q = 0; q < CPW; ++q) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-                ar += __shfl_xor_sync(0xffffffffu, ar, o);
-                ai += __shfl_xor_sync(0xffffffffu, ai, o);
+                ar[q] += __shfl_xor_sync(0xffffffffu, ar[q], o);
+                ai[q] += __shfl_xor_sync(0xffffffffu, ai[q], o);
             }
-            if (lane == 0) sc[j] = cmul(t, make_double2(ar, ai));
+            sc[q] = cmul(t, make_double2(ar[q], ai[q]));
         }
-        __syncthreads();
-        for (int idx = tid; idx < (M - 1 - i) * W; idx += kEvThreads) {
-            const int r = i + 1 + idx / W, j = idx % W;
-            if (j >= nw) continue;
-            const double2 u = cmul(vb[r], sc[j]);
-            S[r * W + j] = make_double2(S[r * W + j].x - u.x, S[r * W + j].y - u.y);
+        for (int r = i + 1 + lane; r < M; r += 32) {
+            const double2 vr = __ldg(v + r);
+#pragma unroll
+            for (int q = 0; q < CPW; ++q) {
+                if (q >= nq) break;
+                double2 *sp = S + (warp + kEvWarps * q) * Mp + r;
+                const double2 u = cmul(vr, sc[q]);
+                *sp = make_double2(sp->x - u.x, sp->y - u.y);
+            }
         }
-        __syncthreads();
     }
+    __syncthreads();
     double2 *V = Vall + (int64_t)b * M * M;
     for (int idx = tid; idx < M * W; idx += kEvThreads) {
         const int r = idx / W, j = idx % W;
-        if (j < nw) V[(int64_t)r * M + c0 + j] = S[idx];
+        if (j < nw) V[(int64_t)r * M + c0 + j] = S[j * Mp + r];
     }
 }
 
@@ -380,7 +396,7 @@ static EvWorkspace ev_layout(int M, int B)
 static int ev_slab(int M)
 {
     int W = 32;
-    while (W > 1 && ((size_t)M * W + M + W) * sizeof(double2) > 200 * 1024) W >>= 1;
+    while (W > 1 && (size_t)(M + 1) * W * sizeof(double2) > 200 * 1024) W >>= 1;
     return W;
 }
 
@@ -405,7 +421,7 @@ int acb_heevd_f64(const void *csm, int num_bins, int num_mics, double *eigval, v
     const EvWorkspace lay = ev_layout(M, B);
     if (workspace_bytes < lay.total) return ACB_ERR_WORKSPACE;
     const int W = ev_slab(M);
-    if (((size_t)M * W + M + W) * sizeof(double2) > 200 * 1024) return ACB_ERR_UNSUPPORTED;
+    if ((size_t)(M + 1) * W * sizeof(double2) > 200 * 1024) return ACB_ERR_UNSUPPORTED;
     cudaStream_t s = as_stream(stream);
     char *ws = static_cast<char *>(workspace);
     double2 *A = reinterpret_cast<double2 *>(ws + lay.A);
@@ -431,11 +447,12 @@ int acb_heevd_f64(const void *csm, int num_bins, int num_mics, double *eigval, v
     heevd_tql_kernel<<<B, kQlThreads, sm2, s>>>(d, e, M, eigval, Z, perm, info);
     st = check_launch();
     if (st) return st;
-    const size_t smem = ((size_t)M * W + M + W) * sizeof(double2);
-    if (cudaFuncSetAttribute(heevd_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    const size_t smem = (size_t)(M + 1) * W * sizeof(double2);
+    // columns per warp: the slab's W columns over the 8 warps
+    auto back = W >= 32 ? heevd_back_kernel<4> : (W >= 16 ? heevd_back_kernel<2> : heevd_back_kernel<1>);
+    if (cudaFuncSetAttribute(back, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return ACB_ERR_CUDA;
-    heevd_back_kernel<<<dim3(B, (M + W - 1) / W), kEvThreads, smem, s>>>(vh, tau, Z, perm, M, W,
-                                                                         static_cast<double2 *>(eigvec));
+    back<<<dim3(B, (M + W - 1) / W), kEvThreads, smem, s>>>(vh, tau, Z, perm, M, W, static_cast<double2 *>(eigvec));
     return check_launch();
 }
 
