@@ -97,6 +97,7 @@ SIGNATURES = {
     'acb_cleansc_workspace_bytes': (ctypes.c_size_t, [_I, ctypes.c_int64, _I, _I]),
     'acb_heevd_workspace_bytes': (ctypes.c_size_t, [_I, _I]),
     'acb_heevd_f64': (_I, [_VP, _I, _I, _VP, _VP, _VP, _VP, ctypes.c_size_t, _VP]),
+    'acb_heevd_select_f64': (_I, [_VP, _I, _I, _I, _VP, _VP, _VP, _VP, ctypes.c_size_t, _VP]),
     'acb_cleansc_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _VP, _VP, _VP, _VP, _I, _D, _I, _VP, _VP,
                              ctypes.c_size_t, _VP]),
     'acb_cleansc_custom_f64': (_I, [ctypes.POINTER(MapParams), _VP, _VP, _I, _D, _I, _VP, _VP, ctypes.c_size_t,

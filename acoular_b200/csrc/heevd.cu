@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kEvThreads) heevd_back_kernel(const double2 *_
                                                                 const double2 *__restrict__ tauall,
                                                                 const double *__restrict__ Zall,
                                                                 const int *__restrict__ permall, int M, int W,
-                                                                double2 *__restrict__ Vall)
+                                                                int ldv, double2 *__restrict__ Vall)
 {
     extern __shared__ double2 bk_sm[];
     const int Mp = M + 1;
@@ -358,11 +358,180 @@ __global__ void __launch_bounds__(kEvThreads) heevd_back_kernel(const double2 *_
         }
     }
     __syncthreads();
-    double2 *V = Vall + (int64_t)b * M * M;
+    double2 *V = Vall + (int64_t)b * M * ldv;   // row stride ldv (M, or the number of selected columns)
     for (int idx = tid; idx < M * W; idx += kEvThreads) {
         const int r = idx / W, j = idx % W;
-        if (j < nw) V[(int64_t)r * M + c0 + j] = S[j * Mp + r];
+        if (j < nw) V[(int64_t)r * ldv + c0 + j] = S[j * Mp + r];
     }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Selected eigenpairs (acb_heevd_select_f64): the eigenvalues of chosen ranks and their eigenvectors
+// only, for consumers that use a few components (BeamformerEig's default n = -1 takes the largest).
+// After the same tridiagonalisation, one warp per selected rank k:
+//   - the k-th smallest eigenvalue of T by multisection: each round the 32 lanes evaluate the Sturm
+//     count (the number of negative pivots of the LDL^T factorisation of T - x I, i.e. of eigenvalues
+//     below x) at 32 points spread over the current interval, which then narrows to the gap between two
+//     neighbouring points (about 33x per round, from the Gershgorin interval down to 2 eps |lambda|, or
+//     eps ||T|| for eigenvalues near zero, the accuracy of the QL iteration);
+//   - its eigenvector by inverse iteration: T - lambda I factored once by Gaussian elimination with
+//     partial pivoting (a tridiagonal factor gains one superdiagonal of fill-in), then three solves from
+//     a fixed start vector, each rescaled by its largest entry; zero pivots are replaced by eps ||T||;
+//   - the back-transformation by the reflectors (heevd_back_kernel on the selected columns).
+// The QL sweeps and their accumulation of all M eigenvectors are skipped.
+// ------------------------------------------------------------------------------------------------
+constexpr int kSelMax = 4;
+
+struct EvSel {
+    int n;
+    int idx[kSelMax];
+};
+
+// Number of eigenvalues of T (diagonal d, squared off-diagonal e2) below x.
+__device__ __forceinline__ int ev_sturm(const double *d, const double *e2, int M, double x, double pivmin)
+{
+    double q = d[0] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    int cnt = q < 0.0;
+    for (int i = 1; i < M; ++i) {
+        q = (d[i] - x) - e2[i - 1] / q;
+        if (fabs(q) < pivmin) q = -pivmin;
+        cnt += q < 0.0;
+    }
+    return cnt;
+}
+
+__host__ __device__ constexpr size_t ev_select_smem(int M, int E)
+{
+    return ((size_t)3 * M + (size_t)5 * M * E) * sizeof(double) + (size_t)M * E;
+}
+
+__global__ void __launch_bounds__(32 * kSelMax) heevd_select_kernel(const double *__restrict__ dall,
+                                                                    const double *__restrict__ eall, int M,
+                                                                    EvSel sel, double *__restrict__ wsel,
+                                                                    double *__restrict__ Zall,
+                                                                    int *__restrict__ permall)
+{
+    extern __shared__ double sl_sm[];
+    double *d = sl_sm;           // [M]
+    double *e = sl_sm + M;       // [M] off-diagonal (e[M - 1] = 0)
+    double *e2 = sl_sm + 2 * M;  // [M] its squares
+    const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    double *u0 = sl_sm + 3 * M + (size_t)w * 5 * M;   // pivots (as reciprocals after the factorisation)
+    double *u1 = u0 + M;                              // first superdiagonal of U
+    double *u2 = u1 + M;                              // second superdiagonal (fill-in)
+    double *mu = u2 + M;                              // multipliers
+    double *y = mu + M;                               // iterate
+    unsigned char *pv = reinterpret_cast<unsigned char *>(sl_sm + 3 * M + (size_t)sel.n * 5 * M) + (size_t)w * M;
+    for (int i = tid; i < M; i += blockDim.x) {
+        d[i] = dall[(int64_t)b * M + i];
+        const double ei = i < M - 1 ? eall[(int64_t)b * M + i] : 0.0;
+        e[i] = ei;
+        e2[i] = ei * ei;
+    }
+    __syncthreads();
+    if (w >= sel.n) return;
+    const double eps = 2.220446049250313e-16;
+    // Gershgorin interval, the norm of T and the pivot floor
+    double lo = INFINITY, hi = -INFINITY, emax2 = 0.0;
+    for (int i = lane; i < M; i += 32) {
+        const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + fabs(e[i]);
+        lo = fmin(lo, d[i] - r);
+        hi = fmax(hi, d[i] + r);
+        emax2 = fmax(emax2, e2[i]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        emax2 = fmax(emax2, __shfl_xor_sync(0xffffffffu, emax2, o));
+    }
+    const double pivmin = 2.2250738585072014e-308 * fmax(1.0, emax2);
+    const double tnorm = fmax(fabs(lo), fabs(hi));
+    const double fudge = 2.0 * eps * tnorm + 2.0 * pivmin;
+    lo -= fudge;
+    hi += fudge;
+    const int k = sel.idx[w];
+    for (int it = 0; it < 64; ++it) {
+        const double width = hi - lo;
+        if (width <= fmax(2.0 * eps * fmax(fabs(lo), fabs(hi)), eps * tnorm) || width <= 4.0 * pivmin) break;
+        const double x = lo + width * (double)(lane + 1) / 33.0;
+        const int c = ev_sturm(d, e2, M, x, pivmin);
+        const unsigned bal = __ballot_sync(0xffffffffu, c > k);   // points above the k-th eigenvalue
+        const double x31 = __shfl_sync(0xffffffffu, x, 31);
+        if (bal == 0) {
+            lo = x31;
+        } else {
+            const int j0 = __ffs(bal) - 1;
+            const double xh = __shfl_sync(0xffffffffu, x, j0);
+            const double xl = __shfl_sync(0xffffffffu, x, j0 > 0 ? j0 - 1 : 0);
+            if (j0 > 0) lo = xl;
+            hi = xh;
+        }
+    }
+    const double lam = 0.5 * (lo + hi);
+    if (lane == 0) {
+        wsel[(int64_t)b * sel.n + w] = lam;
+        const double tiny = tnorm > 0.0 ? eps * tnorm : 2.2250738585072014e-308;
+        // T - lam I = P L U
+        double a = d[0] - lam, bs = M > 1 ? e[0] : 0.0;
+        for (int i = 0; i < M - 1; ++i) {
+            const double l = e[i], m = d[i + 1] - lam, n = i + 2 < M ? e[i + 1] : 0.0;
+            if (fabs(a) >= fabs(l)) {
+                if (fabs(a) < tiny) a = a < 0.0 ? -tiny : tiny;
+                const double f = l / a;
+                pv[i] = 0;
+                u0[i] = a;
+                u1[i] = bs;
+                u2[i] = 0.0;
+                mu[i] = f;
+                a = m - f * bs;
+                bs = n;
+            } else {
+                const double f = a / l;
+                pv[i] = 1;
+                u0[i] = l;
+                u1[i] = m;
+                u2[i] = n;
+                mu[i] = f;
+                a = bs - f * m;
+                bs = -f * n;
+            }
+        }
+        if (fabs(a) < tiny) a = a < 0.0 ? -tiny : tiny;
+        u0[M - 1] = a;
+        for (int i = 0; i < M; ++i) u0[i] = 1.0 / u0[i];
+        for (int i = 0; i < M; ++i) y[i] = 1.0 + 0.25 * (double)((i * 2654435761u) % 1009u) / 1009.0;
+        for (int it = 0; it < 3; ++it) {
+            double cur = y[0];
+            for (int i = 0; i < M - 1; ++i) {
+                const double nx = y[i + 1];
+                if (pv[i]) {
+                    y[i] = nx;
+                    cur -= mu[i] * nx;
+                } else {
+                    y[i] = cur;
+                    cur = nx - mu[i] * cur;
+                }
+            }
+            y[M - 1] = cur * u0[M - 1];
+            if (M > 1) y[M - 2] = (y[M - 2] - u1[M - 2] * y[M - 1]) * u0[M - 2];
+            for (int i = M - 3; i >= 0; --i) y[i] = (y[i] - u1[i] * y[i + 1] - u2[i] * y[i + 2]) * u0[i];
+            double mx = 0.0;
+            for (int i = 0; i < M; ++i) mx = fmax(mx, fabs(y[i]));
+            const double sc = mx > 0.0 ? 1.0 / mx : 1.0;
+            for (int i = 0; i < M; ++i) y[i] *= sc;
+        }
+    }
+    __syncwarp();
+    double ss = 0.0;
+    for (int i = lane; i < M; i += 32) ss += y[i] * y[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    const double inv = ss > 0.0 ? 1.0 / sqrt(ss) : 0.0;
+    double *zc = Zall + (int64_t)b * M * M + (int64_t)w * M;   // column w of Z
+    for (int i = lane; i < M; i += 32) zc[i] = y[i] * inv;
+    if (lane == 0) permall[(int64_t)b * M + w] = w;
 }
 
 struct EvWorkspace {
@@ -452,7 +621,61 @@ int acb_heevd_f64(const void *csm, int num_bins, int num_mics, double *eigval, v
     auto back = W >= 32 ? heevd_back_kernel<4> : (W >= 16 ? heevd_back_kernel<2> : heevd_back_kernel<1>);
     if (cudaFuncSetAttribute(back, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return ACB_ERR_CUDA;
-    back<<<dim3(B, (M + W - 1) / W), kEvThreads, smem, s>>>(vh, tau, Z, perm, M, W, static_cast<double2 *>(eigvec));
+    back<<<dim3(B, (M + W - 1) / W), kEvThreads, smem, s>>>(vh, tau, Z, perm, M, W, M,
+                                                           static_cast<double2 *>(eigvec));
+    return check_launch();
+}
+
+int acb_heevd_select_f64(const void *csm, int num_bins, int num_mics, int num_sel, const int *sel, double *eigval,
+                         void *eigvec, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!csm || !sel || !eigval || !eigvec || !workspace) return ACB_ERR_ARG;
+    const int M = num_mics, B = num_bins, E = num_sel;
+    if (M < 1 || B < 1 || M > 4096 || B > 65535 || E < 1 || E > kSelMax || E > M) return ACB_ERR_SHAPE;
+    EvSel es;
+    es.n = E;
+    for (int j = 0; j < kSelMax; ++j) es.idx[j] = 0;
+    for (int j = 0; j < E; ++j) {
+        if (sel[j] < 0 || sel[j] >= M) return ACB_ERR_ARG;
+        es.idx[j] = sel[j];
+    }
+    const size_t sm3 = ev_select_smem(M, E);
+    if (sm3 > 200 * 1024) return ACB_ERR_UNSUPPORTED;
+    const EvWorkspace lay = ev_layout(M, B);
+    if (workspace_bytes < lay.total) return ACB_ERR_WORKSPACE;
+    cudaStream_t s = as_stream(stream);
+    char *ws = static_cast<char *>(workspace);
+    double2 *A = reinterpret_cast<double2 *>(ws + lay.A);
+    double *d = reinterpret_cast<double *>(ws + lay.d);
+    double *e = reinterpret_cast<double *>(ws + lay.e);
+    double2 *tau = reinterpret_cast<double2 *>(ws + lay.tau);
+    double2 *vh = reinterpret_cast<double2 *>(ws + lay.vh);
+    double *Z = reinterpret_cast<double *>(ws + lay.Z);
+    int *perm = reinterpret_cast<int *>(ws + lay.perm);
+    cudaError_t err = cudaMemcpyAsync(A, csm, (size_t)B * M * M * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+    if (err != cudaSuccess) {
+        set_cuda_error(err);
+        return ACB_ERR_CUDA;
+    }
+    const size_t sm1 = 2 * (size_t)M * sizeof(double2);
+    if (cudaFuncSetAttribute(heevd_tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(heevd_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3) !=
+            cudaSuccess)
+        return ACB_ERR_CUDA;
+    heevd_tridiag_kernel<<<B, kEvThreads, sm1, s>>>(A, M, d, e, tau, vh);
+    int st = check_launch();
+    if (st) return st;
+    heevd_select_kernel<<<B, 32 * E, sm3, s>>>(d, e, M, es, eigval, Z, perm);
+    st = check_launch();
+    if (st) return st;
+    // the E eigenvectors of T sit in columns 0 .. E-1 of each matrix's Z, perm[j] = j: one slab of E columns
+    const size_t smem = (size_t)(M + 1) * E * sizeof(double2);
+    if (cudaFuncSetAttribute(heevd_back_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return ACB_ERR_CUDA;
+    heevd_back_kernel<1><<<dim3(B, 1), kEvThreads, smem, s>>>(vh, tau, Z, perm, M, E, E,
+                                                              static_cast<double2 *>(eigvec));
     return check_launch();
 }
 

@@ -523,6 +523,33 @@ def heevd_f64(csm: torch.Tensor, chunk_bytes: int = 4 << 30):
     return ev, vec, info
 
 
+def heevd_select_f64(csm: torch.Tensor, ranks, chunk_bytes: int = 4 << 30):
+    """Selected eigenpairs of every bin: csm (B, M, M) complex128 on the device, ``ranks`` (1 to 4 ascending
+    ranks, the same for every bin; -1 is the largest) -> (eigvals (B, E) float64, eigvecs (B, M, E)
+    complex128), as the columns ``ranks`` of :func:`heevd_f64`'s result (up to a unit phase per column)."""
+    B, M, _ = csm.shape
+    dev = csm.device
+    sel = [int(r) % M for r in ranks]
+    E = len(sel)
+    if not 1 <= E <= 4:
+        msg = 'between 1 and 4 ranks'
+        raise ValueError(msg)
+    c = csm.to(torch.complex128).contiguous()
+    ev = torch.empty((B, E), dtype=torch.float64, device=dev)
+    vec = torch.empty((B, M, E), dtype=torch.complex128, device=dev)
+    sel_h = (ctypes.c_int * E)(*sel)
+    per = max(1, N.lib().acb_heevd_workspace_bytes(M, 1))
+    step = int(max(1, min(B, chunk_bytes // per)))
+    ws = torch.empty(N.lib().acb_heevd_workspace_bytes(M, step), dtype=torch.uint8, device=dev)
+    for b0 in range(0, B, step):
+        nb = min(step, B - b0)
+        N.check(N.lib().acb_heevd_select_f64(c[b0].data_ptr(), nb, M, E, ctypes.cast(sel_h, ctypes.c_void_p),
+                                             ev[b0].data_ptr(), vec[b0].data_ptr(), ws.data_ptr(), ws.numel(),
+                                             N.stream_handle()),
+                'acb_heevd_select_f64')
+    return ev, vec
+
+
 def cleansc_f64(csm: torch.Tensor, wavenumbers: torch.Tensor, steer_type: str, r_diag: bool, norm: float,
                 n_iter: int = 0, damp: float = 0.6, stopn: int = 3, mpos: torch.Tensor | None = None,
                 gpos: torch.Tensor | None = None, ref=None, r0: torch.Tensor | None = None,

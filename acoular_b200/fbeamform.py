@@ -371,7 +371,8 @@ class BeamformerEig(BeamformerBase):
 
     ``n`` selects the component (0 = smallest eigenvalue ... num_mics - 1; negative counts from the
     largest; default -1, the largest); ``na`` is the resolved index.  The eigen-decomposition runs on
-    the device (``PowerSpectra.evd_device``); the map runs in the plain FP64 form (``acb_map_eig_f64``,
+    the device (``PowerSpectra.evd_device``; for the largest component alone the selected-eigenpair solver
+    ``acb_heevd_select_f64``); the map runs in the plain FP64 form (``acb_map_eig_f64``,
     cost O(G M) per bin and component), with the reference's steering arithmetic.
     """
 
@@ -432,14 +433,26 @@ class BeamformerEig(BeamformerBase):
                           steer_norm=sn)
         return out, sn
 
+    def _components(self, ind):
+        """(lam (B', E), vec (B', M, E), norm) of the bins ``ind``.  The largest component alone (n = -1, the
+        default) comes from the selected-eigenpair solver (``acb_heevd_select_f64``: no QL sweeps, no other
+        eigenvectors) unless the full decomposition is cached already; otherwise ``PowerSpectra.evd_device``."""
+        fd = self.freq_data
+        M = self.steer.mics.num_mics
+        evd = getattr(fd, '_evd_dev', None)
+        cached = evd is not None and evd[0] == getattr(fd, '_cache_key', None)
+        if type(self)._eig_select is BeamformerEig._eig_select and self.na == M - 1 and not cached:
+            csm = fd.csm_device
+            lam, vec = D.heevd_select_f64(csm[torch.as_tensor(ind, device=csm.device)], [M - 1])
+            return lam, vec, self.sig_loss_norm()
+        ev, evec = fd.evd_device
+        return self._eig_select(ev, evec, torch.as_tensor(ind, device=ev.device))
+
     def _calc(self, ind):
         ind = np.asarray(ind, dtype=np.int64)
         if ind.size == 0:
             return
-        ev, evec = self.freq_data.evd_device
-        dev = ev.device
-        ind_d = torch.as_tensor(ind, device=dev)
-        lam, vec, norm = self._eig_select(ev, evec, ind_d)
+        lam, vec, norm = self._components(ind)
         out, _ = self._eig_maps(self._f[ind], lam, vec, norm, self.r_diag)
         out = self._post(out)
         if self.precision == 'float32':

@@ -297,6 +297,19 @@ size_t acb_heevd_workspace_bytes(int num_mics, int num_bins);
 int acb_heevd_f64(const void *csm, int num_bins, int num_mics, double *eigval, void *eigvec, int *info,
                   void *workspace, size_t workspace_bytes, void *stream);
 
+/* Selected eigenpairs of every bin's CSM: the eigenvalues of ascending ranks sel[0 .. num_sel-1] (the same
+ * ranks for every bin, 1 <= num_sel <= 4) and their eigenvectors, as the columns sel of acb_heevd_f64's
+ * result (up to a unit phase factor per column): csm complex128 [B][M][M] (read only) -> eigval float64
+ * [B][num_sel], eigvec complex128 [B][M][num_sel] row-major.  For consumers of a few components
+ * (BeamformerEig n = -1, acoular/fbeamform.py:821-888, uses the largest): Householder tridiagonalisation,
+ * the selected eigenvalues by multisection on Sturm counts, their eigenvectors by inverse iteration, the
+ * back-transformation; no QL sweeps.  Accurate for eigenvalues separated from the others; inside a cluster
+ * of (nearly) equal eigenvalues the vector is some unit vector of the cluster's space, as any solver's is.
+ * Workspace: acb_heevd_workspace_bytes(M, B).  M <= 4096 and (3 M + 5 M num_sel) 8 + M num_sel bytes of
+ * shared memory <= 200 KB (ACB_ERR_UNSUPPORTED above). */
+int acb_heevd_select_f64(const void *csm, int num_bins, int num_mics, int num_sel, const int *sel, double *eigval,
+                         void *eigvec, void *workspace, size_t workspace_bytes, void *stream);
+
 /* Workspace (device bytes) of acb_cleansc_f64 for num_bins bins (n_iter 0 = 2 num_mics iterations). */
 size_t acb_cleansc_workspace_bytes(int num_mics, int64_t num_grid, int num_bins, int n_iter);
 

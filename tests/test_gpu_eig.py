@@ -138,3 +138,57 @@ def test_power_spectra_evd_device_matches_host(golden):
         if wr[b, -1] > 1e3 * max(wr[b, -2], 1e-300):
             ph = np.vdot(vr[b][:, -1], evec[b][:, -1])
             assert abs(abs(ph) - 1.0) <= 1e-9
+
+
+@pytest.mark.parametrize('M', [1, 2, 5, 8, 33, 64, 256, 300])
+def test_heevd_select_against_lapack(M):
+    """acb_heevd_select_f64 (multisection on Sturm counts, inverse iteration, back-transformation) on the same
+    CSM-like matrices: the selected eigenvalues within 1e-12 of numpy's (relative to the largest); each selected
+    vector of unit norm with residual |A v - w v| within 1e-11 of the largest eigenvalue, and, where the
+    eigenvalue is separated from its neighbours by 1e-6 of the largest, equal to numpy's up to a phase."""
+    from acoular_b200 import device as D
+    rng = np.random.RandomState(M + 7)
+    mats = []
+    for _ in range(3):
+        X = rng.randn(2 * M, M) + 1j * rng.randn(2 * M, M)
+        A = X.conj().T @ X / (2 * M)
+        a = np.exp(-1j * rng.uniform(0, 6, M)) / rng.uniform(0.5, 2.0, M)
+        mats.append(A + 40.0 * np.outer(a, a.conj()))
+    a = np.exp(1j * rng.uniform(0, 6, M))
+    mats += [np.zeros((M, M), complex), np.eye(M, dtype=complex), np.outer(a, a.conj())]
+    C = np.stack(mats)
+    for ranks in ([M - 1], [0], sorted({0, M // 2, M - 1})):
+        w, V = D.heevd_select_f64(_dev(C), ranks)
+        w, V = w.cpu().numpy(), V.cpu().numpy()
+        for A, wb, Vb in zip(C, w, V):
+            wr, vr = np.linalg.eigh(A)
+            scale = max(np.abs(wr).max(), 1e-300)
+            for j, r in enumerate(ranks):
+                assert abs(wb[j] - wr[r]) <= 1e-12 * scale
+                v = Vb[:, j]
+                assert abs(np.linalg.norm(v) - 1.0) <= 1e-12
+                assert np.abs(A @ v - wb[j] * v).max() <= 1e-11 * max(scale, 1.0)
+                gap = min([abs(wr[r] - wr[q]) for q in (r - 1, r + 1) if 0 <= q < M] or [scale])
+                if gap > 1e-6 * scale:
+                    assert abs(abs(np.vdot(vr[:, r], v)) - 1.0) <= 1e-9
+
+
+def test_beamformer_eig_selected_path_matches_full(golden):
+    """BeamformerEig n = -1 through the selected-eigenpair solver and through a cached full decomposition
+    (PowerSpectra.evd_device) give the same map to 1e-9 of max on the small fixture's well-separated bins."""
+    import acoular_b200 as ac
+    s = golden('small_kat.npz')
+    g = golden('eig_kat.npz')
+    ps = ac.PowerSpectra(source=ac.TimeSamples(data=s['data'], sample_freq=float(s['fs'])), block_size=128,
+                         window='Hanning', overlap='50%')
+    mics = ac.MicGeom(pos_total=s['mpos'])
+    grid = ac.ImportGrid(pos=s['gpos'])
+    st = ac.SteeringVector(grid=grid, mics=mics)
+    bins = np.asarray(g['s_bins'])
+    sel = np.array(ac.BeamformerEig(freq_data=ps, steer=st, n=-1).result[bins[0]:bins[-1] + 1])
+    ps.evd_device   # cache the full decomposition: the same class now takes its columns
+    full = np.array(ac.BeamformerEig(freq_data=ps, steer=st, n=-1).result[bins[0]:bins[-1] + 1])
+    wr = ps.eigvals
+    for j, b in enumerate(bins):
+        if wr[b, -1] > 1e3 * max(wr[b, -2], 1e-300):
+            assert np.abs(sel[j] - full[j]).max() <= 1e-9 * max(np.abs(full[j]).max(), 1e-300)
