@@ -5,7 +5,8 @@
 //   heevd_tridiag_kernel : Householder reduction to a real symmetric tridiagonal matrix, A = Q T Q^H.
 //                          Step i reflects column i below the diagonal, x -> beta e1 with H = I - tau v v^H
 //                          (beta real, tau complex, v_0 = 1), then updates the trailing matrix
-//                          A22 <- H^H A22 H = A22 - v w^H - w v^H, p = tau A22 v, w = p - (tau/2)(p^H v) v.
+//                          A22 <- H^H A22 H = A22 - v w^H - w v^H, p = tau A22 v, w = p - (tau/2)(p^H v) v,
+//                          on A22's lower triangle only (half the memory traffic of the full update).
 //   heevd_tql_kernel     : eigenvalues and eigenvectors of T by implicit QL sweeps with Wilkinson shifts
 //                          (the EISPACK tql2 scheme), eigenvectors accumulated in Z.  One thread forms a
 //                          sweep's plane rotations from d and e; all threads then apply them to their rows of
@@ -117,12 +118,20 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tridiag_kernel(double2 *__re
             vh[(int64_t)i * M + r] = vr;
         }
         __syncthreads();
-        // p = tau A22 v: a warp per row, lanes along the row
+        // p = tau A22 v: a warp per row, lanes along the row.  Only the lower triangle of A22 is kept up to
+        // date (A is Hermitian): row r's entries right of the diagonal are conj(A[c][r]), read down column r
         for (int r = i + 1 + warp; r < M; r += kEvWarps) {
             const double2 *row = A + (int64_t)r * M;
             double ar = 0.0, ai = 0.0;
             for (int c = i + 1 + lane; c < M; c += 32) {
-                const double2 a = row[c], x = v[c];
+                double2 a;
+                if (c <= r) {
+                    a = row[c];
+                } else {
+                    a = A[(int64_t)c * M + r];
+                    a.y = -a.y;
+                }
+                const double2 x = v[c];
                 ar = fma(a.x, x.x, fma(-a.y, x.y, ar));
                 ai = fma(a.x, x.y, fma(a.y, x.x, ai));
             }
@@ -149,17 +158,17 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tridiag_kernel(double2 *__re
             p[r] = make_double2(p[r].x + t.x, p[r].y + t.y);
         }
         __syncthreads();
-        // A22 -= v w^H + w v^H
-        const int64_t n2 = (int64_t)L * L;
-        for (int64_t idx = tid; idx < n2; idx += kEvThreads) {
-            const int r = i + 1 + (int)(idx / L), c = i + 1 + (int)(idx % L);
-            const double2 vr = v[r], wr = p[r], vc = v[c], wc = p[c];
-            const double2 t1 = cmulc(wc, vr);   // v_r conj(w_c)
-            const double2 t2 = cmulc(vc, wr);   // w_r conj(v_c)
-            double2 a = A[(int64_t)r * M + c];
-            a.x -= t1.x + t2.x;
-            a.y -= t1.y + t2.y;
-            A[(int64_t)r * M + c] = a;
+        // A22 -= v w^H + w v^H on the lower triangle (c <= r): a warp per row, lanes along the row
+        for (int r = i + 1 + warp; r < M; r += kEvWarps) {
+            for (int c = i + 1 + lane; c <= r; c += 32) {
+                const double2 vr = v[r], wr = p[r], vc = v[c], wc = p[c];
+                const double2 t1 = cmulc(wc, vr);   // v_r conj(w_c)
+                const double2 t2 = cmulc(vc, wr);   // w_r conj(v_c)
+                double2 a = A[(int64_t)r * M + c];
+                a.x -= t1.x + t2.x;
+                a.y -= t1.y + t2.y;
+                A[(int64_t)r * M + c] = a;
+            }
         }
         __syncthreads();
     }
