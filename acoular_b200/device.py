@@ -523,6 +523,13 @@ def heevd_f64(csm: torch.Tensor, chunk_bytes: int = 4 << 30):
     return ev, vec, info
 
 
+def heevd_select_supported(num_mics: int, num_ranks: int = 1) -> bool:
+    """Whether acb_heevd_select_f64 takes this size: its per-matrix work arrays, (3 M + 5 M E) doubles and M E
+    pivot flags, must fit 200 KB of shared memory (M up to about 3100 for one rank)."""
+    M, E = int(num_mics), int(num_ranks)
+    return 1 <= E <= 4 and E <= M <= 4096 and (3 * M + 5 * M * E) * 8 + M * E <= 200 * 1024
+
+
 def heevd_select_f64(csm: torch.Tensor, ranks, chunk_bytes: int = 4 << 30):
     """Selected eigenpairs of every bin: csm (B, M, M) complex128 on the device, ``ranks`` (1 to 4 ascending
     ranks, the same for every bin; -1 is the largest) -> (eigvals (B, E) float64, eigvecs (B, M, E)

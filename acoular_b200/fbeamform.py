@@ -441,7 +441,8 @@ class BeamformerEig(BeamformerBase):
         M = self.steer.mics.num_mics
         evd = getattr(fd, '_evd_dev', None)
         cached = evd is not None and evd[0] == getattr(fd, '_cache_key', None)
-        if type(self)._eig_select is BeamformerEig._eig_select and self.na == M - 1 and not cached:
+        if (type(self)._eig_select is BeamformerEig._eig_select and self.na == M - 1 and not cached
+                and D.heevd_select_supported(M, 1)):
             csm = fd.csm_device
             lam, vec = D.heevd_select_f64(csm[torch.as_tensor(ind, device=csm.device)], [M - 1])
             return lam, vec, self.sig_loss_norm()

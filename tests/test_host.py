@@ -232,3 +232,13 @@ def test_noalloc_entry_point_argument_codes_match_workspace_entry_point():
         assert both(p, 0) == (code, code), bad
     big = D.map_params(256, 1000, 100, 'classic', True, 1.0)                 # 100 bins x 544 KB > 32 MiB
     assert L.acb_map_tc_noalloc(ctypes.byref(big), 0, 1, 1, 1, 1, 1, None, None, None) == N.ACB_ERR_SHAPE
+
+
+def test_heevd_select_size_rule():
+    """The selected-eigenpair solver's size rule (its work arrays in 200 KB of shared memory): BeamformerEig
+    takes the full decomposition beyond it."""
+    from acoular_b200 import device as D
+    assert D.heevd_select_supported(1, 1) and D.heevd_select_supported(256, 1) and D.heevd_select_supported(3000, 1)
+    assert not D.heevd_select_supported(3200, 1) and not D.heevd_select_supported(4097, 1)
+    assert D.heevd_select_supported(256, 4) and not D.heevd_select_supported(256, 5)
+    assert not D.heevd_select_supported(2, 3)
