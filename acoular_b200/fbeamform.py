@@ -118,6 +118,20 @@ class LazyBfResult:
         return self.bf._ac.__getitem__(key)
 
 
+def _launch_sizes(n: int, cap: int) -> list:
+    """Bins per map launch for n bins: the bulk in about 7 equal launches of at most ``cap`` bins, then up to
+    three shrinking ones (n / 64, half of it, ...), so that each launch's download overlaps the next launch's
+    computation and the download left after the last launch is a few bins' maps."""
+    tail = []
+    t, rest = min(max(1, n // 64), cap), n
+    while len(tail) < 3 and t >= 1 and rest > 2 * t:
+        tail.append(t)
+        rest -= t
+        t //= 2
+    per = max(1, min(cap, -(-rest // 7)))
+    return [min(per, rest - i) for i in range(0, rest, per)] + tail
+
+
 class BeamformerBase:
     """Delay-and-sum beamformer in the frequency domain, computed on the GPU."""
 
@@ -217,8 +231,6 @@ class BeamformerBase:
         G = gpos.shape[1]
         M = mpos.shape[1]
         cap = self.max_bins_per_launch or max(1, int((1 << 30) // max(1, G * 8 + M * M * 16)))
-        # several launches so that the copy of one overlaps the next one's computation
-        cap = min(cap, max(1, -(-ind.size // 8)))
         norm = self.sig_loss_norm()
         ref = self.steer.ref
         ac_t = torch.from_numpy(self._ac)
@@ -226,8 +238,10 @@ class BeamformerBase:
         compute = torch.cuda.current_stream(dev)
         copy = D.copy_stream(dev)
         pending = []
-        for s0 in range(0, ind.size, cap):
-            sub = ind[s0:s0 + cap]
+        s0 = 0
+        for n in _launch_sizes(ind.size, cap):
+            sub = ind[s0:s0 + n]
+            s0 += n
             contiguous = bool(np.all(np.diff(sub) == 1))
             if contiguous:
                 csm = csm_all[int(sub[0]):int(sub[-1]) + 1]

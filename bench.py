@@ -46,7 +46,7 @@ TC_DTYPE = {'tf32': 'tf32 / f32 accum', 'bf16x3': 'bf16x3 (split) / f32 accum',
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--form', default=None, choices=['tc', 'f64'])

@@ -242,3 +242,15 @@ def test_heevd_select_size_rule():
     assert not D.heevd_select_supported(3200, 1) and not D.heevd_select_supported(4097, 1)
     assert D.heevd_select_supported(256, 4) and not D.heevd_select_supported(256, 5)
     assert not D.heevd_select_supported(2, 3)
+
+
+def test_map_launch_sizes():
+    """BeamformerBase's launch plan: every bin once, in order, no launch above the memory cap, and for the
+    513-bin workload a last launch of a few bins (the download left after the computation)."""
+    from acoular_b200.fbeamform import _launch_sizes
+    for n in (1, 2, 3, 5, 8, 64, 65, 513, 1000):
+        for cap in (1, 7, 30, 10**9):
+            sizes = _launch_sizes(n, cap)
+            assert sum(sizes) == n and min(sizes) >= 1 and max(sizes) <= cap
+    s = _launch_sizes(513, 10**9)
+    assert s[-1] <= 4 and len(s) <= 12
