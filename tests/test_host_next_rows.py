@@ -210,3 +210,21 @@ def test_general_flow_uniform_field_matches_closed_form():
     got, ref = ray.apparent_r(gpos, mpos), exact.apparent_r(gpos, mpos)
     assert np.isfinite(got).all()
     assert np.abs(got - ref).max() <= 3e-3 * ref.max()
+
+
+def test_heevd_select_argument_checks(native):
+    """acb_heevd_select_f64 rejects bad requests before any CUDA call: null pointers (ACB_ERR_ARG), rank counts
+    outside 1..4 or above M (ACB_ERR_SHAPE), ranks outside 0..M-1 (ACB_ERR_ARG), sizes whose work arrays exceed
+    the shared memory (ACB_ERR_UNSUPPORTED) and a short workspace (ACB_ERR_WORKSPACE)."""
+    sel = (ctypes.c_int * 4)(0, 1, 2, 3)
+    ws = native.acb_heevd_workspace_bytes(8, 2)
+    call = native.acb_heevd_select_f64
+    assert call(None, 2, 8, 1, sel, 1, 1, 1, ws, None) == N.ACB_ERR_ARG
+    assert call(1, 2, 8, 1, None, 1, 1, 1, ws, None) == N.ACB_ERR_ARG
+    assert call(1, 2, 8, 0, sel, 1, 1, 1, ws, None) == N.ACB_ERR_SHAPE
+    assert call(1, 2, 8, 5, sel, 1, 1, 1, ws, None) == N.ACB_ERR_SHAPE
+    assert call(1, 2, 3, 4, sel, 1, 1, 1, ws, None) == N.ACB_ERR_SHAPE        # more ranks than mics
+    bad = (ctypes.c_int * 1)(8)
+    assert call(1, 2, 8, 1, bad, 1, 1, 1, ws, None) == N.ACB_ERR_ARG           # rank M
+    assert call(1, 1, 4000, 1, sel, 1, 1, 1, 1 << 40, None) == N.ACB_ERR_UNSUPPORTED
+    assert call(1, 2, 8, 1, sel, 1, 1, 1, ws - 1, None) == N.ACB_ERR_WORKSPACE
