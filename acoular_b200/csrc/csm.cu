@@ -211,14 +211,19 @@ __device__ __forceinline__ void fft_pass_f(float2 *__restrict__ z, int sg, int t
     float2 v[1 << S];
 #pragma unroll
     for (int t = 0; t < (1 << S); ++t) v[t] = z[zpf(base + t * half1)];
+    // the twiddle of point base + t half1 at stage q is entry (task mod half1) + (t mod 2^q) half1 of the
+    // stage's table: 2^q distinct values, each read once
+    const int tb = task & (half1 - 1);
 #pragma unroll
     for (int q = 0; q < S; ++q) {
         const int hf = half1 << q;                       // half the stage length L = 2^(sg + 1 + q)
+        float2 wq[1 << (S - 1)];
+#pragma unroll
+        for (int u = 0; u < (1 << q); ++u) wq[u] = tws[hf + tb + u * half1];
 #pragma unroll
         for (int t = 0; t < (1 << S); ++t) {
             if (t & (1 << q)) continue;
-            const int i0 = base + t * half1;
-            const float2 w = tws[hf + (i0 & (hf - 1))];
+            const float2 w = wq[t & ((1 << q) - 1)];
             const float2 b = v[t + (1 << q)];
             const float br = b.x * w.x - b.y * w.y;
             const float bi = b.x * w.y + b.y * w.x;

@@ -78,7 +78,6 @@ __global__ void __launch_bounds__(kEvThreads) heevd_tridiag_kernel(double2 *__re
     double2 *vh = vhall + (int64_t)b * (M > 1 ? M - 1 : 1) * M;
 
     for (int i = 0; i < M - 1; ++i) {
-        const int L = M - 1 - i;   // length of the column below the diagonal
         for (int r = i + 1 + tid; r < M; r += kEvThreads) v[r] = A[(int64_t)r * M + i];
         __syncthreads();
         double part = 0.0;

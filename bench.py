@@ -67,7 +67,8 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons during the timed region: one nvidia-smi process sampling every
+    100 ms (-lms), started before the region (its first sample awaited, up to 2 s) and stopped after it."""
 
     FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
               'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
@@ -76,28 +77,41 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.rows = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
+        self._first = threading.Event()
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(['nvidia-smi', f'--id={self.gpu}', f'--query-gpu={self.FIELDS}',
-                                      '--format=csv,noheader,nounits'], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.rows.append([x.strip() for x in out.stdout.strip().split(',')])
-            except Exception:  # noqa: BLE001 - clocks are advisory
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.strip().split(',')]
+            if len(parts) >= 5:
+                self.rows.append(parts)
+                self._first.set()
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        try:
+            self._proc = subprocess.Popen(['nvidia-smi', f'--id={self.gpu}', f'--query-gpu={self.FIELDS}',
+                                           '--format=csv,noheader,nounits', '-lms', '100'],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:   # clocks are advisory
+            self._proc = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
+        self._first.wait(2.0)
+        self.rows.clear()   # samples before the timed region starts do not count
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._proc is None:
+            return
+        self._proc.terminate()   # the sampler this object started, by its own handle
+        try:
+            self._proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self._proc.kill()
+            self._proc.wait(timeout=5)
+        self._t.join(timeout=5)
 
     def summary(self):
         if not self.rows:
