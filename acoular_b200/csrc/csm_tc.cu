@@ -14,7 +14,7 @@
 // Work item: one bin x one block of 128 rows (4 row tiles) x 4 column tiles (128 columns) at or
 // right of the block's diagonal.  Persistent CTAs (one per SM) walk the items in bin order; per item
 // the K loop streams 32-window stages of the A (4 tiles) and B (4 tiles) operands through a 6-stage
-// ring of bulk copies (no multicast).  Two TMEM accumulators alternate between items so that the
+// ring of bulk copies into this CTA alone.  Two TMEM accumulators alternate between items so that the
 // epilogue of one item overlaps the MMAs of the next.  All items cost the same, so the CTAs stay in
 // step and the items of a bin run at about the same time, reading the bin's tiles from L2: with
 // items of 4 and 8 column tiles mixed, the CTAs drifted apart by several waves and read the

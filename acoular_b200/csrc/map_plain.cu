@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(256) map_plain_kernel(MapArgs a, const double2
 // ------------------------------------------------------------------------------------------------
 // Staged variant for M <= 256 (one mic chunk): the same steering synthesis and quadratic form, but the
 // CSM rows come through shared memory.  Each warp streams the rows of its 8-row blocks in column
-// chunks of kCB through a two-stage ring that lane 0 fills with bulk copies (cp.async.bulk, no
-// multicast; one copy per row, completion on the stage's mbarrier); the next chunk is in flight while
+// chunks of kCB through a two-stage ring that lane 0 fills with bulk copies (cp.async.bulk into this
+// CTA alone; one copy per row, completion on the stage's mbarrier); the next chunk is in flight while
 // the warp works on the current one.  Every loaded C value then feeds the 32 grid points of the warp
 // from shared memory instead of a broadcast load through L1/L2 per complex FMA, and the masking of the
 // triangle is confined to the diagonal 8 x 8 block.  Sixteen warps (four per scheduler, 128 registers

@@ -1,5 +1,5 @@
 // sm_100a primitives used by the tensor-core kernels: mbarriers with bounded waits, bulk copies
-// (no multicast), TMEM allocation, tcgen05.mma / commit / ld, shared-memory matrix descriptors.
+// (into the issuing CTA alone), TMEM allocation, tcgen05.mma / commit / ld, shared-memory matrix descriptors.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -90,7 +90,7 @@ __host__ __device__ constexpr uint64_t drain_limit_ns(uint64_t limit_ns)
 
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Bulk global -> shared copy completing on an mbarrier (no cluster multicast).
+// Bulk global -> shared copy completing on an mbarrier (into the issuing CTA alone).
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
     asm volatile(
