@@ -31,6 +31,46 @@ def _device_blocks(source, num):
         yield torch.as_tensor(np.ascontiguousarray(b)).to(dev).reshape(b.shape[0], nf, nc)
 
 
+def _host_blocks(blocks):
+    """Numpy blocks (n, rest...) of a generator of device blocks, as ``result(num)`` yields them.
+
+    Each block is copied into page-locked host memory (torch's caching pinned allocator) on the copy stream
+    and handed out one block later, so its download overlaps the computation of the next block.  Every
+    yielded array is a block of its own; the pinned memory returns to the allocator's cache when the caller
+    drops the array, so a consumer that handles one block at a time reuses the same few buffers instead of
+    faulting in fresh host pages for every block.  Blocks above 1 GB are copied synchronously into ordinary
+    host memory (the pinned allocator rounds sizes up to powers of two).
+    """
+    pending = None
+    for b in blocks:
+        if b.numel() * b.element_size() > (1 << 30):   # above 1 GB: a plain synchronous copy, no pinned block
+            if pending is not None:
+                pending[1].synchronize()
+                yield pending[0].numpy().reshape(pending[0].shape[0], -1)
+                pending = None
+            yield b.cpu().numpy().reshape(b.shape[0], -1)
+            continue
+        dev = b.device
+        compute = torch.cuda.current_stream(dev)
+        copy = D.copy_stream(dev)
+        ready = torch.cuda.Event()
+        ready.record(compute)
+        copy.wait_event(ready)
+        host = torch.empty(b.shape, dtype=b.dtype, pin_memory=True)
+        with torch.cuda.stream(copy):
+            host.copy_(b, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(copy)
+        b.record_stream(copy)
+        if pending is not None:
+            pending[1].synchronize()
+            yield pending[0].numpy().reshape(pending[0].shape[0], -1)
+        pending = (host, done)
+    if pending is not None:
+        pending[1].synchronize()
+        yield pending[0].numpy().reshape(pending[0].shape[0], -1)
+
+
 class RFFT:
     """One-sided FFT of real multichannel time data, block by block (acoular/fprocess.py:35-181)."""
 
@@ -149,8 +189,7 @@ class RFFT:
             yield out
 
     def result(self, num: int = 1):
-        for b in self.result_device(num):
-            yield b.cpu().numpy().reshape(b.shape[0], -1)
+        yield from _host_blocks(self.result_device(num))
 
 
 class AutoPowerSpectra:
@@ -213,8 +252,7 @@ class AutoPowerSpectra:
             yield out
 
     def result(self, num: int = 1):
-        for b in self.result_device(num):
-            yield b.cpu().numpy().reshape(b.shape[0], -1)
+        yield from _host_blocks(self.result_device(num))
 
 
 class CrossPowerSpectra(AutoPowerSpectra):
@@ -265,8 +303,7 @@ class CrossPowerSpectra(AutoPowerSpectra):
             yield out
 
     def result(self, num: int = 1):
-        for b in self.result_device(num):
-            yield b.cpu().numpy().reshape(b.shape[0], -1)
+        yield from _host_blocks(self.result_device(num))
 
 
 class _SampleSource:

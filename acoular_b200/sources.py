@@ -57,7 +57,9 @@ class TimeSamples(SamplesGenerator):
 
     @property
     def digest(self) -> str:
-        """Identifier of the data: content hash of a strided sample, computed once per array object.
+        """Identifier of the data: content hash of evenly spaced whole sample rows (about 128 KB, the last
+        row included) with the shape, dtype and sample rate, computed once per array object.  Only the
+        sampled rows leave the device when the data is a CUDA tensor.
 
         Replace ``data`` (assign a new array) after changing samples in place."""
         key = (id(self.data), None if self.data is None else (tuple(self.data.shape), str(self.data.dtype)),
@@ -66,12 +68,21 @@ class TimeSamples(SamplesGenerator):
             h = hashlib.blake2b(digest_size=16)
             if self.data is not None:
                 a = self.data
-                if not isinstance(a, np.ndarray):
-                    a = a.detach().cpu().numpy() if hasattr(a, 'detach') else np.asarray(a)
-                a = np.ascontiguousarray(a)
-                h.update(str((a.shape, a.dtype.str, self.sample_freq)).encode())
-                flat = a.view(np.uint8).reshape(-1)
-                h.update(flat[:: max(1, a.nbytes // (1 << 20))].tobytes())
+                if not hasattr(a, 'detach'):
+                    a = np.asarray(a)
+                shape = tuple(a.shape)
+                h.update(str((shape, str(a.dtype), self.sample_freq)).encode())
+                if a.ndim >= 1 and shape[0] > 0:
+                    row_bytes = max(1, a[0].numel() * a.element_size() if hasattr(a, 'detach') else a[0].nbytes)
+                    step = max(1, shape[0] * row_bytes // (128 << 10))
+                    rows = a[::step]
+                    last = a[shape[0] - 1:]
+                    if hasattr(a, 'detach'):
+                        rows, last = rows.detach().cpu().numpy(), last.detach().cpu().numpy()
+                    h.update(np.ascontiguousarray(rows).tobytes())
+                    h.update(np.ascontiguousarray(last).tobytes())
+                else:
+                    h.update(np.ascontiguousarray(a.detach().cpu().numpy() if hasattr(a, 'detach') else a).tobytes())
             self._digest = '_' + h.hexdigest()
             self._digest_key = key
         return self._digest

@@ -254,3 +254,8 @@ def test_map_launch_sizes():
             assert sum(sizes) == n and min(sizes) >= 1 and max(sizes) <= cap
     s = _launch_sizes(513, 10**9)
     assert s[-1] <= 4 and len(s) <= 12
+    # the 256-mic workload's maps (401 x 401 points, 8 bytes) keep the overlapped plan; a band of 5 bins on a
+    # 41 x 41 grid is one launch, and a cap still splits it
+    assert _launch_sizes(513, 10**9, 160801 * 8) == s
+    assert _launch_sizes(5, 10**9, 1681 * 8) == [5]
+    assert _launch_sizes(5, 2, 1681 * 8) == [2, 2, 1]
