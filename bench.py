@@ -476,11 +476,13 @@ def serving_block(mixed: bool, duration: float, precision: str, verbose: bool = 
         f.result(timeout=120)
     torch.cuda.synchronize()
     rate = 10.0 * n_streams            # real time: each stream sends 0.1 s of data every 0.1 s
-    t_start = time.perf_counter()
-    t_end = t_start + duration
     futs = []
-    t_next = time.perf_counter()
     with ClockSampler(0) as clk:
+        # the arrival schedule starts once the clock sampler is up: arrivals due while it started would
+        # otherwise be submitted together, as a burst that the offered load does not contain
+        t_start = time.perf_counter()
+        t_end = t_start + duration
+        t_next = t_start
         while t_next < t_end:
             t_next += rng.exponential(1.0 / rate)
             delay = t_next - time.perf_counter()
