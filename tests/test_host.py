@@ -259,3 +259,26 @@ def test_map_launch_sizes():
     assert _launch_sizes(513, 10**9, 160801 * 8) == s
     assert _launch_sizes(5, 10**9, 1681 * 8) == [5]
     assert _launch_sizes(5, 2, 1681 * 8) == [2, 2, 1]
+
+
+def test_time_samples_digest():
+    """TimeSamples' content digest: equal for equal samples (another array object), different when a sampled
+    row, the last row, the shape or the sample rate differs; numpy and torch data both work."""
+    import torch
+
+    import acoular_b200 as ac
+    a = np.random.RandomState(3).randn(51200, 64)
+    d = ac.TimeSamples(data=a, sample_freq=51200.0).digest
+    assert ac.TimeSamples(data=a.copy(), sample_freq=51200.0).digest == d
+    b = a.copy()
+    b[0, 5] += 1.0
+    assert ac.TimeSamples(data=b, sample_freq=51200.0).digest != d
+    b = a.copy()
+    b[-1, 0] += 1.0
+    assert ac.TimeSamples(data=b, sample_freq=51200.0).digest != d
+    assert ac.TimeSamples(data=a[:-1], sample_freq=51200.0).digest != d
+    assert ac.TimeSamples(data=a, sample_freq=48000.0).digest != d
+    t = torch.from_numpy(a)
+    assert ac.TimeSamples(data=t, sample_freq=51200.0).digest == ac.TimeSamples(data=t.clone(), sample_freq=51200.0).digest
+    for empty in (np.zeros((0, 4)), np.arange(10.0)):
+        assert ac.TimeSamples(data=empty, sample_freq=1.0).digest.startswith('_')
