@@ -118,6 +118,16 @@ class LazyBfResult:
         return self.bf._ac.__getitem__(key)
 
 
+def _upload(a, dev, dtype=None) -> torch.Tensor:
+    """A host array as a device tensor, copied from page-locked memory without blocking the host.
+
+    ``torch.as_tensor(a, device=...)`` from ordinary host memory waits for all work queued on the stream;
+    inside a chain of launches that wait leaves the GPU idle while the host issues the next launch.  The
+    pinned staging block goes back to torch's cache once the copy is done."""
+    t = torch.as_tensor(np.ascontiguousarray(a, dtype=dtype))
+    return t.pin_memory().to(dev, non_blocking=True)
+
+
 def _launch_sizes(n: int, cap: int, bin_bytes: int = 0) -> list:
     """Bins per map launch for n bins: the bulk in about 7 equal launches of at most ``cap`` bins, then up to
     three shrinking ones (n / 64, half of it, ...), so that each launch's download overlaps the next launch's
@@ -207,8 +217,8 @@ class BeamformerBase:
     def _geometry(self, dev):
         gk = ('geom', self.steer.grid.digest, self.steer.mics.digest, str(dev))
         if getattr(self, '_geom_key', None) != gk:
-            self._mpos_d = torch.as_tensor(np.ascontiguousarray(self.steer.mics.pos, dtype=np.float64), device=dev)
-            self._gpos_d = torch.as_tensor(np.ascontiguousarray(self.steer.grid.pos, dtype=np.float64), device=dev)
+            self._mpos_d = _upload(self.steer.mics.pos, dev, np.float64)
+            self._gpos_d = _upload(self.steer.grid.pos, dev, np.float64)
             self._geom_key = gk
         return self._mpos_d, self._gpos_d
 
@@ -243,16 +253,21 @@ class BeamformerBase:
         compute = torch.cuda.current_stream(dev)
         copy = D.copy_stream(dev)
         pending = []
+        # wave numbers and bin indices of every launch in one upload that does not wait for the stream
+        k_all = _upload(2 * np.pi * self._f[ind] / self.steer.env.c, dev, np.float64)
+        ind_d = None
         s0 = 0
         for n in _launch_sizes(ind.size, cap, G * self._ac.itemsize):
             sub = ind[s0:s0 + n]
-            s0 += n
+            k = k_all[s0:s0 + n]
             contiguous = bool(np.all(np.diff(sub) == 1))
             if contiguous:
                 csm = csm_all[int(sub[0]):int(sub[-1]) + 1]
             else:
-                csm = csm_all.index_select(0, torch.as_tensor(sub, device=dev)).contiguous()
-            k = torch.as_tensor(2 * np.pi * self._f[sub] / self.steer.env.c, dtype=torch.float64, device=dev)
+                if ind_d is None:
+                    ind_d = _upload(ind, dev, np.int64)
+                csm = csm_all.index_select(0, ind_d[s0:s0 + n]).contiguous()
+            s0 += n
             if self.form == 'f64':
                 out = D.map_f64(csm, k, mpos, gpos, self.steer.steer_type, self.r_diag, norm, ref=ref,
                                 clip_negative=self.r_diag, glibc_faithful=self.glibc_faithful)
